@@ -1,0 +1,193 @@
+/*
+ * nestgpu.h -- C ABI of the B200 (sm_100a) engine for NEST's per-min_delay
+ * simulation cycle: node update, spike gather/delivery into ring buffers, and
+ * the spike_recorder sink.
+ *
+ * Plain C: pointers, sizes and status codes only.  Host buffers are owned by
+ * the caller and copied; an engine owns all device memory it allocates.  One
+ * engine is driven by one host thread at a time (the ABI is not re-entrant per
+ * engine); different engines may be driven from different threads.
+ *
+ * Each entry point replaces a piece of the reference's node/kernel interface;
+ * the reference location is given beside it (paths inside nest-simulator).
+ */
+#ifndef NESTGPU_H
+#define NESTGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NG_ABI_VERSION 1
+
+/* status codes (0 = success) */
+#define NG_OK 0
+#define NG_ERR_ARG -1          /* bad argument (BadProperty / BadParameter in the reference) */
+#define NG_ERR_CUDA -2         /* CUDA runtime error or no usable device */
+#define NG_ERR_STATE -3        /* call not valid in the engine's current state (KernelException) */
+#define NG_ERR_NUMERIC -4      /* NumericalInstability (aeif_cond_alpha.cpp:481-490) */
+#define NG_ERR_MEMORY -5       /* device allocation failed */
+#define NG_ERR_CAPACITY -6     /* a device list overflowed (spike list, trace buffer) */
+#define NG_ERR_UNKNOWN_NAME -7 /* unknown parameter/state name (UnaccessedDictionaryEntry) */
+
+/* neuron models on the path */
+#define NG_IAF_PSC_DELTA 0   /* models/iaf_psc_delta.{h,cpp} */
+#define NG_IAF_PSC_EXP 1     /* models/iaf_psc_exp.{h,cpp} */
+#define NG_AEIF_COND_ALPHA 2 /* models/aeif_cond_alpha.{h,cpp} */
+
+/* arithmetic forms */
+#define NG_FP64 0 /* plain: FP64 state and FP64 ring buffers (red.global.add.f64) */
+#define NG_FP32 1 /* precision form: FP32 state, int64 fixed-point ring buffers */
+
+#define NG_MAX_BLOCKS 8
+
+typedef struct ng_engine ng_engine;
+
+/* Network-wide settings, fixed for the engine's lifetime.  A network is a
+ * list of model blocks; neuron indices 0..n_neurons-1 run block by block. */
+typedef struct
+{
+  int32_t device;          /* CUDA device ordinal */
+  int32_t precision;       /* NG_FP64 or NG_FP32 */
+  double h;                /* resolution [ms]: Time::get_resolution().get_ms() (nest_time.h:330) */
+  double tics_per_ms;      /* Time tics per ms, 1000 by default (nest_time.cpp:43) */
+  int32_t min_delay;       /* steps; slice length (connection_manager.cpp:485-530) */
+  int32_t max_delay;       /* steps; ring length is min_delay + max_delay (ring_buffer.cpp:25-46) */
+  int32_t n_blocks;
+  int32_t block_model[ NG_MAX_BLOCKS ];
+  int64_t block_size[ NG_MAX_BLOCKS ];
+  int64_t n_generators;    /* extra spike sources after the neurons (spike_generator ports) */
+  int64_t spike_log_capacity; /* device spike-log entries between drains, 0 = automatic */
+  int64_t start_step;      /* absolute step of the engine's first slice origin (SimulationManager clock_) */
+} ng_config;
+
+/* Counters and timings of an engine. */
+typedef struct
+{
+  int64_t clock_steps;       /* simulated steps so far (SimulationManager::get_time) */
+  int64_t slices;            /* completed min_delay slices */
+  int64_t spikes;            /* neuron spikes emitted (local_spike_counter) */
+  int64_t syn_events;        /* recurrent synaptic events delivered: sum of out-degree x multiplicity */
+  int64_t drive_events;      /* Poisson drive spikes (sum of multiplicities) */
+  double update_ms;          /* device time in node-update kernels (profiling on) */
+  double deliver_ms;         /* device time in delivery kernels (profiling on) */
+  int64_t update_launches;
+  int64_t deliver_launches;
+  double simulate_ms;        /* host wall time inside ng_simulate */
+} ng_stats;
+
+/* Version of this ABI (NG_ABI_VERSION). */
+int ng_abi_version( void );
+
+/* Message of the last error on this host thread (empty if none). */
+const char* ng_last_error( void );
+
+/* Number of usable CUDA devices. */
+int ng_device_count( int32_t* n );
+
+/* Create an engine: allocates state, ring buffers and spike lists on the
+ * device.  Replaces NodeManager::prepare_nodes + Node::init_buffers_
+ * (nestkernel/node_manager.cpp:590-596, node.cpp:75-86) and
+ * EventDeliveryManager::init_moduli (event_delivery_manager.cpp:251-278). */
+int ng_create( const ng_config* cfg, ng_engine** out );
+
+/* Free all device memory of the engine. */
+int ng_destroy( ng_engine* eng );
+
+/* Set `count` values of a parameter or state variable for neurons
+ * first..first+count-1 of block `block`.  Names and units are the model's
+ * internal representation (models/iaf_psc_delta.cpp:94-200 keeps V_m, V_th,
+ * V_reset, V_min relative to E_L: names V_m_rel, V_th_rel, ...).  Replaces
+ * Node::set_status (nestkernel/node.h:420) for the model's Parameters_ and
+ * State_.  `r` is the refractory step counter. */
+int ng_set_var( ng_engine* eng, int32_t block, const char* name, const double* values, int64_t first, int64_t count );
+
+/* Read back a parameter or state variable.  Replaces Node::get_status
+ * (nestkernel/node.h:404) for State_ values. */
+int ng_get_var( ng_engine* eng, int32_t block, const char* name, double* out, int64_t first, int64_t count );
+
+/* Connectivity as CSR over sources 0..n_src-1 (neurons first, then
+ * generator ports): targets are neuron indices, weights in the model's units,
+ * delays in steps (min_delay <= d <= max_delay).  Replaces the per-thread
+ * Connector<static_synapse> tables walked by ConnectionManager::send
+ * (connection_manager.h:910-917, connector_base.h:398-434,
+ * models/static_synapse.h:161-170). */
+int ng_set_connections( ng_engine* eng, int64_t n_src, const int64_t* row_ptr, const int32_t* target,
+  const double* weight, const int32_t* delay_steps );
+
+/* The same connectivity as unordered (source, target, weight, delay) lists;
+ * the engine groups them by source (counting sort, edge order kept within a
+ * source) -- the order in which Connector::send walks a source's run of
+ * connections (connector_base.h:398-434). */
+int ng_set_connections_coo( ng_engine* eng, int64_t n_src, int64_t nnz, const int32_t* source, const int32_t* target,
+  const double* weight, const int32_t* delay_steps );
+
+/* Spikes of generator ports: emission step t_e (spike stamp minus one) and
+ * source index (>= n_neurons), sorted by step.  Replaces
+ * spike_generator::update (models/spike_generator.cpp:320-388). */
+int ng_set_spike_schedule( ng_engine* eng, int64_t n, const int64_t* emit_step, const int32_t* source );
+
+/* Poisson drive per neuron: rate [Hz] (<= 0: none), weight, delay [steps];
+ * a generator draw happens at steps t_g with start < t_g <= stop and arrives
+ * at t_g + delay.  Replaces poisson_generator::update/event_hook
+ * (models/poisson_generator.cpp:125-148) with a counter-based Philox4x32-10
+ * stream keyed by `seed`. */
+int ng_set_poisson( ng_engine* eng, const double* rate_hz, const double* weight, const int32_t* delay_steps,
+  int64_t start_step, int64_t stop_step, uint64_t seed );
+
+/* Which sources (length n_src) have their spikes logged for recorders.
+ * Replaces the device targets of TargetTableDevices::send_to_device
+ * (nestkernel/target_table_devices_impl.h:76-91). */
+int ng_set_recording( ng_engine* eng, const uint8_t* flags );
+
+/* Record the state variables `vars[0..n_vars-1]` of the listed neurons at
+ * every step whose stamp (step + 1) is a multiple of interval_steps.
+ * Replaces the UniversalDataLogger of a multimeter
+ * (nestkernel/universal_data_logger_impl.h:142-180). */
+int ng_set_trace( ng_engine* eng, int64_t n_idx, const int32_t* neuron, int32_t n_vars, const char* const* vars,
+  int32_t interval_steps );
+
+/* Advance the network by n_steps steps: node updates, delivery of each
+ * completed slice into the ring buffers, spike logging.  Partial slices are
+ * handled as SimulationManager::update_ does (simulation_manager.cpp:842-1189).
+ * Replaces SimulationManager::run (simulation_manager.cpp:614-671). */
+int ng_simulate( ng_engine* eng, int64_t n_steps );
+
+/* Number of logged spikes waiting to be drained. */
+int ng_spike_count( ng_engine* eng, int64_t* n );
+
+/* Drain up to `cap` logged spikes as (source, stamp step) in emission order
+ * per drain; *n_out receives the count copied.  Replaces
+ * RecordingBackendMemory::write (recording_backend_memory.cpp:104-112). */
+int ng_get_spikes( ng_engine* eng, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out );
+
+/* Number of trace rows waiting and the drain: a row holds n_vars x n_idx
+ * values (variable-major); row k has stamp first_stamp + k * interval_steps. */
+int ng_trace_count( ng_engine* eng, int64_t* n_rows, int64_t* first_stamp );
+int ng_get_trace( ng_engine* eng, double* out, int64_t max_rows, int64_t* n_rows_out );
+
+/* Counters and timings. */
+int ng_get_stats( ng_engine* eng, ng_stats* out );
+
+/* Time each kernel launch with CUDA events (adds a small overhead). */
+int ng_set_profiling( ng_engine* eng, int32_t on );
+
+/* Run every following launch of this engine on the given cudaStream_t
+ * (NULL: the engine's own stream). */
+int ng_set_stream( ng_engine* eng, void* cuda_stream );
+
+/* Capture full slices as CUDA graphs of `slices_per_graph` slices (0: off). */
+int ng_set_graph_slices( ng_engine* eng, int32_t slices_per_graph );
+
+/* FP64 coefficients the engine computed for a neuron (testing hook):
+ * writes up to `cap` values in the model's order, *n_out the count.  For
+ * iaf_psc_delta: P33, P30, RefractoryCounts; iaf_psc_exp: P11ex, P11in, P22,
+ * P21ex, P21in, P20, RefractoryCounts (models/iaf_psc_exp.cpp:244-285). */
+int ng_debug_coefficients( ng_engine* eng, int32_t block, int64_t index, double* out, int32_t cap, int32_t* n_out );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

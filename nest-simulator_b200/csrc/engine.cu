@@ -1,0 +1,1452 @@
+// engine.cu -- host side of the slice engine and the extern "C" ABI of
+// include/nestgpu.h.
+//
+// The host computes every FP64 coefficient with the C library's exp/expm1
+// by the same formulas as the reference's pre_run_hook functions, dedupes
+// them into coefficient classes, and uploads them; the device never
+// recomputes them.  The slice driver mirrors SimulationManager::update_
+// (nestkernel/simulation_manager.cpp:842-1189): node updates over the lags of
+// a slice, then delivery of the slice's spikes; partial slices are allowed.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <chrono>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/nestgpu.h"
+#include "ng_kernels.cuh"
+
+using namespace ng;
+
+namespace
+{
+
+thread_local std::string g_err;
+
+int
+fail( int code, const std::string& msg )
+{
+  g_err = msg;
+  return code;
+}
+
+#define CU( call )                                                                                       \
+  do                                                                                                     \
+  {                                                                                                      \
+    cudaError_t e_ = ( call );                                                                           \
+    if ( e_ != cudaSuccess )                                                                             \
+      return fail( e_ == cudaErrorMemoryAllocation ? NG_ERR_MEMORY : NG_ERR_CUDA,                        \
+        std::string( #call ) + ": " + cudaGetErrorString( e_ ) );                                        \
+  } while ( 0 )
+
+enum VarKind
+{
+  PARAM = 0,
+  STATE = 1,
+  REFR = 2,
+  ISTEP = 3
+};
+
+struct VarSpec
+{
+  const char* name;
+  int kind;
+  int slot;
+};
+
+// Internal representation of each model's Parameters_ and State_.
+const VarSpec DELTA_VARS[] = { { "tau_m", PARAM, 0 }, { "C_m", PARAM, 1 }, { "t_ref", PARAM, 2 },
+  { "V_th_rel", PARAM, 3 }, { "V_reset_rel", PARAM, 4 }, { "V_min_rel", PARAM, 5 }, { "V_m_rel", STATE, 0 },
+  { "y0", STATE, 1 }, { "I_e", STATE, 2 }, { "r", REFR, 0 }, { nullptr, 0, 0 } };
+const VarSpec EXP_VARS[] = { { "tau_m", PARAM, 0 }, { "C_m", PARAM, 1 }, { "t_ref", PARAM, 2 },
+  { "V_th_rel", PARAM, 3 }, { "V_reset_rel", PARAM, 4 }, { "tau_syn_ex", PARAM, 5 }, { "tau_syn_in", PARAM, 6 },
+  { "V_m_rel", STATE, 0 }, { "I_syn_ex", STATE, 1 }, { "I_syn_in", STATE, 2 }, { "i_0", STATE, 3 },
+  { "i_1", STATE, 4 }, { "I_e", STATE, 5 }, { "r", REFR, 0 }, { nullptr, 0, 0 } };
+const VarSpec AEIF_VARS[] = { { "V_peak", PARAM, 0 }, { "V_reset", PARAM, 1 }, { "t_ref", PARAM, 2 },
+  { "g_L", PARAM, 3 }, { "C_m", PARAM, 4 }, { "E_ex", PARAM, 5 }, { "E_in", PARAM, 6 }, { "E_L", PARAM, 7 },
+  { "Delta_T", PARAM, 8 }, { "tau_w", PARAM, 9 }, { "a", PARAM, 10 }, { "b", PARAM, 11 }, { "V_th", PARAM, 12 },
+  { "tau_syn_ex", PARAM, 13 }, { "tau_syn_in", PARAM, 14 }, { "gsl_error_tol", PARAM, 15 }, { "V_m", STATE, 0 },
+  { "dg_ex", STATE, 1 }, { "g_ex", STATE, 2 }, { "dg_in", STATE, 3 }, { "g_in", STATE, 4 }, { "w", STATE, 5 },
+  { "I_e", STATE, 6 }, { "r", REFR, 0 }, { "integration_step", ISTEP, 0 }, { nullptr, 0, 0 } };
+
+const VarSpec*
+vars_of( int model )
+{
+  return model == NG_IAF_PSC_DELTA ? DELTA_VARS : model == NG_IAF_PSC_EXP ? EXP_VARS : AEIF_VARS;
+}
+int
+n_params( int model )
+{
+  return model == NG_IAF_PSC_DELTA ? 6 : model == NG_IAF_PSC_EXP ? 7 : 16;
+}
+int
+n_states( int model )
+{
+  return model == NG_IAF_PSC_DELTA ? 3 : model == NG_IAF_PSC_EXP ? 6 : 7;
+}
+const VarSpec*
+find_var( int model, const char* name )
+{
+  for ( const VarSpec* v = vars_of( model ); v->name; ++v )
+    if ( std::strcmp( v->name, name ) == 0 )
+      return v;
+  return nullptr;
+}
+
+// Reference defaults (Parameters_::Parameters_ / State_::State_ of each model).
+void
+default_params( int model, std::vector< double >& p )
+{
+  if ( model == NG_IAF_PSC_DELTA )
+    p = { 10.0, 250.0, 2.0, -55.0 - ( -70.0 ), -70.0 - ( -70.0 ), -1.7976931348623157e308 };
+  else if ( model == NG_IAF_PSC_EXP )
+    p = { 10.0, 250.0, 2.0, -55.0 - ( -70.0 ), -70.0 - ( -70.0 ), 2.0, 2.0 };
+  else
+    p = { 0.0, -60.0, 0.0, 30.0, 281.0, 0.0, -85.0, -70.6, 2.0, 144.0, 4.0, 80.5, -50.4, 0.2, 2.0, 1e-6 };
+}
+double
+default_state( int model, int slot )
+{
+  if ( model == NG_AEIF_COND_ALPHA && slot == 0 )
+    return -70.6;
+  return 0.0;
+}
+
+// IAFPropagatorExp::evaluate (libnestutil/iaf_propagator.cpp:42-75,
+// iaf_propagator.h:152-159): P32 with the singular tau_m ~ tau_syn branch.
+double
+propagator_exp( double tau_syn, double tau_m, double c_m, double h )
+{
+  const double beta = tau_syn * tau_m / ( tau_m - tau_syn );
+  const double gamma = beta / c_m;
+  const double inv_tau_syn = 1 / tau_syn;
+  const double inv_tau_m = 1 / tau_m;
+  const double inv_c_m = 1 / c_m;
+  const double inv_beta = ( tau_m - tau_syn ) / ( tau_syn * tau_m );
+  const double exp_h_tau_syn = std::exp( -h * inv_tau_syn );
+  const double expm1_h_tau = std::expm1( h * inv_beta );
+  const double P32 = gamma * exp_h_tau_syn * expm1_h_tau;
+  if ( std::isnormal( P32 ) and P32 > 0 )
+    return P32;
+  const double exp_h_tau = std::exp( -h * inv_tau_m );
+  return h * inv_c_m * exp_h_tau;
+}
+
+// Poisson table (lambda, p_m, F_m, m) for inversion from the mode.
+double4
+poisson_table( double lambda )
+{
+  if ( !( lambda > 0.0 ) )
+    return make_double4( 0.0, 1.0, 1.0, 0.0 );
+  const double m = std::floor( lambda );
+  const double pm = std::exp( -lambda + m * std::log( lambda ) - std::lgamma( m + 1.0 ) );
+  double p = std::exp( -lambda ), F = p;
+  for ( long long k = 1; k <= ( long long ) m; ++k )
+  {
+    p = p * lambda / ( double ) k;
+    F += p;
+  }
+  return make_double4( lambda, pm, F, m );
+}
+
+struct DevBuf
+{
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct ng_engine
+{
+  ng_config cfg {};
+  int prec = NG_FP64;
+  size_t rsz = 8;  // bytes per state element
+  double h = 0.1;
+  int64_t tics_per_step = 100;
+  int64_t N = 0, n_src = 0;
+  int L = 0, C = 2;
+  int sms = 148;
+  cudaStream_t own = nullptr, stream = nullptr;
+
+  struct Blk
+  {
+    int model = 0;
+    int64_t off = 0, n = 0;
+    std::vector< std::vector< double > > par;  // [param][neuron]
+    bool dirty = true;
+    DevBuf st[ MAX_STATE ], r, istep, cls, ctab;
+    int64_t n_classes = 0;
+    std::vector< double > host_ctab;
+    std::vector< int32_t > host_cls;
+  };
+  std::vector< Blk > blk;
+
+  DevBuf ring, row_ptr, real_deg, tdc, w, spk, spk_off, log, rec, pois, pois_w, pois_d, trace_col, trace, sched_step,
+    sched_src, ctl;
+  int32_t tbits = 1;
+  uint32_t tmask = 1, dmask = 0;
+  double fx_inv = 1.0;
+  int64_t nnz_padded = 0, spk_cap = 0, log_cap = 0, n_sched = 0, n_rec = 0;
+  int has_pois = 0;
+  int64_t pois_start = 0, pois_stop = INT64_MAX;
+  uint32_t key0 = 0, key1 = 0;
+  int32_t n_trace_idx = 0, trace_interval = 1, n_trace_vars = 0;
+  int8_t trace_slot[ MAX_STATE ] = { 0, 0, 0, 0, 0, 0, 0, 0 };
+  int64_t trace_rows_cap = 0;
+  std::vector< int64_t > host_sched_step;
+
+  // clock: absolute step = slice origin + from
+  int64_t origin = 0;
+  int32_t from = 0;
+  int64_t slices = 0;
+
+  // drained output
+  std::vector< int32_t > out_src;
+  std::vector< int64_t > out_stamp;
+  std::vector< double > out_trace;
+  int64_t trace_first_stamp = -1;
+  int64_t next_trace_stamp_row = 0;  // absolute row index (stamp / interval) of the next row expected
+
+  Ctl* host_ctl = nullptr;  // pinned
+  ng_stats stats {};
+  int profiling = 0;
+  int graph_slices = 0;
+  cudaGraphExec_t graph = nullptr;
+  int64_t generation = 0, graph_generation = -1;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector< DevBuf* > all;
+  int deliver_ctas = 0;
+
+  ~ng_engine()
+  {
+    cudaSetDevice( cfg.device );
+    if ( graph )
+      cudaGraphExecDestroy( graph );
+    for ( auto& b : blk )
+    {
+      for ( auto& s : b.st )
+        cudaFree( s.p );
+      cudaFree( b.r.p );
+      cudaFree( b.istep.p );
+      cudaFree( b.cls.p );
+      cudaFree( b.ctab.p );
+    }
+    DevBuf* bufs[] = { &ring, &row_ptr, &real_deg, &tdc, &w, &spk, &spk_off, &log, &rec, &pois, &pois_w, &pois_d,
+      &trace_col, &trace, &sched_step, &sched_src, &ctl };
+    for ( DevBuf* b : bufs )
+      cudaFree( b->p );
+    if ( host_ctl )
+      cudaFreeHost( host_ctl );
+    if ( ev0 )
+      cudaEventDestroy( ev0 );
+    if ( ev1 )
+      cudaEventDestroy( ev1 );
+    if ( own )
+      cudaStreamDestroy( own );
+  }
+
+  int
+  alloc( DevBuf& b, size_t bytes )
+  {
+    cudaFree( b.p );
+    b.p = nullptr;
+    b.bytes = 0;
+    if ( bytes == 0 )
+      return NG_OK;
+    CU( cudaMalloc( &b.p, bytes ) );
+    b.bytes = bytes;
+    CU( cudaMemsetAsync( b.p, 0, bytes, stream ) );
+    return NG_OK;
+  }
+
+  int
+  upload( DevBuf& b, const void* src, size_t bytes )
+  {
+    int rc = alloc( b, bytes );
+    if ( rc )
+      return rc;
+    if ( bytes )
+      CU( cudaMemcpyAsync( b.p, src, bytes, cudaMemcpyHostToDevice, stream ) );
+    return NG_OK;
+  }
+
+  int
+  block_of( int64_t i ) const
+  {
+    for ( size_t k = 0; k < blk.size(); ++k )
+      if ( i >= blk[ k ].off && i < blk[ k ].off + blk[ k ].n )
+        return ( int ) k;
+    return -1;
+  }
+
+  int64_t
+  ms_to_steps( double ms ) const
+  {
+    // Time( Time::ms( t ) ).get_steps() (nestkernel/nest_time.h:306-311, 508-521)
+    const int64_t tics = ( int64_t ) ( ms * cfg.tics_per_ms + 0.5 );
+    return ( int64_t ) ( ( double ) ( tics + tics_per_step - 1 ) * ( 1. / ( double ) tics_per_step ) );
+  }
+
+  // pre_run_hook restatements -> coefficient rows (FP64), deduped into classes
+  int
+  build_classes( Blk& b )
+  {
+    std::unordered_map< std::string, int32_t > ids;
+    b.host_ctab.clear();
+    b.host_cls.assign( ( size_t ) b.n, 0 );
+    double row[ CT_STRIDE ];
+    for ( int64_t i = 0; i < b.n; ++i )
+    {
+      std::fill( row, row + CT_STRIDE, 0.0 );
+      const auto& P = b.par;
+      if ( b.model == NG_IAF_PSC_DELTA )
+      {
+        const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ];
+        if ( !( c_m > 0 ) || !( tau_m > 0 ) || P[ 2 ][ i ] < 0 )
+          return fail( NG_ERR_ARG, "iaf_psc_delta: C_m and tau_m must be > 0, t_ref >= 0" );
+        if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
+          return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
+        row[ 0 ] = std::exp( -h / tau_m );
+        row[ 1 ] = 1 / c_m * ( 1 - row[ 0 ] ) * tau_m;
+        row[ 2 ] = P[ 3 ][ i ];
+        row[ 3 ] = P[ 4 ][ i ];
+        row[ 4 ] = P[ 5 ][ i ];
+        row[ 5 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+      }
+      else if ( b.model == NG_IAF_PSC_EXP )
+      {
+        const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ], tex = P[ 5 ][ i ], tin = P[ 6 ][ i ];
+        if ( !( c_m > 0 ) || !( tau_m > 0 ) || !( tex > 0 ) || !( tin > 0 ) || P[ 2 ][ i ] < 0 )
+          return fail( NG_ERR_ARG, "iaf_psc_exp: capacitance and time constants must be > 0, t_ref >= 0" );
+        if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
+          return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
+        const double P11ex = std::exp( -h / tex );
+        const double P11in = std::exp( -h / tin );
+        const double P22 = std::exp( -h / tau_m );
+        row[ 0 ] = P22;
+        row[ 1 ] = propagator_exp( tex, tau_m, c_m, h );
+        row[ 2 ] = propagator_exp( tin, tau_m, c_m, h );
+        row[ 3 ] = tau_m / c_m * ( 1.0 - P22 );
+        row[ 4 ] = P11ex;
+        row[ 5 ] = P11in;
+        row[ 6 ] = P[ 3 ][ i ];
+        row[ 7 ] = P[ 4 ][ i ];
+        row[ 8 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+        row[ 9 ] = 1. - P11ex;
+      }
+      else
+      {
+        for ( int k = 0; k < 15; ++k )
+          row[ k ] = P[ k == 0 ? 0 : k == 1 ? 1 : k + 1 ][ i ];
+        // order: V_peak, V_reset, g_L, C_m, E_ex, E_in, E_L, Delta_T, tau_w, a, b, V_th, tau_ex, tau_in, tol
+        row[ 14 ] = P[ 15 ][ i ];
+        const double Vpeak = P[ 0 ][ i ], Vreset = P[ 1 ][ i ], Vth = P[ 12 ][ i ], DT = P[ 8 ][ i ];
+        if ( Vreset >= Vpeak )
+          return fail( NG_ERR_ARG, "Ensure that: V_reset < V_peak ." );
+        if ( DT < 0. )
+          return fail( NG_ERR_ARG, "Delta_T must be positive." );
+        if ( Vpeak < Vth )
+          return fail( NG_ERR_ARG, "V_peak >= V_th required." );
+        if ( !( P[ 4 ][ i ] > 0 ) )
+          return fail( NG_ERR_ARG, "Capacitance must be strictly positive." );
+        if ( !( P[ 13 ][ i ] > 0 ) || !( P[ 14 ][ i ] > 0 ) || !( P[ 9 ][ i ] > 0 ) )
+          return fail( NG_ERR_ARG, "All time constants must be strictly positive." );
+        if ( !( P[ 15 ][ i ] > 0 ) )
+          return fail( NG_ERR_ARG, "The gsl_error_tol must be strictly positive." );
+        if ( P[ 2 ][ i ] < 0 )
+          return fail( NG_ERR_ARG, "Refractory time cannot be negative." );
+        row[ 15 ] = 1.0 * M_E / P[ 13 ][ i ];
+        row[ 16 ] = 1.0 * M_E / P[ 14 ][ i ];
+        row[ 17 ] = DT > 0. ? Vpeak : Vth;
+        row[ 18 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+      }
+      std::string key( reinterpret_cast< const char* >( row ), sizeof( row ) );
+      auto it = ids.find( key );
+      int32_t id;
+      if ( it == ids.end() )
+      {
+        id = ( int32_t ) ids.size();
+        ids.emplace( std::move( key ), id );
+        b.host_ctab.insert( b.host_ctab.end(), row, row + CT_STRIDE );
+      }
+      else
+      {
+        id = it->second;
+      }
+      b.host_cls[ ( size_t ) i ] = id;
+    }
+    b.n_classes = ( int64_t ) ids.size();
+    int rc = upload( b.ctab, b.host_ctab.data(), b.host_ctab.size() * sizeof( double ) );
+    if ( rc )
+      return rc;
+    rc = upload( b.cls, b.host_cls.data(), b.host_cls.size() * sizeof( int32_t ) );
+    if ( rc )
+      return rc;
+    b.dirty = false;
+    ++generation;
+    return NG_OK;
+  }
+
+  Net
+  net() const
+  {
+    Net d {};
+    d.N = N;
+    d.n_src = n_src;
+    d.L = L;
+    d.C = C;
+    d.min_delay = cfg.min_delay;
+    d.tbits = tbits;
+    d.tmask = tmask;
+    d.dmask = dmask;
+    d.ring = ring.p;
+    d.fx_inv = fx_inv;
+    d.row_ptr = ( const int64_t* ) row_ptr.p;
+    d.real_deg = ( const int32_t* ) real_deg.p;
+    d.edge_tdc = ( const uint32_t* ) tdc.p;
+    d.edge_w = w.p;
+    d.spk = ( int4* ) spk.p;
+    d.spk_off = ( long long* ) spk_off.p;
+    d.spk_cap = spk_cap;
+    d.log = ( uint2* ) log.p;
+    d.log_cap = log_cap;
+    d.rec = ( const uint8_t* ) rec.p;
+    d.pois = ( const double4* ) pois.p;
+    d.pois_w = ( const double* ) pois_w.p;
+    d.pois_d = ( const int32_t* ) pois_d.p;
+    d.pois_start = pois_start;
+    d.pois_stop = pois_stop;
+    d.key0 = key0;
+    d.key1 = key1;
+    d.has_pois = has_pois;
+    d.trace_col = n_trace_idx > 0 ? ( const int32_t* ) trace_col.p : nullptr;
+    d.trace = ( double* ) trace.p;
+    d.n_trace_idx = n_trace_idx;
+    d.trace_interval = trace_interval;
+    d.n_trace_vars = n_trace_vars;
+    for ( int k = 0; k < MAX_STATE; ++k )
+      d.trace_slot[ k ] = trace_slot[ k ];
+    d.trace_rows = trace_rows_cap;
+    d.sched_step = ( const int64_t* ) sched_step.p;
+    d.sched_src = ( const int32_t* ) sched_src.p;
+    d.n_sched = n_sched;
+    d.ctl = ( Ctl* ) ctl.p;
+    return d;
+  }
+
+  Block
+  dblock( const Blk& b ) const
+  {
+    Block k {};
+    k.off = b.off;
+    k.n = b.n;
+    k.model = b.model;
+    k.cls = ( const int32_t* ) b.cls.p;
+    k.ctab = ( const double* ) b.ctab.p;
+    for ( int s = 0; s < MAX_STATE; ++s )
+      k.s[ s ] = b.st[ s ].p;
+    k.r = ( int32_t* ) b.r.p;
+    k.istep = ( double* ) b.istep.p;
+    return k;
+  }
+
+  void
+  launch_update( const Net& d, int from_, int to_ )
+  {
+    for ( size_t k = 0; k < blk.size(); ++k )
+    {
+      const Blk& b = blk[ k ];
+      const int sched = ( k == 0 ) ? 1 : 0;
+      const Block db = dblock( b );
+      if ( b.model == NG_AEIF_COND_ALPHA )
+      {
+        const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( b.n + 127 ) / 128 );
+        if ( prec == NG_FP64 )
+          k_update_aeif< double, false ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched, h );
+        else
+          k_update_aeif< float, true ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched, h );
+      }
+      else
+      {
+        const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( b.n + 255 ) / 256 );
+        if ( b.model == NG_IAF_PSC_DELTA )
+        {
+          if ( prec == NG_FP64 )
+            k_update_delta< double, false ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+          else
+            k_update_delta< float, true ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+        }
+        else
+        {
+          if ( prec == NG_FP64 )
+            k_update_exp< double, false ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+          else
+            k_update_exp< float, true ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+        }
+      }
+    }
+  }
+
+  void
+  launch_deliver( const Net& d )
+  {
+    const unsigned grid = ( unsigned ) deliver_ctas;
+    if ( prec == NG_FP64 )
+      k_deliver< false ><<< grid, 256, 0, stream >>>( d );
+    else
+      k_deliver< true ><<< grid, 256, 0, stream >>>( d );
+  }
+
+  int
+  run_slice_range( const Net& d, int from_, int to_ )
+  {
+    if ( profiling )
+      CU( cudaEventRecord( ev0, stream ) );
+    launch_update( d, from_, to_ );
+    CU( cudaGetLastError() );
+    if ( profiling )
+    {
+      CU( cudaEventRecord( ev1, stream ) );
+      CU( cudaEventSynchronize( ev1 ) );
+      float ms = 0;
+      CU( cudaEventElapsedTime( &ms, ev0, ev1 ) );
+      stats.update_ms += ms;
+    }
+    stats.update_launches += ( int64_t ) blk.size();
+    if ( to_ == cfg.min_delay )
+    {
+      if ( profiling )
+        CU( cudaEventRecord( ev0, stream ) );
+      launch_deliver( d );
+      CU( cudaGetLastError() );
+      if ( profiling )
+      {
+        CU( cudaEventRecord( ev1, stream ) );
+        CU( cudaEventSynchronize( ev1 ) );
+        float ms = 0;
+        CU( cudaEventElapsedTime( &ms, ev0, ev1 ) );
+        stats.deliver_ms += ms;
+      }
+      stats.deliver_launches += 1;
+    }
+    return NG_OK;
+  }
+
+  int
+  ensure_graph( const Net& d )
+  {
+    if ( graph && graph_generation == generation )
+      return NG_OK;
+    if ( graph )
+    {
+      cudaGraphExecDestroy( graph );
+      graph = nullptr;
+    }
+    cudaGraph_t g;
+    CU( cudaStreamBeginCapture( stream, cudaStreamCaptureModeThreadLocal ) );
+    for ( int s = 0; s < graph_slices; ++s )
+    {
+      launch_update( d, 0, cfg.min_delay );
+      launch_deliver( d );
+    }
+    CU( cudaStreamEndCapture( stream, &g ) );
+    cudaError_t e = cudaGraphInstantiate( &graph, g, 0 );
+    cudaGraphDestroy( g );
+    if ( e != cudaSuccess )
+      return fail( NG_ERR_CUDA, std::string( "cudaGraphInstantiate: " ) + cudaGetErrorString( e ) );
+    graph_generation = generation;
+    return NG_OK;
+  }
+
+  // enqueue n steps without host synchronisation
+  int
+  enqueue_steps( int64_t n )
+  {
+    const Net d = net();
+    while ( n > 0 )
+    {
+      if ( from == 0 && graph_slices > 0 && !profiling && n >= ( int64_t ) graph_slices * cfg.min_delay )
+      {
+        int rc = ensure_graph( d );
+        if ( rc )
+          return rc;
+        CU( cudaGraphLaunch( graph, stream ) );
+        const int64_t st = ( int64_t ) graph_slices * cfg.min_delay;
+        origin += st;
+        slices += graph_slices;
+        n -= st;
+        stats.update_launches += ( int64_t ) graph_slices * ( int64_t ) blk.size();
+        stats.deliver_launches += graph_slices;
+        continue;
+      }
+      const int to_ = ( int ) std::min< int64_t >( from + n, cfg.min_delay );
+      int rc = run_slice_range( d, from, to_ );
+      if ( rc )
+        return rc;
+      n -= to_ - from;
+      if ( to_ == cfg.min_delay )
+      {
+        origin += cfg.min_delay;
+        from = 0;
+        slices += 1;
+      }
+      else
+      {
+        from = to_;
+      }
+    }
+    return NG_OK;
+  }
+
+  int
+  prepare()
+  {
+    for ( auto& b : blk )
+      if ( b.dirty )
+      {
+        int rc = build_classes( b );
+        if ( rc )
+          return rc;
+      }
+    return NG_OK;
+  }
+
+  // one group: set ctl, enqueue, sync, drain
+  int
+  run_group( int64_t n )
+  {
+    const int64_t clock = origin + from;
+    const int64_t row0 = ( clock + 1 + trace_interval - 1 ) / trace_interval;
+    k_set_ctl<<< 1, 1, 0, stream >>>( ( Ctl* ) ctl.p, clock, row0, 1 );
+    CU( cudaGetLastError() );
+    int rc = enqueue_steps( n );
+    if ( rc )
+      return rc;
+    CU( cudaMemcpyAsync( host_ctl, ctl.p, sizeof( Ctl ), cudaMemcpyDeviceToHost, stream ) );
+    CU( cudaStreamSynchronize( stream ) );
+    const Ctl& c = *host_ctl;
+    if ( c.err & ERR_NUMERIC )
+      return fail( NG_ERR_NUMERIC, "NumericalInstability: aeif_cond_alpha state exploded (V_m < -1e3 or |w| > 1e6)" );
+    if ( c.err & ( ERR_SPIKE_LIST | ERR_LOG | ERR_TRACE ) )
+      return fail( NG_ERR_CAPACITY, "device spike list, spike log or trace buffer overflowed (err word "
+          + std::to_string( c.err ) + ")" );
+    // drain the spike log
+    const int64_t nl = ( int64_t ) c.log_count;
+    if ( nl > 0 )
+    {
+      std::vector< uint2 > tmp( ( size_t ) nl );
+      CU( cudaMemcpy( tmp.data(), log.p, sizeof( uint2 ) * ( size_t ) nl, cudaMemcpyDeviceToHost ) );
+      for ( const uint2& e : tmp )
+      {
+        const uint32_t mult = e.y >> 24;
+        const int64_t stamp = clock + ( int64_t ) ( e.y & 0xFFFFFFu );
+        for ( uint32_t m = 0; m < mult; ++m )
+        {
+          out_src.push_back( ( int32_t ) e.x );
+          out_stamp.push_back( stamp );
+        }
+      }
+    }
+    // drain the trace rows of this group
+    if ( n_trace_idx > 0 )
+    {
+      const int64_t end = origin + from;
+      const int64_t row_end = end / trace_interval;  // last complete row index
+      const int64_t rows = row_end - row0 + 1;
+      if ( rows > 0 )
+      {
+        const size_t cnt = ( size_t ) rows * ( size_t ) n_trace_idx * ( size_t ) n_trace_vars;
+        const size_t old = out_trace.size();
+        out_trace.resize( old + cnt );
+        CU( cudaMemcpy( out_trace.data() + old, trace.p, cnt * sizeof( double ), cudaMemcpyDeviceToHost ) );
+        if ( trace_first_stamp < 0 )
+          trace_first_stamp = row0 * trace_interval;
+      }
+    }
+    stats.spikes = ( int64_t ) c.n_spikes;
+    stats.syn_events = ( int64_t ) c.syn_events;
+    stats.drive_events = ( int64_t ) c.drive_events;
+    return NG_OK;
+  }
+
+  int
+  simulate( int64_t n )
+  {
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = prepare();
+    if ( rc )
+      return rc;
+    // group size: bounded by the spike-log and trace capacities
+    const int64_t per_step = std::max< int64_t >( 1, n_rec );
+    int64_t by_log = ( log_cap - n_sched ) / per_step;
+    if ( by_log < 1 )
+      return fail( NG_ERR_CAPACITY, "spike log capacity too small for one step" );
+    int64_t gmax = std::min< int64_t >( by_log, ( 1 << 24 ) - 2 );
+    if ( n_trace_idx > 0 )
+      gmax = std::min< int64_t >( gmax, ( trace_rows_cap - 1 ) * trace_interval );
+    if ( gmax < 1 )
+      return fail( NG_ERR_CAPACITY, "trace buffer too small" );
+    // keep groups to whole graph chunks where possible
+    const int64_t chunk = graph_slices > 0 ? ( int64_t ) graph_slices * cfg.min_delay : cfg.min_delay;
+    if ( gmax > chunk )
+      gmax = ( gmax / chunk ) * chunk;
+    while ( n > 0 )
+    {
+      const int64_t g = std::min( n, gmax );
+      rc = run_group( g );
+      if ( rc )
+        return rc;
+      n -= g;
+    }
+    stats.clock_steps = origin + from;
+    stats.slices = slices;
+    stats.simulate_ms += std::chrono::duration< double, std::milli >( std::chrono::steady_clock::now() - t0 ).count();
+    return NG_OK;
+  }
+};
+
+extern "C" {
+
+int
+ng_abi_version( void )
+{
+  return NG_ABI_VERSION;
+}
+
+const char*
+ng_last_error( void )
+{
+  return g_err.c_str();
+}
+
+int
+ng_device_count( int32_t* n )
+{
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount( &c );
+  if ( e != cudaSuccess )
+  {
+    *n = 0;
+    return fail( NG_ERR_CUDA, std::string( "cudaGetDeviceCount: " ) + cudaGetErrorString( e ) );
+  }
+  *n = c;
+  return NG_OK;
+}
+
+int
+ng_create( const ng_config* cfg, ng_engine** out )
+{
+  if ( !cfg || !out )
+    return fail( NG_ERR_ARG, "ng_create: null argument" );
+  *out = nullptr;
+  if ( cfg->precision != NG_FP64 && cfg->precision != NG_FP32 )
+    return fail( NG_ERR_ARG, "ng_create: precision must be NG_FP64 or NG_FP32" );
+  if ( !( cfg->h > 0 ) || !( cfg->tics_per_ms > 0 ) )
+    return fail( NG_ERR_ARG, "ng_create: resolution and tics_per_ms must be > 0" );
+  if ( cfg->min_delay < 1 || cfg->max_delay < cfg->min_delay )
+    return fail( NG_ERR_ARG, "ng_create: need 1 <= min_delay <= max_delay (steps)" );
+  if ( cfg->n_blocks < 1 || cfg->n_blocks > NG_MAX_BLOCKS )
+    return fail( NG_ERR_ARG, "ng_create: n_blocks out of range" );
+  int64_t N = 0;
+  for ( int k = 0; k < cfg->n_blocks; ++k )
+  {
+    if ( cfg->block_model[ k ] < 0 || cfg->block_model[ k ] > 2 || cfg->block_size[ k ] < 0 )
+      return fail( NG_ERR_ARG, "ng_create: bad block model or size" );
+    N += cfg->block_size[ k ];
+  }
+  if ( N < 1 || N >= ( 1ll << 30 ) || cfg->n_generators < 0 )
+    return fail( NG_ERR_ARG, "ng_create: neuron count out of range" );
+  int ndev = 0;
+  if ( cudaGetDeviceCount( &ndev ) != cudaSuccess || ndev == 0 )
+    return fail( NG_ERR_CUDA, "ng_create: no CUDA device available (the engine has no CPU fallback)" );
+  if ( cfg->device < 0 || cfg->device >= ndev )
+    return fail( NG_ERR_ARG, "ng_create: device ordinal out of range" );
+  CU( cudaSetDevice( cfg->device ) );
+  auto* e = new ng_engine();
+  e->cfg = *cfg;
+  e->prec = cfg->precision;
+  e->rsz = e->prec == NG_FP64 ? 8 : 4;
+  // Time::set_resolution: tics per step rounded, h = MS_PER_TIC * tics (nest_time.cpp:88-104)
+  e->tics_per_step = ( int64_t ) std::floor( cfg->tics_per_ms * cfg->h + 0.5 );
+  if ( e->tics_per_step < 1 )
+  {
+    delete e;
+    return fail( NG_ERR_ARG, "ng_create: resolution below one tic" );
+  }
+  e->h = ( 1 / cfg->tics_per_ms ) * ( double ) e->tics_per_step;
+  e->N = N;
+  e->n_src = N + cfg->n_generators;
+  e->L = cfg->min_delay + cfg->max_delay;
+  if ( cfg->start_step < 0 )
+  {
+    delete e;
+    return fail( NG_ERR_ARG, "ng_create: start_step must be >= 0" );
+  }
+  e->origin = cfg->start_step;
+  cudaDeviceProp prop;
+  if ( cudaGetDeviceProperties( &prop, cfg->device ) == cudaSuccess )
+    e->sms = prop.multiProcessorCount;
+  int rc = NG_OK;
+  auto bail = [ & ]( int code ) {
+    delete e;
+    return code;
+  };
+  if ( cudaStreamCreateWithFlags( &e->own, cudaStreamNonBlocking ) != cudaSuccess )
+    return bail( fail( NG_ERR_CUDA, "cudaStreamCreate failed" ) );
+  e->stream = e->own;
+  cudaEventCreate( &e->ev0 );
+  cudaEventCreate( &e->ev1 );
+  if ( cudaMallocHost( &e->host_ctl, sizeof( Ctl ) ) != cudaSuccess )
+    return bail( fail( NG_ERR_MEMORY, "cudaMallocHost failed" ) );
+  std::memset( e->host_ctl, 0, sizeof( Ctl ) );
+  int64_t off = 0;
+  for ( int k = 0; k < cfg->n_blocks; ++k )
+  {
+    ng_engine::Blk b;
+    b.model = cfg->block_model[ k ];
+    b.off = off;
+    b.n = cfg->block_size[ k ];
+    off += b.n;
+    std::vector< double > dp;
+    default_params( b.model, dp );
+    b.par.resize( ( size_t ) n_params( b.model ) );
+    for ( int p = 0; p < n_params( b.model ); ++p )
+      b.par[ p ].assign( ( size_t ) b.n, dp[ p ] );
+    e->blk.push_back( std::move( b ) );
+  }
+  for ( auto& b : e->blk )
+  {
+    for ( int s = 0; s < n_states( b.model ); ++s )
+    {
+      if ( ( rc = e->alloc( b.st[ s ], ( size_t ) b.n * e->rsz ) ) )
+        return bail( rc );
+      const double dv = default_state( b.model, s );
+      if ( dv != 0.0 )
+      {
+        std::vector< char > tmp( ( size_t ) b.n * e->rsz );
+        for ( int64_t i = 0; i < b.n; ++i )
+        {
+          if ( e->rsz == 8 )
+            reinterpret_cast< double* >( tmp.data() )[ i ] = dv;
+          else
+            reinterpret_cast< float* >( tmp.data() )[ i ] = ( float ) dv;
+        }
+        if ( ( rc = e->upload( b.st[ s ], tmp.data(), tmp.size() ) ) )
+          return bail( rc );
+      }
+    }
+    if ( ( rc = e->alloc( b.r, ( size_t ) b.n * sizeof( int32_t ) ) ) )
+      return bail( rc );
+    if ( b.model == NG_AEIF_COND_ALPHA )
+    {
+      std::vector< double > hs( ( size_t ) b.n, e->h );
+      if ( ( rc = e->upload( b.istep, hs.data(), hs.size() * sizeof( double ) ) ) )
+        return bail( rc );
+    }
+  }
+  // ring [L][C][N]
+  if ( ( rc = e->alloc( e->ring, ( size_t ) e->L * e->C * ( size_t ) N * 8 ) ) )
+    return bail( rc );
+  // empty CSR: every source has no edges
+  std::vector< int64_t > rp( ( size_t ) e->n_src + 1, 0 );
+  if ( ( rc = e->upload( e->row_ptr, rp.data(), rp.size() * sizeof( int64_t ) ) ) )
+    return bail( rc );
+  if ( ( rc = e->alloc( e->real_deg, ( size_t ) e->n_src * sizeof( int32_t ) ) ) )
+    return bail( rc );
+  if ( ( rc = e->alloc( e->tdc, 16 ) ) || ( rc = e->alloc( e->w, 32 ) ) )
+    return bail( rc );
+  e->tbits = 1;
+  while ( ( 1ll << e->tbits ) < N )
+    ++e->tbits;
+  if ( e->tbits > 30 )
+    return bail( fail( NG_ERR_ARG, "ng_create: too many neurons for the packed edge format" ) );
+  e->tmask = ( 1u << e->tbits ) - 1u;
+  const int dbits = 31 - e->tbits;
+  e->dmask = ( 1u << dbits ) - 1u;
+  if ( ( int64_t ) cfg->max_delay > ( int64_t ) e->dmask )
+    return bail( fail( NG_ERR_ARG, "ng_create: max_delay does not fit the packed edge format for this network size" ) );
+  e->spk_cap = std::min< int64_t >( e->n_src * ( int64_t ) cfg->min_delay, ( 1ll << 24 ) - 1 );
+  if ( ( rc = e->alloc( e->spk, ( size_t ) e->spk_cap * sizeof( int4 ) ) ) )
+    return bail( rc );
+  if ( ( rc = e->alloc( e->spk_off, ( size_t ) e->spk_cap * sizeof( long long ) ) ) )
+    return bail( rc );
+  e->log_cap = cfg->spike_log_capacity > 0 ? cfg->spike_log_capacity
+                                           : std::max< int64_t >( 1 << 22, 64 * e->n_src );
+  e->log_cap = std::min< int64_t >( e->log_cap, 1ll << 28 );
+  if ( ( rc = e->alloc( e->log, ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
+    return bail( rc );
+  if ( ( rc = e->alloc( e->rec, ( size_t ) e->n_src ) ) )
+    return bail( rc );
+  if ( ( rc = e->alloc( e->ctl, sizeof( Ctl ) ) ) )
+    return bail( rc );
+  {
+    const long long o = ( long long ) cfg->start_step;
+    if ( cudaMemcpyAsync( ( char* ) e->ctl.p + offsetof( Ctl, origin ), &o, sizeof( o ), cudaMemcpyHostToDevice,
+           e->stream )
+      != cudaSuccess )
+      return bail( fail( NG_ERR_CUDA, "ng_create: control block upload failed" ) );
+  }
+  e->deliver_ctas = std::max( 1, std::min( e->sms * 4, 1 ) );
+  if ( cudaStreamSynchronize( e->stream ) != cudaSuccess )
+    return bail( fail( NG_ERR_CUDA, "ng_create: device initialisation failed" ) );
+  *out = e;
+  return NG_OK;
+}
+
+int
+ng_destroy( ng_engine* eng )
+{
+  delete eng;
+  return NG_OK;
+}
+
+static int
+check_range( ng_engine* e, int32_t block, int64_t first, int64_t count )
+{
+  if ( !e )
+    return fail( NG_ERR_ARG, "null engine" );
+  if ( block < 0 || block >= ( int32_t ) e->blk.size() )
+    return fail( NG_ERR_ARG, "block index out of range" );
+  if ( first < 0 || count < 0 || first + count > e->blk[ block ].n )
+    return fail( NG_ERR_ARG, "neuron range out of bounds" );
+  return NG_OK;
+}
+
+int
+ng_set_var( ng_engine* e, int32_t block, const char* name, const double* values, int64_t first, int64_t count )
+{
+  int rc = check_range( e, block, first, count );
+  if ( rc )
+    return rc;
+  if ( !name || ( count > 0 && !values ) )
+    return fail( NG_ERR_ARG, "ng_set_var: null argument" );
+  auto& b = e->blk[ block ];
+  const VarSpec* v = find_var( b.model, name );
+  if ( !v )
+    return fail( NG_ERR_UNKNOWN_NAME, std::string( "unknown variable '" ) + name + "' for this model" );
+  cudaSetDevice( e->cfg.device );
+  if ( count == 0 )
+    return NG_OK;
+  if ( v->kind == PARAM )
+  {
+    std::copy( values, values + count, b.par[ v->slot ].begin() + first );
+    b.dirty = true;
+    return NG_OK;
+  }
+  if ( v->kind == REFR )
+  {
+    std::vector< int32_t > tmp( ( size_t ) count );
+    for ( int64_t i = 0; i < count; ++i )
+      tmp[ i ] = ( int32_t ) values[ i ];
+    CU( cudaMemcpyAsync( ( int32_t* ) b.r.p + first, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    return NG_OK;
+  }
+  if ( v->kind == ISTEP )
+  {
+    CU( cudaMemcpyAsync( ( double* ) b.istep.p + first, values, ( size_t ) count * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    return NG_OK;
+  }
+  if ( e->rsz == 8 )
+  {
+    CU( cudaMemcpyAsync( ( double* ) b.st[ v->slot ].p + first, values, ( size_t ) count * 8, cudaMemcpyHostToDevice,
+      e->stream ) );
+  }
+  else
+  {
+    std::vector< float > tmp( ( size_t ) count );
+    for ( int64_t i = 0; i < count; ++i )
+      tmp[ i ] = ( float ) values[ i ];
+    CU( cudaMemcpyAsync( ( float* ) b.st[ v->slot ].p + first, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice,
+      e->stream ) );
+  }
+  CU( cudaStreamSynchronize( e->stream ) );
+  return NG_OK;
+}
+
+int
+ng_get_var( ng_engine* e, int32_t block, const char* name, double* out, int64_t first, int64_t count )
+{
+  int rc = check_range( e, block, first, count );
+  if ( rc )
+    return rc;
+  if ( !name || ( count > 0 && !out ) )
+    return fail( NG_ERR_ARG, "ng_get_var: null argument" );
+  auto& b = e->blk[ block ];
+  const VarSpec* v = find_var( b.model, name );
+  if ( !v )
+    return fail( NG_ERR_UNKNOWN_NAME, std::string( "unknown variable '" ) + name + "' for this model" );
+  cudaSetDevice( e->cfg.device );
+  if ( count == 0 )
+    return NG_OK;
+  if ( v->kind == PARAM )
+  {
+    std::copy( b.par[ v->slot ].begin() + first, b.par[ v->slot ].begin() + first + count, out );
+    return NG_OK;
+  }
+  if ( v->kind == REFR )
+  {
+    std::vector< int32_t > tmp( ( size_t ) count );
+    CU( cudaMemcpyAsync( tmp.data(), ( int32_t* ) b.r.p + first, tmp.size() * 4, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    for ( int64_t i = 0; i < count; ++i )
+      out[ i ] = tmp[ i ];
+    return NG_OK;
+  }
+  if ( v->kind == ISTEP )
+  {
+    CU( cudaMemcpyAsync( out, ( double* ) b.istep.p + first, ( size_t ) count * 8, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    return NG_OK;
+  }
+  if ( e->rsz == 8 )
+  {
+    CU( cudaMemcpyAsync( out, ( double* ) b.st[ v->slot ].p + first, ( size_t ) count * 8, cudaMemcpyDeviceToHost,
+      e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  else
+  {
+    std::vector< float > tmp( ( size_t ) count );
+    CU( cudaMemcpyAsync( tmp.data(), ( float* ) b.st[ v->slot ].p + first, tmp.size() * 4, cudaMemcpyDeviceToHost,
+      e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    for ( int64_t i = 0; i < count; ++i )
+      out[ i ] = tmp[ i ];
+  }
+  return NG_OK;
+}
+
+int
+ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const int32_t* target, const double* weight,
+  const int32_t* delay_steps )
+{
+  if ( !e || !row_ptr )
+    return fail( NG_ERR_ARG, "ng_set_connections: null argument" );
+  if ( n_src != e->n_src )
+    return fail( NG_ERR_ARG, "ng_set_connections: n_src must equal n_neurons + n_generators" );
+  const int64_t nnz = row_ptr[ n_src ];
+  if ( row_ptr[ 0 ] != 0 || nnz < 0 || ( nnz > 0 && ( !target || !weight || !delay_steps ) ) )
+    return fail( NG_ERR_ARG, "ng_set_connections: bad CSR" );
+  cudaSetDevice( e->cfg.device );
+  std::vector< int64_t > prow( ( size_t ) n_src + 1, 0 );
+  std::vector< int32_t > rdeg( ( size_t ) n_src, 0 );
+  for ( int64_t s = 0; s < n_src; ++s )
+  {
+    const int64_t deg = row_ptr[ s + 1 ] - row_ptr[ s ];
+    if ( deg < 0 || deg > INT32_MAX )
+      return fail( NG_ERR_ARG, "ng_set_connections: row pointers must be non-decreasing" );
+    rdeg[ s ] = ( int32_t ) deg;
+    prow[ s + 1 ] = prow[ s ] + ( ( deg + 3 ) & ~3ll );
+  }
+  const int64_t np = prow[ n_src ];
+  // per-edge channel and effective weight by the target's model
+  std::vector< int > model_of_block;
+  std::vector< int64_t > bend;
+  for ( auto& b : e->blk )
+  {
+    model_of_block.push_back( b.model );
+    bend.push_back( b.off + b.n );
+  }
+  std::vector< uint32_t > tdc( ( size_t ) std::max< int64_t >( np, 4 ), 0u );
+  std::vector< double > weff( ( size_t ) std::max< int64_t >( np, 4 ), 0.0 );
+  double maxabs = 0.0;
+  for ( int64_t s = 0; s < n_src; ++s )
+  {
+    int64_t k = prow[ s ];
+    for ( int64_t j = row_ptr[ s ]; j < row_ptr[ s + 1 ]; ++j, ++k )
+    {
+      const int64_t t = target[ j ];
+      const int32_t d = delay_steps[ j ];
+      if ( t < 0 || t >= e->N )
+        return fail( NG_ERR_ARG, "ng_set_connections: target out of range" );
+      if ( d < e->cfg.min_delay || d > e->cfg.max_delay )
+        return fail( NG_ERR_ARG, "ng_set_connections: delay outside [min_delay, max_delay]" );
+      const double wv = weight[ j ];
+      if ( !std::isfinite( wv ) )
+        return fail( NG_ERR_ARG, "ng_set_connections: weight not finite" );
+      const int bk = ( int ) ( std::upper_bound( bend.begin(), bend.end(), t ) - bend.begin() );
+      const int model = model_of_block[ bk ];
+      uint32_t ch = 0;
+      double we = wv;
+      if ( model == NG_IAF_PSC_EXP )
+        ch = wv > 0 ? 0u : 1u;  // iaf_psc_exp.cpp:351-362
+      else if ( model == NG_AEIF_COND_ALPHA && !( wv > 0.0 ) )
+      {
+        ch = 1u;  // aeif_cond_alpha.cpp:536-550 stores -w in the inhibitory buffer
+        we = -wv;
+      }
+      tdc[ k ] = ( uint32_t ) t | ( ( uint32_t ) d << e->tbits ) | ( ch << 31 );
+      weff[ k ] = we;
+      maxabs = std::max( maxabs, std::fabs( we ) );
+    }
+  }
+  int rc;
+  if ( ( rc = e->upload( e->row_ptr, prow.data(), prow.size() * sizeof( int64_t ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->real_deg, rdeg.data(), rdeg.size() * sizeof( int32_t ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->tdc, tdc.data(), tdc.size() * sizeof( uint32_t ) ) ) )
+    return rc;
+  if ( e->prec == NG_FP64 )
+  {
+    if ( ( rc = e->upload( e->w, weff.data(), weff.size() * sizeof( double ) ) ) )
+      return rc;
+    e->fx_inv = 1.0;
+  }
+  else
+  {
+    // int32 fixed point with a power-of-two scale: |w| * 2^S < 2^31
+    int S = 0;
+    if ( maxabs > 0 )
+    {
+      S = ( int ) std::floor( std::log2( 2147483647.0 / maxabs ) );
+      S = std::max( -30, std::min( S, 60 ) );
+      while ( S > -30 && std::ldexp( maxabs, S ) >= 2147483647.0 )
+        --S;
+    }
+    std::vector< int32_t > wf( weff.size(), 0 );
+    for ( size_t k = 0; k < weff.size(); ++k )
+      wf[ k ] = ( int32_t ) std::llrint( std::ldexp( weff[ k ], S ) );
+    if ( ( rc = e->upload( e->w, wf.data(), wf.size() * sizeof( int32_t ) ) ) )
+      return rc;
+    e->fx_inv = std::ldexp( 1.0, -S );
+  }
+  e->nnz_padded = np;
+  // delivery grid: enough CTAs for the expected events of a slice, at most 4 per SM
+  const int64_t quads = np / 4;
+  const int64_t want = std::max< int64_t >( 1, quads / 256 / 8 );
+  e->deliver_ctas = ( int ) std::min< int64_t >( want, ( int64_t ) e->sms * 4 );
+  CU( cudaStreamSynchronize( e->stream ) );
+  ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_set_connections_coo( ng_engine* e, int64_t n_src, int64_t nnz, const int32_t* source, const int32_t* target,
+  const double* weight, const int32_t* delay_steps )
+{
+  if ( !e || nnz < 0 || ( nnz > 0 && ( !source || !target || !weight || !delay_steps ) ) )
+    return fail( NG_ERR_ARG, "ng_set_connections_coo: bad argument" );
+  if ( n_src != e->n_src )
+    return fail( NG_ERR_ARG, "ng_set_connections_coo: n_src must equal n_neurons + n_generators" );
+  std::vector< int64_t > row( ( size_t ) n_src + 1, 0 );
+  for ( int64_t k = 0; k < nnz; ++k )
+  {
+    const int32_t s = source[ k ];
+    if ( s < 0 || s >= n_src )
+      return fail( NG_ERR_ARG, "ng_set_connections_coo: source out of range" );
+    ++row[ ( size_t ) s + 1 ];
+  }
+  for ( int64_t s = 0; s < n_src; ++s )
+    row[ s + 1 ] += row[ s ];
+  std::vector< int64_t > pos( row.begin(), row.end() - 1 );
+  std::vector< int32_t > tg( ( size_t ) std::max< int64_t >( nnz, 1 ) );
+  std::vector< double > ww( ( size_t ) std::max< int64_t >( nnz, 1 ) );
+  std::vector< int32_t > dd( ( size_t ) std::max< int64_t >( nnz, 1 ) );
+  for ( int64_t k = 0; k < nnz; ++k )
+  {
+    const int64_t j = pos[ source[ k ] ]++;
+    tg[ j ] = target[ k ];
+    ww[ j ] = weight[ k ];
+    dd[ j ] = delay_steps[ k ];
+  }
+  return ng_set_connections( e, n_src, row.data(), tg.data(), ww.data(), dd.data() );
+}
+
+int
+ng_set_spike_schedule( ng_engine* e, int64_t n, const int64_t* emit_step, const int32_t* source )
+{
+  if ( !e || n < 0 || ( n > 0 && ( !emit_step || !source ) ) )
+    return fail( NG_ERR_ARG, "ng_set_spike_schedule: bad argument" );
+  cudaSetDevice( e->cfg.device );
+  for ( int64_t i = 0; i < n; ++i )
+  {
+    if ( i > 0 && emit_step[ i ] < emit_step[ i - 1 ] )
+      return fail( NG_ERR_ARG, "ng_set_spike_schedule: steps must be sorted" );
+    if ( source[ i ] < 0 || source[ i ] >= e->n_src )
+      return fail( NG_ERR_ARG, "ng_set_spike_schedule: source out of range" );
+  }
+  int rc;
+  if ( ( rc = e->upload( e->sched_step, emit_step, ( size_t ) n * sizeof( int64_t ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->sched_src, source, ( size_t ) n * sizeof( int32_t ) ) ) )
+    return rc;
+  e->n_sched = n;
+  // the spike list must also hold the generator spikes of one slice
+  const int64_t need = std::min< int64_t >( e->n_src * ( int64_t ) e->cfg.min_delay + n, ( 1ll << 24 ) - 1 );
+  if ( need > e->spk_cap )
+  {
+    e->spk_cap = need;
+    if ( ( rc = e->alloc( e->spk, ( size_t ) e->spk_cap * sizeof( int4 ) ) ) )
+      return rc;
+    if ( ( rc = e->alloc( e->spk_off, ( size_t ) e->spk_cap * sizeof( long long ) ) ) )
+      return rc;
+  }
+  if ( e->log_cap < 2 * n + 4 * e->n_src )
+  {
+    e->log_cap = 2 * n + 4 * e->n_src;
+    if ( ( rc = e->alloc( e->log, ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
+      return rc;
+  }
+  // consume entries already in the past
+  const int64_t clock = e->origin + e->from;
+  int64_t pos = 0;
+  while ( pos < n && emit_step[ pos ] < clock )
+    ++pos;
+  CU( cudaMemcpyAsync( ( char* ) e->ctl.p + offsetof( Ctl, sched_pos ), &pos, sizeof( long long ),
+    cudaMemcpyHostToDevice, e->stream ) );
+  CU( cudaStreamSynchronize( e->stream ) );
+  ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const int32_t* delay_steps,
+  int64_t start_step, int64_t stop_step, uint64_t seed )
+{
+  if ( !e || !rate_hz || !weight || !delay_steps )
+    return fail( NG_ERR_ARG, "ng_set_poisson: null argument" );
+  cudaSetDevice( e->cfg.device );
+  const int64_t n = e->N;
+  std::vector< double4 > tab( ( size_t ) n );
+  bool any = false;
+  for ( int64_t i = 0; i < n; ++i )
+  {
+    if ( rate_hz[ i ] > 0 && ( delay_steps[ i ] < e->cfg.min_delay || delay_steps[ i ] > e->cfg.max_delay ) )
+      return fail( NG_ERR_ARG, "ng_set_poisson: delay outside [min_delay, max_delay]" );
+    // lambda = h * rate * 1e-3 (models/poisson_generator.cpp:114)
+    const double lam = rate_hz[ i ] > 0 ? e->h * rate_hz[ i ] * 1e-3 : 0.0;
+    tab[ i ] = poisson_table( lam );
+    any = any || lam > 0;
+  }
+  int rc;
+  if ( ( rc = e->upload( e->pois, tab.data(), tab.size() * sizeof( double4 ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->pois_w, weight, ( size_t ) n * sizeof( double ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->pois_d, delay_steps, ( size_t ) n * sizeof( int32_t ) ) ) )
+    return rc;
+  e->has_pois = any ? 1 : 0;
+  e->pois_start = start_step;
+  e->pois_stop = stop_step;
+  e->key0 = ( uint32_t ) seed;
+  e->key1 = ( uint32_t ) ( seed >> 32 );
+  CU( cudaStreamSynchronize( e->stream ) );
+  ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_set_recording( ng_engine* e, const uint8_t* flags )
+{
+  if ( !e || !flags )
+    return fail( NG_ERR_ARG, "ng_set_recording: null argument" );
+  cudaSetDevice( e->cfg.device );
+  int64_t nr = 0;
+  for ( int64_t i = 0; i < e->n_src; ++i )
+    nr += flags[ i ] ? 1 : 0;
+  std::vector< uint8_t > f( flags, flags + e->n_src );
+  int rc = e->upload( e->rec, f.data(), f.size() );
+  if ( rc )
+    return rc;
+  e->n_rec = nr;
+  CU( cudaStreamSynchronize( e->stream ) );
+  ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_set_trace( ng_engine* e, int64_t n_idx, const int32_t* neuron, int32_t n_vars, const char* const* vars,
+  int32_t interval_steps )
+{
+  if ( !e || n_idx < 0 || ( n_idx > 0 && ( !neuron || !vars || n_vars < 1 ) ) || interval_steps < 1
+    || n_vars > MAX_STATE || n_vars < 0 )
+    return fail( NG_ERR_ARG, "ng_set_trace: bad argument" );
+  cudaSetDevice( e->cfg.device );
+  std::vector< int32_t > col( ( size_t ) e->N, -1 );
+  int model = -1;
+  for ( int64_t k = 0; k < n_idx; ++k )
+  {
+    const int32_t i = neuron[ k ];
+    if ( i < 0 || i >= e->N || col[ i ] >= 0 )
+      return fail( NG_ERR_ARG, "ng_set_trace: neuron index out of range or repeated" );
+    col[ i ] = ( int32_t ) k;
+    const int bk = e->block_of( i );
+    if ( model >= 0 && e->blk[ bk ].model != model )
+      return fail( NG_ERR_ARG, "ng_set_trace: traced neurons must share one model" );
+    model = e->blk[ bk ].model;
+  }
+  int8_t slots[ MAX_STATE ] = { 0, 0, 0, 0, 0, 0, 0, 0 };
+  if ( n_idx > 0 )
+  {
+    for ( int32_t v = 0; v < n_vars; ++v )
+    {
+      const VarSpec* vs = vars[ v ] ? find_var( model, vars[ v ] ) : nullptr;
+      if ( !vs || vs->kind != STATE )
+        return fail( NG_ERR_UNKNOWN_NAME, std::string( "ng_set_trace: '" ) + ( vars[ v ] ? vars[ v ] : "(null)" )
+            + "' is not a recordable state of this model" );
+      slots[ v ] = ( int8_t ) vs->slot;
+    }
+  }
+  int rc = e->upload( e->trace_col, col.data(), col.size() * sizeof( int32_t ) );
+  if ( rc )
+    return rc;
+  e->n_trace_idx = n_idx > 0 ? ( int32_t ) n_idx : 0;
+  e->n_trace_vars = n_idx > 0 ? n_vars : 0;
+  std::copy( slots, slots + MAX_STATE, e->trace_slot );
+  e->trace_interval = interval_steps;
+  // rows held per group: bounded to 256 MB
+  const int64_t per_row = std::max< int64_t >( 1, n_idx * std::max< int32_t >( 1, n_vars ) ) * 8;
+  e->trace_rows_cap = std::max< int64_t >( 2, std::min< int64_t >( ( 256ll << 20 ) / per_row, 1 << 20 ) );
+  if ( n_idx > 0 && ( rc = e->alloc( e->trace, ( size_t ) ( e->trace_rows_cap * per_row ) ) ) )
+    return rc;
+  e->out_trace.clear();
+  e->trace_first_stamp = -1;
+  CU( cudaStreamSynchronize( e->stream ) );
+  ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_simulate( ng_engine* e, int64_t n_steps )
+{
+  if ( !e || n_steps < 0 )
+    return fail( NG_ERR_ARG, "ng_simulate: bad argument" );
+  CU( cudaSetDevice( e->cfg.device ) );
+  return e->simulate( n_steps );
+}
+
+int
+ng_spike_count( ng_engine* e, int64_t* n )
+{
+  if ( !e || !n )
+    return fail( NG_ERR_ARG, "ng_spike_count: null argument" );
+  *n = ( int64_t ) e->out_src.size();
+  return NG_OK;
+}
+
+int
+ng_get_spikes( ng_engine* e, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out )
+{
+  if ( !e || !n_out || cap < 0 || ( cap > 0 && ( !source || !stamp ) ) )
+    return fail( NG_ERR_ARG, "ng_get_spikes: bad argument" );
+  const int64_t k = std::min< int64_t >( cap, ( int64_t ) e->out_src.size() );
+  std::copy( e->out_src.begin(), e->out_src.begin() + k, source );
+  std::copy( e->out_stamp.begin(), e->out_stamp.begin() + k, stamp );
+  e->out_src.erase( e->out_src.begin(), e->out_src.begin() + k );
+  e->out_stamp.erase( e->out_stamp.begin(), e->out_stamp.begin() + k );
+  *n_out = k;
+  return NG_OK;
+}
+
+int
+ng_trace_count( ng_engine* e, int64_t* n_rows, int64_t* first_stamp )
+{
+  if ( !e || !n_rows || !first_stamp )
+    return fail( NG_ERR_ARG, "ng_trace_count: null argument" );
+  const int64_t w = ( int64_t ) e->n_trace_idx * e->n_trace_vars;
+  *n_rows = w > 0 ? ( int64_t ) e->out_trace.size() / w : 0;
+  *first_stamp = e->trace_first_stamp;
+  return NG_OK;
+}
+
+int
+ng_get_trace( ng_engine* e, double* out, int64_t max_rows, int64_t* n_rows_out )
+{
+  if ( !e || !n_rows_out || max_rows < 0 || ( max_rows > 0 && !out ) )
+    return fail( NG_ERR_ARG, "ng_get_trace: bad argument" );
+  if ( e->n_trace_idx == 0 )
+  {
+    *n_rows_out = 0;
+    return NG_OK;
+  }
+  const int64_t w = ( int64_t ) e->n_trace_idx * e->n_trace_vars;
+  const int64_t rows = std::min< int64_t >( max_rows, ( int64_t ) e->out_trace.size() / w );
+  const size_t cnt = ( size_t ) ( rows * w );
+  std::copy( e->out_trace.begin(), e->out_trace.begin() + cnt, out );
+  e->out_trace.erase( e->out_trace.begin(), e->out_trace.begin() + cnt );
+  if ( rows > 0 )
+    e->trace_first_stamp += rows * e->trace_interval;
+  if ( e->out_trace.empty() )
+    e->trace_first_stamp = -1;
+  *n_rows_out = rows;
+  return NG_OK;
+}
+
+int
+ng_get_stats( ng_engine* e, ng_stats* out )
+{
+  if ( !e || !out )
+    return fail( NG_ERR_ARG, "ng_get_stats: null argument" );
+  e->stats.clock_steps = e->origin + e->from;
+  e->stats.slices = e->slices;
+  *out = e->stats;
+  return NG_OK;
+}
+
+int
+ng_set_profiling( ng_engine* e, int32_t on )
+{
+  if ( !e )
+    return fail( NG_ERR_ARG, "null engine" );
+  e->profiling = on ? 1 : 0;
+  return NG_OK;
+}
+
+int
+ng_set_stream( ng_engine* e, void* cuda_stream )
+{
+  if ( !e )
+    return fail( NG_ERR_ARG, "null engine" );
+  e->stream = cuda_stream ? ( cudaStream_t ) cuda_stream : e->own;
+  if ( e->graph )
+  {
+    cudaGraphExecDestroy( e->graph );
+    e->graph = nullptr;
+  }
+  return NG_OK;
+}
+
+int
+ng_set_graph_slices( ng_engine* e, int32_t slices_per_graph )
+{
+  if ( !e || slices_per_graph < 0 || slices_per_graph > 4096 )
+    return fail( NG_ERR_ARG, "ng_set_graph_slices: bad argument" );
+  e->graph_slices = slices_per_graph;
+  ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_debug_coefficients( ng_engine* e, int32_t block, int64_t index, double* out, int32_t cap, int32_t* n_out )
+{
+  int rc = check_range( e, block, index, 1 );
+  if ( rc )
+    return rc;
+  auto& b = e->blk[ block ];
+  if ( b.dirty && ( rc = e->build_classes( b ) ) )
+    return rc;
+  const double* row = b.host_ctab.data() + ( size_t ) b.host_cls[ ( size_t ) index ] * CT_STRIDE;
+  std::vector< double > v;
+  if ( b.model == NG_IAF_PSC_DELTA )
+    v = { row[ 0 ], row[ 1 ], row[ 5 ] };
+  else if ( b.model == NG_IAF_PSC_EXP )
+    v = { row[ 4 ], row[ 5 ], row[ 0 ], row[ 1 ], row[ 2 ], row[ 3 ], row[ 8 ] };
+  else
+    v = { row[ 15 ], row[ 16 ], row[ 17 ], row[ 18 ] };
+  const int32_t k = std::min< int32_t >( cap, ( int32_t ) v.size() );
+  std::copy( v.begin(), v.begin() + k, out );
+  *n_out = k;
+  return NG_OK;
+}
+
+}  // extern "C"

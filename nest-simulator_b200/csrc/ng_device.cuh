@@ -1,0 +1,164 @@
+// ng_device.cuh -- device-side data layout and helpers of the slice engine.
+//
+// HBM layout (one engine = one network, N neurons, L = min_delay + max_delay):
+//   state     SoA arrays per model block, FP64 (plain) or FP32 (precision form)
+//   classes   per-neuron class id -> row of FP64 coefficients (propagators,
+//             thresholds, refractory counts) computed on the host
+//   ring      [L][C][N] FP64 (plain) or int64 fixed point (precision form),
+//             C = 2 input channels (excitatory / inhibitory)
+//   CSR       row_ptr[n_src+1] (rows padded to multiples of 4 edges),
+//             packed edge word tgt | delay << tbits | channel << 31 (u32),
+//             weight FP64 (plain) or int32 fixed point (precision form)
+//   spikes    per-slice list of (source, emission step mod L, multiplicity)
+//             with the prefix offsets of their padded out-degrees
+//   log       (source, stamp - log_base | multiplicity << 24) for recorders
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ng
+{
+
+constexpr int CT_STRIDE = 20;  // doubles per coefficient-class row
+constexpr int MAX_STATE = 8;
+constexpr uint32_t DRIVE_STREAM = 0x504F4953u;
+constexpr int ERR_NUMERIC = 1;
+constexpr int ERR_SPIKE_LIST = 2;
+constexpr int ERR_LOG = 4;
+constexpr int ERR_TRACE = 8;
+constexpr int SPK_SHIFT = 40;
+constexpr unsigned long long EV_MASK = ( 1ull << SPK_SHIFT ) - 1ull;
+
+// Control block in device memory, shared by all kernels of an engine.
+struct Ctl
+{
+  unsigned long long spk_packed;  // (spikes << 40) | padded events of the open slice
+  unsigned long long log_count;
+  unsigned long long syn_events;
+  unsigned long long drive_events;
+  unsigned long long n_spikes;
+  long long origin;     // slice origin [steps]
+  long long log_base;   // stamp offset of the log entries
+  long long trace_row0; // first trace row index held in the buffer
+  long long sched_pos;  // next unconsumed scheduled generator spike
+  int deliver_done;     // finished CTAs of the running delivery launch
+  int err;
+};
+
+struct Block
+{
+  int64_t off, n;
+  int model;
+  const int32_t* cls;
+  const double* ctab;
+  void* s[ MAX_STATE ];
+  int32_t* r;
+  double* istep;
+};
+
+struct Net
+{
+  int64_t N, n_src;
+  int32_t L, C, min_delay;
+  int32_t tbits;
+  uint32_t tmask, dmask;
+  void* ring;
+  double fx_inv;  // precision form: 2^-S of the fixed-point weights
+  const int64_t* row_ptr;
+  const int32_t* real_deg;
+  const uint32_t* edge_tdc;
+  const void* edge_w;
+  int4* spk;
+  long long* spk_off;
+  int64_t spk_cap;
+  uint2* log;
+  int64_t log_cap;
+  const uint8_t* rec;
+  const double4* pois;  // lambda, p_m, F_m, m
+  const double* pois_w;
+  const int32_t* pois_d;
+  int64_t pois_start, pois_stop;
+  uint32_t key0, key1;
+  int has_pois;
+  const int32_t* trace_col;
+  double* trace;
+  int32_t n_trace_idx, trace_interval, n_trace_vars;
+  int8_t trace_slot[ MAX_STATE ];
+  int64_t trace_rows;
+  const int64_t* sched_step;
+  const int32_t* sched_src;
+  int64_t n_sched;
+  Ctl* ctl;
+};
+
+// ---------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11), u53 and Poisson inversion from the
+// mode.  Identical arithmetic on host and device: only integer ops, exact
+// int->double conversions, and IEEE multiplies/divides/adds (no contraction).
+// ---------------------------------------------------------------------
+__host__ __device__ inline void
+philox4x32_10( uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t out[ 4 ] )
+{
+#pragma unroll
+  for ( int r = 0; r < 10; ++r )
+  {
+    if ( r > 0 )
+    {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint64_t p0 = ( uint64_t ) 0xD2511F53u * c0;
+    const uint64_t p1 = ( uint64_t ) 0xCD9E8D57u * c2;
+    const uint32_t n0 = ( uint32_t ) ( p1 >> 32 ) ^ c1 ^ k0;
+    const uint32_t n1 = ( uint32_t ) p1;
+    const uint32_t n2 = ( uint32_t ) ( p0 >> 32 ) ^ c3 ^ k1;
+    const uint32_t n3 = ( uint32_t ) p0;
+    c0 = n0;
+    c1 = n1;
+    c2 = n2;
+    c3 = n3;
+  }
+  out[ 0 ] = c0;
+  out[ 1 ] = c1;
+  out[ 2 ] = c2;
+  out[ 3 ] = c3;
+}
+
+__host__ __device__ inline double
+u53( uint32_t a, uint32_t b )
+{
+  return ( ( double ) ( a >> 5 ) * 67108864.0 + ( double ) ( b >> 6 ) ) * ( 1.0 / 9007199254740992.0 );
+}
+
+// tab = (lambda, p_m, F_m, m): walk from the mode m up while u > F or down
+// while u <= F - p.
+__host__ __device__ inline long long
+poisson_from_mode( double4 tab, double u )
+{
+  const double lam = tab.x;
+  long long k = ( long long ) tab.w;
+  double p = tab.y, F = tab.z;
+  if ( u > F )
+  {
+    const long long kmax = k + 100000;
+    while ( u > F && k < kmax )
+    {
+      k += 1;
+      p = p * lam / ( double ) k;
+      F += p;
+      if ( p == 0.0 )
+        break;
+    }
+    return k;
+  }
+  while ( k > 0 && u <= F - p )
+  {
+    F -= p;
+    p = p * ( double ) k / lam;
+    k -= 1;
+  }
+  return k;
+}
+
+}  // namespace ng

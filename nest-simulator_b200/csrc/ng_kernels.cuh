@@ -1,0 +1,766 @@
+// ng_kernels.cuh -- sm_100a kernels of one min_delay slice.
+//
+// Per slice: one node-update launch per model block (thread per neuron, the
+// lags of the slice in registers, warp-ballot spike compaction, Philox drive
+// fused), then one delivery launch (source-spike-driven scatter over the CSR
+// with 128-bit edge loads and red.global adds into the ring buffers).  The
+// delivery launch's last CTA closes the slice: it resets the spike list and
+// advances the device clock, so a run of slices needs no host round trip and
+// can be captured as one CUDA graph.
+//
+// Compiled with -fmad=false: every FP64 multiply and add rounds on its own as
+// in the reference's x86-64 build, which makes the plain form bit-exact where
+// the ring sums are order independent.
+#pragma once
+
+#include "ng_device.cuh"
+
+namespace ng
+{
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template < typename T >
+__device__ __forceinline__ T
+ld_volatile( const T* p )
+{
+  return *( const volatile T* ) p;
+}
+
+__device__ __forceinline__ long long
+warp_sum_ll( long long v )
+{
+#pragma unroll
+  for ( int o = 16; o > 0; o >>= 1 )
+    v += __shfl_xor_sync( FULL, v, o );
+  return v;
+}
+
+// Append this lane's spike (if any) to the slice's spike list and the
+// recorder log.  Must be called by all 32 lanes of the warp.
+__device__ __forceinline__ void
+warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, long long stamp )
+{
+  const unsigned m = __ballot_sync( FULL, spk );
+  if ( m == 0 )
+    return;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = ( 1u << lane ) - 1u;
+  long long pdeg = 0, rdeg = 0;
+  if ( spk )
+  {
+    pdeg = d.row_ptr[ src + 1 ] - d.row_ptr[ src ];
+    rdeg = ( long long ) d.real_deg[ src ] * mult;
+  }
+  long long incl = pdeg;
+#pragma unroll
+  for ( int o = 1; o < 32; o <<= 1 )
+  {
+    const long long v = __shfl_up_sync( FULL, incl, o );
+    if ( lane >= o )
+      incl += v;
+  }
+  const long long tot = __shfl_sync( FULL, incl, 31 );
+  const long long rtot = warp_sum_ll( rdeg );
+  const long long mtot = warp_sum_ll( spk ? ( long long ) mult : 0ll );
+  unsigned long long base = 0;
+  if ( lane == 0 )
+  {
+    base = atomicAdd( &d.ctl->spk_packed,
+      ( ( unsigned long long ) __popc( m ) << SPK_SHIFT ) | ( unsigned long long ) tot );
+    atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
+    atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) mtot );
+  }
+  base = __shfl_sync( FULL, base, 0 );
+  if ( spk )
+  {
+    const long long idx = ( long long ) ( base >> SPK_SHIFT ) + __popc( m & lt );
+    const long long off = ( long long ) ( base & EV_MASK ) + incl - pdeg;
+    if ( idx < d.spk_cap )
+    {
+      d.spk[ idx ] = make_int4( src, tmod, mult, 0 );
+      d.spk_off[ idx ] = off;
+    }
+    else
+    {
+      atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+    }
+  }
+  const bool lg = spk && ( d.rec == nullptr || d.rec[ src ] );
+  const unsigned lm = __ballot_sync( FULL, lg );
+  if ( lm )
+  {
+    unsigned long long lb = 0;
+    if ( lane == 0 )
+      lb = atomicAdd( &d.ctl->log_count, ( unsigned long long ) __popc( lm ) );
+    lb = __shfl_sync( FULL, lb, 0 );
+    if ( lg )
+    {
+      const long long li = ( long long ) lb + __popc( lm & lt );
+      if ( li < d.log_cap )
+      {
+        const uint32_t rel = ( uint32_t ) ( stamp - ld_volatile( &d.ctl->log_base ) );
+        const uint32_t mu = ( uint32_t ) ( mult < 255 ? mult : 255 );
+        d.log[ li ] = make_uint2( ( uint32_t ) src, rel | ( mu << 24 ) );
+      }
+      else
+      {
+        atomicOr( &d.ctl->err, ERR_LOG );
+      }
+    }
+  }
+}
+
+// Poisson drive value for neuron i at step t (generator step t - delay).
+template < typename Real >
+__device__ __forceinline__ Real
+drive( const Net& d, int64_t i, long long t, long long& cnt )
+{
+  if ( !d.has_pois )
+    return Real( 0 );
+  const double4 tab = d.pois[ i ];
+  if ( !( tab.x > 0.0 ) )
+    return Real( 0 );
+  const long long tg = t - d.pois_d[ i ];
+  if ( !( d.pois_start < tg && tg <= d.pois_stop ) || tg < 0 )
+    return Real( 0 );
+  uint32_t o[ 4 ];
+  philox4x32_10( ( uint32_t ) i, ( uint32_t ) tg, ( uint32_t ) ( ( unsigned long long ) tg >> 32 ), DRIVE_STREAM,
+    d.key0, d.key1, o );
+  const long long k = poisson_from_mode( tab, u53( o[ 0 ], o[ 1 ] ) );
+  cnt += k;
+  if ( k <= 0 )
+    return Real( 0 );
+  return ( Real ) ( d.pois_w[ i ] * ( double ) k );
+}
+
+template < typename Real, bool FIX >
+__device__ __forceinline__ Real
+ring_take( const Net& d, int slot, int ch, int64_t i )
+{
+  const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + i;
+  if constexpr ( FIX )
+  {
+    long long* ring = ( long long* ) d.ring;
+    const long long v = ring[ idx ];
+    ring[ idx ] = 0;
+    return ( Real ) ( ( double ) v * d.fx_inv );
+  }
+  else
+  {
+    double* ring = ( double* ) d.ring;
+    const double v = ring[ idx ];
+    ring[ idx ] = 0.0;
+    return ( Real ) v;
+  }
+}
+
+// vals[slot] holds the model's state variables in slot order.
+__device__ __forceinline__ void
+trace_put( const Net& d, int64_t i, long long stamp, const double* vals )
+{
+  if ( d.trace_col == nullptr || ( stamp % d.trace_interval ) != 0 )
+    return;
+  const int32_t col = d.trace_col[ i ];
+  if ( col < 0 )
+    return;
+  const long long row = stamp / d.trace_interval - ld_volatile( &d.ctl->trace_row0 );
+  if ( row >= 0 && row < d.trace_rows )
+  {
+    for ( int v = 0; v < d.n_trace_vars; ++v )
+      d.trace[ ( row * d.n_trace_vars + v ) * d.n_trace_idx + col ] = vals[ d.trace_slot[ v ] ];
+  }
+  else
+  {
+    atomicOr( &d.ctl->err, ERR_TRACE );
+  }
+}
+
+__device__ __forceinline__ void
+flush_drive_count( const Net& d, long long cnt )
+{
+  const long long s = warp_sum_ll( cnt );
+  if ( ( threadIdx.x & 31 ) == 0 && s > 0 )
+    atomicAdd( &d.ctl->drive_events, ( unsigned long long ) s );
+}
+
+// Scheduled generator spikes with emission step in [origin+from, origin+to):
+// one warp consumes them in order (CTA 0 of the first block's launch).
+__device__ __forceinline__ void
+append_scheduled( const Net& d, long long origin, int from, int to )
+{
+  if ( d.n_sched == 0 )
+    return;
+  long long pos = ld_volatile( &d.ctl->sched_pos );
+  const int lane = threadIdx.x & 31;
+  const long long lo = origin + from, hi = origin + to;
+  for ( ;; )
+  {
+    const long long p = pos + lane;
+    const bool in_range = p < d.n_sched;
+    const long long st = in_range ? d.sched_step[ p ] : hi;
+    const bool consumed = in_range && st < hi;
+    const bool emit = consumed && st >= lo;
+    const int32_t src = emit ? d.sched_src[ p ] : 0;
+    warp_append( d, emit, src, emit ? ( int32_t ) ( st % d.L ) : 0, 1, st + 1 );
+    const unsigned cm = __ballot_sync( FULL, consumed );
+    pos += __popc( cm );
+    if ( cm != FULL )
+      break;
+  }
+  if ( lane == 0 )
+    d.ctl->sched_pos = pos;
+}
+
+// ---------------------------------------------------------------------
+// iaf_psc_delta (models/iaf_psc_delta.cpp:272-329)
+// ctab: P33, P30, V_th, V_reset, V_min, RefractoryCounts
+// state: s0 = y3 (V_m - E_L), s1 = y0, s2 = I_e
+// ---------------------------------------------------------------------
+template < typename Real, bool FIX >
+__global__ void __launch_bounds__( 256 )
+k_update_delta( Net d, Block b, int from, int to, int sched )
+{
+  const long long origin = ld_volatile( &d.ctl->origin );
+  if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
+    append_scheduled( d, origin, from, to );
+  const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = li < b.n;
+  const int64_t i = b.off + ( act ? li : 0 );
+  Real* sV = ( Real* ) b.s[ 0 ];
+  Real* sy0 = ( Real* ) b.s[ 1 ];
+  const Real* sIe = ( const Real* ) b.s[ 2 ];
+  Real V = 0, y0 = 0, Ie = 0, P33 = 0, P30 = 0, Vth = 0, Vreset = 0, Vmin = 0;
+  int r = 0, refr = 0;
+  if ( act )
+  {
+    const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
+    P33 = ( Real ) ct[ 0 ];
+    P30 = ( Real ) ct[ 1 ];
+    Vth = ( Real ) ct[ 2 ];
+    Vreset = ( Real ) ct[ 3 ];
+    Vmin = ( Real ) ct[ 4 ];
+    refr = ( int ) ct[ 5 ];
+    V = sV[ li ];
+    y0 = sy0[ li ];
+    Ie = sIe[ li ];
+    r = b.r[ li ];
+  }
+  long long t = origin + from;
+  int slot = ( int ) ( t % d.L );
+  long long dcnt = 0;
+  for ( int lag = from; lag < to; ++lag, ++t )
+  {
+    bool spk = false;
+    if ( act )
+    {
+      Real in = ring_take< Real, FIX >( d, slot, 0, i );
+      const Real dv = drive< Real >( d, i, t, dcnt );
+      if ( dv != Real( 0 ) )
+        in = in + dv;
+      if ( r == 0 )
+      {
+        V = P30 * ( y0 + Ie ) + P33 * V + in;
+        V = ( V < Vmin ? Vmin : V );
+      }
+      else
+      {
+        --r;
+      }
+      if ( V >= Vth )
+      {
+        r = refr;
+        V = Vreset;
+        spk = true;
+      }
+      y0 = Real( 0 );
+    }
+    warp_append( d, spk, ( int32_t ) i, slot, 1, t + 1 );
+    if ( act && d.trace_col )
+    {
+      const double vals[ 3 ] = { ( double ) V, ( double ) y0, ( double ) Ie };
+      trace_put( d, i, t + 1, vals );
+    }
+    if ( ++slot == d.L )
+      slot = 0;
+  }
+  flush_drive_count( d, dcnt );
+  if ( act )
+  {
+    sV[ li ] = V;
+    sy0[ li ] = y0;
+    b.r[ li ] = r;
+  }
+}
+
+// ---------------------------------------------------------------------
+// iaf_psc_exp (models/iaf_psc_exp.cpp:288-348)
+// ctab: P22, P21ex, P21in, P20, P11ex, P11in, Theta, V_reset, RefractoryCounts, 1-P11ex
+// state: s0 = V_m - E_L, s1 = i_syn_ex, s2 = i_syn_in, s3 = i_0, s4 = i_1, s5 = I_e
+// ---------------------------------------------------------------------
+template < typename Real, bool FIX >
+__global__ void __launch_bounds__( 256 )
+k_update_exp( Net d, Block b, int from, int to, int sched )
+{
+  const long long origin = ld_volatile( &d.ctl->origin );
+  if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
+    append_scheduled( d, origin, from, to );
+  const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = li < b.n;
+  const int64_t i = b.off + ( act ? li : 0 );
+  Real* s0 = ( Real* ) b.s[ 0 ];
+  Real* s1 = ( Real* ) b.s[ 1 ];
+  Real* s2 = ( Real* ) b.s[ 2 ];
+  Real* s3 = ( Real* ) b.s[ 3 ];
+  Real* s4 = ( Real* ) b.s[ 4 ];
+  const Real* s5 = ( const Real* ) b.s[ 5 ];
+  Real V = 0, iex = 0, iin = 0, i0 = 0, i1 = 0, Ie = 0;
+  Real P22 = 0, P21ex = 0, P21in = 0, P20 = 0, P11ex = 0, P11in = 0, Theta = 0, Vreset = 0, omP11ex = 0;
+  int r = 0, refr = 0;
+  if ( act )
+  {
+    const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
+    P22 = ( Real ) ct[ 0 ];
+    P21ex = ( Real ) ct[ 1 ];
+    P21in = ( Real ) ct[ 2 ];
+    P20 = ( Real ) ct[ 3 ];
+    P11ex = ( Real ) ct[ 4 ];
+    P11in = ( Real ) ct[ 5 ];
+    Theta = ( Real ) ct[ 6 ];
+    Vreset = ( Real ) ct[ 7 ];
+    refr = ( int ) ct[ 8 ];
+    omP11ex = ( Real ) ct[ 9 ];
+    V = s0[ li ];
+    iex = s1[ li ];
+    iin = s2[ li ];
+    i0 = s3[ li ];
+    i1 = s4[ li ];
+    Ie = s5[ li ];
+    r = b.r[ li ];
+  }
+  long long t = origin + from;
+  int slot = ( int ) ( t % d.L );
+  long long dcnt = 0;
+  for ( int lag = from; lag < to; ++lag, ++t )
+  {
+    bool spk = false;
+    if ( act )
+    {
+      if ( r == 0 )
+        V = V * P22 + iex * P21ex + iin * P21in + ( Ie + i0 ) * P20;
+      else
+        --r;
+      iex *= P11ex;
+      iin *= P11in;
+      iex += omP11ex * i1;
+      Real ex = ring_take< Real, FIX >( d, slot, 0, i );
+      Real inh = ring_take< Real, FIX >( d, slot, 1, i );
+      const Real dv = drive< Real >( d, i, t, dcnt );
+      if ( dv != Real( 0 ) )
+      {
+        if ( dv > Real( 0 ) )
+          ex = ex + dv;
+        else
+          inh = inh + dv;
+      }
+      iex += ex;
+      iin += inh;
+      if ( V >= Theta )
+      {
+        r = refr;
+        V = Vreset;
+        spk = true;
+      }
+      i0 = Real( 0 );
+      i1 = Real( 0 );
+    }
+    warp_append( d, spk, ( int32_t ) i, slot, 1, t + 1 );
+    if ( act && d.trace_col )
+    {
+      const double vals[ 6 ] = { ( double ) V, ( double ) iex, ( double ) iin, ( double ) i0, ( double ) i1,
+        ( double ) Ie };
+      trace_put( d, i, t + 1, vals );
+    }
+    if ( ++slot == d.L )
+      slot = 0;
+  }
+  flush_drive_count( d, dcnt );
+  if ( act )
+  {
+    s0[ li ] = V;
+    s1[ li ] = iex;
+    s2[ li ] = iin;
+    s3[ li ] = i0;
+    s4[ li ] = i1;
+    b.r[ li ] = r;
+  }
+}
+
+// ---------------------------------------------------------------------
+// aeif_cond_alpha (models/aeif_cond_alpha.cpp:74-126, 450-533) with a
+// per-neuron adaptive Runge-Kutta-Fehlberg 4(5) step in FP64.
+// ctab: V_peak, V_reset, g_L, C_m, E_ex, E_in, E_L, Delta_T, tau_w, a, b, V_th,
+//       tau_syn_ex, tau_syn_in, tol, g0_ex, g0_in, V_peak_eff, RefractoryCounts
+// state: s0..s5 = V, dg_ex, g_ex, dg_in, g_in, w; s6 = I_e; istep (FP64)
+// ---------------------------------------------------------------------
+struct AeifPar
+{
+  double V_peak, V_reset, g_L, C_m, E_ex, E_in, E_L, Delta_T, tau_w, a, b, V_th, tau_ex, tau_in, I_e;
+};
+
+__device__ __forceinline__ void
+aeif_rhs( const AeifPar& p, bool refr, const double* y, double* f )
+{
+  const double V = refr ? p.V_reset : fmin( y[ 0 ], p.V_peak );
+  const double I_syn_exc = y[ 2 ] * ( V - p.E_ex );
+  const double I_syn_inh = y[ 4 ] * ( V - p.E_in );
+  const double I_spike = p.Delta_T == 0. ? 0. : ( p.g_L * p.Delta_T * exp( ( V - p.V_th ) / p.Delta_T ) );
+  f[ 0 ] = refr ? 0. : ( -p.g_L * ( V - p.E_L ) + I_spike - I_syn_exc - I_syn_inh - y[ 5 ] + p.I_e ) / p.C_m;
+  f[ 1 ] = -y[ 1 ] / p.tau_ex;
+  f[ 2 ] = y[ 1 ] - y[ 2 ] / p.tau_ex;
+  f[ 3 ] = -y[ 3 ] / p.tau_in;
+  f[ 4 ] = y[ 3 ] - y[ 4 ] / p.tau_in;
+  f[ 5 ] = ( p.a * ( V - p.E_L ) - y[ 5 ] ) / p.tau_w;
+}
+
+// Fehlberg 4(5): advance with the fifth-order weights; error = 5th - 4th.
+__device__ __forceinline__ void
+rkf45( const AeifPar& p, bool refr, const double* y, const double* k1, double hs, double* yn, double* err, double* fout )
+{
+  double k2[ 6 ], k3[ 6 ], k4[ 6 ], k5[ 6 ], k6[ 6 ], yt[ 6 ];
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+    yt[ i ] = y[ i ] + ( 1.0 / 4.0 ) * hs * k1[ i ];
+  aeif_rhs( p, refr, yt, k2 );
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+    yt[ i ] = y[ i ] + hs * ( ( 3.0 / 32.0 ) * k1[ i ] + ( 9.0 / 32.0 ) * k2[ i ] );
+  aeif_rhs( p, refr, yt, k3 );
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+    yt[ i ] = y[ i ] + hs * ( ( 1932.0 / 2197.0 ) * k1[ i ] + ( -7200.0 / 2197.0 ) * k2[ i ] + ( 7296.0 / 2197.0 ) * k3[ i ] );
+  aeif_rhs( p, refr, yt, k4 );
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+    yt[ i ] = y[ i ]
+      + hs * ( ( 439.0 / 216.0 ) * k1[ i ] + ( -8.0 ) * k2[ i ] + ( 3680.0 / 513.0 ) * k3[ i ] + ( -845.0 / 4104.0 ) * k4[ i ] );
+  aeif_rhs( p, refr, yt, k5 );
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+    yt[ i ] = y[ i ]
+      + hs * ( ( -8.0 / 27.0 ) * k1[ i ] + 2.0 * k2[ i ] + ( -3544.0 / 2565.0 ) * k3[ i ] + ( 1859.0 / 4104.0 ) * k4[ i ]
+        + ( -11.0 / 40.0 ) * k5[ i ] );
+  aeif_rhs( p, refr, yt, k6 );
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+  {
+    const double d5 = ( 16.0 / 135.0 ) * k1[ i ] + ( 6656.0 / 12825.0 ) * k3[ i ] + ( 28561.0 / 56430.0 ) * k4[ i ]
+      + ( -9.0 / 50.0 ) * k5[ i ] + ( 2.0 / 55.0 ) * k6[ i ];
+    yn[ i ] = y[ i ] + hs * d5;
+    err[ i ] = hs
+      * ( ( 1.0 / 360.0 ) * k1[ i ] + ( -128.0 / 4275.0 ) * k3[ i ] + ( -2197.0 / 75240.0 ) * k4[ i ]
+        + ( 1.0 / 50.0 ) * k5[ i ] + ( 2.0 / 55.0 ) * k6[ i ] );
+  }
+  aeif_rhs( p, refr, yn, fout );
+}
+
+// Step-size control with D_i = tol + tol * h |y'_i|; q = 5 (stepper order).
+__device__ __forceinline__ int
+control_yp( double tol, const double* err, const double* f, double& hs )
+{
+  const double h_old = hs;
+  double rmax = 2.2250738585072014e-308;
+#pragma unroll
+  for ( int i = 0; i < 6; ++i )
+  {
+    const double D0 = tol * fabs( h_old * f[ i ] ) + tol;
+    const double r = fabs( err[ i ] ) / fabs( D0 );
+    rmax = r > rmax ? r : rmax;
+  }
+  if ( rmax > 1.1 )
+  {
+    double r = 0.9 / pow( rmax, 1.0 / 5.0 );
+    if ( r < 0.2 )
+      r = 0.2;
+    hs = r * h_old;
+    return -1;
+  }
+  if ( rmax < 0.5 )
+  {
+    double r = 0.9 / pow( rmax, 1.0 / 6.0 );
+    if ( r > 5.0 )
+      r = 5.0;
+    if ( r < 1.0 )
+      r = 1.0;
+    hs = r * h_old;
+    return 1;
+  }
+  return 0;
+}
+
+template < typename Real, bool FIX >
+__global__ void __launch_bounds__( 128 )
+k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
+{
+  const long long origin = ld_volatile( &d.ctl->origin );
+  if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
+    append_scheduled( d, origin, from, to );
+  const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = li < b.n;
+  const int64_t i = b.off + ( act ? li : 0 );
+  Real* sy[ 6 ];
+#pragma unroll
+  for ( int k = 0; k < 6; ++k )
+    sy[ k ] = ( Real* ) b.s[ k ];
+  AeifPar p {};
+  double y[ 6 ] = { 0, 0, 0, 0, 0, 0 };
+  double tol = 0, g0ex = 0, g0in = 0, Vpk = 0, hs = h;
+  int r = 0, refr = 0;
+  if ( act )
+  {
+    const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
+    p.V_peak = ct[ 0 ];
+    p.V_reset = ct[ 1 ];
+    p.g_L = ct[ 2 ];
+    p.C_m = ct[ 3 ];
+    p.E_ex = ct[ 4 ];
+    p.E_in = ct[ 5 ];
+    p.E_L = ct[ 6 ];
+    p.Delta_T = ct[ 7 ];
+    p.tau_w = ct[ 8 ];
+    p.a = ct[ 9 ];
+    p.b = ct[ 10 ];
+    p.V_th = ct[ 11 ];
+    p.tau_ex = ct[ 12 ];
+    p.tau_in = ct[ 13 ];
+    tol = ct[ 14 ];
+    g0ex = ct[ 15 ];
+    g0in = ct[ 16 ];
+    Vpk = ct[ 17 ];
+    refr = ( int ) ct[ 18 ];
+    p.I_e = ( double ) ( ( const Real* ) b.s[ 6 ] )[ li ];
+#pragma unroll
+    for ( int k = 0; k < 6; ++k )
+      y[ k ] = ( double ) sy[ k ][ li ];
+    r = b.r[ li ];
+    hs = b.istep[ li ];
+  }
+  long long t = origin + from;
+  int slot = ( int ) ( t % d.L );
+  long long dcnt = 0;
+  bool unstable = false;
+  for ( int lag = from; lag < to; ++lag, ++t )
+  {
+    int mult = 0;
+    if ( act && !unstable )
+    {
+      double tt = 0.0;
+      int guard = 0;
+      while ( tt < h )
+      {
+        // one accepted sub-step (evolve_apply), retried on rejection
+        const double t0 = tt;
+        const double dt = h - t0;
+        double h0 = hs;
+        double k1[ 6 ], yn[ 6 ], err[ 6 ], fo[ 6 ];
+        aeif_rhs( p, r > 0, y, k1 );
+        for ( ;; )
+        {
+          bool final_step = false;
+          if ( h0 > dt )
+          {
+            h0 = dt;
+            final_step = true;
+          }
+          rkf45( p, r > 0, y, k1, h0, yn, err, fo );
+          tt = final_step ? h : t0 + h0;
+          const double h_old = h0;
+          const int adj = control_yp( tol, err, fo, h0 );
+          if ( adj < 0 )
+          {
+            const double t_next = tt + h0;
+            if ( fabs( h0 ) < fabs( h_old ) && t_next != tt && ++guard < 100000 )
+              continue;
+            h0 = h_old;
+          }
+          break;
+        }
+#pragma unroll
+        for ( int k = 0; k < 6; ++k )
+          y[ k ] = yn[ k ];
+        hs = h0;
+        if ( y[ 0 ] < -1e3 || y[ 5 ] < -1e6 || y[ 5 ] > 1e6 || ++guard >= 100000 )
+        {
+          unstable = true;
+          break;
+        }
+        if ( r > 0 )
+        {
+          y[ 0 ] = p.V_reset;
+        }
+        else if ( y[ 0 ] >= Vpk )
+        {
+          y[ 0 ] = p.V_reset;
+          y[ 5 ] += p.b;
+          r = refr > 0 ? refr + 1 : 0;
+          ++mult;
+        }
+      }
+      if ( r > 0 )
+        --r;
+      Real ex = ring_take< Real, FIX >( d, slot, 0, i );
+      Real inh = ring_take< Real, FIX >( d, slot, 1, i );
+      const Real dv = drive< Real >( d, i, t, dcnt );
+      if ( dv != Real( 0 ) )
+      {
+        if ( dv > Real( 0 ) )
+          ex = ex + dv;
+        else
+          inh = inh - dv;
+      }
+      y[ 1 ] += ( double ) ex * g0ex;
+      y[ 3 ] += ( double ) inh * g0in;
+      if constexpr ( sizeof( Real ) == 4 )
+      {
+#pragma unroll
+        for ( int k = 0; k < 6; ++k )
+          y[ k ] = ( double ) ( float ) y[ k ];
+      }
+    }
+    warp_append( d, mult > 0, ( int32_t ) i, slot, mult, t + 1 );
+    if ( act && d.trace_col )
+    {
+      const double vals[ 7 ] = { y[ 0 ], y[ 1 ], y[ 2 ], y[ 3 ], y[ 4 ], y[ 5 ], p.I_e };
+      trace_put( d, i, t + 1, vals );
+    }
+    if ( ++slot == d.L )
+      slot = 0;
+  }
+  flush_drive_count( d, dcnt );
+  if ( unstable )
+    atomicOr( &d.ctl->err, ERR_NUMERIC );
+  if ( act )
+  {
+#pragma unroll
+    for ( int k = 0; k < 6; ++k )
+      sy[ k ][ li ] = ( Real ) y[ k ];
+    b.r[ li ] = r;
+    b.istep[ li ] = hs;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Delivery: every spike of the closing slice, every out-edge, one red.global
+// add into ring[(t_emit + d) mod L][channel][target]
+// (EventDeliveryManager::deliver_events_ -> Connector::send -> handle,
+// event_delivery_manager.cpp:599-700, connector_base.h:398-434).
+// Work item = 4 consecutive edges of one (padded) CSR row; the spike owning
+// an item is found by binary search over the spikes' event offsets, staged
+// in shared memory when the list is short.
+// ---------------------------------------------------------------------
+constexpr int SMEM_SPIKES = 2048;
+
+template < bool FIX >
+__global__ void __launch_bounds__( 256 )
+k_deliver( Net d )
+{
+  __shared__ long long s_off[ SMEM_SPIKES ];
+  __shared__ int s_last;
+  const unsigned long long packed = ld_volatile( &d.ctl->spk_packed );
+  long long nspk = ( long long ) ( packed >> SPK_SHIFT );
+  const long long nev = ( long long ) ( packed & EV_MASK );
+  const bool ok = nspk <= d.spk_cap && ( ld_volatile( &d.ctl->err ) & ERR_SPIKE_LIST ) == 0;
+  const long long nq = ok ? ( nev >> 2 ) : 0;
+  const bool use_sm = nspk <= SMEM_SPIKES;
+  if ( use_sm && nq > 0 )
+  {
+    for ( long long k = threadIdx.x; k < nspk; k += blockDim.x )
+      s_off[ k ] = d.spk_off[ k ];
+    __syncthreads();
+  }
+  const long long* off = use_sm ? s_off : d.spk_off;
+  const long long stride = ( long long ) gridDim.x * blockDim.x;
+  for ( long long q = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride )
+  {
+    const long long e0 = q << 2;
+    long long lo = 0, hi = nspk;
+    while ( hi - lo > 1 )
+    {
+      const long long mid = ( lo + hi ) >> 1;
+      if ( off[ mid ] <= e0 )
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int4 sp = d.spk[ lo ];
+    const long long row = d.row_ptr[ sp.x ];
+    const long long edge = row + ( e0 - off[ lo ] );
+    if ( edge + 4 > d.row_ptr[ sp.x + 1 ] )
+      continue;
+    const uint4 tdc = *reinterpret_cast< const uint4* >( d.edge_tdc + edge );
+    const uint32_t tw[ 4 ] = { tdc.x, tdc.y, tdc.z, tdc.w };
+    if constexpr ( FIX )
+    {
+      const int4 w4 = *reinterpret_cast< const int4* >( ( const int32_t* ) d.edge_w + edge );
+      const int32_t ww[ 4 ] = { w4.x, w4.y, w4.z, w4.w };
+      unsigned long long* ring = ( unsigned long long* ) d.ring;
+#pragma unroll
+      for ( int k = 0; k < 4; ++k )
+      {
+        if ( ww[ k ] == 0 )
+          continue;
+        const uint32_t tgt = tw[ k ] & d.tmask;
+        int slot = sp.y + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
+        if ( slot >= d.L )
+          slot -= d.L;
+        const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
+        atomicAdd( ring + idx, ( unsigned long long ) ( ( long long ) ww[ k ] * ( long long ) sp.z ) );
+      }
+    }
+    else
+    {
+      const double2* wp = reinterpret_cast< const double2* >( ( const double* ) d.edge_w + edge );
+      const double2 wa = wp[ 0 ], wb = wp[ 1 ];
+      const double ww[ 4 ] = { wa.x, wa.y, wb.x, wb.y };
+      double* ring = ( double* ) d.ring;
+#pragma unroll
+      for ( int k = 0; k < 4; ++k )
+      {
+        if ( ww[ k ] == 0.0 )
+          continue;
+        const uint32_t tgt = tw[ k ] & d.tmask;
+        int slot = sp.y + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
+        if ( slot >= d.L )
+          slot -= d.L;
+        const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
+        atomicAdd( ring + idx, sp.z == 1 ? ww[ k ] : ww[ k ] * ( double ) sp.z );
+      }
+    }
+  }
+  __syncthreads();
+  if ( threadIdx.x == 0 )
+  {
+    __threadfence();
+    s_last = atomicAdd( &d.ctl->deliver_done, 1 ) == ( int ) gridDim.x - 1;
+  }
+  __syncthreads();
+  if ( s_last && threadIdx.x == 0 )
+  {
+    d.ctl->spk_packed = 0ull;
+    d.ctl->deliver_done = 0;
+    d.ctl->origin = d.ctl->origin + d.min_delay;
+    __threadfence();
+  }
+}
+
+// Host-side ctl edits between groups (log drain, trace window).
+__global__ void
+k_set_ctl( Ctl* ctl, long long log_base, long long trace_row0, int reset_log )
+{
+  if ( reset_log )
+    ctl->log_count = 0ull;
+  ctl->log_base = log_base;
+  ctl->trace_row0 = trace_row0;
+}
+
+}  // namespace ng

@@ -1,0 +1,274 @@
+"""ctypes binding of the engine's C ABI (include/nestgpu.h).
+
+The product path is this library and nothing else: if ``libnestgpu.so`` is
+missing or no CUDA device is present, the calls raise -- there is no CPU
+fallback.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnestgpu.so")
+
+NG_OK = 0
+NG_ERR_ARG = -1
+NG_ERR_CUDA = -2
+NG_ERR_STATE = -3
+NG_ERR_NUMERIC = -4
+NG_ERR_MEMORY = -5
+NG_ERR_CAPACITY = -6
+NG_ERR_UNKNOWN_NAME = -7
+
+NG_IAF_PSC_DELTA, NG_IAF_PSC_EXP, NG_AEIF_COND_ALPHA = 0, 1, 2
+NG_FP64, NG_FP32 = 0, 1
+NG_MAX_BLOCKS = 8
+
+#: every symbol include/nestgpu.h declares
+EXPORTED = [
+    "ng_abi_version", "ng_last_error", "ng_device_count", "ng_create", "ng_destroy", "ng_set_var", "ng_get_var",
+    "ng_set_connections", "ng_set_connections_coo", "ng_set_spike_schedule", "ng_set_poisson", "ng_set_recording", "ng_set_trace",
+    "ng_simulate", "ng_spike_count", "ng_get_spikes", "ng_trace_count", "ng_get_trace", "ng_get_stats",
+    "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients",
+]
+
+
+class NGConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("h", ctypes.c_double),
+        ("tics_per_ms", ctypes.c_double),
+        ("min_delay", ctypes.c_int32),
+        ("max_delay", ctypes.c_int32),
+        ("n_blocks", ctypes.c_int32),
+        ("block_model", ctypes.c_int32 * NG_MAX_BLOCKS),
+        ("block_size", ctypes.c_int64 * NG_MAX_BLOCKS),
+        ("n_generators", ctypes.c_int64),
+        ("spike_log_capacity", ctypes.c_int64),
+        ("start_step", ctypes.c_int64),
+    ]
+
+
+class NGStats(ctypes.Structure):
+    _fields_ = [
+        ("clock_steps", ctypes.c_int64),
+        ("slices", ctypes.c_int64),
+        ("spikes", ctypes.c_int64),
+        ("syn_events", ctypes.c_int64),
+        ("drive_events", ctypes.c_int64),
+        ("update_ms", ctypes.c_double),
+        ("deliver_ms", ctypes.c_double),
+        ("update_launches", ctypes.c_int64),
+        ("deliver_launches", ctypes.c_int64),
+        ("simulate_ms", ctypes.c_double),
+    ]
+
+
+class EngineError(RuntimeError):
+    """Error status returned by the engine's C ABI."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"nestgpu error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load libnestgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                          "or `make -C nest-simulator_b200/csrc`; the engine has no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    sig = {
+        "ng_abi_version": ([], ctypes.c_int),
+        "ng_last_error": ([], ctypes.c_char_p),
+        "ng_device_count": ([P], ctypes.c_int),
+        "ng_create": ([P, P], ctypes.c_int),
+        "ng_destroy": ([P], ctypes.c_int),
+        "ng_set_var": ([P, i32, ctypes.c_char_p, P, i64, i64], ctypes.c_int),
+        "ng_get_var": ([P, i32, ctypes.c_char_p, P, i64, i64], ctypes.c_int),
+        "ng_set_connections": ([P, i64, P, P, P, P], ctypes.c_int),
+        "ng_set_connections_coo": ([P, i64, i64, P, P, P, P], ctypes.c_int),
+        "ng_set_spike_schedule": ([P, i64, P, P], ctypes.c_int),
+        "ng_set_poisson": ([P, P, P, P, i64, i64, ctypes.c_uint64], ctypes.c_int),
+        "ng_set_recording": ([P, P], ctypes.c_int),
+        "ng_set_trace": ([P, i64, P, i32, P, i32], ctypes.c_int),
+        "ng_simulate": ([P, i64], ctypes.c_int),
+        "ng_spike_count": ([P, P], ctypes.c_int),
+        "ng_get_spikes": ([P, P, P, i64, P], ctypes.c_int),
+        "ng_trace_count": ([P, P, P], ctypes.c_int),
+        "ng_get_trace": ([P, P, i64, P], ctypes.c_int),
+        "ng_get_stats": ([P, P], ctypes.c_int),
+        "ng_set_profiling": ([P, i32], ctypes.c_int),
+        "ng_set_stream": ([P, P], ctypes.c_int),
+        "ng_set_graph_slices": ([P, i32], ctypes.c_int),
+        "ng_debug_coefficients": ([P, i32, i64, P, i32, P], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+def check(rc):
+    if rc != NG_OK:
+        raise EngineError(rc, load().ng_last_error().decode(errors="replace"))
+
+
+def device_count():
+    n = ctypes.c_int32(0)
+    rc = load().ng_device_count(ctypes.byref(n))
+    return n.value if rc == NG_OK else 0
+
+
+class Engine:
+    """Thin owner of one ng_engine handle."""
+
+    def __init__(self, blocks, h, min_delay, max_delay, n_generators=0, precision=NG_FP64, device=0,
+                 tics_per_ms=1000.0, spike_log_capacity=0, start_step=0):
+        L = load()
+        cfg = NGConfig()
+        cfg.device = int(device)
+        cfg.precision = int(precision)
+        cfg.h = float(h)
+        cfg.tics_per_ms = float(tics_per_ms)
+        cfg.min_delay = int(min_delay)
+        cfg.max_delay = int(max_delay)
+        if len(blocks) > NG_MAX_BLOCKS:
+            raise ValueError("too many model blocks")
+        cfg.n_blocks = len(blocks)
+        for k, (model, n) in enumerate(blocks):
+            cfg.block_model[k] = int(model)
+            cfg.block_size[k] = int(n)
+        cfg.n_generators = int(n_generators)
+        cfg.spike_log_capacity = int(spike_log_capacity)
+        cfg.start_step = int(start_step)
+        self.handle = ctypes.c_void_p()
+        self.L = L
+        check(L.ng_create(ctypes.byref(cfg), ctypes.byref(self.handle)))
+        self.blocks = list(blocks)
+        self.n_trace = 0
+        self.n_trace_vars = 0
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            self.L.ng_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_var(self, block, name, values, first=0):
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        check(self.L.ng_set_var(self.handle, int(block), name.encode(), _p(v), int(first), len(v)))
+
+    def get_var(self, block, name, first=0, count=None):
+        if count is None:
+            count = self.blocks[block][1] - first
+        out = np.empty(int(count), dtype=np.float64)
+        check(self.L.ng_get_var(self.handle, int(block), name.encode(), _p(out), int(first), int(count)))
+        return out
+
+    def set_connections(self, row_ptr, target, weight, delay_steps):
+        row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        target = np.ascontiguousarray(target, dtype=np.int32)
+        weight = np.ascontiguousarray(weight, dtype=np.float64)
+        delay_steps = np.ascontiguousarray(delay_steps, dtype=np.int32)
+        check(self.L.ng_set_connections(self.handle, len(row_ptr) - 1, _p(row_ptr), _p(target), _p(weight),
+                                        _p(delay_steps)))
+
+    def set_connections_coo(self, source, target, weight, delay_steps, n_src):
+        source = np.ascontiguousarray(source, dtype=np.int32)
+        target = np.ascontiguousarray(target, dtype=np.int32)
+        weight = np.ascontiguousarray(weight, dtype=np.float64)
+        delay_steps = np.ascontiguousarray(delay_steps, dtype=np.int32)
+        check(self.L.ng_set_connections_coo(self.handle, int(n_src), len(source), _p(source), _p(target),
+                                            _p(weight), _p(delay_steps)))
+
+    def set_spike_schedule(self, emit_step, source):
+        emit_step = np.ascontiguousarray(emit_step, dtype=np.int64)
+        source = np.ascontiguousarray(source, dtype=np.int32)
+        check(self.L.ng_set_spike_schedule(self.handle, len(emit_step), _p(emit_step), _p(source)))
+
+    def set_poisson(self, rate_hz, weight, delay_steps, start_step, stop_step, seed):
+        r = np.ascontiguousarray(rate_hz, dtype=np.float64)
+        w = np.ascontiguousarray(weight, dtype=np.float64)
+        d = np.ascontiguousarray(delay_steps, dtype=np.int32)
+        check(self.L.ng_set_poisson(self.handle, _p(r), _p(w), _p(d), int(start_step), int(stop_step),
+                                    int(seed) & (2**64 - 1)))
+
+    def set_recording(self, flags):
+        f = np.ascontiguousarray(flags, dtype=np.uint8)
+        check(self.L.ng_set_recording(self.handle, _p(f)))
+
+    def set_trace(self, neurons, var_names, interval_steps):
+        idx = np.ascontiguousarray(neurons, dtype=np.int32)
+        names = [ctypes.c_char_p(v.encode()) for v in var_names]
+        arr = (ctypes.c_char_p * max(1, len(names)))(*names)
+        check(self.L.ng_set_trace(self.handle, len(idx), _p(idx), len(names), ctypes.cast(arr, ctypes.c_void_p),
+                                  int(interval_steps)))
+        self.n_trace = len(idx)
+        self.n_trace_vars = len(names)
+
+    def simulate(self, n_steps):
+        check(self.L.ng_simulate(self.handle, int(n_steps)))
+
+    def spikes(self):
+        n = ctypes.c_int64(0)
+        check(self.L.ng_spike_count(self.handle, ctypes.byref(n)))
+        src = np.empty(n.value, dtype=np.int32)
+        st = np.empty(n.value, dtype=np.int64)
+        got = ctypes.c_int64(0)
+        check(self.L.ng_get_spikes(self.handle, _p(src), _p(st), n.value, ctypes.byref(got)))
+        return src[:got.value], st[:got.value]
+
+    def trace(self):
+        """Drain trace rows: (first_stamp, array [rows, n_vars, n_neurons])."""
+        rows = ctypes.c_int64(0)
+        first = ctypes.c_int64(0)
+        check(self.L.ng_trace_count(self.handle, ctypes.byref(rows), ctypes.byref(first)))
+        width = max(1, self.n_trace * self.n_trace_vars)
+        out = np.empty(rows.value * width, dtype=np.float64)
+        got = ctypes.c_int64(0)
+        check(self.L.ng_get_trace(self.handle, _p(out), rows.value, ctypes.byref(got)))
+        return first.value, out[:got.value * width].reshape(got.value, max(1, self.n_trace_vars),
+                                                            max(1, self.n_trace))
+
+    def stats(self):
+        s = NGStats()
+        check(self.L.ng_get_stats(self.handle, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in NGStats._fields_}
+
+    def set_profiling(self, on):
+        check(self.L.ng_set_profiling(self.handle, 1 if on else 0))
+
+    def set_stream(self, stream_ptr):
+        check(self.L.ng_set_stream(self.handle, ctypes.c_void_p(int(stream_ptr) if stream_ptr else 0)))
+
+    def set_graph_slices(self, k):
+        check(self.L.ng_set_graph_slices(self.handle, int(k)))
+
+    def coefficients(self, block, index):
+        out = np.empty(32, dtype=np.float64)
+        n = ctypes.c_int32(0)
+        check(self.L.ng_debug_coefficients(self.handle, int(block), int(index), _p(out), 32, ctypes.byref(n)))
+        return out[:n.value]

@@ -1,0 +1,18 @@
+#!/bin/sh
+# Compiles the reference's own propagator sources (libnestutil/iaf_propagator.cpp,
+# libnestutil/numerics.cpp) with g++ directly into oracle/_ref/libnestprop.so,
+# for pinning the oracle's and the engine's FP64 coefficients.  The
+# reference's build system is not used; its generated config.h is replaced by
+# an empty header (these two files need none of its macros).
+# Usage: oracle/build_ref.sh [reference root, default /root/reference]
+set -e
+REF=${1:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+[ -f "$REF/libnestutil/iaf_propagator.cpp" ] || { echo "reference sources not found under $REF" >&2; exit 1; }
+mkdir -p "$OUT/include"
+: > "$OUT/include/config.h"
+CXX=${CXX:-/usr/bin/g++}
+$CXX -std=c++20 -O2 -fPIC -ffp-contract=off -shared -I"$OUT/include" -I"$REF/libnestutil" \
+  -o "$OUT/libnestprop.so" "$REF/libnestutil/iaf_propagator.cpp" "$REF/libnestutil/numerics.cpp" "$HERE/ref_shim.cpp"
+echo "built $OUT/libnestprop.so"

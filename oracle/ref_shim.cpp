@@ -1,0 +1,10 @@
+// ref_shim.cpp -- extern "C" entry into the reference's own propagator code
+// (libnestutil/iaf_propagator.cpp, compiled from the reference sources by
+// oracle/build_ref.sh).  TEST INFRASTRUCTURE ONLY.
+#include "iaf_propagator.h"
+
+extern "C" double
+ref_iaf_propagator_exp( double tau_syn, double tau_m, double c_m, double h )
+{
+  return IAFPropagatorExp( tau_syn, tau_m, c_m ).evaluate( h );
+}
