@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark of the min_delay-slice engine on the Poisson-driven
+iaf_psc_exp network (12,500 neurons, K_E=1,000, K_I=250, 1.5625e7 synapses,
+8 kHz drive, delay 1.5 ms, h = 0.1 ms).
+
+One step = Simulate(1000 ms) of the network (10,000 node-update steps in 667
+min_delay slices).  Metric: recurrent synaptic events per second, i.e.
+(sum over emitted spikes of the source's out-degree) / device time, summed
+over all ranks.  Also reported: real-time factor, the FP32/fixed-point form,
+end-to-end throughput through the C ABI with host buffers, the roofline of
+the dominant kernel, and a CPU baseline (the oracle port on the host cores).
+
+Usage:
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+N > 1 runs under torchrun: independent replicas, one per GPU (the path has
+no cross-GPU exchange); the time is the max over ranks.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "nest-simulator_b200"), ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "syn_events_per_s"
+UNIT = "syn events/s"
+WORKLOAD = ("Poisson-driven iaf_psc_exp network: 12,500 neurons (10,000 exc, 2,500 inh), fixed_indegree "
+            "K_E=1,000 K_I=250 (1.5625e7 synapses), J=87.8 pA, g=5, delay 1.5 ms, 8 kHz Poisson drive, "
+            "dt=0.1 ms, 1,000 ms per step")
+SIM_MS = 1000.0
+
+# algorithmic bytes (Measurement)
+B_EVENT = {"fp64": 4 + 8 + 16, "fp32": 4 + 4 + 16}      # edge word + weight + ring read-modify-write
+B_NEURON_LAUNCH = {"fp64": 144, "fp32": 100}            # state r/w, I_e, class id, drive table per launch
+B_NEURON_LAG = {"fp64": 32, "fp32": 32}                 # 2 ring channels read + cleared per step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch", type=int, default=8, help="config-1 networks advanced together (batched form)")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def start(self):
+        def run():
+            first = True
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                if first:
+                    self._started.set()
+                    first = False
+                self._stop.wait(0.1)
+
+        self._started = threading.Event()
+        self._th = threading.Thread(target=run, daemon=True)
+        self._th.start()
+        self._started.wait(timeout=10)
+
+    def stop(self):
+        self._stop.set()
+        if self._th:
+            self._th.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 4 + k and s[4 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl" if args.impl == "engine" else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(x, pg, device=None):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, pg, device=None):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def build(nest, precision, seed):
+    from nestgpu import workloads
+
+    pop, sr = workloads.c1(nest, precision=precision, seed=seed)
+    return pop, sr
+
+
+def cpu_baseline(K, sample_ms=100.0):
+    """The oracle port (C, OpenMP, all host cores) on the same network."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = os.cpu_count() or 1
+    net, c = O.net_from_kernel(K, nthreads=threads)
+    steps = int(round(sample_ms / K.h))
+    net.run(int(round(50.0 / K.h)), nthreads=threads)  # warm-up: 50 ms
+    e0 = net.syn_events
+    t0 = time.perf_counter()
+    net.run(steps, nthreads=threads)
+    dt = time.perf_counter() - t0
+    ev = net.syn_events - e0
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample_ms:.0f} ms of simulated time of the same network after 50 ms warm-up "
+                      f"({ev} synaptic events in {dt:.2f} s, RTF {dt / (sample_ms / 1000):.2f})"}
+
+
+def run_reference(args):
+    """Reference arm: the oracle port of the reference's CPU path, all host cores."""
+    # no process group: rank 0 alone does the CPU work, the others exit at once
+    rank = int(os.environ.get("RANK", "0"))
+    pg = None
+    if rank != 0:
+        return
+    import nestgpu as nest
+    from nestgpu.kernel import KERNEL
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    build(nest, "fp64", 4242)
+    threads = os.cpu_count() or 1
+    net, c = O.net_from_kernel(KERNEL, nthreads=threads)
+    sample_ms = float(os.environ.get("NG_BENCH_SAMPLE_MS", "200"))
+    steps = int(round(sample_ms / KERNEL.h))
+    for _ in range(args.warmup):
+        net.run(steps, nthreads=threads)
+    e0 = net.syn_events
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.run(steps, nthreads=threads)
+    dt = time.perf_counter() - t0
+    ev = net.syn_events - e0
+    value = ev / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample_per_step_ms": sample_ms, "rtf": dt / (args.steps * sample_ms / 1e3)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample_ms:.0f} ms of simulated time per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def e2e_run(c, K, precision, sim_steps, seed):
+    """One step through the C ABI with host buffers: create the engine,
+    copy graph/state/drive from pinned host memory, simulate, copy the
+    spikes back, destroy."""
+    import torch
+
+    from nestgpu import _abi
+
+    st = K.models[c["blocks"][0]["model"]]
+    prec = _abi.NG_FP32 if precision == "fp32" else _abi.NG_FP64
+    eng = _abi.Engine([(b["engine_model"], b["n"]) for b in c["blocks"]], K.h, c["min_delay"], c["max_delay"],
+                      n_generators=len(c["gen_ids"]), precision=prec, device=torch.cuda.current_device())
+    h2d = 0
+    for k, ev in st.engine_vars.items():
+        eng.set_var(0, ev, c["host_state"][k])
+        h2d += c["host_state"][k].nbytes
+    eng.set_connections(c["row_ptr"], c["tgt_sorted"], c["w_sorted"], c["d_sorted"])
+    h2d += c["row_ptr"].nbytes + c["tgt_sorted"].nbytes + c["w_sorted"].nbytes + c["d_sorted"].nbytes
+    start, stop = c["pois_window"]
+    eng.set_poisson(c["pois_rate"], c["pois_w"], c["pois_d"], start, stop, seed)
+    h2d += c["pois_rate"].nbytes + c["pois_w"].nbytes + c["pois_d"].nbytes
+    eng.set_recording(c["rec_flags"])
+    h2d += c["rec_flags"].nbytes
+    eng.set_graph_slices(K.graph_slices)
+    eng.simulate(sim_steps)
+    src, stamp = eng.spikes()
+    d2h = 8 * len(src)
+    ev = eng.stats()["syn_events"]
+    eng.close()
+    return ev, h2d, d2h
+
+
+def pinned(a):
+    import torch
+
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    t.numpy()[...] = a
+    return t.numpy()
+
+
+def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg):
+    """Build, warm up, time K steps, profile kernels, and (optionally) run e2e."""
+    import torch
+
+    from nestgpu import workloads
+
+    if copies == 1:
+        workloads.c1(nest, precision=precision, seed=seed)
+    else:
+        workloads.brunel_exp_batch(nest, copies, precision=precision, seed=seed)
+    nest.set(device=local)
+    nest.Prepare()
+    eng = KERNEL.engine
+    stream = torch.cuda.current_stream(dev)
+    eng.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        nest.Run(SIM_MS)
+    s0 = eng.stats()
+    sampler = ClockSampler(local)
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.steps):
+        nest.Run(SIM_MS)
+    e_end.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    if pg is not None:
+        pg.barrier()
+    ms = e_start.elapsed_time(e_end)
+    s1 = eng.stats()
+    ev = s1["syn_events"] - s0["syn_events"]
+    ms_max = max_over_ranks(ms, pg, dev)
+    ev_all = sum_over_ranks(ev, pg, dev)
+    # per-kernel device times: event record nodes around every kernel inside the graphs
+    eng.set_profiling(True)
+    p0 = eng.stats()
+    nest.Run(SIM_MS)
+    p1 = eng.stats()
+    eng.set_profiling(False)
+    upd_ms = p1["update_ms"] - p0["update_ms"]
+    del_ms = p1["deliver_ms"] - p0["deliver_ms"]
+    n_upd = p1["update_launches"] - p0["update_launches"]
+    n_del = p1["deliver_launches"] - p0["deliver_launches"]
+    ev_prof = p1["syn_events"] - p0["syn_events"]
+    c = KERNEL.compiled
+    md = c["min_delay"]
+    N = c["N"]
+    upd_bytes = N * (B_NEURON_LAUNCH[precision] + B_NEURON_LAG[precision] * md)
+    del_bytes = ev_prof / max(1, n_del) * B_EVENT[precision]
+
+    def kern(launches, tot_ms, nbytes):
+        avg = tot_ms / max(1, launches)
+        return {"launches": launches, "avg_us": 1e3 * avg, "alg_bytes_per_launch": nbytes,
+                "achieved_gbs": nbytes / (avg * 1e-3) / 1e9 if avg > 0 else None}
+
+    kernels = {"k_update_iaf2": kern(n_upd, upd_ms, upd_bytes), "k_deliver": kern(n_del, del_ms, del_bytes)}
+    res = {"ms": ms_max, "events": ev_all, "clocks": clocks, "kernels": kernels, "copies": copies,
+           "launches": (s1["update_launches"] - s0["update_launches"]) +
+                       (s1["deliver_launches"] - s0["deliver_launches"]) + 1,
+           "spikes": s1["spikes"] - s0["spikes"], "form": form, "precision": precision}
+    res["value"] = ev_all / (ms_max * 1e-3)
+    res["rtf"] = ms_max / args.steps / SIM_MS
+    # end to end through the C ABI with host buffers
+    if not args.no_e2e:
+        src = c["src"].astype(np.int64)
+        order = np.argsort(src, kind="stable")
+        counts = np.bincount(src, minlength=c["n_src"])
+        row_ptr = np.zeros(c["n_src"] + 1, dtype=np.int64)
+        np.cumsum(counts, out=row_ptr[1:])
+        st = KERNEL.models[c["blocks"][0]["model"]]
+        cc = dict(c)
+        cc["row_ptr"] = pinned(row_ptr)
+        cc["tgt_sorted"] = pinned(c["tgt"][order].astype(np.int32))
+        cc["w_sorted"] = pinned(c["w"][order].astype(np.float64))
+        cc["d_sorted"] = pinned(c["d"][order].astype(np.int32))
+        cc["host_state"] = {k: pinned(st.data[k][:N].astype(np.float64)) for k in st.engine_vars}
+        cc["pois_rate"] = pinned(c["pois_rate"])
+        cc["pois_w"] = pinned(c["pois_w"])
+        cc["pois_d"] = pinned(c["pois_d"].astype(np.int32))
+        cc["rec_flags"] = pinned(c["rec_flags"])
+        del src, order, counts
+        sim_steps = KERNEL.ms_to_steps_exact(SIM_MS)
+        e2e_run(cc, KERNEL, precision, sim_steps, seed)  # warm-up
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        tot_ev = 0
+        for _ in range(args.steps):
+            ev_e, h2d, d2h = e2e_run(cc, KERNEL, precision, sim_steps, seed)
+            tot_ev += ev_e
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+        wall_max = max_over_ranks(wall, pg, dev)
+        tot_all = sum_over_ranks(tot_ev, pg, dev)
+        res["e2e"] = {"value": tot_all / wall_max, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                      "d2h_bytes_per_step": int(d2h)}
+    nest.ResetKernel()
+    return res
+
+
+def run_engine(args):
+    import torch
+
+    ws, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import nestgpu as nest
+    from nestgpu.kernel import KERNEL
+
+    seed = 4242 + 1000 * rank
+    plain = measure(args, nest, KERNEL, "plain", "fp64", 1, seed, local, dev, pg)
+    single32 = measure(args, nest, KERNEL, "single", "fp32", 1, seed, local, dev, pg)
+    batched = measure(args, nest, KERNEL, "batched", "fp32", args.batch, seed, local, dev, pg) \
+        if args.batch > 1 else single32
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from nestgpu import workloads
+
+        workloads.c1(nest, precision="fp64", seed=seed)
+        cpu = cpu_baseline(KERNEL)
+        nest.ResetKernel()
+    r = batched
+    peak, peak_kind = load_peaks()
+    dom_name, dom = max(r["kernels"].items(), key=lambda kv: kv[1]["avg_us"] * kv[1]["launches"])
+    ach = dom["achieved_gbs"]
+
+    def brief(x):
+        return {"value": x["value"], "rtf": x["rtf"], "e2e": x.get("e2e"), "spikes_per_step": x["spikes"] /
+                max(1, args.steps + 1), "kernels": {k: {"avg_us": v["avg_us"], "achieved_gbs": v["achieved_gbs"]}
+                                                    for k, v in x["kernels"].items()}}
+
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+i64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": "batched FP32 state + int64 fixed-point rings",
+                   "networks_per_gpu": r["copies"], "global_batch": r["copies"] * ws,
+                   "parallelism": f"replicas{ws}", "l2": "graph larger than L2 (no flush needed)",
+                   "rtf_per_network": r["rtf"],
+                   "plain_fp64_single_network": brief(plain), "fp32_single_network": brief(single32),
+                   "batched_over_plain": r["value"] / plain["value"]},
+        "gpu_launches": int(r["launches"]),
+        "clocks": r["clocks"],
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": (ach / peak) if ach else None, "peak_kind": peak_kind, "traffic": None,
+                     "kernels": r["kernels"]},
+        "e2e": r.get("e2e"),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

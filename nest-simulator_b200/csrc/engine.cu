@@ -155,6 +155,31 @@ poisson_table( double lambda )
   return make_double4( lambda, pm, F, m );
 }
 
+// CDF table of Poisson(lambda): cdf[k] = P(X <= k), summed upward in FP64,
+// up to 1 - cdf < 1e-17 or 256 entries; the last entry is set to 1 so the
+// search always ends.  Returns false when the table would be too long.
+bool
+poisson_cdf_table( double lambda, std::vector< double >& cdf )
+{
+  cdf.clear();
+  if ( lambda > 100.0 )
+    return false;
+  double p = std::exp( -lambda ), F = p;
+  cdf.push_back( F );
+  for ( int k = 1; k < 256; ++k )
+  {
+    p = p * lambda / ( double ) k;
+    F += p;
+    cdf.push_back( F );
+    if ( 1.0 - F < 1e-17 && ( double ) k > lambda )
+      break;
+  }
+  if ( 1.0 - F > 1e-15 )
+    return false;
+  cdf.back() = 1.0;
+  return true;
+}
+
 struct DevBuf
 {
   void* p = nullptr;
@@ -188,8 +213,8 @@ struct ng_engine
   };
   std::vector< Blk > blk;
 
-  DevBuf ring, row_ptr, real_deg, tdc, w, spk, spk_off, log, rec, pois, pois_w, pois_d, trace_col, trace, sched_step,
-    sched_src, ctl;
+  DevBuf ring, row_ptr, real_deg, tdc, w, spk, spk_off, log, rec, pois, pois_w, pois_d, pois_ref, pois_cdf, trace_col,
+    trace, sched_step, sched_src, ctl;
   int32_t tbits = 1;
   uint32_t tmask = 1, dmask = 0;
   double fx_inv = 1.0;
@@ -218,17 +243,30 @@ struct ng_engine
   ng_stats stats {};
   int profiling = 0;
   int graph_slices = 0;
-  cudaGraphExec_t graph = nullptr;
-  int64_t generation = 0, graph_generation = -1;
+  // instantiated graphs of k full slices (k in {graph_slices, 16, 4, 1}),
+  // plain or with an event pair around every kernel (profiling)
+  struct GraphEntry
+  {
+    int slices = 0;
+    bool prof = false;
+    int64_t gen = -1;
+    cudaGraphExec_t exec = nullptr;
+    std::vector< cudaEvent_t > ev;
+  };
+  std::vector< GraphEntry > graphs;
+  int64_t generation = 0;
+  std::vector< uint8_t > rec_host;
+  double log_per_step = 1.0;  // bound on recorded neuron spikes per step (refractoriness)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector< DevBuf* > all;
   int deliver_ctas = 0;
+  int max_lanes = 32;             // 1: always one thread per neuron
+  int64_t one_thread_min_n = 20000;  // block size from which one thread per neuron fills the GPU
 
   ~ng_engine()
   {
     cudaSetDevice( cfg.device );
-    if ( graph )
-      cudaGraphExecDestroy( graph );
+    drop_graphs();
     for ( auto& b : blk )
     {
       for ( auto& s : b.st )
@@ -239,7 +277,7 @@ struct ng_engine
       cudaFree( b.ctab.p );
     }
     DevBuf* bufs[] = { &ring, &row_ptr, &real_deg, &tdc, &w, &spk, &spk_off, &log, &rec, &pois, &pois_w, &pois_d,
-      &trace_col, &trace, &sched_step, &sched_src, &ctl };
+      &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -421,6 +459,8 @@ struct ng_engine
     d.pois = ( const double4* ) pois.p;
     d.pois_w = ( const double* ) pois_w.p;
     d.pois_d = ( const int32_t* ) pois_d.p;
+    d.pois_cdf_ref = ( const int2* ) pois_ref.p;
+    d.pois_cdf = ( const double* ) pois_cdf.p;
     d.pois_start = pois_start;
     d.pois_stop = pois_stop;
     d.key0 = key0;
@@ -475,22 +515,46 @@ struct ng_engine
       }
       else
       {
-        const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( b.n + 255 ) / 256 );
-        if ( b.model == NG_IAF_PSC_DELTA )
-        {
-          if ( prec == NG_FP64 )
-            k_update_delta< double, false ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
-          else
-            k_update_delta< float, true ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
-        }
-        else
-        {
-          if ( prec == NG_FP64 )
-            k_update_exp< double, false ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
-          else
-            k_update_exp< float, true ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
-        }
+        launch_iaf( d, db, b.model, from_, to_, sched );
       }
+    }
+  }
+
+  template < typename Real, bool FIX, int MODEL >
+  void
+  launch_iaf_g( const Net& d, const Block& db, int from_, int to_, int sched )
+  {
+    const int span = to_ - from_;
+    // one thread per neuron for 1-2 step slices and for networks large enough
+    // to fill the GPU that way; the two-phase kernel otherwise
+    if ( span <= 2 || db.n >= one_thread_min_n || max_lanes == 1 )
+    {
+      const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 255 ) / 256 );
+      k_update_iaf< Real, FIX, MODEL ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+    }
+    else
+    {
+      const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + P2_NB - 1 ) / P2_NB );
+      k_update_iaf2< Real, FIX, MODEL ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+    }
+  }
+
+  void
+  launch_iaf( const Net& d, const Block& db, int model, int from_, int to_, int sched )
+  {
+    if ( model == NG_IAF_PSC_DELTA )
+    {
+      if ( prec == NG_FP64 )
+        launch_iaf_g< double, false, NG_IAF_PSC_DELTA >( d, db, from_, to_, sched );
+      else
+        launch_iaf_g< float, true, NG_IAF_PSC_DELTA >( d, db, from_, to_, sched );
+    }
+    else
+    {
+      if ( prec == NG_FP64 )
+        launch_iaf_g< double, false, NG_IAF_PSC_EXP >( d, db, from_, to_, sched );
+      else
+        launch_iaf_g< float, true, NG_IAF_PSC_EXP >( d, db, from_, to_, sched );
     }
   }
 
@@ -539,51 +603,117 @@ struct ng_engine
     return NG_OK;
   }
 
-  int
-  ensure_graph( const Net& d )
+  void
+  drop_graphs()
   {
-    if ( graph && graph_generation == generation )
-      return NG_OK;
-    if ( graph )
+    for ( auto& g : graphs )
     {
-      cudaGraphExecDestroy( graph );
-      graph = nullptr;
+      if ( g.exec )
+        cudaGraphExecDestroy( g.exec );
+      for ( cudaEvent_t ev : g.ev )
+        cudaEventDestroy( ev );
     }
-    cudaGraph_t g;
+    graphs.clear();
+  }
+
+  int
+  get_graph( const Net& d, int k, bool prof, GraphEntry** out )
+  {
+    for ( auto& g : graphs )
+      if ( g.slices == k && g.prof == prof && g.gen == generation )
+      {
+        *out = &g;
+        return NG_OK;
+      }
+    // stale graphs of an older configuration are rebuilt
+    for ( auto it = graphs.begin(); it != graphs.end(); )
+    {
+      if ( it->gen != generation )
+      {
+        if ( it->exec )
+          cudaGraphExecDestroy( it->exec );
+        for ( cudaEvent_t ev : it->ev )
+          cudaEventDestroy( ev );
+        it = graphs.erase( it );
+      }
+      else
+        ++it;
+    }
+    GraphEntry g;
+    g.slices = k;
+    g.prof = prof;
+    g.gen = generation;
+    if ( prof )
+    {
+      g.ev.resize( ( size_t ) 4 * k );
+      for ( auto& ev : g.ev )
+        CU( cudaEventCreate( &ev ) );
+    }
+    cudaGraph_t cg;
     CU( cudaStreamBeginCapture( stream, cudaStreamCaptureModeThreadLocal ) );
-    for ( int s = 0; s < graph_slices; ++s )
+    // event record nodes inside the graph (external events) bracket every kernel
+    for ( int sl = 0; sl < k; ++sl )
     {
+      if ( prof )
+        cudaEventRecordWithFlags( g.ev[ 4 * sl + 0 ], stream, cudaEventRecordExternal );
       launch_update( d, 0, cfg.min_delay );
+      if ( prof )
+      {
+        cudaEventRecordWithFlags( g.ev[ 4 * sl + 1 ], stream, cudaEventRecordExternal );
+        cudaEventRecordWithFlags( g.ev[ 4 * sl + 2 ], stream, cudaEventRecordExternal );
+      }
       launch_deliver( d );
+      if ( prof )
+        cudaEventRecordWithFlags( g.ev[ 4 * sl + 3 ], stream, cudaEventRecordExternal );
     }
-    CU( cudaStreamEndCapture( stream, &g ) );
-    cudaError_t e = cudaGraphInstantiate( &graph, g, 0 );
-    cudaGraphDestroy( g );
+    CU( cudaStreamEndCapture( stream, &cg ) );
+    cudaError_t e = cudaGraphInstantiate( &g.exec, cg, 0 );
+    cudaGraphDestroy( cg );
     if ( e != cudaSuccess )
       return fail( NG_ERR_CUDA, std::string( "cudaGraphInstantiate: " ) + cudaGetErrorString( e ) );
-    graph_generation = generation;
+    graphs.push_back( std::move( g ) );
+    *out = &graphs.back();
     return NG_OK;
   }
 
-  // enqueue n steps without host synchronisation
+  // enqueue n steps without host synchronisation (except when profiling)
   int
   enqueue_steps( int64_t n )
   {
     const Net d = net();
     while ( n > 0 )
     {
-      if ( from == 0 && graph_slices > 0 && !profiling && n >= ( int64_t ) graph_slices * cfg.min_delay )
+      if ( from == 0 && graph_slices > 0 && n >= cfg.min_delay )
       {
-        int rc = ensure_graph( d );
+        // largest graph chunk that fits: graph_slices, 16, 4 or 1 slices
+        const int64_t full = n / cfg.min_delay;
+        int k = 1;
+        for ( int cand : { graph_slices, 16, 4 } )
+          if ( cand <= graph_slices && cand <= full && cand > k )
+            k = cand;
+        GraphEntry* g = nullptr;
+        int rc = get_graph( d, k, profiling != 0, &g );
         if ( rc )
           return rc;
-        CU( cudaGraphLaunch( graph, stream ) );
-        const int64_t st = ( int64_t ) graph_slices * cfg.min_delay;
+        CU( cudaGraphLaunch( g->exec, stream ) );
+        if ( profiling )
+        {
+          CU( cudaStreamSynchronize( stream ) );
+          for ( int sl = 0; sl < k; ++sl )
+          {
+            float a = 0, b2 = 0;
+            CU( cudaEventElapsedTime( &a, g->ev[ 4 * sl + 0 ], g->ev[ 4 * sl + 1 ] ) );
+            CU( cudaEventElapsedTime( &b2, g->ev[ 4 * sl + 2 ], g->ev[ 4 * sl + 3 ] ) );
+            stats.update_ms += a;
+            stats.deliver_ms += b2;
+          }
+        }
+        const int64_t st = ( int64_t ) k * cfg.min_delay;
         origin += st;
-        slices += graph_slices;
+        slices += k;
         n -= st;
-        stats.update_launches += ( int64_t ) graph_slices * ( int64_t ) blk.size();
-        stats.deliver_launches += graph_slices;
+        stats.update_launches += ( int64_t ) k * ( int64_t ) blk.size();
+        stats.deliver_launches += k;
         continue;
       }
       const int to_ = ( int ) std::min< int64_t >( from + n, cfg.min_delay );
@@ -605,18 +735,47 @@ struct ng_engine
     return NG_OK;
   }
 
+  // bound on recorded neuron spikes per step: a neuron with refractory
+  // count R emits at most one logged entry per R + 1 steps
+  void
+  update_log_bound()
+  {
+    double bound = 0.0;
+    for ( const auto& b : blk )
+    {
+      const int ri = b.model == NG_IAF_PSC_DELTA ? 5 : b.model == NG_IAF_PSC_EXP ? 8 : 18;
+      for ( int64_t j = 0; j < b.n; ++j )
+      {
+        const int64_t i = b.off + j;
+        if ( rec_host.empty() || !rec_host[ ( size_t ) i ] )
+          continue;
+        const double R = b.host_cls.empty() ? 0.0 : b.host_ctab[ ( size_t ) b.host_cls[ ( size_t ) j ] * CT_STRIDE + ri ];
+        bound += 1.0 / ( R + 1.0 );
+      }
+    }
+    log_per_step = std::max( bound, 1.0 );
+  }
+
   int
   prepare()
   {
+    bool rebuilt = false;
     for ( auto& b : blk )
       if ( b.dirty )
       {
         int rc = build_classes( b );
         if ( rc )
           return rc;
+        rebuilt = true;
       }
+    if ( rebuilt || log_bound_dirty )
+    {
+      update_log_bound();
+      log_bound_dirty = false;
+    }
     return NG_OK;
   }
+  bool log_bound_dirty = true;
 
   // one group: set ctl, enqueue, sync, drain
   int
@@ -684,8 +843,8 @@ struct ng_engine
     if ( rc )
       return rc;
     // group size: bounded by the spike-log and trace capacities
-    const int64_t per_step = std::max< int64_t >( 1, n_rec );
-    int64_t by_log = ( log_cap - n_sched ) / per_step;
+    // over S steps a recorded neuron logs at most S / (R + 1) + 1 entries
+    int64_t by_log = ( int64_t ) std::floor( ( double ) ( log_cap - n_sched - n_rec ) / log_per_step );
     if ( by_log < 1 )
       return fail( NG_ERR_CAPACITY, "spike log capacity too small for one step" );
     int64_t gmax = std::min< int64_t >( by_log, ( 1 << 24 ) - 2 );
@@ -893,7 +1052,19 @@ ng_create( const ng_config* cfg, ng_engine** out )
       != cudaSuccess )
       return bail( fail( NG_ERR_CUDA, "ng_create: control block upload failed" ) );
   }
-  e->deliver_ctas = std::max( 1, std::min( e->sms * 4, 1 ) );
+  e->deliver_ctas = 1;
+  if ( const char* ml = std::getenv( "NG_MAX_LANES" ) )
+  {
+    const int v = std::atoi( ml );
+    if ( v == 1 || v == 32 )
+      e->max_lanes = v;
+  }
+  if ( const char* tn = std::getenv( "NG_ONE_THREAD_MIN_N" ) )
+  {
+    const long long v = std::atoll( tn );
+    if ( v > 0 )
+      e->one_thread_min_n = v;
+  }
   if ( cudaStreamSynchronize( e->stream ) != cudaSuccess )
     return bail( fail( NG_ERR_CUDA, "ng_create: device initialisation failed" ) );
   *out = e;
@@ -1218,6 +1389,9 @@ ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const
   cudaSetDevice( e->cfg.device );
   const int64_t n = e->N;
   std::vector< double4 > tab( ( size_t ) n );
+  std::vector< int2 > ref( ( size_t ) n, make_int2( 0, 0 ) );
+  std::vector< double > cdf;
+  std::unordered_map< double, int2 > tables;  // one CDF table per distinct lambda
   bool any = false;
   for ( int64_t i = 0; i < n; ++i )
   {
@@ -1226,10 +1400,31 @@ ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const
     // lambda = h * rate * 1e-3 (models/poisson_generator.cpp:114)
     const double lam = rate_hz[ i ] > 0 ? e->h * rate_hz[ i ] * 1e-3 : 0.0;
     tab[ i ] = poisson_table( lam );
-    any = any || lam > 0;
+    if ( !( lam > 0 ) )
+      continue;
+    any = true;
+    auto it = tables.find( lam );
+    if ( it == tables.end() )
+    {
+      int2 r2 = make_int2( ( int ) cdf.size(), -1 );
+      std::vector< double > t2;
+      if ( poisson_cdf_table( lam, t2 ) )
+      {
+        r2.y = ( int ) t2.size();
+        cdf.insert( cdf.end(), t2.begin(), t2.end() );
+      }
+      it = tables.emplace( lam, r2 ).first;
+    }
+    ref[ i ] = it->second;
   }
+  if ( cdf.empty() )
+    cdf.push_back( 1.0 );
   int rc;
   if ( ( rc = e->upload( e->pois, tab.data(), tab.size() * sizeof( double4 ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->pois_ref, ref.data(), ref.size() * sizeof( int2 ) ) ) )
+    return rc;
+  if ( ( rc = e->upload( e->pois_cdf, cdf.data(), cdf.size() * sizeof( double ) ) ) )
     return rc;
   if ( ( rc = e->upload( e->pois_w, weight, ( size_t ) n * sizeof( double ) ) ) )
     return rc;
@@ -1255,6 +1450,8 @@ ng_set_recording( ng_engine* e, const uint8_t* flags )
   for ( int64_t i = 0; i < e->n_src; ++i )
     nr += flags[ i ] ? 1 : 0;
   std::vector< uint8_t > f( flags, flags + e->n_src );
+  e->rec_host = f;
+  e->log_bound_dirty = true;
   int rc = e->upload( e->rec, f.data(), f.size() );
   if ( rc )
     return rc;
@@ -1408,11 +1605,7 @@ ng_set_stream( ng_engine* e, void* cuda_stream )
   if ( !e )
     return fail( NG_ERR_ARG, "null engine" );
   e->stream = cuda_stream ? ( cudaStream_t ) cuda_stream : e->own;
-  if ( e->graph )
-  {
-    cudaGraphExecDestroy( e->graph );
-    e->graph = nullptr;
-  }
+  e->drop_graphs();
   return NG_OK;
 }
 

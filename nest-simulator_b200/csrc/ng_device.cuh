@@ -75,7 +75,9 @@ struct Net
   uint2* log;
   int64_t log_cap;
   const uint8_t* rec;
-  const double4* pois;  // lambda, p_m, F_m, m
+  const double4* pois;  // lambda, p_m, F_m, m (walk from the mode, long tables)
+  const int2* pois_cdf_ref;  // per neuron: (offset, length) into pois_cdf; length 0 = no drive, -1 = walk
+  const double* pois_cdf;    // concatenated CDF tables, one per distinct rate
   const double* pois_w;
   const int32_t* pois_d;
   int64_t pois_start, pois_stop;

@@ -19,6 +19,8 @@ namespace ng
 {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int NG_IAF_PSC_DELTA_ID = 0;
+constexpr int NG_IAF_PSC_EXP_ID = 1;
 
 template < typename T >
 __device__ __forceinline__ T
@@ -46,10 +48,11 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
     return;
   const int lane = threadIdx.x & 31;
   const unsigned lt = ( 1u << lane ) - 1u;
-  long long pdeg = 0, rdeg = 0;
+  long long pdeg = 0, rdeg = 0, row = 0;
   if ( spk )
   {
-    pdeg = d.row_ptr[ src + 1 ] - d.row_ptr[ src ];
+    row = d.row_ptr[ src ];
+    pdeg = d.row_ptr[ src + 1 ] - row;
     rdeg = ( long long ) d.real_deg[ src ] * mult;
   }
   long long incl = pdeg;
@@ -78,7 +81,8 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
     const long long off = ( long long ) ( base & EV_MASK ) + incl - pdeg;
     if ( idx < d.spk_cap )
     {
-      d.spk[ idx ] = make_int4( src, tmod, mult, 0 );
+      // entry: CSR row start (lo, hi), emission slot, multiplicity
+      d.spk[ idx ] = make_int4( ( int ) ( unsigned ) ( row & 0xffffffffll ), ( int ) ( row >> 32 ), tmod, mult );
       d.spk_off[ idx ] = off;
     }
     else
@@ -111,27 +115,139 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
   }
 }
 
-// Poisson drive value for neuron i at step t (generator step t - delay).
+// Append all spikes of a chunk of up to 32 lags at once: bit k of `mask` is
+// a spike of this lane's neuron at lag k (emission step t0 + k, ring slot
+// (slot0 + k) mod L).  One spike-list and one log reservation per warp and
+// chunk, issued together, instead of an atomic round trip per lag.  Must be
+// called by all 32 lanes.
+__device__ __forceinline__ void
+warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long t0 )
+{
+  const int cnt = __popc( mask );
+  if ( __ballot_sync( FULL, cnt > 0 ) == 0 )
+    return;
+  const int lane = threadIdx.x & 31;
+  long long pdeg = 0, rdeg = 0, row = 0;
+  const bool lg = cnt > 0 && ( d.rec == nullptr || d.rec[ src ] );
+  if ( cnt > 0 )
+  {
+    row = d.row_ptr[ src ];
+    pdeg = d.row_ptr[ src + 1 ] - row;
+    rdeg = d.real_deg[ src ];
+  }
+  long long c_incl = cnt, e_incl = cnt * pdeg, l_incl = lg ? cnt : 0;
+#pragma unroll
+  for ( int o = 1; o < 32; o <<= 1 )
+  {
+    const long long a = __shfl_up_sync( FULL, c_incl, o );
+    const long long b = __shfl_up_sync( FULL, e_incl, o );
+    const long long c = __shfl_up_sync( FULL, l_incl, o );
+    if ( lane >= o )
+    {
+      c_incl += a;
+      e_incl += b;
+      l_incl += c;
+    }
+  }
+  const long long tot_c = __shfl_sync( FULL, c_incl, 31 );
+  const long long tot_e = __shfl_sync( FULL, e_incl, 31 );
+  const long long tot_l = __shfl_sync( FULL, l_incl, 31 );
+  const long long rtot = warp_sum_ll( cnt * rdeg );
+  unsigned long long base = 0, lbase = 0;
+  if ( lane == 0 )
+  {
+    base = atomicAdd( &d.ctl->spk_packed, ( ( unsigned long long ) tot_c << SPK_SHIFT ) | ( unsigned long long ) tot_e );
+    if ( tot_l > 0 )
+      lbase = atomicAdd( &d.ctl->log_count, ( unsigned long long ) tot_l );
+    atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
+    atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) tot_c );
+  }
+  base = __shfl_sync( FULL, base, 0 );
+  lbase = __shfl_sync( FULL, lbase, 0 );
+  if ( cnt == 0 )
+    return;
+  long long idx = ( long long ) ( base >> SPK_SHIFT ) + c_incl - cnt;
+  long long off = ( long long ) ( base & EV_MASK ) + e_incl - cnt * pdeg;
+  long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
+  const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
+  unsigned m = mask;
+  while ( m )
+  {
+    const int k = __ffs( m ) - 1;
+    m &= m - 1;
+    int slot = slot0 + k;
+    if ( slot >= d.L )
+      slot -= d.L;
+    if ( idx < d.spk_cap )
+    {
+      d.spk[ idx ] = make_int4( ( int ) ( unsigned ) ( row & 0xffffffffll ), ( int ) ( row >> 32 ), slot, 1 );
+      d.spk_off[ idx ] = off;
+    }
+    else
+    {
+      atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+    }
+    ++idx;
+    off += pdeg;
+    if ( lg )
+    {
+      if ( li < d.log_cap )
+        d.log[ li ] = make_uint2( ( uint32_t ) src, ( uint32_t ) ( t0 + k + 1 - lb0 ) | ( 1u << 24 ) );
+      else
+        atomicOr( &d.ctl->err, ERR_LOG );
+      ++li;
+    }
+  }
+}
+
+// Read the slice origin once per CTA (a load by every warp of a large grid
+// queues thousands of requests on one L2 line).  Call from all threads.
+__device__ __forceinline__ long long
+cta_origin( const Net& d )
+{
+  __shared__ long long s_origin;
+  if ( threadIdx.x == 0 )
+    s_origin = ld_volatile( &d.ctl->origin );
+  __syncthreads();
+  return s_origin;
+}
+
+// Poisson drive value for neuron i at step t (generator step t - delay):
+// inversion over the neuron's precomputed CDF table (cdf[k] = P(X <= k)),
+// or, for tables too long to store, the walk from the mode.
 template < typename Real >
 __device__ __forceinline__ Real
 drive( const Net& d, int64_t i, long long t, long long& cnt )
 {
   if ( !d.has_pois )
     return Real( 0 );
-  const double4 tab = d.pois[ i ];
-  if ( !( tab.x > 0.0 ) )
+  const int2 tb = __ldg( d.pois_cdf_ref + i );
+  if ( tb.y == 0 )
     return Real( 0 );
-  const long long tg = t - d.pois_d[ i ];
+  const long long tg = t - __ldg( d.pois_d + i );
   if ( !( d.pois_start < tg && tg <= d.pois_stop ) || tg < 0 )
     return Real( 0 );
   uint32_t o[ 4 ];
   philox4x32_10( ( uint32_t ) i, ( uint32_t ) tg, ( uint32_t ) ( ( unsigned long long ) tg >> 32 ), DRIVE_STREAM,
     d.key0, d.key1, o );
-  const long long k = poisson_from_mode( tab, u53( o[ 0 ], o[ 1 ] ) );
+  const double u = u53( o[ 0 ], o[ 1 ] );
+  long long k;
+  if ( tb.y > 0 )
+  {
+    const double* cdf = d.pois_cdf + tb.x;
+    int j = 0;
+    while ( j < tb.y - 1 && u > __ldg( cdf + j ) )
+      ++j;
+    k = j;
+  }
+  else
+  {
+    k = poisson_from_mode( d.pois[ i ], u );
+  }
   cnt += k;
   if ( k <= 0 )
     return Real( 0 );
-  return ( Real ) ( d.pois_w[ i ] * ( double ) k );
+  return ( Real ) ( __ldg( d.pois_w + i ) * ( double ) k );
 }
 
 template < typename Real, bool FIX >
@@ -176,12 +292,22 @@ trace_put( const Net& d, int64_t i, long long stamp, const double* vals )
   }
 }
 
+// Drive counts: warp sums, then one atomic per CTA (a same-address atomic
+// per warp serialises thousands of L2 atomics at large grids).  Must be
+// called by every thread of the CTA.
 __device__ __forceinline__ void
 flush_drive_count( const Net& d, long long cnt )
 {
+  __shared__ unsigned long long s_cnt;
+  if ( threadIdx.x == 0 )
+    s_cnt = 0ull;
+  __syncthreads();
   const long long s = warp_sum_ll( cnt );
   if ( ( threadIdx.x & 31 ) == 0 && s > 0 )
-    atomicAdd( &d.ctl->drive_events, ( unsigned long long ) s );
+    atomicAdd( &s_cnt, ( unsigned long long ) s );
+  __syncthreads();
+  if ( threadIdx.x == 0 && s_cnt > 0 )
+    atomicAdd( &d.ctl->drive_events, s_cnt );
 }
 
 // Scheduled generator spikes with emission step in [origin+from, origin+to):
@@ -213,185 +339,385 @@ append_scheduled( const Net& d, long long origin, int from, int to )
 }
 
 // ---------------------------------------------------------------------
-// iaf_psc_delta (models/iaf_psc_delta.cpp:272-329)
-// ctab: P33, P30, V_th, V_reset, V_min, RefractoryCounts
-// state: s0 = y3 (V_m - E_L), s1 = y0, s2 = I_e
+// iaf_psc_delta (models/iaf_psc_delta.cpp:272-329) and iaf_psc_exp
+// (models/iaf_psc_exp.cpp:288-348), one thread per neuron.
+//
+// Used for slices of one or two steps and for large networks, where one
+// thread per neuron already gives enough warps to hide memory latency.  The
+// lags run in order in registers; spikes are collected as a bit mask per
+// chunk of up to 32 lags and appended once per chunk (warp_append_mask).
+//
+// iaf_psc_delta ctab: P33, P30, V_th, V_reset, V_min, RefractoryCounts
+//               state: s0 = y3 (V_m - E_L), s1 = y0, s2 = I_e
+// iaf_psc_exp   ctab: P22, P21ex, P21in, P20, P11ex, P11in, Theta, V_reset,
+//                     RefractoryCounts, 1 - P11ex
+//               state: s0 = V_m - E_L, s1 = i_syn_ex, s2 = i_syn_in,
+//                      s3 = i_0, s4 = i_1, s5 = I_e
 // ---------------------------------------------------------------------
-template < typename Real, bool FIX >
+template < typename Real, bool FIX, int MODEL >
 __global__ void __launch_bounds__( 256 )
-k_update_delta( Net d, Block b, int from, int to, int sched )
+k_update_iaf( Net d, Block b, int from, int to, int sched )
 {
-  const long long origin = ld_volatile( &d.ctl->origin );
+  const long long origin = cta_origin( d );
   if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
     append_scheduled( d, origin, from, to );
   const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = li < b.n;
   const int64_t i = b.off + ( act ? li : 0 );
-  Real* sV = ( Real* ) b.s[ 0 ];
-  Real* sy0 = ( Real* ) b.s[ 1 ];
-  const Real* sIe = ( const Real* ) b.s[ 2 ];
-  Real V = 0, y0 = 0, Ie = 0, P33 = 0, P30 = 0, Vth = 0, Vreset = 0, Vmin = 0;
+  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
+  Real* s0 = ( Real* ) b.s[ 0 ];
+  Real* s1 = ( Real* ) b.s[ 1 ];
+  Real* s2 = ( Real* ) b.s[ 2 ];
+  Real* s3 = ( Real* ) b.s[ 3 ];
+  Real* s4 = ( Real* ) b.s[ 4 ];
+  Real V = 0, x1 = 0, x2 = 0, i0 = 0, i1 = 0, Ie = 0;
+  Real c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, Vth = 0, Vreset = 0, c9 = 0;
   int r = 0, refr = 0;
   if ( act )
   {
     const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
-    P33 = ( Real ) ct[ 0 ];
-    P30 = ( Real ) ct[ 1 ];
-    Vth = ( Real ) ct[ 2 ];
-    Vreset = ( Real ) ct[ 3 ];
-    Vmin = ( Real ) ct[ 4 ];
-    refr = ( int ) ct[ 5 ];
-    V = sV[ li ];
-    y0 = sy0[ li ];
-    Ie = sIe[ li ];
+    if constexpr ( EXP )
+    {
+      c0 = ( Real ) ct[ 0 ];
+      c1 = ( Real ) ct[ 1 ];
+      c2 = ( Real ) ct[ 2 ];
+      c3 = ( Real ) ct[ 3 ];
+      c4 = ( Real ) ct[ 4 ];
+      c5 = ( Real ) ct[ 5 ];
+      Vth = ( Real ) ct[ 6 ];
+      Vreset = ( Real ) ct[ 7 ];
+      refr = ( int ) ct[ 8 ];
+      c9 = ( Real ) ct[ 9 ];
+      V = s0[ li ];
+      x1 = s1[ li ];
+      x2 = s2[ li ];
+      i0 = s3[ li ];
+      i1 = s4[ li ];
+      Ie = ( ( const Real* ) b.s[ 5 ] )[ li ];
+    }
+    else
+    {
+      c0 = ( Real ) ct[ 0 ];
+      c1 = ( Real ) ct[ 1 ];
+      Vth = ( Real ) ct[ 2 ];
+      Vreset = ( Real ) ct[ 3 ];
+      c2 = ( Real ) ct[ 4 ];
+      refr = ( int ) ct[ 5 ];
+      V = s0[ li ];
+      x1 = s1[ li ];
+      Ie = s2[ li ];
+    }
     r = b.r[ li ];
   }
-  long long t = origin + from;
-  int slot = ( int ) ( t % d.L );
   long long dcnt = 0;
-  for ( int lag = from; lag < to; ++lag, ++t )
+  for ( int cb = from; cb < to; cb += 32 )
   {
-    bool spk = false;
-    if ( act )
+    const int nl = min( 32, to - cb );
+    const long long t0 = origin + cb;
+    const int slot0 = ( int ) ( t0 % d.L );
+    int slot = slot0;
+    unsigned smask = 0;
+    for ( int k = 0; k < nl; ++k )
     {
-      Real in = ring_take< Real, FIX >( d, slot, 0, i );
-      const Real dv = drive< Real >( d, i, t, dcnt );
-      if ( dv != Real( 0 ) )
-        in = in + dv;
-      if ( r == 0 )
+      if ( act )
       {
-        V = P30 * ( y0 + Ie ) + P33 * V + in;
-        V = ( V < Vmin ? Vmin : V );
+        Real ex = ring_take< Real, FIX >( d, slot, 0, i );
+        Real inh = 0;
+        if constexpr ( EXP )
+          inh = ring_take< Real, FIX >( d, slot, 1, i );
+        const Real dv = drive< Real >( d, i, t0 + k, dcnt );
+        if ( dv != Real( 0 ) )
+        {
+          if constexpr ( EXP )
+          {
+            if ( dv > Real( 0 ) )
+              ex = ex + dv;
+            else
+              inh = inh + dv;
+          }
+          else
+          {
+            ex = ex + dv;
+          }
+        }
+        bool spk = false;
+        if constexpr ( EXP )
+        {
+          if ( r == 0 )
+            V = V * c0 + x1 * c1 + x2 * c2 + ( Ie + i0 ) * c3;
+          else
+            --r;
+          x1 *= c4;
+          x2 *= c5;
+          x1 += c9 * i1;
+          x1 += ex;
+          x2 += inh;
+          if ( V >= Vth )
+          {
+            r = refr;
+            V = Vreset;
+            spk = true;
+          }
+          i0 = Real( 0 );
+          i1 = Real( 0 );
+        }
+        else
+        {
+          if ( r == 0 )
+          {
+            V = c1 * ( x1 + Ie ) + c0 * V + ex;
+            V = ( V < c2 ? c2 : V );
+          }
+          else
+          {
+            --r;
+          }
+          if ( V >= Vth )
+          {
+            r = refr;
+            V = Vreset;
+            spk = true;
+          }
+          x1 = Real( 0 );
+        }
+        if ( spk )
+          smask |= 1u << k;
+        if ( d.trace_col )
+        {
+          if constexpr ( EXP )
+          {
+            const double vals[ 6 ] = { ( double ) V, ( double ) x1, ( double ) x2, ( double ) i0, ( double ) i1,
+              ( double ) Ie };
+            trace_put( d, i, t0 + k + 1, vals );
+          }
+          else
+          {
+            const double vals[ 3 ] = { ( double ) V, ( double ) x1, ( double ) Ie };
+            trace_put( d, i, t0 + k + 1, vals );
+          }
+        }
       }
-      else
-      {
-        --r;
-      }
-      if ( V >= Vth )
-      {
-        r = refr;
-        V = Vreset;
-        spk = true;
-      }
-      y0 = Real( 0 );
+      if ( ++slot == d.L )
+        slot = 0;
     }
-    warp_append( d, spk, ( int32_t ) i, slot, 1, t + 1 );
-    if ( act && d.trace_col )
-    {
-      const double vals[ 3 ] = { ( double ) V, ( double ) y0, ( double ) Ie };
-      trace_put( d, i, t + 1, vals );
-    }
-    if ( ++slot == d.L )
-      slot = 0;
+    warp_append_mask( d, smask, ( int32_t ) i, slot0, t0 );
   }
   flush_drive_count( d, dcnt );
   if ( act )
   {
-    sV[ li ] = V;
-    sy0[ li ] = y0;
+    s0[ li ] = V;
+    s1[ li ] = x1;
+    if constexpr ( EXP )
+    {
+      s2[ li ] = x2;
+      s3[ li ] = i0;
+      s4[ li ] = i1;
+    }
     b.r[ li ] = r;
   }
 }
 
 // ---------------------------------------------------------------------
-// iaf_psc_exp (models/iaf_psc_exp.cpp:288-348)
-// ctab: P22, P21ex, P21in, P20, P11ex, P11in, Theta, V_reset, RefractoryCounts, 1-P11ex
-// state: s0 = V_m - E_L, s1 = i_syn_ex, s2 = i_syn_in, s3 = i_0, s4 = i_1, s5 = I_e
+// Two-phase variant for slices of 3 or more lags.  A CTA serves 32 neurons.
+// Phase 1: all 256 threads read and clear the ring slots and draw the
+// Poisson drive of the CTA's (neuron, lag) pairs -- the state-independent,
+// latency-heavy part -- into shared memory, coalesced across neurons.
+// Phase 2: warp 0 runs the state recurrence, one lane per neuron, reading
+// its inputs from shared memory, and appends each lag's spikes with one
+// ballot.  Same arithmetic, in the same order, as k_update_iaf.
 // ---------------------------------------------------------------------
-template < typename Real, bool FIX >
+constexpr int P2_NB = 32;  // neurons per CTA
+constexpr int P2_CH = 32;  // lags per chunk
+
+template < typename Real, bool FIX, int MODEL >
 __global__ void __launch_bounds__( 256 )
-k_update_exp( Net d, Block b, int from, int to, int sched )
+k_update_iaf2( Net d, Block b, int from, int to, int sched )
 {
-  const long long origin = ld_volatile( &d.ctl->origin );
+  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
+  __shared__ Real s_ex[ P2_CH ][ P2_NB ];
+  __shared__ Real s_in[ EXP ? P2_CH : 1 ][ P2_NB ];
+  const long long origin = cta_origin( d );
   if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
     append_scheduled( d, origin, from, to );
-  const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = li < b.n;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t nb0 = ( int64_t ) blockIdx.x * P2_NB;
+  const int64_t li = nb0 + lane;
+  const bool act = warp == 0 && li < b.n;
   const int64_t i = b.off + ( act ? li : 0 );
   Real* s0 = ( Real* ) b.s[ 0 ];
   Real* s1 = ( Real* ) b.s[ 1 ];
   Real* s2 = ( Real* ) b.s[ 2 ];
   Real* s3 = ( Real* ) b.s[ 3 ];
   Real* s4 = ( Real* ) b.s[ 4 ];
-  const Real* s5 = ( const Real* ) b.s[ 5 ];
-  Real V = 0, iex = 0, iin = 0, i0 = 0, i1 = 0, Ie = 0;
-  Real P22 = 0, P21ex = 0, P21in = 0, P20 = 0, P11ex = 0, P11in = 0, Theta = 0, Vreset = 0, omP11ex = 0;
+  Real V = 0, x1 = 0, x2 = 0, i0 = 0, i1 = 0, Ie = 0;
+  Real c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, Vth = 0, Vreset = 0, c9 = 0;
   int r = 0, refr = 0;
   if ( act )
   {
     const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
-    P22 = ( Real ) ct[ 0 ];
-    P21ex = ( Real ) ct[ 1 ];
-    P21in = ( Real ) ct[ 2 ];
-    P20 = ( Real ) ct[ 3 ];
-    P11ex = ( Real ) ct[ 4 ];
-    P11in = ( Real ) ct[ 5 ];
-    Theta = ( Real ) ct[ 6 ];
-    Vreset = ( Real ) ct[ 7 ];
-    refr = ( int ) ct[ 8 ];
-    omP11ex = ( Real ) ct[ 9 ];
-    V = s0[ li ];
-    iex = s1[ li ];
-    iin = s2[ li ];
-    i0 = s3[ li ];
-    i1 = s4[ li ];
-    Ie = s5[ li ];
+    if constexpr ( EXP )
+    {
+      c0 = ( Real ) ct[ 0 ];
+      c1 = ( Real ) ct[ 1 ];
+      c2 = ( Real ) ct[ 2 ];
+      c3 = ( Real ) ct[ 3 ];
+      c4 = ( Real ) ct[ 4 ];
+      c5 = ( Real ) ct[ 5 ];
+      Vth = ( Real ) ct[ 6 ];
+      Vreset = ( Real ) ct[ 7 ];
+      refr = ( int ) ct[ 8 ];
+      c9 = ( Real ) ct[ 9 ];
+      V = s0[ li ];
+      x1 = s1[ li ];
+      x2 = s2[ li ];
+      i0 = s3[ li ];
+      i1 = s4[ li ];
+      Ie = ( ( const Real* ) b.s[ 5 ] )[ li ];
+    }
+    else
+    {
+      c0 = ( Real ) ct[ 0 ];
+      c1 = ( Real ) ct[ 1 ];
+      Vth = ( Real ) ct[ 2 ];
+      Vreset = ( Real ) ct[ 3 ];
+      c2 = ( Real ) ct[ 4 ];
+      refr = ( int ) ct[ 5 ];
+      V = s0[ li ];
+      x1 = s1[ li ];
+      Ie = s2[ li ];
+    }
     r = b.r[ li ];
   }
-  long long t = origin + from;
-  int slot = ( int ) ( t % d.L );
   long long dcnt = 0;
-  for ( int lag = from; lag < to; ++lag, ++t )
+  for ( int cb = from; cb < to; cb += P2_CH )
   {
-    bool spk = false;
-    if ( act )
+    const int nl = min( P2_CH, to - cb );
+    const long long t0 = origin + cb;
+    const int slot0 = ( int ) ( t0 % d.L );
+    // ---- phase 1: inputs of (neuron q, lag k), item j = k * 32 + q
+    for ( int j = threadIdx.x; j < nl * P2_NB; j += blockDim.x )
     {
-      if ( r == 0 )
-        V = V * P22 + iex * P21ex + iin * P21in + ( Ie + i0 ) * P20;
-      else
-        --r;
-      iex *= P11ex;
-      iin *= P11in;
-      iex += omP11ex * i1;
-      Real ex = ring_take< Real, FIX >( d, slot, 0, i );
-      Real inh = ring_take< Real, FIX >( d, slot, 1, i );
-      const Real dv = drive< Real >( d, i, t, dcnt );
-      if ( dv != Real( 0 ) )
+      const int k = j >> 5;
+      const int q = j & 31;
+      const int64_t lq = nb0 + q;
+      Real ex = 0, inh = 0;
+      if ( lq < b.n )
       {
-        if ( dv > Real( 0 ) )
-          ex = ex + dv;
-        else
-          inh = inh + dv;
+        const int64_t iq = b.off + lq;
+        int slot = slot0 + k;
+        if ( slot >= d.L )
+          slot -= d.L;
+        ex = ring_take< Real, FIX >( d, slot, 0, iq );
+        if constexpr ( EXP )
+          inh = ring_take< Real, FIX >( d, slot, 1, iq );
+        const Real dv = drive< Real >( d, iq, t0 + k, dcnt );
+        if ( dv != Real( 0 ) )
+        {
+          if constexpr ( EXP )
+          {
+            if ( dv > Real( 0 ) )
+              ex = ex + dv;
+            else
+              inh = inh + dv;
+          }
+          else
+          {
+            ex = ex + dv;
+          }
+        }
       }
-      iex += ex;
-      iin += inh;
-      if ( V >= Theta )
-      {
-        r = refr;
-        V = Vreset;
-        spk = true;
-      }
-      i0 = Real( 0 );
-      i1 = Real( 0 );
+      s_ex[ k ][ q ] = ex;
+      if constexpr ( EXP )
+        s_in[ k ][ q ] = inh;
     }
-    warp_append( d, spk, ( int32_t ) i, slot, 1, t + 1 );
-    if ( act && d.trace_col )
+    __syncthreads();
+    // ---- phase 2: the recurrence, one lane per neuron
+    if ( warp == 0 )
     {
-      const double vals[ 6 ] = { ( double ) V, ( double ) iex, ( double ) iin, ( double ) i0, ( double ) i1,
-        ( double ) Ie };
-      trace_put( d, i, t + 1, vals );
+      int slot = slot0;
+      unsigned smask = 0;
+      for ( int k = 0; k < nl; ++k )
+      {
+        bool spk = false;
+        if ( act )
+        {
+          const Real in_ex = s_ex[ k ][ lane ];
+          if constexpr ( EXP )
+          {
+            const Real in_in = s_in[ k ][ lane ];
+            if ( r == 0 )
+              V = V * c0 + x1 * c1 + x2 * c2 + ( Ie + i0 ) * c3;
+            else
+              --r;
+            x1 *= c4;
+            x2 *= c5;
+            x1 += c9 * i1;
+            x1 += in_ex;
+            x2 += in_in;
+            if ( V >= Vth )
+            {
+              r = refr;
+              V = Vreset;
+              spk = true;
+            }
+            i0 = Real( 0 );
+            i1 = Real( 0 );
+          }
+          else
+          {
+            if ( r == 0 )
+            {
+              V = c1 * ( x1 + Ie ) + c0 * V + in_ex;
+              V = ( V < c2 ? c2 : V );
+            }
+            else
+            {
+              --r;
+            }
+            if ( V >= Vth )
+            {
+              r = refr;
+              V = Vreset;
+              spk = true;
+            }
+            x1 = Real( 0 );
+          }
+        }
+        if ( spk )
+          smask |= 1u << k;
+        if ( act && d.trace_col )
+        {
+          if constexpr ( EXP )
+          {
+            const double vals[ 6 ] = { ( double ) V, ( double ) x1, ( double ) x2, ( double ) i0, ( double ) i1,
+              ( double ) Ie };
+            trace_put( d, i, t0 + k + 1, vals );
+          }
+          else
+          {
+            const double vals[ 3 ] = { ( double ) V, ( double ) x1, ( double ) Ie };
+            trace_put( d, i, t0 + k + 1, vals );
+          }
+        }
+        if ( ++slot == d.L )
+          slot = 0;
+      }
+      warp_append_mask( d, smask, ( int32_t ) i, slot0, t0 );
     }
-    if ( ++slot == d.L )
-      slot = 0;
+    __syncthreads();
   }
   flush_drive_count( d, dcnt );
   if ( act )
   {
     s0[ li ] = V;
-    s1[ li ] = iex;
-    s2[ li ] = iin;
-    s3[ li ] = i0;
-    s4[ li ] = i1;
+    s1[ li ] = x1;
+    if constexpr ( EXP )
+    {
+      s2[ li ] = x2;
+      s3[ li ] = i0;
+      s4[ li ] = i1;
+    }
     b.r[ li ] = r;
   }
 }
@@ -502,7 +828,7 @@ template < typename Real, bool FIX >
 __global__ void __launch_bounds__( 128 )
 k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
 {
-  const long long origin = ld_volatile( &d.ctl->origin );
+  const long long origin = cta_origin( d );
   if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
     append_scheduled( d, origin, from, to );
   const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
@@ -658,27 +984,40 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
 // an item is found by binary search over the spikes' event offsets, staged
 // in shared memory when the list is short.
 // ---------------------------------------------------------------------
-constexpr int SMEM_SPIKES = 2048;
+constexpr int SMEM_SPIKES = 1024;
 
 template < bool FIX >
 __global__ void __launch_bounds__( 256 )
 k_deliver( Net d )
 {
   __shared__ long long s_off[ SMEM_SPIKES ];
+  __shared__ int4 s_spk[ SMEM_SPIKES ];
   __shared__ int s_last;
-  const unsigned long long packed = ld_volatile( &d.ctl->spk_packed );
-  long long nspk = ( long long ) ( packed >> SPK_SHIFT );
+  __shared__ unsigned long long s_packed;
+  __shared__ int s_err;
+  if ( threadIdx.x == 0 )
+  {
+    s_packed = ld_volatile( &d.ctl->spk_packed );
+    s_err = ld_volatile( &d.ctl->err );
+  }
+  __syncthreads();
+  const unsigned long long packed = s_packed;
+  const long long nspk = ( long long ) ( packed >> SPK_SHIFT );
   const long long nev = ( long long ) ( packed & EV_MASK );
-  const bool ok = nspk <= d.spk_cap && ( ld_volatile( &d.ctl->err ) & ERR_SPIKE_LIST ) == 0;
+  const bool ok = nspk <= d.spk_cap && ( s_err & ERR_SPIKE_LIST ) == 0;
   const long long nq = ok ? ( nev >> 2 ) : 0;
   const bool use_sm = nspk <= SMEM_SPIKES;
-  if ( use_sm && nq > 0 )
+  if ( use_sm && nq > 0 && ( long long ) blockIdx.x * blockDim.x < nq )
   {
     for ( long long k = threadIdx.x; k < nspk; k += blockDim.x )
+    {
       s_off[ k ] = d.spk_off[ k ];
+      s_spk[ k ] = d.spk[ k ];
+    }
     __syncthreads();
   }
   const long long* off = use_sm ? s_off : d.spk_off;
+  const int4* spl = use_sm ? s_spk : d.spk;
   const long long stride = ( long long ) gridDim.x * blockDim.x;
   for ( long long q = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride )
   {
@@ -692,16 +1031,14 @@ k_deliver( Net d )
       else
         hi = mid;
     }
-    const int4 sp = d.spk[ lo ];
-    const long long row = d.row_ptr[ sp.x ];
-    const long long edge = row + ( e0 - off[ lo ] );
-    if ( edge + 4 > d.row_ptr[ sp.x + 1 ] )
-      continue;
-    const uint4 tdc = *reinterpret_cast< const uint4* >( d.edge_tdc + edge );
+    const int4 sp = spl[ lo ];
+    // off[lo] <= e0 < off[lo + 1]: the quad lies inside this spike's padded row
+    const long long edge = ( ( ( long long ) sp.y << 32 ) | ( unsigned ) sp.x ) + ( e0 - off[ lo ] );
+    const uint4 tdc = __ldg( reinterpret_cast< const uint4* >( d.edge_tdc + edge ) );
     const uint32_t tw[ 4 ] = { tdc.x, tdc.y, tdc.z, tdc.w };
     if constexpr ( FIX )
     {
-      const int4 w4 = *reinterpret_cast< const int4* >( ( const int32_t* ) d.edge_w + edge );
+      const int4 w4 = __ldg( reinterpret_cast< const int4* >( ( const int32_t* ) d.edge_w + edge ) );
       const int32_t ww[ 4 ] = { w4.x, w4.y, w4.z, w4.w };
       unsigned long long* ring = ( unsigned long long* ) d.ring;
 #pragma unroll
@@ -710,17 +1047,17 @@ k_deliver( Net d )
         if ( ww[ k ] == 0 )
           continue;
         const uint32_t tgt = tw[ k ] & d.tmask;
-        int slot = sp.y + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
+        int slot = sp.z + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
         if ( slot >= d.L )
           slot -= d.L;
         const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
-        atomicAdd( ring + idx, ( unsigned long long ) ( ( long long ) ww[ k ] * ( long long ) sp.z ) );
+        atomicAdd( ring + idx, ( unsigned long long ) ( ( long long ) ww[ k ] * ( long long ) sp.w ) );
       }
     }
     else
     {
       const double2* wp = reinterpret_cast< const double2* >( ( const double* ) d.edge_w + edge );
-      const double2 wa = wp[ 0 ], wb = wp[ 1 ];
+      const double2 wa = __ldg( wp ), wb = __ldg( wp + 1 );
       const double ww[ 4 ] = { wa.x, wa.y, wb.x, wb.y };
       double* ring = ( double* ) d.ring;
 #pragma unroll
@@ -729,11 +1066,11 @@ k_deliver( Net d )
         if ( ww[ k ] == 0.0 )
           continue;
         const uint32_t tgt = tw[ k ] & d.tmask;
-        int slot = sp.y + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
+        int slot = sp.z + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
         if ( slot >= d.L )
           slot -= d.L;
         const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
-        atomicAdd( ring + idx, sp.z == 1 ? ww[ k ] : ww[ k ] * ( double ) sp.z );
+        atomicAdd( ring + idx, sp.w == 1 ? ww[ k ] : ww[ k ] * ( double ) sp.w );
       }
     }
   }

@@ -596,6 +596,8 @@ class Kernel:
         self.time_simulate = time.perf_counter() - t0
 
     def simulate(self, t_ms):
+        if self.ms_to_steps_exact(t_ms) < 0:
+            raise KernelException("Simulation time must be >= 0")
         self.prepare()
         self.run(t_ms)
         self.cleanup()

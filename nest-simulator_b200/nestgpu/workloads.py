@@ -38,3 +38,30 @@ def brunel_exp(nest, n_exc=10000, n_inh=2500, k_exc=1000, k_inh=250, J=87.8, g=5
 
 def c1(nest, precision="fp64", seed=4242):
     return brunel_exp(nest, precision=precision, seed=seed)
+
+
+def brunel_exp_batch(nest, copies, n_exc=10000, n_inh=2500, k_exc=1000, k_inh=250, J=87.8, g=5.0, rate=8000.0,
+                     delay=1.5, tau_syn=0.5, seed=4242, precision="fp32", record=True):
+    """`copies` independent realizations of the Brunel-type iaf_psc_exp network
+    in one kernel: the engine advances them together (one node-update and one
+    delivery launch per slice for all of them, concatenated CSRs)."""
+    nest.ResetKernel()
+    nest.set(resolution=0.1, rng_seed=seed, precision=precision)
+    N = n_exc + n_inh
+    rng = np.random.default_rng(seed)
+    pops, recs = [], []
+    for _ in range(copies):
+        pop = nest.Create("iaf_psc_exp", N, params={"tau_syn_ex": tau_syn, "tau_syn_in": tau_syn})
+        pop.set(V_m=rng.normal(-58.0, 10.0, N))
+        nest.Connect(pop[:n_exc], pop, {"rule": "fixed_indegree", "indegree": k_exc, "allow_autapses": False},
+                     {"weight": J, "delay": delay})
+        nest.Connect(pop[n_exc:], pop, {"rule": "fixed_indegree", "indegree": k_inh, "allow_autapses": False},
+                     {"weight": -g * J, "delay": delay})
+        pg = nest.Create("poisson_generator", params={"rate": rate})
+        nest.Connect(pg, pop, syn_spec={"weight": J, "delay": delay})
+        if record:
+            sr = nest.Create("spike_recorder")
+            nest.Connect(pop, sr, syn_spec={"delay": delay})
+            recs.append(sr)
+        pops.append(pop)
+    return pops, recs

@@ -83,14 +83,50 @@ u53( uint32_t a, uint32_t b )
   return ( ( double ) ( a >> 5 ) * 67108864.0 + ( double ) ( b >> 6 ) ) * ( 1.0 / 9007199254740992.0 );
 }
 
-/* Poisson(lambda) by inversion from the mode (Kemp & Kemp 1991): start at
- * m = floor(lambda) with p_m and F_m = P(X <= m) precomputed, walk down while
- * u <= F - p, else up while u > F.  Only +, *, / after the precomputation. */
+/* Poisson(lambda) by inversion: the smallest k with u <= F(k), read from a
+ * precomputed CDF table, or for long tables by walking from the mode
+ * (Kemp & Kemp 1991): start at m = floor(lambda) with p_m and F_m = P(X <= m)
+ * precomputed, walk down while u <= F - p, else up while u > F. */
 typedef struct
 {
   double lambda, pm, Fm;
   int64_t m;
+  double* cdf; /* cdf[k] = P(X <= k), last entry 1; NULL: walk from the mode */
+  int len;
 } pois_tab;
+
+/* CDF table, summed upward in FP64 until 1 - F < 1e-17 (k > lambda) or 256
+ * entries; the last entry is set to 1.  No table for lambda > 100 or when the
+ * tail is not reached. */
+static void
+pois_cdf_table( pois_tab* t )
+{
+  t->cdf = NULL;
+  t->len = 0;
+  const double lambda = t->lambda;
+  if ( !( lambda > 0.0 ) || lambda > 100.0 )
+    return;
+  double* c = malloc( sizeof( double ) * 256 );
+  double p = exp( -lambda ), F = p;
+  int n = 0;
+  c[ n++ ] = F;
+  for ( int k = 1; k < 256; ++k )
+  {
+    p = p * lambda / ( double ) k;
+    F += p;
+    c[ n++ ] = F;
+    if ( 1.0 - F < 1e-17 && ( double ) k > lambda )
+      break;
+  }
+  if ( 1.0 - F > 1e-15 )
+  {
+    free( c );
+    return;
+  }
+  c[ n - 1 ] = 1.0;
+  t->cdf = c;
+  t->len = n;
+}
 
 static pois_tab
 pois_prepare( double lambda )
@@ -98,6 +134,8 @@ pois_prepare( double lambda )
   pois_tab t;
   t.lambda = lambda;
   t.m = ( int64_t ) floor( lambda );
+  t.cdf = NULL;
+  t.len = 0;
   if ( lambda <= 0.0 )
   {
     t.m = 0;
@@ -114,12 +152,20 @@ pois_prepare( double lambda )
     F += p;
   }
   t.Fm = F;
+  pois_cdf_table( &t );
   return t;
 }
 
 static inline int64_t
 pois_draw( const pois_tab* t, double u )
 {
+  if ( t->cdf )
+  {
+    int j = 0;
+    while ( j < t->len - 1 && u > t->cdf[ j ] )
+      ++j;
+    return j;
+  }
   int64_t k = t->m;
   double p = t->pm, F = t->Fm;
   if ( u > F )
@@ -147,7 +193,9 @@ int64_t
 orc_poisson_draw( double lambda, double u )
 {
   pois_tab t = pois_prepare( lambda );
-  return pois_draw( &t, u );
+  const int64_t k = pois_draw( &t, u );
+  free( t.cdf );
+  return k;
 }
 
 /* ---------------------------------------------------------------------
@@ -371,6 +419,9 @@ orc_destroy( orc_net* net )
   free( net->part_d );
   free( net->sched_step );
   free( net->sched_src );
+  if ( net->pois )
+    for ( int64_t i = 0; i < net->n; ++i )
+      free( net->pois[ i ].cdf );
   free( net->pois );
   free( net->pois_w );
   free( net->pois_d );
@@ -541,6 +592,9 @@ int
 orc_set_poisson( orc_net* net, const double* rate_hz, const double* w, const int32_t* d, int64_t start_step,
   int64_t stop_step, uint64_t seed )
 {
+  if ( net->pois )
+    for ( int64_t i = 0; i < net->n; ++i )
+      free( net->pois[ i ].cdf );
   free( net->pois );
   free( net->pois_w );
   free( net->pois_d );

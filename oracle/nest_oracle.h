@@ -22,7 +22,7 @@
  *   - poisson_generator drive: a draw per target per generator step t_g with
  *     start < t_g <= stop, arriving at t_g + d (models/poisson_generator.cpp:
  *     125-148, nestkernel/stimulation_device.cpp:47-57).  The draw itself uses
- *     a counter-based Philox4x32-10 stream and inversion-from-the-mode, so the
+ *     a counter-based Philox4x32-10 stream and inversion over a CDF table, so the
  *     drive is statistically (not bitwise) equal to the reference's
  *     std::poisson_distribution over mt19937_64.
  *
@@ -92,7 +92,7 @@ double orc_iaf_propagator_exp( double tau_syn, double tau_m, double c_m, double 
 /* Philox4x32-10 block (Salmon et al., SC'11) for known-answer tests. */
 void orc_philox4x32( const uint32_t ctr[ 4 ], const uint32_t key[ 2 ], int rounds, uint32_t out[ 4 ] );
 
-/* Poisson draw by inversion from the mode with host-precomputed (m, p_m, F_m). */
+/* Poisson draw by inversion (CDF table, or the walk from the mode for long tables). */
 int64_t orc_poisson_draw( double lambda, double u );
 
 #ifdef __cplusplus

@@ -274,11 +274,50 @@ def make_c1_stats(nest):
             cv[i] = isi.std() / isi.mean()
     pop_counts = np.bincount(np.rint(t / 1.0).astype(np.int64), minlength=1001)
     ks = nest.GetKernelStatus()
+    # spread of the population statistics across network realizations
+    seed_rates, seed_cvs = [], []
+    for seed in (1, 2, 3, 5, 6):
+        r, c = _c1_once(nest, seed)
+        seed_rates.append(r)
+        seed_cvs.append(c)
     np.savez_compressed(os.path.join(HERE, "c1_exp_poisson_stats.npz"),
                         counts=counts.astype(np.int32), cv=cv, pop_counts_1ms=pop_counts.astype(np.int32),
                         ref_wall_s=np.float64(wall), ref_threads=np.int64(8),
-                        time_simulate=np.float64(ks.get("time_simulate", np.nan)))
+                        time_simulate=np.float64(ks.get("time_simulate", np.nan)),
+                        seed_rates=np.array(seed_rates), seed_mean_cv=np.array(seed_cvs))
     print("c1: rate", counts.mean(), "Hz; mean CV", np.nanmean(cv), "; wall", wall)
+
+
+def _c1_once(nest, seed):
+    """Mean rate and mean CV-ISI of one realization of the config-1 network."""
+    nest.ResetKernel()
+    nest.set(resolution=0.1, local_num_threads=8, rng_seed=seed)
+    NE, NI = 10000, 2500
+    N = NE + NI
+    pop = nest.Create("iaf_psc_exp", N, params={"tau_syn_ex": 0.5, "tau_syn_in": 0.5})
+    pop.set(V_m=list(np.random.default_rng(seed).normal(-58.0, 10.0, N)))
+    nest.Connect(pop[:NE], pop, {"rule": "fixed_indegree", "indegree": 1000, "allow_autapses": False},
+                 {"weight": 87.8, "delay": 1.5})
+    nest.Connect(pop[NE:], pop, {"rule": "fixed_indegree", "indegree": 250, "allow_autapses": False},
+                 {"weight": -5.0 * 87.8, "delay": 1.5})
+    pg = nest.Create("poisson_generator", params={"rate": 8000.0})
+    nest.Connect(pg, pop, syn_spec={"weight": 87.8, "delay": 1.5})
+    sr = nest.Create("spike_recorder")
+    nest.Connect(pop, sr, syn_spec={"delay": 1.5})
+    nest.Simulate(1000.0)
+    snd = np.asarray(sr.events["senders"], dtype=np.int64) - 1
+    t = np.asarray(sr.events["times"])
+    o = np.lexsort((t, snd))
+    snd, t = snd[o], t[o]
+    cvs = []
+    starts = np.searchsorted(snd, np.arange(N))
+    ends = np.searchsorted(snd, np.arange(N), side="right")
+    for i in range(N):
+        ts = t[starts[i]:ends[i]]
+        if len(ts) >= 3:
+            isi = np.diff(ts)
+            cvs.append(isi.std() / isi.mean())
+    return len(t) / N, float(np.mean(cvs))
 
 
 def make_aeif_lsodar():
