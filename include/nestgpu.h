@@ -187,6 +187,60 @@ int ng_set_graph_slices( ng_engine* eng, int32_t slices_per_graph );
  * P21ex, P21in, P20, RefractoryCounts (models/iaf_psc_exp.cpp:244-285). */
 int ng_debug_coefficients( ng_engine* eng, int32_t block, int64_t index, double* out, int32_t cap, int32_t* n_out );
 
+/* ---------------------------------------------------------------------
+ * Allocation-free entry point.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory on the path that steps a
+ * network: a host framework that owns all device memory through its own
+ * allocator or pool and forbids foreign allocations, or a closed-loop
+ * controller that steps a small network every control tick and cannot take
+ * an allocation's implicit synchronisation and latency.  It simulates a
+ * small iaf_psc_delta network in the plain FP64 form (the same arithmetic as
+ * ng_simulate) from inputs and into outputs that the caller owns in device
+ * memory, and calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ * Its ring buffer, spike list and counters live in one file-scope device
+ * array of NG_NOALLOC_SCRATCH_BYTES that every GPU which loads the library
+ * holds until the process exits.  Networks whose scratch
+ * ((min_delay + max_delay) * n * 8 + n * min_delay * 8 bytes + 256) does not
+ * fit are rejected with NG_ERR_CAPACITY.  Every call starts a fresh run (it
+ * zeroes the ring and counters) and shares the one array, so calls that
+ * overlap on the GPU race: serialise them (one stream, or events).  The
+ * first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  The call
+ * is asynchronous on `cuda_stream`; spikes beyond out_cap are counted in
+ * *out_count but not written.
+ * --------------------------------------------------------------------- */
+#define NG_NOALLOC_SCRATCH_BYTES ( 16u << 20 )
+
+typedef struct
+{
+  int64_t n;                  /* neurons */
+  int32_t min_delay;          /* steps */
+  int32_t max_delay;          /* steps */
+  int64_t start_step;         /* absolute step of the first slice origin, a multiple of min_delay */
+  const double* P33;          /* per neuron: exp(-h / tau_m) */
+  const double* P30;          /* per neuron: 1 / C_m * (1 - P33) * tau_m */
+  const double* V_th_rel;     /* per neuron, relative to E_L */
+  const double* V_reset_rel;  /* per neuron, relative to E_L */
+  const double* V_min_rel;    /* per neuron, relative to E_L */
+  const double* I_e;          /* per neuron [pA] */
+  const int32_t* refr_counts; /* per neuron: refractory steps */
+  double* V_m_rel;            /* in/out: membrane potential relative to E_L */
+  int32_t* r;                 /* in/out: refractory step counter */
+  const int64_t* row_ptr;     /* CSR over the n neurons (n + 1 entries) */
+  const int32_t* target;      /* edge target neuron */
+  const double* weight;       /* edge weight [mV] */
+  const int32_t* delay;       /* edge delay [steps], min_delay <= d <= max_delay */
+  int32_t* out_src;           /* out: spike sources */
+  int64_t* out_stamp;         /* out: spike stamps (emission step + 1) */
+  int64_t out_cap;            /* capacity of out_src / out_stamp */
+  unsigned long long* out_count; /* out: number of spikes emitted */
+} ng_noalloc_net;
+
+/* Simulate n_steps of `net` with no memory allocation (see above). */
+int ng_simulate_noalloc( const ng_noalloc_net* net, int64_t n_steps, void* cuda_stream );
+
 #ifdef __cplusplus
 }
 #endif

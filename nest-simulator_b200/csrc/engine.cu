@@ -871,6 +871,13 @@ struct ng_engine
   }
 };
 
+// error text of entry points compiled in other files of the library
+void
+ng_internal_set_error( const char* msg )
+{
+  g_err = msg;
+}
+
 extern "C" {
 
 int

@@ -31,7 +31,7 @@ EXPORTED = [
     "ng_abi_version", "ng_last_error", "ng_device_count", "ng_create", "ng_destroy", "ng_set_var", "ng_get_var",
     "ng_set_connections", "ng_set_connections_coo", "ng_set_spike_schedule", "ng_set_poisson", "ng_set_recording", "ng_set_trace",
     "ng_simulate", "ng_spike_count", "ng_get_spikes", "ng_trace_count", "ng_get_trace", "ng_get_stats",
-    "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients",
+    "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients", "ng_simulate_noalloc",
 ]
 
 
