@@ -61,6 +61,12 @@ typedef struct
   int64_t n_generators;    /* extra spike sources after the neurons (spike_generator ports) */
   int64_t spike_log_capacity; /* device spike-log entries between drains, 0 = automatic */
   int64_t start_step;      /* absolute step of the engine's first slice origin (SimulationManager clock_) */
+  /* serving: networks are added and removed while the engine runs (ng_net_*);
+   * block_size[0] is then the neuron capacity of the pool */
+  int32_t serving;
+  int32_t max_networks;    /* serving: network slots */
+  int64_t edge_capacity;   /* serving: edge pool, padding included */
+  double max_abs_weight;   /* serving, FP32 form: largest |weight| (sets the fixed-point scale) */
 } ng_config;
 
 /* Counters and timings of an engine. */
@@ -186,6 +192,100 @@ int ng_set_graph_slices( ng_engine* eng, int32_t slices_per_graph );
  * iaf_psc_delta: P33, P30, RefractoryCounts; iaf_psc_exp: P11ex, P11in, P22,
  * P21ex, P21in, P20, RefractoryCounts (models/iaf_psc_exp.cpp:244-285). */
 int ng_debug_coefficients( ng_engine* eng, int32_t block, int64_t index, double* out, int32_t cap, int32_t* n_out );
+
+/* ---------------------------------------------------------------------
+ * Serving: independent networks admitted into and retired from one engine
+ * while it runs (continuous batching).  All networks share the engine's
+ * model (block 0), resolution and min/max delay; each has its own clock
+ * origin, duration and drive seed.  A network draws the same drive and
+ * produces the same spikes wherever and whenever it is admitted (its Philox
+ * counters use network-local neuron indices and steps; the FP32 form's
+ * int64 ring sums are order independent).  No counterpart in the reference,
+ * which runs one network per kernel.
+ * --------------------------------------------------------------------- */
+
+/* fixed_indegree connectivity drawn on the device (nestkernel/conn_builder.cpp
+ * FixedInDegreeBuilder, with a Philox stream instead of the reference's RNG):
+ * every target gets k_exc sources from neurons [0, n_exc) and k_inh from
+ * [n_exc, n), weights w_exc / w_inh, one delay. */
+typedef struct
+{
+  int64_t n_exc;
+  int32_t k_exc, k_inh;
+  double w_exc, w_inh;
+  int32_t delay_steps;
+  int32_t allow_autapses;
+  uint64_t seed;
+} ng_fixed_indegree;
+
+/* pairwise_bernoulli connectivity drawn on the device (nestkernel/conn_builder.h:716
+ * BernoulliBuilder, with a Philox stream): the network's neurons form
+ * populations in order; a (source, target) pair of populations (i, j) is
+ * connected with probability p[i * NG_MAX_POPS + j]; weights and delays are
+ * normal per source type (index 1: excitatory population, 0: inhibitory),
+ * delays clipped to [h, d_max_ms] and rounded to steps. */
+#define NG_MAX_POPS 16
+typedef struct
+{
+  int32_t n_pops;
+  int64_t pop_size[ NG_MAX_POPS ];
+  int32_t pop_exc[ NG_MAX_POPS ];
+  double p[ NG_MAX_POPS * NG_MAX_POPS ];
+  double w_mean[ 2 ], w_sd[ 2 ];
+  double d_mean_ms[ 2 ], d_sd_ms[ 2 ];
+  double d_max_ms;
+  int32_t allow_autapses;
+  uint64_t seed;
+} ng_pairwise_bernoulli;
+
+typedef struct
+{
+  int64_t n;                        /* neurons */
+  int64_t steps;                    /* steps to simulate from admission */
+  uint64_t seed;                    /* Philox key of the network's drive */
+  int32_t record;                   /* log the network's spikes */
+  int32_t n_vars;                   /* per-neuron parameter/state arrays (model's internal names) */
+  const char* const* var_names;
+  const double* const* var_values;
+  int64_t nnz;                      /* explicit edges (local neuron indices), or ... */
+  const int32_t* source;
+  const int32_t* target;
+  const double* weight;
+  const int32_t* delay_steps;
+  const ng_fixed_indegree* build;   /* ... connectivity drawn on the device (nnz ignored) */
+  const double* poisson_rate;       /* per neuron [Hz] (NULL: no drive) */
+  const double* poisson_weight;
+  const int32_t* poisson_delay;
+  const ng_pairwise_bernoulli* build_pb; /* or pairwise_bernoulli connectivity drawn on the device */
+} ng_net_desc;
+
+/* Admit a network at the current clock (a slice boundary).  Returns
+ * NG_ERR_CAPACITY, and changes nothing, when its neurons or edges do not
+ * fit the free pool right now (admission by device-memory footprint). */
+int ng_net_add( ng_engine* eng, const ng_net_desc* desc, int32_t* net_id );
+
+/* Steps simulated so far and whether the network has reached its duration. */
+int ng_net_poll( ng_engine* eng, int32_t net_id, int64_t* steps_done, int32_t* finished );
+
+/* Drain the network's logged spikes: local neuron index and local stamp. */
+int ng_net_spikes( ng_engine* eng, int32_t net_id, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out );
+
+/* Read a state variable of the network's neurons (length n). */
+int ng_net_get_var( ng_engine* eng, int32_t net_id, const char* name, double* out );
+
+/* The network's connections in network-local ids, grouped by source
+ * (GetConnections, nestkernel/nest.cpp:get_connections, with the fields
+ * source, target, weight, delay of nestkernel/connection_manager.cpp:
+ * get_connections).  With source == NULL only *n_out (the count) is set;
+ * otherwise cap must hold all of them. */
+int ng_net_get_connections( ng_engine* eng, int32_t net_id, int32_t* source, int32_t* target, double* weight,
+  int32_t* delay_steps, int64_t cap, int64_t* n_out );
+
+/* Retire the network and free its neurons, edges and slot. */
+int ng_net_remove( ng_engine* eng, int32_t net_id );
+
+/* Free neurons and edges of the pool (largest free runs). */
+int ng_net_capacity( ng_engine* eng, int64_t* free_neurons, int64_t* free_edges );
 
 /* ---------------------------------------------------------------------
  * Allocation-free entry point.  No counterpart in the reference.

@@ -19,8 +19,11 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
+
 #include "../../include/nestgpu.h"
 #include "ng_kernels.cuh"
+#include "ng_serving.cuh"
 
 using namespace ng;
 
@@ -213,12 +216,13 @@ struct ng_engine
   };
   std::vector< Blk > blk;
 
-  DevBuf ring, row_ptr, real_deg, tdc, w, spk, spk_off, log, rec, pois, pois_w, pois_d, pois_ref, pois_cdf, trace_col,
+  DevBuf ring, row_beg, row_len, real_deg, tdc, w, ent, log, rec, pois, pois_w, pois_d, pois_ref, pois_cdf, trace_col,
     trace, sched_step, sched_src, ctl;
   int32_t tbits = 1;
   uint32_t tmask = 1, dmask = 0;
   double fx_inv = 1.0;
-  int64_t nnz_padded = 0, spk_cap = 0, log_cap = 0, n_sched = 0, n_rec = 0;
+  int64_t nnz_padded = 0, ent_cap = 0, log_cap = 0, n_sched = 0, n_rec = 0;
+  int64_t chunks_all_src = 0, chunks_max_gen = 0;  // for the delivery work capacity
   int has_pois = 0;
   int64_t pois_start = 0, pois_stop = INT64_MAX;
   uint32_t key0 = 0, key1 = 0;
@@ -260,6 +264,162 @@ struct ng_engine
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector< DevBuf* > all;
   int deliver_ctas = 0;
+
+  // ---- serving: networks added to and removed from the running engine
+  bool serving = false;
+  DevBuf d_nid, d_step0, d_until, d_off, d_key, sc_src, sc_cnt, sc_fill, sc_beg, sc_plen, sc_total, sc_sb;
+  std::vector< int32_t > nid_host;
+  struct NetInfo
+  {
+    bool used = false;
+    int64_t off = 0, n = 0, e0 = 0, ne = 0, step0 = 0, until = 0;
+    bool rec = false;
+    double log_rate = 0.0;
+    std::vector< int32_t > src;
+    std::vector< int64_t > stamp;
+  };
+  std::vector< NetInfo > nets;
+  std::map< int64_t, int64_t > free_neurons, free_edges;  // run start -> length
+  std::unordered_map< std::string, int32_t > cls_ids;     // engine-wide coefficient classes
+  int64_t cls_cap = 0, cdf_cap = 0;
+  std::vector< double > cdf_host;
+  std::unordered_map< double, int2 > cdf_tables;
+  int fx_S = 0;
+
+  static bool
+  take_run( std::map< int64_t, int64_t >& fl, int64_t len, int64_t* start )
+  {
+    if ( len == 0 )
+    {
+      *start = 0;
+      return true;
+    }
+    for ( auto it = fl.begin(); it != fl.end(); ++it )
+      if ( it->second >= len )
+      {
+        *start = it->first;
+        const int64_t rest = it->second - len, s2 = it->first + len;
+        fl.erase( it );
+        if ( rest > 0 )
+          fl[ s2 ] = rest;
+        return true;
+      }
+    return false;
+  }
+
+  static void
+  give_run( std::map< int64_t, int64_t >& fl, int64_t start, int64_t len )
+  {
+    if ( len <= 0 )
+      return;
+    auto it = fl.emplace( start, len ).first;
+    auto nx = std::next( it );
+    if ( nx != fl.end() && it->first + it->second == nx->first )
+    {
+      it->second += nx->second;
+      fl.erase( nx );
+    }
+    if ( it != fl.begin() )
+    {
+      auto pv = std::prev( it );
+      if ( pv->first + pv->second == it->first )
+      {
+        pv->second += it->second;
+        fl.erase( it );
+      }
+    }
+  }
+
+  // pools of a serving engine: every array sized for the capacity up front,
+  // so admitting or retiring a network changes no device pointer and the
+  // captured slice graphs stay valid
+  int
+  setup_serving()
+  {
+    int rc;
+    const int64_t E = cfg.edge_capacity;
+    const int nmax = cfg.max_networks;
+    nets.assign( ( size_t ) nmax, NetInfo() );
+    nid_host.assign( ( size_t ) N, -1 );
+    if ( ( rc = alloc( d_nid, ( size_t ) N * 4 ) ) )
+      return rc;
+    k_fill_i32<<< ( unsigned ) ( ( N + 255 ) / 256 ), 256, 0, stream >>>( ( int32_t* ) d_nid.p, N, -1 );
+    if ( ( rc = alloc( d_step0, ( size_t ) nmax * 8 ) ) || ( rc = alloc( d_until, ( size_t ) nmax * 8 ) )
+      || ( rc = alloc( d_off, ( size_t ) nmax * 8 ) ) || ( rc = alloc( d_key, ( size_t ) nmax * 8 ) ) )
+      return rc;
+    if ( ( rc = alloc( tdc, ( size_t ) E * 4 ) ) || ( rc = alloc( w, ( size_t ) E * ( prec == NG_FP64 ? 8 : 4 ) ) ) )
+      return rc;
+    chunks_all_src = E / CHUNK_EDGES + N;
+    if ( ( rc = resize_work() ) )
+      return rc;
+    Blk& b = blk[ 0 ];
+    cls_cap = 1 << 16;
+    if ( ( rc = alloc( b.ctab, ( size_t ) cls_cap * CT_STRIDE * 8 ) ) || ( rc = alloc( b.cls, ( size_t ) N * 4 ) ) )
+      return rc;
+    b.host_cls.assign( ( size_t ) N, 0 );
+    b.dirty = false;
+    cdf_cap = 1 << 20;
+    if ( ( rc = alloc( pois_cdf, ( size_t ) cdf_cap * 8 ) ) || ( rc = alloc( pois_ref, ( size_t ) N * 8 ) )
+      || ( rc = alloc( pois, ( size_t ) N * sizeof( double4 ) ) ) || ( rc = alloc( pois_w, ( size_t ) N * 8 ) )
+      || ( rc = alloc( pois_d, ( size_t ) N * 4 ) ) )
+      return rc;
+    has_pois = 1;
+    if ( ( rc = alloc( rec, ( size_t ) N ) ) )
+      return rc;
+    rec_host.assign( ( size_t ) N, 0 );
+    free_neurons.clear();
+    free_edges.clear();
+    free_neurons[ 0 ] = N;
+    free_edges[ 0 ] = E;
+    // one fixed-point scale for every network (FP32 form)
+    const double mx = cfg.max_abs_weight > 0 ? cfg.max_abs_weight : 1e4;
+    fx_S = ( int ) std::floor( std::log2( 2147483647.0 / mx ) );
+    fx_S = std::max( -30, std::min( fx_S, 60 ) );
+    fx_inv = prec == NG_FP64 ? 1.0 : std::ldexp( 1.0, -fx_S );
+    log_per_step = 1.0;
+    serving = true;
+    ++generation;
+    CU( cudaStreamSynchronize( stream ) );
+    return NG_OK;
+  }
+
+  // channel word and stored weight of an edge into the block-0 model
+  void
+  edge_word( double wv, uint32_t* ch, double* we ) const
+  {
+    const int model = blk[ 0 ].model;
+    *ch = 0;
+    *we = wv;
+    if ( model == NG_IAF_PSC_EXP )
+      *ch = wv > 0 ? 0u : 1u;
+    else if ( model == NG_AEIF_COND_ALPHA && !( wv > 0.0 ) )
+    {
+      *ch = 1u;
+      *we = -wv;
+    }
+  }
+
+  int
+  grow( DevBuf& b, size_t bytes )
+  {
+    if ( b.bytes >= bytes )
+      return NG_OK;
+    return alloc( b, bytes );
+  }
+
+  // delivery work per slice: every source spiking at every lag, each spike
+  // queueing ceil(padded degree / 128) chunks, plus the generator spikes
+  int
+  resize_work()
+  {
+    int64_t need = ( int64_t ) cfg.min_delay * chunks_all_src + n_sched * chunks_max_gen + 1024;
+    need = std::min< int64_t >( need, 1ll << 28 );
+    if ( need <= ent_cap )
+      return NG_OK;
+    ent_cap = need;
+    ++generation;
+    return alloc( ent, ( size_t ) ent_cap * sizeof( int4 ) );
+  }
   int max_lanes = 32;             // 1: always one thread per neuron
   int64_t one_thread_min_n = 20000;  // block size from which one thread per neuron fills the GPU
 
@@ -276,7 +436,7 @@ struct ng_engine
       cudaFree( b.cls.p );
       cudaFree( b.ctab.p );
     }
-    DevBuf* bufs[] = { &ring, &row_ptr, &real_deg, &tdc, &w, &spk, &spk_off, &log, &rec, &pois, &pois_w, &pois_d,
+    DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
       &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
@@ -333,6 +493,76 @@ struct ng_engine
   }
 
   // pre_run_hook restatements -> coefficient rows (FP64), deduped into classes
+  // pre_run_hook restatement for neuron i of block b: one coefficient row
+  int
+  coef_row( const Blk& b, int64_t i, double* row ) const
+  {
+  std::fill( row, row + CT_STRIDE, 0.0 );
+  const auto& P = b.par;
+  if ( b.model == NG_IAF_PSC_DELTA )
+  {
+    const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ];
+    if ( !( c_m > 0 ) || !( tau_m > 0 ) || P[ 2 ][ i ] < 0 )
+      return fail( NG_ERR_ARG, "iaf_psc_delta: C_m and tau_m must be > 0, t_ref >= 0" );
+    if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
+      return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
+    row[ 0 ] = std::exp( -h / tau_m );
+    row[ 1 ] = 1 / c_m * ( 1 - row[ 0 ] ) * tau_m;
+    row[ 2 ] = P[ 3 ][ i ];
+    row[ 3 ] = P[ 4 ][ i ];
+    row[ 4 ] = P[ 5 ][ i ];
+    row[ 5 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+  }
+  else if ( b.model == NG_IAF_PSC_EXP )
+  {
+    const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ], tex = P[ 5 ][ i ], tin = P[ 6 ][ i ];
+    if ( !( c_m > 0 ) || !( tau_m > 0 ) || !( tex > 0 ) || !( tin > 0 ) || P[ 2 ][ i ] < 0 )
+      return fail( NG_ERR_ARG, "iaf_psc_exp: capacitance and time constants must be > 0, t_ref >= 0" );
+    if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
+      return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
+    const double P11ex = std::exp( -h / tex );
+    const double P11in = std::exp( -h / tin );
+    const double P22 = std::exp( -h / tau_m );
+    row[ 0 ] = P22;
+    row[ 1 ] = propagator_exp( tex, tau_m, c_m, h );
+    row[ 2 ] = propagator_exp( tin, tau_m, c_m, h );
+    row[ 3 ] = tau_m / c_m * ( 1.0 - P22 );
+    row[ 4 ] = P11ex;
+    row[ 5 ] = P11in;
+    row[ 6 ] = P[ 3 ][ i ];
+    row[ 7 ] = P[ 4 ][ i ];
+    row[ 8 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+    row[ 9 ] = 1. - P11ex;
+  }
+  else
+  {
+    for ( int k = 0; k < 15; ++k )
+      row[ k ] = P[ k == 0 ? 0 : k == 1 ? 1 : k + 1 ][ i ];
+    // order: V_peak, V_reset, g_L, C_m, E_ex, E_in, E_L, Delta_T, tau_w, a, b, V_th, tau_ex, tau_in, tol
+    row[ 14 ] = P[ 15 ][ i ];
+    const double Vpeak = P[ 0 ][ i ], Vreset = P[ 1 ][ i ], Vth = P[ 12 ][ i ], DT = P[ 8 ][ i ];
+    if ( Vreset >= Vpeak )
+      return fail( NG_ERR_ARG, "Ensure that: V_reset < V_peak ." );
+    if ( DT < 0. )
+      return fail( NG_ERR_ARG, "Delta_T must be positive." );
+    if ( Vpeak < Vth )
+      return fail( NG_ERR_ARG, "V_peak >= V_th required." );
+    if ( !( P[ 4 ][ i ] > 0 ) )
+      return fail( NG_ERR_ARG, "Capacitance must be strictly positive." );
+    if ( !( P[ 13 ][ i ] > 0 ) || !( P[ 14 ][ i ] > 0 ) || !( P[ 9 ][ i ] > 0 ) )
+      return fail( NG_ERR_ARG, "All time constants must be strictly positive." );
+    if ( !( P[ 15 ][ i ] > 0 ) )
+      return fail( NG_ERR_ARG, "The gsl_error_tol must be strictly positive." );
+    if ( P[ 2 ][ i ] < 0 )
+      return fail( NG_ERR_ARG, "Refractory time cannot be negative." );
+    row[ 15 ] = 1.0 * M_E / P[ 13 ][ i ];
+    row[ 16 ] = 1.0 * M_E / P[ 14 ][ i ];
+    row[ 17 ] = DT > 0. ? Vpeak : Vth;
+    row[ 18 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+  }
+  return NG_OK;
+  }
+
   int
   build_classes( Blk& b )
   {
@@ -342,69 +572,9 @@ struct ng_engine
     double row[ CT_STRIDE ];
     for ( int64_t i = 0; i < b.n; ++i )
     {
-      std::fill( row, row + CT_STRIDE, 0.0 );
-      const auto& P = b.par;
-      if ( b.model == NG_IAF_PSC_DELTA )
-      {
-        const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ];
-        if ( !( c_m > 0 ) || !( tau_m > 0 ) || P[ 2 ][ i ] < 0 )
-          return fail( NG_ERR_ARG, "iaf_psc_delta: C_m and tau_m must be > 0, t_ref >= 0" );
-        if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
-          return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
-        row[ 0 ] = std::exp( -h / tau_m );
-        row[ 1 ] = 1 / c_m * ( 1 - row[ 0 ] ) * tau_m;
-        row[ 2 ] = P[ 3 ][ i ];
-        row[ 3 ] = P[ 4 ][ i ];
-        row[ 4 ] = P[ 5 ][ i ];
-        row[ 5 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
-      }
-      else if ( b.model == NG_IAF_PSC_EXP )
-      {
-        const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ], tex = P[ 5 ][ i ], tin = P[ 6 ][ i ];
-        if ( !( c_m > 0 ) || !( tau_m > 0 ) || !( tex > 0 ) || !( tin > 0 ) || P[ 2 ][ i ] < 0 )
-          return fail( NG_ERR_ARG, "iaf_psc_exp: capacitance and time constants must be > 0, t_ref >= 0" );
-        if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
-          return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
-        const double P11ex = std::exp( -h / tex );
-        const double P11in = std::exp( -h / tin );
-        const double P22 = std::exp( -h / tau_m );
-        row[ 0 ] = P22;
-        row[ 1 ] = propagator_exp( tex, tau_m, c_m, h );
-        row[ 2 ] = propagator_exp( tin, tau_m, c_m, h );
-        row[ 3 ] = tau_m / c_m * ( 1.0 - P22 );
-        row[ 4 ] = P11ex;
-        row[ 5 ] = P11in;
-        row[ 6 ] = P[ 3 ][ i ];
-        row[ 7 ] = P[ 4 ][ i ];
-        row[ 8 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
-        row[ 9 ] = 1. - P11ex;
-      }
-      else
-      {
-        for ( int k = 0; k < 15; ++k )
-          row[ k ] = P[ k == 0 ? 0 : k == 1 ? 1 : k + 1 ][ i ];
-        // order: V_peak, V_reset, g_L, C_m, E_ex, E_in, E_L, Delta_T, tau_w, a, b, V_th, tau_ex, tau_in, tol
-        row[ 14 ] = P[ 15 ][ i ];
-        const double Vpeak = P[ 0 ][ i ], Vreset = P[ 1 ][ i ], Vth = P[ 12 ][ i ], DT = P[ 8 ][ i ];
-        if ( Vreset >= Vpeak )
-          return fail( NG_ERR_ARG, "Ensure that: V_reset < V_peak ." );
-        if ( DT < 0. )
-          return fail( NG_ERR_ARG, "Delta_T must be positive." );
-        if ( Vpeak < Vth )
-          return fail( NG_ERR_ARG, "V_peak >= V_th required." );
-        if ( !( P[ 4 ][ i ] > 0 ) )
-          return fail( NG_ERR_ARG, "Capacitance must be strictly positive." );
-        if ( !( P[ 13 ][ i ] > 0 ) || !( P[ 14 ][ i ] > 0 ) || !( P[ 9 ][ i ] > 0 ) )
-          return fail( NG_ERR_ARG, "All time constants must be strictly positive." );
-        if ( !( P[ 15 ][ i ] > 0 ) )
-          return fail( NG_ERR_ARG, "The gsl_error_tol must be strictly positive." );
-        if ( P[ 2 ][ i ] < 0 )
-          return fail( NG_ERR_ARG, "Refractory time cannot be negative." );
-        row[ 15 ] = 1.0 * M_E / P[ 13 ][ i ];
-        row[ 16 ] = 1.0 * M_E / P[ 14 ][ i ];
-        row[ 17 ] = DT > 0. ? Vpeak : Vth;
-        row[ 18 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
-      }
+      int rc = coef_row( b, i, row );
+      if ( rc )
+        return rc;
       std::string key( reinterpret_cast< const char* >( row ), sizeof( row ) );
       auto it = ids.find( key );
       int32_t id;
@@ -446,13 +616,13 @@ struct ng_engine
     d.dmask = dmask;
     d.ring = ring.p;
     d.fx_inv = fx_inv;
-    d.row_ptr = ( const int64_t* ) row_ptr.p;
+    d.row_beg = ( const int64_t* ) row_beg.p;
+    d.row_len = ( const int32_t* ) row_len.p;
     d.real_deg = ( const int32_t* ) real_deg.p;
     d.edge_tdc = ( const uint32_t* ) tdc.p;
     d.edge_w = w.p;
-    d.spk = ( int4* ) spk.p;
-    d.spk_off = ( long long* ) spk_off.p;
-    d.spk_cap = spk_cap;
+    d.ent = ( int4* ) ent.p;
+    d.ent_cap = ent_cap;
     d.log = ( uint2* ) log.p;
     d.log_cap = log_cap;
     d.rec = ( const uint8_t* ) rec.p;
@@ -474,6 +644,11 @@ struct ng_engine
     for ( int k = 0; k < MAX_STATE; ++k )
       d.trace_slot[ k ] = trace_slot[ k ];
     d.trace_rows = trace_rows_cap;
+    d.nid = serving ? ( const int32_t* ) d_nid.p : nullptr;
+    d.net_step0 = ( const long long* ) d_step0.p;
+    d.net_until = ( const long long* ) d_until.p;
+    d.net_off = ( const long long* ) d_off.p;
+    d.net_key = ( const uint2* ) d_key.p;
     d.sched_step = ( const int64_t* ) sched_step.p;
     d.sched_src = ( const int32_t* ) sched_src.p;
     d.n_sched = n_sched;
@@ -761,14 +936,14 @@ struct ng_engine
   {
     bool rebuilt = false;
     for ( auto& b : blk )
-      if ( b.dirty )
+      if ( b.dirty && !serving )
       {
         int rc = build_classes( b );
         if ( rc )
           return rc;
         rebuilt = true;
       }
-    if ( rebuilt || log_bound_dirty )
+    if ( ( rebuilt || log_bound_dirty ) && !serving )
     {
       update_log_bound();
       log_bound_dirty = false;
@@ -806,6 +981,20 @@ struct ng_engine
       {
         const uint32_t mult = e.y >> 24;
         const int64_t stamp = clock + ( int64_t ) ( e.y & 0xFFFFFFu );
+        if ( serving )
+        {
+          const int32_t id = nid_host[ e.x ];
+          if ( id >= 0 && nets[ id ].used )
+          {
+            NetInfo& nw = nets[ id ];
+            for ( uint32_t m = 0; m < mult; ++m )
+            {
+              nw.src.push_back( ( int32_t ) ( e.x - nw.off ) );
+              nw.stamp.push_back( stamp - nw.step0 );
+            }
+          }
+          continue;
+        }
         for ( uint32_t m = 0; m < mult; ++m )
         {
           out_src.push_back( ( int32_t ) e.x );
@@ -1021,8 +1210,9 @@ ng_create( const ng_config* cfg, ng_engine** out )
   if ( ( rc = e->alloc( e->ring, ( size_t ) e->L * e->C * ( size_t ) N * 8 ) ) )
     return bail( rc );
   // empty CSR: every source has no edges
-  std::vector< int64_t > rp( ( size_t ) e->n_src + 1, 0 );
-  if ( ( rc = e->upload( e->row_ptr, rp.data(), rp.size() * sizeof( int64_t ) ) ) )
+  if ( ( rc = e->alloc( e->row_beg, ( size_t ) e->n_src * sizeof( int64_t ) ) ) )
+    return bail( rc );
+  if ( ( rc = e->alloc( e->row_len, ( size_t ) e->n_src * sizeof( int32_t ) ) ) )
     return bail( rc );
   if ( ( rc = e->alloc( e->real_deg, ( size_t ) e->n_src * sizeof( int32_t ) ) ) )
     return bail( rc );
@@ -1038,10 +1228,10 @@ ng_create( const ng_config* cfg, ng_engine** out )
   e->dmask = ( 1u << dbits ) - 1u;
   if ( ( int64_t ) cfg->max_delay > ( int64_t ) e->dmask )
     return bail( fail( NG_ERR_ARG, "ng_create: max_delay does not fit the packed edge format for this network size" ) );
-  e->spk_cap = std::min< int64_t >( e->n_src * ( int64_t ) cfg->min_delay, ( 1ll << 24 ) - 1 );
-  if ( ( rc = e->alloc( e->spk, ( size_t ) e->spk_cap * sizeof( int4 ) ) ) )
-    return bail( rc );
-  if ( ( rc = e->alloc( e->spk_off, ( size_t ) e->spk_cap * sizeof( long long ) ) ) )
+  if ( e->L >= 65536 )
+    return bail( fail( NG_ERR_ARG, "ng_create: min_delay + max_delay must be below 65536 steps" ) );
+  e->ent_cap = 1024;
+  if ( ( rc = e->alloc( e->ent, ( size_t ) e->ent_cap * sizeof( int4 ) ) ) )
     return bail( rc );
   e->log_cap = cfg->spike_log_capacity > 0 ? cfg->spike_log_capacity
                                            : std::max< int64_t >( 1 << 22, 64 * e->n_src );
@@ -1060,6 +1250,15 @@ ng_create( const ng_config* cfg, ng_engine** out )
       return bail( fail( NG_ERR_CUDA, "ng_create: control block upload failed" ) );
   }
   e->deliver_ctas = 1;
+  if ( cfg->serving )
+  {
+    if ( cfg->n_blocks != 1 || cfg->n_generators != 0 || cfg->edge_capacity < 4 || cfg->max_networks < 1 )
+      return bail( fail( NG_ERR_ARG, "ng_create: serving needs one model block, no generators, an edge capacity "
+                                     "and network slots" ) );
+    if ( ( rc = e->setup_serving() ) )
+      return bail( rc );
+    e->deliver_ctas = e->sms * 4;
+  }
   if ( const char* ml = std::getenv( "NG_MAX_LANES" ) )
   {
     const int v = std::atoi( ml );
@@ -1268,8 +1467,15 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
     }
   }
   int rc;
-  if ( ( rc = e->upload( e->row_ptr, prow.data(), prow.size() * sizeof( int64_t ) ) ) )
-    return rc;
+  {
+    std::vector< int32_t > plen( ( size_t ) n_src );
+    for ( int64_t sidx = 0; sidx < n_src; ++sidx )
+      plen[ sidx ] = ( int32_t ) ( prow[ sidx + 1 ] - prow[ sidx ] );
+    if ( ( rc = e->upload( e->row_beg, prow.data(), ( size_t ) n_src * sizeof( int64_t ) ) ) )
+      return rc;
+    if ( ( rc = e->upload( e->row_len, plen.data(), plen.size() * sizeof( int32_t ) ) ) )
+      return rc;
+  }
   if ( ( rc = e->upload( e->real_deg, rdeg.data(), rdeg.size() * sizeof( int32_t ) ) ) )
     return rc;
   if ( ( rc = e->upload( e->tdc, tdc.data(), tdc.size() * sizeof( uint32_t ) ) ) )
@@ -1299,9 +1505,20 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
     e->fx_inv = std::ldexp( 1.0, -S );
   }
   e->nnz_padded = np;
-  // delivery grid: enough CTAs for the expected events of a slice, at most 4 per SM
-  const int64_t quads = np / 4;
-  const int64_t want = std::max< int64_t >( 1, quads / 256 / 8 );
+  e->chunks_all_src = 0;
+  e->chunks_max_gen = 0;
+  for ( int64_t sidx = 0; sidx < n_src; ++sidx )
+  {
+    const int64_t nch = ( prow[ sidx + 1 ] - prow[ sidx ] + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
+    if ( sidx < e->N )
+      e->chunks_all_src += nch;
+    else
+      e->chunks_max_gen = std::max( e->chunks_max_gen, nch );
+  }
+  if ( ( rc = e->resize_work() ) )
+    return rc;
+  // delivery grid: a warp per chunk; up to 4 CTAs of 8 warps per SM, fewer for small graphs
+  const int64_t want = std::max< int64_t >( 1, e->chunks_all_src / 64 );
   e->deliver_ctas = ( int ) std::min< int64_t >( want, ( int64_t ) e->sms * 4 );
   CU( cudaStreamSynchronize( e->stream ) );
   ++e->generation;
@@ -1359,16 +1576,9 @@ ng_set_spike_schedule( ng_engine* e, int64_t n, const int64_t* emit_step, const 
   if ( ( rc = e->upload( e->sched_src, source, ( size_t ) n * sizeof( int32_t ) ) ) )
     return rc;
   e->n_sched = n;
-  // the spike list must also hold the generator spikes of one slice
-  const int64_t need = std::min< int64_t >( e->n_src * ( int64_t ) e->cfg.min_delay + n, ( 1ll << 24 ) - 1 );
-  if ( need > e->spk_cap )
-  {
-    e->spk_cap = need;
-    if ( ( rc = e->alloc( e->spk, ( size_t ) e->spk_cap * sizeof( int4 ) ) ) )
-      return rc;
-    if ( ( rc = e->alloc( e->spk_off, ( size_t ) e->spk_cap * sizeof( long long ) ) ) )
-      return rc;
-  }
+  // the delivery work must also hold the generator spikes of one slice
+  if ( ( rc = e->resize_work() ) )
+    return rc;
   if ( e->log_cap < 2 * n + 4 * e->n_src )
   {
     e->log_cap = 2 * n + 4 * e->n_src;
@@ -1623,6 +1833,575 @@ ng_set_graph_slices( ng_engine* e, int32_t slices_per_graph )
     return fail( NG_ERR_ARG, "ng_set_graph_slices: bad argument" );
   e->graph_slices = slices_per_graph;
   ++e->generation;
+  return NG_OK;
+}
+
+static int
+net_check( ng_engine* e, int32_t id )
+{
+  if ( !e || !e->serving )
+    return fail( NG_ERR_STATE, "not a serving engine (ng_config.serving = 0)" );
+  if ( id < 0 || id >= ( int32_t ) e->nets.size() || !e->nets[ id ].used )
+    return fail( NG_ERR_ARG, "unknown network id" );
+  return NG_OK;
+}
+
+int
+ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
+{
+  if ( !e || !desc || !net_id )
+    return fail( NG_ERR_ARG, "ng_net_add: null argument" );
+  if ( !e->serving )
+    return fail( NG_ERR_STATE, "ng_net_add: not a serving engine (ng_config.serving = 0)" );
+  if ( e->from != 0 )
+    return fail( NG_ERR_STATE, "ng_net_add: networks are admitted at slice boundaries" );
+  const int64_t n = desc->n;
+  if ( n < 1 || desc->steps < 0 || desc->n_vars < 0 || ( desc->n_vars > 0 && ( !desc->var_names || !desc->var_values ) ) )
+    return fail( NG_ERR_ARG, "ng_net_add: bad network description" );
+  const ng_fixed_indegree* fb = desc->build;
+  const ng_pairwise_bernoulli* pb = desc->build_pb;
+  if ( pb )
+  {
+    if ( fb || pb->n_pops < 1 || pb->n_pops > NG_MAX_POPS )
+      return fail( NG_ERR_ARG, "ng_net_add: bad pairwise_bernoulli description" );
+    int64_t tot = 0;
+    for ( int j = 0; j < pb->n_pops; ++j )
+    {
+      if ( pb->pop_size[ j ] < 0 )
+        return fail( NG_ERR_ARG, "ng_net_add: negative population size" );
+      tot += pb->pop_size[ j ];
+      for ( int i = 0; i < pb->n_pops; ++i )
+        if ( !( pb->p[ i * NG_MAX_POPS + j ] >= 0.0 && pb->p[ i * NG_MAX_POPS + j ] <= 1.0 ) )
+          return fail( NG_ERR_ARG, "ng_net_add: connection probability outside [0, 1]" );
+    }
+    if ( tot != n )
+      return fail( NG_ERR_ARG, "ng_net_add: population sizes do not add up to n" );
+  }
+  if ( fb && ( fb->n_exc < 0 || fb->n_exc > n || fb->k_exc < 0 || fb->k_inh < 0 || ( fb->k_exc > 0 && fb->n_exc == 0 )
+               || ( fb->k_inh > 0 && fb->n_exc == n ) ) )
+    return fail( NG_ERR_ARG, "ng_net_add: bad fixed_indegree description" );
+  if ( !fb && desc->nnz > 0 && ( !desc->source || !desc->target || !desc->weight || !desc->delay_steps ) )
+    return fail( NG_ERR_ARG, "ng_net_add: edges without arrays" );
+  cudaSetDevice( e->cfg.device );
+  int32_t id = -1;
+  for ( size_t k = 0; k < e->nets.size(); ++k )
+    if ( !e->nets[ k ].used )
+    {
+      id = ( int32_t ) k;
+      break;
+    }
+  if ( id < 0 )
+    return fail( NG_ERR_CAPACITY, "ng_net_add: no free network slot" );
+  // host side of explicit edges: rows padded to multiples of 4
+  std::vector< int64_t > prow;
+  std::vector< int32_t > rdeg;
+  int64_t ne_need;
+  if ( pb )
+    ne_need = 0;  // known after the counting pass
+  else if ( fb )
+    ne_need = n * ( int64_t ) ( fb->k_exc + fb->k_inh ) + 3 * n;
+  else
+  {
+    prow.assign( ( size_t ) n + 1, 0 );
+    rdeg.assign( ( size_t ) n, 0 );
+    for ( int64_t k = 0; k < desc->nnz; ++k )
+    {
+      if ( desc->source[ k ] < 0 || desc->source[ k ] >= n || desc->target[ k ] < 0 || desc->target[ k ] >= n )
+        return fail( NG_ERR_ARG, "ng_net_add: edge endpoint outside the network" );
+      ++rdeg[ desc->source[ k ] ];
+    }
+    for ( int64_t sidx = 0; sidx < n; ++sidx )
+      prow[ sidx + 1 ] = prow[ sidx ] + ( ( rdeg[ sidx ] + 3 ) & ~3 );
+    ne_need = prow[ n ];
+  }
+  int64_t n0 = 0, e0 = 0;
+  if ( !ng_engine::take_run( e->free_neurons, n, &n0 ) )
+    return fail( NG_ERR_CAPACITY, "ng_net_add: not enough free neurons in the pool" );
+  if ( !ng_engine::take_run( e->free_edges, ne_need, &e0 ) )
+  {
+    ng_engine::give_run( e->free_neurons, n0, n );
+    return fail( NG_ERR_CAPACITY, "ng_net_add: not enough free edges in the pool" );
+  }
+  auto undo = [ & ]( int code ) {
+    ng_engine::give_run( e->free_neurons, n0, n );
+    ng_engine::give_run( e->free_edges, e0, ne_need );
+    return code;
+  };
+  auto& b = e->blk[ 0 ];
+  const int model = b.model;
+  // parameters (host copies) and state (device) of the region
+  std::vector< double > defaults;
+  default_params( model, defaults );
+  for ( int p2 = 0; p2 < n_params( model ); ++p2 )
+    std::fill( b.par[ p2 ].begin() + n0, b.par[ p2 ].begin() + n0 + n, defaults[ p2 ] );
+  std::vector< const double* > state_src( MAX_STATE, nullptr );
+  for ( int32_t v = 0; v < desc->n_vars; ++v )
+  {
+    const VarSpec* vs = desc->var_names[ v ] ? find_var( model, desc->var_names[ v ] ) : nullptr;
+    if ( !vs || !desc->var_values[ v ] )
+      return undo( fail( NG_ERR_UNKNOWN_NAME, std::string( "ng_net_add: unknown variable '" )
+                                                + ( desc->var_names[ v ] ? desc->var_names[ v ] : "(null)" ) + "'" ) );
+    if ( vs->kind == PARAM )
+      std::copy( desc->var_values[ v ], desc->var_values[ v ] + n, b.par[ vs->slot ].begin() + n0 );
+    else if ( vs->kind == STATE )
+      state_src[ vs->slot ] = desc->var_values[ v ];
+  }
+  {
+    std::vector< char > tmp( ( size_t ) n * e->rsz );
+    for ( int sl = 0; sl < n_states( model ); ++sl )
+    {
+      for ( int64_t i = 0; i < n; ++i )
+      {
+        const double v = state_src[ sl ] ? state_src[ sl ][ i ] : default_state( model, sl );
+        if ( e->rsz == 8 )
+          reinterpret_cast< double* >( tmp.data() )[ i ] = v;
+        else
+          reinterpret_cast< float* >( tmp.data() )[ i ] = ( float ) v;
+      }
+      CU( cudaMemcpyAsync( ( char* ) b.st[ sl ].p + n0 * e->rsz, tmp.data(), tmp.size(), cudaMemcpyHostToDevice,
+        e->stream ) );
+      CU( cudaStreamSynchronize( e->stream ) );
+    }
+    CU( cudaMemsetAsync( ( int32_t* ) b.r.p + n0, 0, ( size_t ) n * 4, e->stream ) );
+    if ( model == NG_AEIF_COND_ALPHA )
+    {
+      std::vector< double > hs( ( size_t ) n, e->h );
+      CU( cudaMemcpyAsync( ( double* ) b.istep.p + n0, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice, e->stream ) );
+      CU( cudaStreamSynchronize( e->stream ) );
+    }
+  }
+  // coefficient classes, shared by all networks
+  double row[ CT_STRIDE ];
+  double log_rate = 0.0;
+  const int ri = model == NG_IAF_PSC_DELTA ? 5 : model == NG_IAF_PSC_EXP ? 8 : 18;
+  const int64_t first_new = ( int64_t ) e->cls_ids.size();
+  for ( int64_t i = n0; i < n0 + n; ++i )
+  {
+    std::fill( row, row + CT_STRIDE, 0.0 );
+    int rc = e->coef_row( b, i, row );
+    if ( rc )
+      return undo( rc );
+    std::string key( reinterpret_cast< const char* >( row ), sizeof( row ) );
+    auto it = e->cls_ids.find( key );
+    int32_t cid;
+    if ( it == e->cls_ids.end() )
+    {
+      cid = ( int32_t ) e->cls_ids.size();
+      if ( cid >= e->cls_cap )
+        return undo( fail( NG_ERR_CAPACITY, "ng_net_add: coefficient class table full" ) );
+      e->cls_ids.emplace( std::move( key ), cid );
+      b.host_ctab.insert( b.host_ctab.end(), row, row + CT_STRIDE );
+    }
+    else
+      cid = it->second;
+    b.host_cls[ ( size_t ) i ] = cid;
+    log_rate += 1.0 / ( row[ ri ] + 1.0 );
+  }
+  const int64_t n_cls = ( int64_t ) e->cls_ids.size();
+  if ( n_cls > first_new )
+    CU( cudaMemcpyAsync( ( double* ) b.ctab.p + first_new * CT_STRIDE, b.host_ctab.data() + first_new * CT_STRIDE,
+      ( size_t ) ( n_cls - first_new ) * CT_STRIDE * 8, cudaMemcpyHostToDevice, e->stream ) );
+  CU( cudaMemcpyAsync( ( int32_t* ) b.cls.p + n0, b.host_cls.data() + n0, ( size_t ) n * 4, cudaMemcpyHostToDevice,
+    e->stream ) );
+  // edges of the region
+  const bool fx = e->prec != NG_FP64;
+  const size_t wsz = fx ? 4 : 8;
+  if ( ne_need > 0 )
+  {
+    CU( cudaMemsetAsync( ( uint32_t* ) e->tdc.p + e0, 0, ( size_t ) ne_need * 4, e->stream ) );
+    CU( cudaMemsetAsync( ( char* ) e->w.p + e0 * wsz, 0, ( size_t ) ne_need * wsz, e->stream ) );
+  }
+  auto to_fixed = [ & ]( double wv, int32_t* out ) {
+    const double sc = std::ldexp( wv, e->fx_S );
+    if ( !( std::fabs( sc ) < 2147483647.0 ) )
+      return false;
+    *out = ( int32_t ) std::llrint( sc );
+    return true;
+  };
+  int64_t ne_used = ne_need;
+  if ( pb )
+  {
+    PbSpec sp {};
+    sp.n_pops = pb->n_pops;
+    sp.pop_lo[ 0 ] = 0;
+    int nb = 0;
+    for ( int j = 0; j < pb->n_pops; ++j )
+    {
+      sp.pop_lo[ j + 1 ] = sp.pop_lo[ j ] + pb->pop_size[ j ];
+      sp.pop_exc[ j ] = pb->pop_exc[ j ];
+      nb += ( int ) ( ( pb->pop_size[ j ] + PB_BLOCK - 1 ) / PB_BLOCK );
+    }
+    for ( int i = 0; i < pb->n_pops; ++i )
+      for ( int j = 0; j < pb->n_pops; ++j )
+      {
+        const double pp = pb->p[ i * NG_MAX_POPS + j ];
+        sp.inv_log1mp[ i * PB_MAX_POPS + j ] = pp <= 0.0 ? NAN : pp >= 1.0 ? 0.0 : 1.0 / std::log1p( -pp );
+      }
+    for ( int k = 0; k < 2; ++k )
+    {
+      sp.w_mean[ k ] = pb->w_mean[ k ];
+      sp.w_sd[ k ] = pb->w_sd[ k ];
+      sp.d_mean[ k ] = pb->d_mean_ms[ k ];
+      sp.d_sd[ k ] = pb->d_sd_ms[ k ];
+    }
+    sp.h = e->h;
+    sp.min_steps = e->cfg.min_delay;
+    sp.max_steps = e->cfg.max_delay;
+    sp.d_max = std::min( pb->d_max_ms, e->cfg.max_delay * e->h );
+    sp.allow_aut = pb->allow_autapses;
+    sp.key0 = ( uint32_t ) pb->seed;
+    sp.key1 = ( uint32_t ) ( pb->seed >> 32 );
+    sp.nb = nb;
+    const int64_t items = n * ( int64_t ) nb;
+    int rc;
+    if ( ( rc = e->grow( e->sc_sb, ( size_t ) std::max< int64_t >( items, 1 ) * 4 ) )
+      || ( rc = e->grow( e->sc_cnt, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_beg, ( size_t ) n * 8 ) )
+      || ( rc = e->grow( e->sc_plen, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_total, 8 ) ) )
+      return undo( rc );
+    const unsigned g = ( unsigned ) std::max< int64_t >( 1, ( items + 255 ) / 256 );
+    const bool ex_m = model == NG_IAF_PSC_EXP, ae_m = model == NG_AEIF_COND_ALPHA;
+    const double fxs = std::ldexp( 1.0, e->fx_S );
+    k_pb_pass< double ><<< g, 256, 0, e->stream >>>( sp, n, false, ( int* ) e->sc_sb.p, nullptr, 0, 0, e->tbits, ex_m,
+      ae_m, 1.0, nullptr, nullptr );
+    k_pb_rowsum<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, nb, ( const int* ) e->sc_sb.p,
+      ( int32_t* ) e->sc_cnt.p );
+    k_fi_scan<<< 1, 1024, 0, e->stream >>>( n, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->sc_beg.p,
+      ( int32_t* ) e->sc_plen.p, ( long long* ) e->sc_total.p );
+    long long total = 0;
+    CU( cudaMemcpyAsync( &total, e->sc_total.p, 8, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    if ( !ng_engine::take_run( e->free_edges, total, &e0 ) )
+      return undo( fail( NG_ERR_CAPACITY, "ng_net_add: not enough free edges in the pool" ) );
+    ne_need = total;
+    ne_used = total;
+    CU( cudaMemsetAsync( ( uint32_t* ) e->tdc.p + e0, 0, ( size_t ) total * 4, e->stream ) );
+    CU( cudaMemsetAsync( ( char* ) e->w.p + e0 * wsz, 0, ( size_t ) total * wsz, e->stream ) );
+    if ( fx )
+      k_pb_pass< int32_t ><<< g, 256, 0, e->stream >>>( sp, n, true, ( int* ) e->sc_sb.p, ( const int64_t* ) e->sc_beg.p,
+        n0, e0, e->tbits, ex_m, ae_m, fxs, ( uint32_t* ) e->tdc.p, ( int32_t* ) e->w.p );
+    else
+      k_pb_pass< double ><<< g, 256, 0, e->stream >>>( sp, n, true, ( int* ) e->sc_sb.p, ( const int64_t* ) e->sc_beg.p,
+        n0, e0, e->tbits, ex_m, ae_m, 1.0, ( uint32_t* ) e->tdc.p, ( double* ) e->w.p );
+    k_fi_rows<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, n0, e0, ( const int64_t* ) e->sc_beg.p,
+      ( const int32_t* ) e->sc_plen.p, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->row_beg.p,
+      ( int32_t* ) e->row_len.p, ( int32_t* ) e->real_deg.p );
+    CU( cudaGetLastError() );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  else if ( fb )
+  {
+    const int K = fb->k_exc + fb->k_inh;
+    const int64_t nk = n * K;
+    if ( fb->delay_steps < e->cfg.min_delay || fb->delay_steps > e->cfg.max_delay )
+      return undo( fail( NG_ERR_ARG, "ng_net_add: delay outside [min_delay, max_delay]" ) );
+    int rc;
+    if ( ( rc = e->grow( e->sc_src, ( size_t ) std::max< int64_t >( nk, 1 ) * 4 ) )
+      || ( rc = e->grow( e->sc_cnt, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_fill, ( size_t ) n * 4 ) )
+      || ( rc = e->grow( e->sc_beg, ( size_t ) n * 8 ) ) || ( rc = e->grow( e->sc_plen, ( size_t ) n * 4 ) )
+      || ( rc = e->grow( e->sc_total, 8 ) ) )
+      return undo( rc );
+    CU( cudaMemsetAsync( e->sc_cnt.p, 0, ( size_t ) n * 4, e->stream ) );
+    CU( cudaMemsetAsync( e->sc_fill.p, 0, ( size_t ) n * 4, e->stream ) );
+    const unsigned g = ( unsigned ) std::max< int64_t >( 1, ( nk + 255 ) / 256 );
+    if ( nk > 0 )
+      k_fi_draw<<< g, 256, 0, e->stream >>>( n, fb->n_exc, fb->k_exc, fb->k_inh, fb->allow_autapses,
+        ( uint32_t ) fb->seed, ( uint32_t ) ( fb->seed >> 32 ), ( int32_t* ) e->sc_src.p, ( int32_t* ) e->sc_cnt.p );
+    k_fi_scan<<< 1, 1024, 0, e->stream >>>( n, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->sc_beg.p,
+      ( int32_t* ) e->sc_plen.p, ( long long* ) e->sc_total.p );
+    uint32_t chx, chi;
+    double wex, win;
+    e->edge_word( fb->w_exc, &chx, &wex );
+    e->edge_word( fb->w_inh, &chi, &win );
+    const uint32_t dword = ( uint32_t ) fb->delay_steps << e->tbits;
+    const uint32_t wordx = dword | ( chx << 31 ), wordi = dword | ( chi << 31 );
+    if ( nk > 0 )
+    {
+      if ( fx )
+      {
+        int32_t fwx = 0, fwi = 0;
+        if ( !to_fixed( wex, &fwx ) || !to_fixed( win, &fwi ) )
+          return undo( fail( NG_ERR_ARG, "ng_net_add: weight above the engine's max_abs_weight" ) );
+        k_fi_scatter< int32_t ><<< g, 256, 0, e->stream >>>( n, fb->k_exc, fb->k_inh, ( const int32_t* ) e->sc_src.p,
+          ( const int64_t* ) e->sc_beg.p, ( int32_t* ) e->sc_fill.p, n0, e0, wordx, wordi, fwx, fwi,
+          ( uint32_t* ) e->tdc.p, ( int32_t* ) e->w.p );
+      }
+      else
+      {
+        k_fi_scatter< double ><<< g, 256, 0, e->stream >>>( n, fb->k_exc, fb->k_inh, ( const int32_t* ) e->sc_src.p,
+          ( const int64_t* ) e->sc_beg.p, ( int32_t* ) e->sc_fill.p, n0, e0, wordx, wordi, wex, win,
+          ( uint32_t* ) e->tdc.p, ( double* ) e->w.p );
+      }
+    }
+    k_fi_rows<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, n0, e0, ( const int64_t* ) e->sc_beg.p,
+      ( const int32_t* ) e->sc_plen.p, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->row_beg.p,
+      ( int32_t* ) e->row_len.p, ( int32_t* ) e->real_deg.p );
+    CU( cudaGetLastError() );
+    long long total = 0;
+    CU( cudaMemcpyAsync( &total, e->sc_total.p, 8, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    ne_used = total;
+  }
+  else
+  {
+    const int64_t np = prow[ n ];
+    std::vector< int64_t > pos( prow.begin(), prow.end() - 1 );
+    std::vector< uint32_t > tw( ( size_t ) std::max< int64_t >( np, 1 ), 0u );
+    std::vector< double > wd( fx ? 0 : ( size_t ) std::max< int64_t >( np, 1 ), 0.0 );
+    std::vector< int32_t > wi( fx ? ( size_t ) std::max< int64_t >( np, 1 ) : 0, 0 );
+    for ( int64_t k = 0; k < desc->nnz; ++k )
+    {
+      const int32_t d = desc->delay_steps[ k ];
+      if ( d < e->cfg.min_delay || d > e->cfg.max_delay )
+        return undo( fail( NG_ERR_ARG, "ng_net_add: delay outside [min_delay, max_delay]" ) );
+      uint32_t ch;
+      double we;
+      e->edge_word( desc->weight[ k ], &ch, &we );
+      const int64_t j = pos[ desc->source[ k ] ]++;
+      tw[ j ] = ( uint32_t ) ( n0 + desc->target[ k ] ) | ( ( uint32_t ) d << e->tbits ) | ( ch << 31 );
+      if ( fx )
+      {
+        if ( !to_fixed( we, &wi[ j ] ) )
+          return undo( fail( NG_ERR_ARG, "ng_net_add: weight above the engine's max_abs_weight" ) );
+      }
+      else
+        wd[ j ] = we;
+    }
+    if ( np > 0 )
+    {
+      CU( cudaMemcpyAsync( ( uint32_t* ) e->tdc.p + e0, tw.data(), ( size_t ) np * 4, cudaMemcpyHostToDevice, e->stream ) );
+      if ( fx )
+        CU( cudaMemcpyAsync( ( int32_t* ) e->w.p + e0, wi.data(), ( size_t ) np * 4, cudaMemcpyHostToDevice, e->stream ) );
+      else
+        CU( cudaMemcpyAsync( ( double* ) e->w.p + e0, wd.data(), ( size_t ) np * 8, cudaMemcpyHostToDevice, e->stream ) );
+    }
+    std::vector< int64_t > beg( ( size_t ) n );
+    std::vector< int32_t > plen( ( size_t ) n );
+    for ( int64_t sidx = 0; sidx < n; ++sidx )
+    {
+      beg[ sidx ] = e0 + prow[ sidx ];
+      plen[ sidx ] = ( int32_t ) ( prow[ sidx + 1 ] - prow[ sidx ] );
+    }
+    CU( cudaMemcpyAsync( ( int64_t* ) e->row_beg.p + n0, beg.data(), ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int32_t* ) e->row_len.p + n0, plen.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int32_t* ) e->real_deg.p + n0, rdeg.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice,
+      e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  // give back the unused tail of the edge reservation
+  if ( ne_used < ne_need )
+    ng_engine::give_run( e->free_edges, e0 + ne_used, ne_need - ne_used );
+  // drive: Poisson tables and CDF references of the region
+  {
+    std::vector< double4 > tab( ( size_t ) n );
+    std::vector< int2 > ref( ( size_t ) n, make_int2( 0, 0 ) );
+    std::vector< double > pw( ( size_t ) n, 0.0 );
+    std::vector< int32_t > pd( ( size_t ) n, e->cfg.min_delay );
+    const int64_t cdf_old = ( int64_t ) e->cdf_host.size();
+    for ( int64_t i = 0; i < n; ++i )
+    {
+      const double rate = desc->poisson_rate ? desc->poisson_rate[ i ] : 0.0;
+      const double lam = rate > 0 ? e->h * rate * 1e-3 : 0.0;
+      tab[ i ] = poisson_table( lam );
+      if ( !( lam > 0 ) )
+        continue;
+      pw[ i ] = desc->poisson_weight ? desc->poisson_weight[ i ] : 0.0;
+      pd[ i ] = desc->poisson_delay ? desc->poisson_delay[ i ] : e->cfg.min_delay;
+      if ( pd[ i ] < e->cfg.min_delay || pd[ i ] > e->cfg.max_delay )
+        return undo( fail( NG_ERR_ARG, "ng_net_add: Poisson delay outside [min_delay, max_delay]" ) );
+      auto it = e->cdf_tables.find( lam );
+      if ( it == e->cdf_tables.end() )
+      {
+        int2 r2 = make_int2( ( int ) e->cdf_host.size(), -1 );
+        std::vector< double > t2;
+        if ( poisson_cdf_table( lam, t2 ) )
+        {
+          if ( ( int64_t ) ( e->cdf_host.size() + t2.size() ) > e->cdf_cap )
+            return undo( fail( NG_ERR_CAPACITY, "ng_net_add: Poisson table pool full" ) );
+          r2.y = ( int ) t2.size();
+          e->cdf_host.insert( e->cdf_host.end(), t2.begin(), t2.end() );
+        }
+        it = e->cdf_tables.emplace( lam, r2 ).first;
+      }
+      ref[ i ] = it->second;
+    }
+    const int64_t cdf_new = ( int64_t ) e->cdf_host.size();
+    if ( cdf_new > cdf_old )
+      CU( cudaMemcpyAsync( ( double* ) e->pois_cdf.p + cdf_old, e->cdf_host.data() + cdf_old,
+        ( size_t ) ( cdf_new - cdf_old ) * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( double4* ) e->pois.p + n0, tab.data(), ( size_t ) n * sizeof( double4 ), cudaMemcpyHostToDevice,
+      e->stream ) );
+    CU( cudaMemcpyAsync( ( int2* ) e->pois_ref.p + n0, ref.data(), ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( double* ) e->pois_w.p + n0, pw.data(), ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int32_t* ) e->pois_d.p + n0, pd.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  // recording, network table, ids, and a clean ring region
+  CU( cudaMemsetAsync( ( uint8_t* ) e->rec.p + n0, desc->record ? 1 : 0, ( size_t ) n, e->stream ) );
+  std::fill( e->rec_host.begin() + n0, e->rec_host.begin() + n0 + n, ( uint8_t ) ( desc->record ? 1 : 0 ) );
+  const long long step0 = e->origin, until = e->origin + desc->steps, off = n0;
+  const uint2 key = make_uint2( ( uint32_t ) desc->seed, ( uint32_t ) ( desc->seed >> 32 ) );
+  CU( cudaMemcpyAsync( ( long long* ) e->d_step0.p + id, &step0, 8, cudaMemcpyHostToDevice, e->stream ) );
+  CU( cudaMemcpyAsync( ( long long* ) e->d_until.p + id, &until, 8, cudaMemcpyHostToDevice, e->stream ) );
+  CU( cudaMemcpyAsync( ( long long* ) e->d_off.p + id, &off, 8, cudaMemcpyHostToDevice, e->stream ) );
+  CU( cudaMemcpyAsync( ( uint2* ) e->d_key.p + id, &key, 8, cudaMemcpyHostToDevice, e->stream ) );
+  k_fill_i32<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( ( int32_t* ) e->d_nid.p + n0, n, id );
+  CU( cudaMemset2DAsync( ( char* ) e->ring.p + n0 * 8, ( size_t ) e->N * 8, 0, ( size_t ) n * 8, ( size_t ) e->L * e->C,
+    e->stream ) );
+  CU( cudaGetLastError() );
+  CU( cudaStreamSynchronize( e->stream ) );
+  std::fill( e->nid_host.begin() + n0, e->nid_host.begin() + n0 + n, id );
+  auto& nw = e->nets[ id ];
+  nw = ng_engine::NetInfo();
+  nw.used = true;
+  nw.off = n0;
+  nw.n = n;
+  nw.e0 = e0;
+  nw.ne = ne_used;
+  nw.step0 = step0;
+  nw.until = until;
+  nw.rec = desc->record != 0;
+  nw.log_rate = desc->record ? log_rate : 0.0;
+  e->n_rec += desc->record ? n : 0;
+  e->log_per_step = std::max( 1.0, e->log_per_step + nw.log_rate );
+  *net_id = id;
+  return NG_OK;
+}
+
+int
+ng_net_poll( ng_engine* e, int32_t id, int64_t* steps_done, int32_t* finished )
+{
+  int rc = net_check( e, id );
+  if ( rc )
+    return rc;
+  const auto& nw = e->nets[ id ];
+  const int64_t clock = e->origin + e->from;
+  if ( steps_done )
+    *steps_done = std::min( clock, nw.until ) - nw.step0;
+  if ( finished )
+    *finished = clock >= nw.until ? 1 : 0;
+  return NG_OK;
+}
+
+int
+ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out )
+{
+  int rc = net_check( e, id );
+  if ( rc )
+    return rc;
+  if ( !n_out || cap < 0 || ( cap > 0 && ( !source || !stamp ) ) )
+    return fail( NG_ERR_ARG, "ng_net_spikes: bad argument" );
+  auto& nw = e->nets[ id ];
+  const int64_t k = std::min< int64_t >( cap, ( int64_t ) nw.src.size() );
+  std::copy( nw.src.begin(), nw.src.begin() + k, source );
+  std::copy( nw.stamp.begin(), nw.stamp.begin() + k, stamp );
+  nw.src.erase( nw.src.begin(), nw.src.begin() + k );
+  nw.stamp.erase( nw.stamp.begin(), nw.stamp.begin() + k );
+  *n_out = k;
+  return NG_OK;
+}
+
+int
+ng_net_get_var( ng_engine* e, int32_t id, const char* name, double* out )
+{
+  int rc = net_check( e, id );
+  if ( rc )
+    return rc;
+  const auto& nw = e->nets[ id ];
+  return ng_get_var( e, 0, name, out, nw.off, nw.n );
+}
+
+int
+ng_net_get_connections( ng_engine* e, int32_t id, int32_t* source, int32_t* target, double* weight,
+  int32_t* delay_steps, int64_t cap, int64_t* n_out )
+{
+  int rc = net_check( e, id );
+  if ( rc )
+    return rc;
+  if ( !n_out || cap < 0 || ( cap > 0 && ( !source || !target || !weight || !delay_steps ) ) )
+    return fail( NG_ERR_ARG, "ng_net_get_connections: bad argument" );
+  cudaSetDevice( e->cfg.device );
+  const auto& nw = e->nets[ id ];
+  std::vector< int64_t > beg( ( size_t ) nw.n );
+  std::vector< int32_t > deg( ( size_t ) nw.n );
+  CU( cudaMemcpyAsync( beg.data(), ( int64_t* ) e->row_beg.p + nw.off, ( size_t ) nw.n * 8, cudaMemcpyDeviceToHost,
+    e->stream ) );
+  CU( cudaMemcpyAsync( deg.data(), ( int32_t* ) e->real_deg.p + nw.off, ( size_t ) nw.n * 4, cudaMemcpyDeviceToHost,
+    e->stream ) );
+  CU( cudaStreamSynchronize( e->stream ) );
+  int64_t total = 0;
+  for ( int32_t d : deg )
+    total += d;
+  *n_out = total;
+  if ( !source )
+    return NG_OK;  // count only
+  if ( cap < total )
+    return fail( NG_ERR_ARG, "ng_net_get_connections: output smaller than the network's connection count" );
+  const bool fx = e->prec != NG_FP64;
+  std::vector< uint32_t > tw( ( size_t ) std::max< int64_t >( nw.ne, 1 ) );
+  std::vector< char > wb( ( size_t ) std::max< int64_t >( nw.ne, 1 ) * ( fx ? 4 : 8 ) );
+  if ( nw.ne > 0 )
+  {
+    CU( cudaMemcpyAsync( tw.data(), ( uint32_t* ) e->tdc.p + nw.e0, ( size_t ) nw.ne * 4, cudaMemcpyDeviceToHost,
+      e->stream ) );
+    CU( cudaMemcpyAsync( wb.data(), ( char* ) e->w.p + nw.e0 * ( fx ? 4 : 8 ), ( size_t ) nw.ne * ( fx ? 4 : 8 ),
+      cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  const bool aeif = e->blk[ 0 ].model == NG_AEIF_COND_ALPHA;
+  const double inv_fx = std::ldexp( 1.0, -e->fx_S );
+  int64_t k = 0;
+  for ( int64_t s2 = 0; s2 < nw.n; ++s2 )
+    for ( int32_t j = 0; j < deg[ s2 ]; ++j, ++k )
+    {
+      const int64_t q = beg[ s2 ] - nw.e0 + j;
+      const uint32_t word = tw[ ( size_t ) q ];
+      double wv = fx ? reinterpret_cast< const int32_t* >( wb.data() )[ q ] * inv_fx
+                     : reinterpret_cast< const double* >( wb.data() )[ q ];
+      if ( aeif && ( word >> 31 ) )
+        wv = -wv;
+      source[ k ] = ( int32_t ) s2;
+      target[ k ] = ( int32_t ) ( ( int64_t ) ( word & e->tmask ) - nw.off );
+      delay_steps[ k ] = ( int32_t ) ( ( word >> e->tbits ) & e->dmask );
+      weight[ k ] = wv;
+    }
+  return NG_OK;
+}
+
+int
+ng_net_remove( ng_engine* e, int32_t id )
+{
+  int rc = net_check( e, id );
+  if ( rc )
+    return rc;
+  cudaSetDevice( e->cfg.device );
+  auto& nw = e->nets[ id ];
+  k_fill_i32<<< ( unsigned ) ( ( nw.n + 255 ) / 256 ), 256, 0, e->stream >>>( ( int32_t* ) e->d_nid.p + nw.off, nw.n, -1 );
+  CU( cudaMemsetAsync( ( int32_t* ) e->row_len.p + nw.off, 0, ( size_t ) nw.n * 4, e->stream ) );
+  CU( cudaMemsetAsync( ( uint8_t* ) e->rec.p + nw.off, 0, ( size_t ) nw.n, e->stream ) );
+  CU( cudaGetLastError() );
+  CU( cudaStreamSynchronize( e->stream ) );
+  std::fill( e->nid_host.begin() + nw.off, e->nid_host.begin() + nw.off + nw.n, -1 );
+  std::fill( e->rec_host.begin() + nw.off, e->rec_host.begin() + nw.off + nw.n, ( uint8_t ) 0 );
+  ng_engine::give_run( e->free_neurons, nw.off, nw.n );
+  ng_engine::give_run( e->free_edges, nw.e0, nw.ne );
+  e->n_rec -= nw.rec ? nw.n : 0;
+  e->log_per_step = std::max( 1.0, e->log_per_step - nw.log_rate );
+  nw = ng_engine::NetInfo();
+  return NG_OK;
+}
+
+int
+ng_net_capacity( ng_engine* e, int64_t* free_neurons, int64_t* free_edges )
+{
+  if ( !e || !e->serving || !free_neurons || !free_edges )
+    return fail( NG_ERR_STATE, "ng_net_capacity: not a serving engine" );
+  int64_t a = 0, b2 = 0;
+  for ( auto& kv : e->free_neurons )
+    a = std::max( a, kv.second );
+  for ( auto& kv : e->free_edges )
+    b2 = std::max( b2, kv.second );
+  *free_neurons = a;
+  *free_edges = b2;
   return NG_OK;
 }
 

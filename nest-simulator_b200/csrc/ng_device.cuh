@@ -6,11 +6,13 @@
 //             thresholds, refractory counts) computed on the host
 //   ring      [L][C][N] FP64 (plain) or int64 fixed point (precision form),
 //             C = 2 input channels (excitatory / inhibitory)
-//   CSR       row_ptr[n_src+1] (rows padded to multiples of 4 edges),
+//   CSR       row_beg[n_src] (int64) and row_len[n_src] (int32): a source's
+//             row, padded to a multiple of 4 edges (rows of the networks of a
+//             serving engine live anywhere in the edge pool),
 //             packed edge word tgt | delay << tbits | channel << 31 (u32),
 //             weight FP64 (plain) or int32 fixed point (precision form)
-//   spikes    per-slice list of (source, emission step mod L, multiplicity)
-//             with the prefix offsets of their padded out-degrees
+//   edge work per-slice list of edge chunks of the spikes to deliver: (row
+//             start, up to 128 edges, emission slot, multiplicity)
 //   log       (source, stamp - log_base | multiplicity << 24) for recorders
 #pragma once
 
@@ -27,13 +29,12 @@ constexpr int ERR_NUMERIC = 1;
 constexpr int ERR_SPIKE_LIST = 2;
 constexpr int ERR_LOG = 4;
 constexpr int ERR_TRACE = 8;
-constexpr int SPK_SHIFT = 40;
-constexpr unsigned long long EV_MASK = ( 1ull << SPK_SHIFT ) - 1ull;
+constexpr int CHUNK_EDGES = 128;  // edges per delivery work item: 32 lanes x 4 edges
 
 // Control block in device memory, shared by all kernels of an engine.
 struct Ctl
 {
-  unsigned long long spk_packed;  // (spikes << 40) | padded events of the open slice
+  unsigned long long n_ent;       // edge chunks queued for delivery in the open slice
   unsigned long long log_count;
   unsigned long long syn_events;
   unsigned long long drive_events;
@@ -65,13 +66,13 @@ struct Net
   uint32_t tmask, dmask;
   void* ring;
   double fx_inv;  // precision form: 2^-S of the fixed-point weights
-  const int64_t* row_ptr;
+  const int64_t* row_beg;
+  const int32_t* row_len;
   const int32_t* real_deg;
   const uint32_t* edge_tdc;
   const void* edge_w;
-  int4* spk;
-  long long* spk_off;
-  int64_t spk_cap;
+  int4* ent;  // edge chunks: row start (lo, hi), edge count, slot | multiplicity << 16
+  int64_t ent_cap;
   uint2* log;
   int64_t log_cap;
   const uint8_t* rec;
@@ -88,6 +89,12 @@ struct Net
   int32_t n_trace_idx, trace_interval, n_trace_vars;
   int8_t trace_slot[ MAX_STATE ];
   int64_t trace_rows;
+  // networks of a serving engine (nid == nullptr: one network, always on)
+  const int32_t* nid;            // per neuron: network id, -1 = free
+  const long long* net_step0;    // per network: admission step (its local time 0)
+  const long long* net_until;    // per network: first step it no longer simulates
+  const long long* net_off;      // per network: first neuron
+  const uint2* net_key;          // per network: Philox key of its drive
   const int64_t* sched_step;
   const int32_t* sched_src;
   int64_t n_sched;

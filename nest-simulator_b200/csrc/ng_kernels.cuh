@@ -38,8 +38,23 @@ warp_sum_ll( long long v )
   return v;
 }
 
-// Append this lane's spike (if any) to the slice's spike list and the
-// recorder log.  Must be called by all 32 lanes of the warp.
+// Queue the edge chunks of one spike: ceil(pdeg / 128) work items.
+__device__ __forceinline__ void
+put_chunks( const Net& d, long long idx, long long row, long long pdeg, int slot, int mult )
+{
+  for ( long long c = 0; c < pdeg; c += CHUNK_EDGES, ++idx )
+  {
+    const long long r = row + c;
+    const int ne = ( int ) ( pdeg - c < CHUNK_EDGES ? pdeg - c : CHUNK_EDGES );
+    if ( idx < d.ent_cap )
+      d.ent[ idx ] = make_int4( ( int ) ( unsigned ) ( r & 0xffffffffll ), ( int ) ( r >> 32 ), ne, slot | ( mult << 16 ) );
+    else
+      atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+  }
+}
+
+// Append this lane's spike (if any, with its multiplicity) to the slice's
+// delivery work and the recorder log.  Must be called by all 32 lanes.
 __device__ __forceinline__ void
 warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, long long stamp )
 {
@@ -48,14 +63,15 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
     return;
   const int lane = threadIdx.x & 31;
   const unsigned lt = ( 1u << lane ) - 1u;
-  long long pdeg = 0, rdeg = 0, row = 0;
+  long long pdeg = 0, rdeg = 0, row = 0, nch = 0;
   if ( spk )
   {
-    row = d.row_ptr[ src ];
-    pdeg = d.row_ptr[ src + 1 ] - row;
+    row = d.row_beg[ src ];
+    pdeg = d.row_len[ src ];
     rdeg = ( long long ) d.real_deg[ src ] * mult;
+    nch = ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
   }
-  long long incl = pdeg;
+  long long incl = nch;
 #pragma unroll
   for ( int o = 1; o < 32; o <<= 1 )
   {
@@ -66,60 +82,43 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
   const long long tot = __shfl_sync( FULL, incl, 31 );
   const long long rtot = warp_sum_ll( rdeg );
   const long long mtot = warp_sum_ll( spk ? ( long long ) mult : 0ll );
-  unsigned long long base = 0;
+  const bool lg = spk && ( d.rec == nullptr || d.rec[ src ] );
+  const unsigned lm = __ballot_sync( FULL, lg );
+  unsigned long long base = 0, lb = 0;
   if ( lane == 0 )
   {
-    base = atomicAdd( &d.ctl->spk_packed,
-      ( ( unsigned long long ) __popc( m ) << SPK_SHIFT ) | ( unsigned long long ) tot );
+    if ( tot > 0 )
+      base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot );
+    if ( lm )
+      lb = atomicAdd( &d.ctl->log_count, ( unsigned long long ) __popc( lm ) );
     atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
     atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) mtot );
   }
   base = __shfl_sync( FULL, base, 0 );
-  if ( spk )
+  lb = __shfl_sync( FULL, lb, 0 );
+  if ( spk && nch > 0 )
+    put_chunks( d, ( long long ) base + incl - nch, row, pdeg, tmod, mult );
+  if ( lg )
   {
-    const long long idx = ( long long ) ( base >> SPK_SHIFT ) + __popc( m & lt );
-    const long long off = ( long long ) ( base & EV_MASK ) + incl - pdeg;
-    if ( idx < d.spk_cap )
+    const long long li = ( long long ) lb + __popc( lm & lt );
+    if ( li < d.log_cap )
     {
-      // entry: CSR row start (lo, hi), emission slot, multiplicity
-      d.spk[ idx ] = make_int4( ( int ) ( unsigned ) ( row & 0xffffffffll ), ( int ) ( row >> 32 ), tmod, mult );
-      d.spk_off[ idx ] = off;
+      const uint32_t rel = ( uint32_t ) ( stamp - ld_volatile( &d.ctl->log_base ) );
+      const uint32_t mu = ( uint32_t ) ( mult < 255 ? mult : 255 );
+      d.log[ li ] = make_uint2( ( uint32_t ) src, rel | ( mu << 24 ) );
     }
     else
     {
-      atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
-    }
-  }
-  const bool lg = spk && ( d.rec == nullptr || d.rec[ src ] );
-  const unsigned lm = __ballot_sync( FULL, lg );
-  if ( lm )
-  {
-    unsigned long long lb = 0;
-    if ( lane == 0 )
-      lb = atomicAdd( &d.ctl->log_count, ( unsigned long long ) __popc( lm ) );
-    lb = __shfl_sync( FULL, lb, 0 );
-    if ( lg )
-    {
-      const long long li = ( long long ) lb + __popc( lm & lt );
-      if ( li < d.log_cap )
-      {
-        const uint32_t rel = ( uint32_t ) ( stamp - ld_volatile( &d.ctl->log_base ) );
-        const uint32_t mu = ( uint32_t ) ( mult < 255 ? mult : 255 );
-        d.log[ li ] = make_uint2( ( uint32_t ) src, rel | ( mu << 24 ) );
-      }
-      else
-      {
-        atomicOr( &d.ctl->err, ERR_LOG );
-      }
+      atomicOr( &d.ctl->err, ERR_LOG );
     }
   }
 }
 
 // Append all spikes of a chunk of up to 32 lags at once: bit k of `mask` is
 // a spike of this lane's neuron at lag k (emission step t0 + k, ring slot
-// (slot0 + k) mod L).  One spike-list and one log reservation per warp and
-// chunk, issued together, instead of an atomic round trip per lag.  Must be
-// called by all 32 lanes.
+// (slot0 + k) mod L).  One work and one log reservation per warp and chunk,
+// issued together, instead of an atomic round trip per lag.  Must be called
+// by all 32 lanes.
 __device__ __forceinline__ void
 warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long t0 )
 {
@@ -127,47 +126,46 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
   if ( __ballot_sync( FULL, cnt > 0 ) == 0 )
     return;
   const int lane = threadIdx.x & 31;
-  long long pdeg = 0, rdeg = 0, row = 0;
+  long long pdeg = 0, rdeg = 0, row = 0, nch = 0;
   const bool lg = cnt > 0 && ( d.rec == nullptr || d.rec[ src ] );
   if ( cnt > 0 )
   {
-    row = d.row_ptr[ src ];
-    pdeg = d.row_ptr[ src + 1 ] - row;
+    row = d.row_beg[ src ];
+    pdeg = d.row_len[ src ];
     rdeg = d.real_deg[ src ];
+    nch = ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
   }
-  long long c_incl = cnt, e_incl = cnt * pdeg, l_incl = lg ? cnt : 0;
+  long long e_incl = cnt * nch, l_incl = lg ? cnt : 0;
 #pragma unroll
   for ( int o = 1; o < 32; o <<= 1 )
   {
-    const long long a = __shfl_up_sync( FULL, c_incl, o );
     const long long b = __shfl_up_sync( FULL, e_incl, o );
     const long long c = __shfl_up_sync( FULL, l_incl, o );
     if ( lane >= o )
     {
-      c_incl += a;
       e_incl += b;
       l_incl += c;
     }
   }
-  const long long tot_c = __shfl_sync( FULL, c_incl, 31 );
   const long long tot_e = __shfl_sync( FULL, e_incl, 31 );
   const long long tot_l = __shfl_sync( FULL, l_incl, 31 );
   const long long rtot = warp_sum_ll( cnt * rdeg );
+  const long long ctot = warp_sum_ll( cnt );
   unsigned long long base = 0, lbase = 0;
   if ( lane == 0 )
   {
-    base = atomicAdd( &d.ctl->spk_packed, ( ( unsigned long long ) tot_c << SPK_SHIFT ) | ( unsigned long long ) tot_e );
+    if ( tot_e > 0 )
+      base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot_e );
     if ( tot_l > 0 )
       lbase = atomicAdd( &d.ctl->log_count, ( unsigned long long ) tot_l );
     atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
-    atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) tot_c );
+    atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) ctot );
   }
   base = __shfl_sync( FULL, base, 0 );
   lbase = __shfl_sync( FULL, lbase, 0 );
   if ( cnt == 0 )
     return;
-  long long idx = ( long long ) ( base >> SPK_SHIFT ) + c_incl - cnt;
-  long long off = ( long long ) ( base & EV_MASK ) + e_incl - cnt * pdeg;
+  long long idx = ( long long ) base + e_incl - cnt * nch;
   long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
   const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
   unsigned m = mask;
@@ -178,17 +176,9 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
     int slot = slot0 + k;
     if ( slot >= d.L )
       slot -= d.L;
-    if ( idx < d.spk_cap )
-    {
-      d.spk[ idx ] = make_int4( ( int ) ( unsigned ) ( row & 0xffffffffll ), ( int ) ( row >> 32 ), slot, 1 );
-      d.spk_off[ idx ] = off;
-    }
-    else
-    {
-      atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
-    }
-    ++idx;
-    off += pdeg;
+    if ( nch > 0 )
+      put_chunks( d, idx, row, pdeg, slot, 1 );
+    idx += nch;
     if ( lg )
     {
       if ( li < d.log_cap )
@@ -198,6 +188,17 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
       ++li;
     }
   }
+}
+
+// Steps at which neuron i is simulated: [.., until); a free neuron of a
+// serving engine never is.
+__device__ __forceinline__ long long
+active_until( const Net& d, int64_t i )
+{
+  if ( d.nid == nullptr )
+    return 0x7fffffffffffffffll;
+  const int id = d.nid[ i ];
+  return id < 0 ? -1ll : d.net_until[ id ];
 }
 
 // Read the slice origin once per CTA (a load by every warp of a large grid
@@ -224,12 +225,26 @@ drive( const Net& d, int64_t i, long long t, long long& cnt )
   const int2 tb = __ldg( d.pois_cdf_ref + i );
   if ( tb.y == 0 )
     return Real( 0 );
-  const long long tg = t - __ldg( d.pois_d + i );
+  // counter = (neuron, generator step) in the network's local numbering,
+  // key = the network's seed: a network draws the same drive wherever and
+  // whenever it is placed
+  long long tl = t, il = i;
+  uint32_t k0 = d.key0, k1 = d.key1;
+  if ( d.nid )
+  {
+    const int id = d.nid[ i ];
+    const uint2 kk = d.net_key[ id ];
+    tl = t - d.net_step0[ id ];
+    il = i - d.net_off[ id ];
+    k0 = kk.x;
+    k1 = kk.y;
+  }
+  const long long tg = tl - __ldg( d.pois_d + i );
   if ( !( d.pois_start < tg && tg <= d.pois_stop ) || tg < 0 )
     return Real( 0 );
   uint32_t o[ 4 ];
-  philox4x32_10( ( uint32_t ) i, ( uint32_t ) tg, ( uint32_t ) ( ( unsigned long long ) tg >> 32 ), DRIVE_STREAM,
-    d.key0, d.key1, o );
+  philox4x32_10( ( uint32_t ) il, ( uint32_t ) tg, ( uint32_t ) ( ( unsigned long long ) tg >> 32 ), DRIVE_STREAM,
+    k0, k1, o );
   const double u = u53( o[ 0 ], o[ 1 ] );
   long long k;
   if ( tb.y > 0 )
@@ -364,6 +379,7 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
   const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = li < b.n;
   const int64_t i = b.off + ( act ? li : 0 );
+  const long long until = act ? active_until( d, i ) : -1ll;
   constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
   Real* s0 = ( Real* ) b.s[ 0 ];
   Real* s1 = ( Real* ) b.s[ 1 ];
@@ -410,36 +426,58 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
     r = b.r[ li ];
   }
   long long dcnt = 0;
+  constexpr int SUB = 8;  // lags whose inputs are gathered before the recurrence runs over them
   for ( int cb = from; cb < to; cb += 32 )
   {
     const int nl = min( 32, to - cb );
     const long long t0 = origin + cb;
     const int slot0 = ( int ) ( t0 % d.L );
-    int slot = slot0;
     unsigned smask = 0;
-    for ( int k = 0; k < nl; ++k )
+    for ( int sb = 0; sb < nl; sb += SUB )
     {
-      if ( act )
+      // inputs of up to SUB lags: independent loads and draws, overlapped
+      Real in_ex[ SUB ], in_in[ SUB ];
+#pragma unroll
+      for ( int q = 0; q < SUB; ++q )
       {
-        Real ex = ring_take< Real, FIX >( d, slot, 0, i );
-        Real inh = 0;
-        if constexpr ( EXP )
-          inh = ring_take< Real, FIX >( d, slot, 1, i );
-        const Real dv = drive< Real >( d, i, t0 + k, dcnt );
-        if ( dv != Real( 0 ) )
+        in_ex[ q ] = Real( 0 );
+        in_in[ q ] = Real( 0 );
+        const int k = sb + q;
+        if ( act && k < nl && t0 + k < until )
         {
+          int slot = slot0 + k;
+          if ( slot >= d.L )
+            slot -= d.L;
+          Real ex = ring_take< Real, FIX >( d, slot, 0, i );
+          Real inh = 0;
           if constexpr ( EXP )
+            inh = ring_take< Real, FIX >( d, slot, 1, i );
+          const Real dv = drive< Real >( d, i, t0 + k, dcnt );
+          if ( dv != Real( 0 ) )
           {
-            if ( dv > Real( 0 ) )
-              ex = ex + dv;
+            if constexpr ( EXP )
+            {
+              if ( dv > Real( 0 ) )
+                ex = ex + dv;
+              else
+                inh = inh + dv;
+            }
             else
-              inh = inh + dv;
+            {
+              ex = ex + dv;
+            }
           }
-          else
-          {
-            ex = ex + dv;
-          }
+          in_ex[ q ] = ex;
+          in_in[ q ] = inh;
         }
+      }
+      // the recurrence over these lags, in order
+#pragma unroll
+      for ( int q = 0; q < SUB; ++q )
+      {
+        const int k = sb + q;
+        if ( !act || k >= nl || t0 + k >= until )
+          continue;
         bool spk = false;
         if constexpr ( EXP )
         {
@@ -450,8 +488,8 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
           x1 *= c4;
           x2 *= c5;
           x1 += c9 * i1;
-          x1 += ex;
-          x2 += inh;
+          x1 += in_ex[ q ];
+          x2 += in_in[ q ];
           if ( V >= Vth )
           {
             r = refr;
@@ -465,7 +503,7 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
         {
           if ( r == 0 )
           {
-            V = c1 * ( x1 + Ie ) + c0 * V + ex;
+            V = c1 * ( x1 + Ie ) + c0 * V + in_ex[ q ];
             V = ( V < c2 ? c2 : V );
           }
           else
@@ -497,8 +535,6 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
           }
         }
       }
-      if ( ++slot == d.L )
-        slot = 0;
     }
     warp_append_mask( d, smask, ( int32_t ) i, slot0, t0 );
   }
@@ -545,6 +581,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
   const int64_t li = nb0 + lane;
   const bool act = warp == 0 && li < b.n;
   const int64_t i = b.off + ( act ? li : 0 );
+  const long long until = act ? active_until( d, i ) : -1ll;
   Real* s0 = ( Real* ) b.s[ 0 ];
   Real* s1 = ( Real* ) b.s[ 1 ];
   Real* s2 = ( Real* ) b.s[ 2 ];
@@ -602,7 +639,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
       const int q = j & 31;
       const int64_t lq = nb0 + q;
       Real ex = 0, inh = 0;
-      if ( lq < b.n )
+      if ( lq < b.n && t0 + k < active_until( d, b.off + lq ) )
       {
         const int64_t iq = b.off + lq;
         int slot = slot0 + k;
@@ -640,7 +677,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
       for ( int k = 0; k < nl; ++k )
       {
         bool spk = false;
-        if ( act )
+        if ( act && t0 + k < until )
         {
           const Real in_ex = s_ex[ k ][ lane ];
           if constexpr ( EXP )
@@ -686,7 +723,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
         }
         if ( spk )
           smask |= 1u << k;
-        if ( act && d.trace_col )
+        if ( act && t0 + k < until && d.trace_col )
         {
           if constexpr ( EXP )
           {
@@ -834,6 +871,7 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
   const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = li < b.n;
   const int64_t i = b.off + ( act ? li : 0 );
+  const long long until = act ? active_until( d, i ) : -1ll;
   Real* sy[ 6 ];
 #pragma unroll
   for ( int k = 0; k < 6; ++k )
@@ -878,7 +916,8 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
   for ( int lag = from; lag < to; ++lag, ++t )
   {
     int mult = 0;
-    if ( act && !unstable )
+    const bool live = act && t < until;
+    if ( live && !unstable )
     {
       double tt = 0.0;
       int guard = 0;
@@ -954,7 +993,7 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
       }
     }
     warp_append( d, mult > 0, ( int32_t ) i, slot, mult, t + 1 );
-    if ( act && d.trace_col )
+    if ( live && d.trace_col )
     {
       const double vals[ 7 ] = { y[ 0 ], y[ 1 ], y[ 2 ], y[ 3 ], y[ 4 ], y[ 5 ], p.I_e };
       trace_put( d, i, t + 1, vals );
@@ -980,60 +1019,37 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
 // add into ring[(t_emit + d) mod L][channel][target]
 // (EventDeliveryManager::deliver_events_ -> Connector::send -> handle,
 // event_delivery_manager.cpp:599-700, connector_base.h:398-434).
-// Work item = 4 consecutive edges of one (padded) CSR row; the spike owning
-// an item is found by binary search over the spikes' event offsets, staged
-// in shared memory when the list is short.
+// Work item = one edge chunk (<= 128 edges of one padded CSR row) queued by
+// the update kernel when the spike was emitted; a warp takes a chunk, each
+// lane loads 4 edges (one 16-byte edge-word load, 32 or 16 bytes of
+// weights) and issues their adds.
 // ---------------------------------------------------------------------
-constexpr int SMEM_SPIKES = 1024;
-
 template < bool FIX >
 __global__ void __launch_bounds__( 256 )
 k_deliver( Net d )
 {
-  __shared__ long long s_off[ SMEM_SPIKES ];
-  __shared__ int4 s_spk[ SMEM_SPIKES ];
-  __shared__ int s_last;
-  __shared__ unsigned long long s_packed;
+  __shared__ unsigned long long s_nent;
   __shared__ int s_err;
+  __shared__ int s_last;
   if ( threadIdx.x == 0 )
   {
-    s_packed = ld_volatile( &d.ctl->spk_packed );
+    s_nent = ld_volatile( &d.ctl->n_ent );
     s_err = ld_volatile( &d.ctl->err );
   }
   __syncthreads();
-  const unsigned long long packed = s_packed;
-  const long long nspk = ( long long ) ( packed >> SPK_SHIFT );
-  const long long nev = ( long long ) ( packed & EV_MASK );
-  const bool ok = nspk <= d.spk_cap && ( s_err & ERR_SPIKE_LIST ) == 0;
-  const long long nq = ok ? ( nev >> 2 ) : 0;
-  const bool use_sm = nspk <= SMEM_SPIKES;
-  if ( use_sm && nq > 0 && ( long long ) blockIdx.x * blockDim.x < nq )
+  const bool ok = ( long long ) s_nent <= d.ent_cap && ( s_err & ERR_SPIKE_LIST ) == 0;
+  const long long nent = ok ? ( long long ) s_nent : 0;
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ( ( long long ) gridDim.x * blockDim.x ) >> 5;
+  for ( long long e = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5; e < nent; e += nwarps )
   {
-    for ( long long k = threadIdx.x; k < nspk; k += blockDim.x )
-    {
-      s_off[ k ] = d.spk_off[ k ];
-      s_spk[ k ] = d.spk[ k ];
-    }
-    __syncthreads();
-  }
-  const long long* off = use_sm ? s_off : d.spk_off;
-  const int4* spl = use_sm ? s_spk : d.spk;
-  const long long stride = ( long long ) gridDim.x * blockDim.x;
-  for ( long long q = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride )
-  {
-    const long long e0 = q << 2;
-    long long lo = 0, hi = nspk;
-    while ( hi - lo > 1 )
-    {
-      const long long mid = ( lo + hi ) >> 1;
-      if ( off[ mid ] <= e0 )
-        lo = mid;
-      else
-        hi = mid;
-    }
-    const int4 sp = spl[ lo ];
-    // off[lo] <= e0 < off[lo + 1]: the quad lies inside this spike's padded row
-    const long long edge = ( ( ( long long ) sp.y << 32 ) | ( unsigned ) sp.x ) + ( e0 - off[ lo ] );
+    const int4 en = d.ent[ e ];  // the same 16 bytes for the whole warp
+    const int j = lane << 2;
+    if ( j >= en.z )
+      continue;
+    const long long edge = ( ( ( long long ) en.y << 32 ) | ( unsigned ) en.x ) + j;
+    const int slot0 = en.w & 0xffff;
+    const int mult = en.w >> 16;
     const uint4 tdc = __ldg( reinterpret_cast< const uint4* >( d.edge_tdc + edge ) );
     const uint32_t tw[ 4 ] = { tdc.x, tdc.y, tdc.z, tdc.w };
     if constexpr ( FIX )
@@ -1047,11 +1063,11 @@ k_deliver( Net d )
         if ( ww[ k ] == 0 )
           continue;
         const uint32_t tgt = tw[ k ] & d.tmask;
-        int slot = sp.z + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
+        int slot = slot0 + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
         if ( slot >= d.L )
           slot -= d.L;
         const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
-        atomicAdd( ring + idx, ( unsigned long long ) ( ( long long ) ww[ k ] * ( long long ) sp.w ) );
+        atomicAdd( ring + idx, ( unsigned long long ) ( ( long long ) ww[ k ] * ( long long ) mult ) );
       }
     }
     else
@@ -1066,14 +1082,15 @@ k_deliver( Net d )
         if ( ww[ k ] == 0.0 )
           continue;
         const uint32_t tgt = tw[ k ] & d.tmask;
-        int slot = sp.z + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
+        int slot = slot0 + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
         if ( slot >= d.L )
           slot -= d.L;
         const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
-        atomicAdd( ring + idx, sp.w == 1 ? ww[ k ] : ww[ k ] * ( double ) sp.w );
+        atomicAdd( ring + idx, mult == 1 ? ww[ k ] : ww[ k ] * ( double ) mult );
       }
     }
   }
+  // the last CTA to finish closes the slice
   __syncthreads();
   if ( threadIdx.x == 0 )
   {
@@ -1083,7 +1100,7 @@ k_deliver( Net d )
   __syncthreads();
   if ( s_last && threadIdx.x == 0 )
   {
-    d.ctl->spk_packed = 0ull;
+    d.ctl->n_ent = 0ull;
     d.ctl->deliver_done = 0;
     d.ctl->origin = d.ctl->origin + d.min_delay;
     __threadfence();

@@ -1,0 +1,303 @@
+// ng_serving.cuh -- device kernels of the serving engine: fixed_indegree
+// connectivity drawn on the GPU into a network's region of the edge pool,
+// and the per-region bookkeeping (network ids, rows).
+//
+// Graph construction follows the reference's FixedInDegreeBuilder
+// (nestkernel/conn_builder.cpp:1508-...): every target draws k_exc sources
+// uniformly from the excitatory range and k_inh from the inhibitory range,
+// multapses allowed, autapses redrawn unless allowed.  The draws come from a
+// Philox4x32-10 stream keyed by the network's graph seed, counter (target,
+// draw index, attempt), so a network's graph depends on its seed only.  The
+// edges are then grouped by source with a counting sort (histogram, scan of
+// the padded row lengths, scatter).
+#pragma once
+
+#include "ng_device.cuh"
+
+namespace ng
+{
+
+constexpr uint32_t CONN_STREAM = 0x434F4E4Eu;
+
+// uniform integer in [0, size) from a 32-bit draw (multiply-high)
+__device__ __forceinline__ int64_t
+uniform_below( uint32_t u, int64_t size )
+{
+  return ( int64_t ) ( ( ( unsigned long long ) u * ( unsigned long long ) size ) >> 32 );
+}
+
+__global__ void
+k_fi_draw( int64_t n, int64_t n_exc, int k_exc, int k_inh, int allow_aut, uint32_t key0, uint32_t key1,
+  int32_t* tmp_src, int32_t* cnt )
+{
+  const int K = k_exc + k_inh;
+  const int64_t idx = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( idx >= n * K )
+    return;
+  const int64_t t = idx / K;
+  const int j = ( int ) ( idx - t * K );
+  const bool ex = j < k_exc;
+  const int64_t base = ex ? 0 : n_exc;
+  const int64_t size = ex ? n_exc : n - n_exc;
+  int64_t src = base;
+  for ( int attempt = 0; attempt < 64; ++attempt )
+  {
+    uint32_t o[ 4 ];
+    philox4x32_10( ( uint32_t ) t, ( uint32_t ) j, ( uint32_t ) attempt, CONN_STREAM, key0, key1, o );
+    src = base + uniform_below( o[ 0 ], size );
+    if ( allow_aut || src != t )
+      break;
+  }
+  tmp_src[ idx ] = ( int32_t ) src;
+  atomicAdd( &cnt[ src ], 1 );
+}
+
+// Exclusive scan of the padded row lengths (one CTA of 1024 threads; each
+// thread sums a contiguous run of sources, then a block scan of the runs).
+__global__ void __launch_bounds__( 1024 )
+k_fi_scan( int64_t n, const int32_t* cnt, int64_t* beg, int32_t* plen, long long* total )
+{
+  __shared__ long long s_part[ 1024 ];
+  const int t = threadIdx.x;
+  const int64_t per = ( n + 1023 ) / 1024;
+  const int64_t lo = t * per, hi = min( n, lo + per );
+  long long sum = 0;
+  for ( int64_t s = lo; s < hi; ++s )
+    sum += ( cnt[ s ] + 3 ) & ~3;
+  s_part[ t ] = sum;
+  __syncthreads();
+  for ( int o = 1; o < 1024; o <<= 1 )
+  {
+    const long long v = t >= o ? s_part[ t - o ] : 0;
+    __syncthreads();
+    s_part[ t ] += v;
+    __syncthreads();
+  }
+  long long run = s_part[ t ] - sum;
+  for ( int64_t s = lo; s < hi; ++s )
+  {
+    const int p = ( cnt[ s ] + 3 ) & ~3;
+    beg[ s ] = run;
+    plen[ s ] = p;
+    run += p;
+  }
+  if ( t == 1023 )
+    *total = s_part[ 1023 ];
+}
+
+// Place every drawn edge into its source's row of the network's region.
+template < typename W >
+__global__ void
+k_fi_scatter( int64_t n, int k_exc, int k_inh, const int32_t* tmp_src, const int64_t* beg, int32_t* fill,
+  int64_t n0, int64_t e0, uint32_t word_exc, uint32_t word_inh, W w_exc, W w_inh, uint32_t* tdc, W* w )
+{
+  const int K = k_exc + k_inh;
+  const int64_t idx = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( idx >= n * K )
+    return;
+  const int64_t t = idx / K;
+  const int j = ( int ) ( idx - t * K );
+  const int32_t src = tmp_src[ idx ];
+  const int64_t e = e0 + beg[ src ] + atomicAdd( &fill[ src ], 1 );
+  const bool ex = j < k_exc;
+  tdc[ e ] = ( uint32_t ) ( n0 + t ) | ( ex ? word_exc : word_inh );
+  w[ e ] = ex ? w_exc : w_inh;
+}
+
+// Rows of the region's sources: begin, padded length, real degree.
+__global__ void
+k_fi_rows( int64_t n, int64_t n0, int64_t e0, const int64_t* beg, const int32_t* plen, const int32_t* cnt,
+  int64_t* row_beg, int32_t* row_len, int32_t* real_deg )
+{
+  const int64_t s = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( s >= n )
+    return;
+  row_beg[ n0 + s ] = e0 + beg[ s ];
+  row_len[ n0 + s ] = plen[ s ];
+  real_deg[ n0 + s ] = cnt[ s ];
+}
+
+__global__ void
+k_fill_i32( int32_t* p, int64_t n, int32_t v )
+{
+  const int64_t k = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( k < n )
+    p[ k ] = v;
+}
+
+}  // namespace ng
+
+namespace ng
+{
+
+// ---------------------------------------------------------------------
+// pairwise_bernoulli connectivity drawn on the device (the reference's
+// BernoulliBuilder, nestkernel/conn_builder.h:716, with Philox streams):
+// every (source, target) pair of source population i and target population
+// j is connected with probability p[i][j].  Targets are walked in blocks of
+// PB_BLOCK; inside a block the next connected target is found by geometric
+// skipping, gap = floor(log(u) / log(1 - p)).  Weights and delays are
+// normal per source type (excitatory / inhibitory), delays clipped to
+// [h, d_max] and rounded to steps as Time::delay_ms_to_steps does (then
+// raised to the engine's min_delay where that is longer than one step).
+// Pass 1 counts the edges of every (source, block); pass 2 regenerates the
+// same draws and writes them into the source's row.
+// ---------------------------------------------------------------------
+constexpr int PB_BLOCK = 1024;
+constexpr uint32_t PB_STREAM = 0x50425244u;  // target draws
+constexpr uint32_t WD_STREAM = 0x57444C59u;  // weight / delay draws
+constexpr int PB_MAX_POPS = 16;
+
+struct PbSpec
+{
+  int n_pops;
+  long long pop_lo[ PB_MAX_POPS + 1 ];
+  int pop_exc[ PB_MAX_POPS ];
+  double inv_log1mp[ PB_MAX_POPS * PB_MAX_POPS ];  // 1 / log(1 - p), 0: p = 1, NaN: p = 0
+  double w_mean[ 2 ], w_sd[ 2 ];                  // [inhibitory, excitatory] source
+  double d_mean[ 2 ], d_sd[ 2 ];                  // ms
+  double h, d_max;                                // ms
+  int min_steps, max_steps;                       // delay bounds of the engine
+  int allow_aut;
+  uint32_t key0, key1;
+  int nb;                                         // target blocks in the network
+};
+
+__device__ __forceinline__ int
+pop_of( const PbSpec& sp, long long i )
+{
+  int j = 0;
+  while ( j + 1 < sp.n_pops && i >= sp.pop_lo[ j + 1 ] )
+    ++j;
+  return j;
+}
+
+// block b covers targets [lo, hi) of one target population
+__device__ __forceinline__ void
+block_range( const PbSpec& sp, int b, long long& lo, long long& hi, int& pj )
+{
+  int acc = 0;
+  for ( int j = 0; j < sp.n_pops; ++j )
+  {
+    const long long sz = sp.pop_lo[ j + 1 ] - sp.pop_lo[ j ];
+    const int nbj = ( int ) ( ( sz + PB_BLOCK - 1 ) / PB_BLOCK );
+    if ( b < acc + nbj )
+    {
+      lo = sp.pop_lo[ j ] + ( long long ) ( b - acc ) * PB_BLOCK;
+      hi = min( lo + PB_BLOCK, sp.pop_lo[ j + 1 ] );
+      pj = j;
+      return;
+    }
+    acc += nbj;
+  }
+  lo = hi = 0;
+  pj = 0;
+}
+
+__device__ __forceinline__ double
+unit_open( uint32_t x )
+{
+  return ( ( double ) x + 0.5 ) * ( 1.0 / 4294967296.0 );
+}
+
+// pass 1 (write == false): count into cnt_sb; pass 2: write the edges
+template < typename W >
+__global__ void
+k_pb_pass( PbSpec sp, long long n, bool write, int* cnt_sb, const int64_t* beg, long long n0, long long e0, int tbits,
+  bool exp_model, bool aeif_model, double fx_scale, uint32_t* tdc, W* w )
+{
+  const long long idx = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( idx >= n * sp.nb )
+    return;
+  const long long s = idx / sp.nb;
+  const int b = ( int ) ( idx - s * sp.nb );
+  long long lo, hi;
+  int pj;
+  block_range( sp, b, lo, hi, pj );
+  const int pi = pop_of( sp, s );
+  const double inv = sp.inv_log1mp[ pi * PB_MAX_POPS + pj ];
+  if ( isnan( inv ) )
+  {
+    if ( !write )
+      cnt_sb[ idx ] = 0;
+    return;
+  }
+  long long off = 0;
+  int c_max = 0x7fffffff;
+  if ( write )
+  {
+    off = beg[ s ];
+    for ( int bb = 0; bb < b; ++bb )
+      off += cnt_sb[ s * sp.nb + bb ];
+    c_max = cnt_sb[ idx ];  // pass 2 never writes past what pass 1 counted
+  }
+  const int ex = sp.pop_exc[ pi ] ? 1 : 0;
+  long long pos = lo - 1;
+  int c = 0;
+  uint32_t o[ 4 ];
+  int q = 4;
+  uint32_t k = 0;
+  for ( ;; )
+  {
+    if ( q == 4 )
+    {
+      philox4x32_10( ( uint32_t ) s, ( uint32_t ) b, k++, PB_STREAM, sp.key0, sp.key1, o );
+      q = 0;
+    }
+    const double u = unit_open( o[ q++ ] );
+    const double gap = inv == 0.0 ? 0.0 : floor( log( u ) * inv );
+    if ( !( gap < ( double ) ( hi - 1 - pos ) ) )  // the next target lies past the block (or gap is inf)
+      break;
+    pos += ( long long ) gap + 1;
+    if ( !sp.allow_aut && pos == s )
+      continue;
+    if ( c >= c_max )
+      break;
+    if ( write )
+    {
+      uint32_t r[ 4 ];
+      philox4x32_10( ( uint32_t ) s, ( uint32_t ) b, ( uint32_t ) c, WD_STREAM, sp.key0, sp.key1, r );
+      // Box-Muller: two normals from two uniforms
+      const double rr = sqrt( -2.0 * log( unit_open( r[ 0 ] ) ) );
+      const double th = 6.283185307179586 * unit_open( r[ 1 ] );
+      const double z0 = rr * cos( th ), z1 = rr * sin( th );
+      double wv = sp.w_mean[ ex ] + sp.w_sd[ ex ] * z0;
+      double dms = sp.d_mean[ ex ] + sp.d_sd[ ex ] * z1;
+      dms = fmin( fmax( dms, sp.h ), sp.d_max );
+      int dst = ( int ) floor( dms / sp.h + 0.5 );
+      dst = max( sp.min_steps, min( dst, sp.max_steps ) );
+      uint32_t ch = 0;
+      if ( exp_model )
+        ch = wv > 0 ? 0u : 1u;
+      else if ( aeif_model && !( wv > 0.0 ) )
+      {
+        ch = 1u;
+        wv = -wv;
+      }
+      const long long e = e0 + off + c;
+      tdc[ e ] = ( uint32_t ) ( n0 + pos ) | ( ( uint32_t ) dst << tbits ) | ( ch << 31 );
+      if constexpr ( sizeof( W ) == 4 )
+        w[ e ] = ( W ) llrint( fmin( fmax( wv * fx_scale, -2147483647.0 ), 2147483647.0 ) );
+      else
+        w[ e ] = ( W ) wv;
+    }
+    ++c;
+  }
+  if ( !write )
+    cnt_sb[ idx ] = c;
+}
+
+// per-source totals of pass 1
+__global__ void
+k_pb_rowsum( long long n, int nb, const int* cnt_sb, int32_t* cnt )
+{
+  const long long s = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( s >= n )
+    return;
+  long long t = 0;
+  for ( int b = 0; b < nb; ++b )
+    t += cnt_sb[ s * nb + b ];
+  cnt[ s ] = ( int32_t ) t;
+}
+
+}  // namespace ng

@@ -31,7 +31,9 @@ EXPORTED = [
     "ng_abi_version", "ng_last_error", "ng_device_count", "ng_create", "ng_destroy", "ng_set_var", "ng_get_var",
     "ng_set_connections", "ng_set_connections_coo", "ng_set_spike_schedule", "ng_set_poisson", "ng_set_recording", "ng_set_trace",
     "ng_simulate", "ng_spike_count", "ng_get_spikes", "ng_trace_count", "ng_get_trace", "ng_get_stats",
-    "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients", "ng_simulate_noalloc",
+    "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients", "ng_net_add", "ng_net_poll",
+    "ng_net_spikes", "ng_net_get_var", "ng_net_get_connections", "ng_net_remove", "ng_net_capacity",
+    "ng_simulate_noalloc",
 ]
 
 
@@ -49,6 +51,83 @@ class NGConfig(ctypes.Structure):
         ("n_generators", ctypes.c_int64),
         ("spike_log_capacity", ctypes.c_int64),
         ("start_step", ctypes.c_int64),
+        ("serving", ctypes.c_int32),
+        ("max_networks", ctypes.c_int32),
+        ("edge_capacity", ctypes.c_int64),
+        ("max_abs_weight", ctypes.c_double),
+    ]
+
+
+class NGFixedIndegree(ctypes.Structure):
+    _fields_ = [
+        ("n_exc", ctypes.c_int64),
+        ("k_exc", ctypes.c_int32),
+        ("k_inh", ctypes.c_int32),
+        ("w_exc", ctypes.c_double),
+        ("w_inh", ctypes.c_double),
+        ("delay_steps", ctypes.c_int32),
+        ("allow_autapses", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+NG_MAX_POPS = 16
+
+
+class NGPairwiseBernoulli(ctypes.Structure):
+    _fields_ = [
+        ("n_pops", ctypes.c_int32),
+        ("pop_size", ctypes.c_int64 * NG_MAX_POPS),
+        ("pop_exc", ctypes.c_int32 * NG_MAX_POPS),
+        ("p", ctypes.c_double * (NG_MAX_POPS * NG_MAX_POPS)),
+        ("w_mean", ctypes.c_double * 2),
+        ("w_sd", ctypes.c_double * 2),
+        ("d_mean_ms", ctypes.c_double * 2),
+        ("d_sd_ms", ctypes.c_double * 2),
+        ("d_max_ms", ctypes.c_double),
+        ("allow_autapses", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+    ]
+
+    @classmethod
+    def make(cls, pop_size, pop_exc, p, w_mean, w_sd, d_mean_ms, d_sd_ms, d_max_ms, allow_autapses=0, seed=0):
+        """p[i][j]: probability that a neuron of population i projects to one
+        of population j; w_*/d_*: (inhibitory source, excitatory source)."""
+        k = len(pop_size)
+        if not 1 <= k <= NG_MAX_POPS:
+            raise ValueError("1 to 16 populations")
+        s = cls(n_pops=k, d_max_ms=float(d_max_ms), allow_autapses=int(allow_autapses), seed=int(seed) & (2**64 - 1))
+        pp = np.asarray(p, dtype=np.float64).reshape(k, k)
+        for i in range(k):
+            s.pop_size[i] = int(pop_size[i])
+            s.pop_exc[i] = 1 if pop_exc[i] else 0
+            for j in range(k):
+                s.p[i * NG_MAX_POPS + j] = float(pp[i, j])
+        for a in range(2):
+            s.w_mean[a], s.w_sd[a] = float(w_mean[a]), float(w_sd[a])
+            s.d_mean_ms[a], s.d_sd_ms[a] = float(d_mean_ms[a]), float(d_sd_ms[a])
+        return s
+
+
+class NGNetDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int64),
+        ("steps", ctypes.c_int64),
+        ("seed", ctypes.c_uint64),
+        ("record", ctypes.c_int32),
+        ("n_vars", ctypes.c_int32),
+        ("var_names", ctypes.c_void_p),
+        ("var_values", ctypes.c_void_p),
+        ("nnz", ctypes.c_int64),
+        ("source", ctypes.c_void_p),
+        ("target", ctypes.c_void_p),
+        ("weight", ctypes.c_void_p),
+        ("delay_steps", ctypes.c_void_p),
+        ("build", ctypes.c_void_p),
+        ("poisson_rate", ctypes.c_void_p),
+        ("poisson_weight", ctypes.c_void_p),
+        ("poisson_delay", ctypes.c_void_p),
+        ("build_pb", ctypes.c_void_p),
     ]
 
 
@@ -113,6 +192,13 @@ def load():
         "ng_set_stream": ([P, P], ctypes.c_int),
         "ng_set_graph_slices": ([P, i32], ctypes.c_int),
         "ng_debug_coefficients": ([P, i32, i64, P, i32, P], ctypes.c_int),
+        "ng_net_add": ([P, P, P], ctypes.c_int),
+        "ng_net_poll": ([P, i32, P, P], ctypes.c_int),
+        "ng_net_spikes": ([P, i32, P, P, i64, P], ctypes.c_int),
+        "ng_net_get_var": ([P, i32, ctypes.c_char_p, P], ctypes.c_int),
+        "ng_net_get_connections": ([P, i32, P, P, P, P, i64, P], ctypes.c_int),
+        "ng_net_remove": ([P, i32], ctypes.c_int),
+        "ng_net_capacity": ([P, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -141,7 +227,8 @@ class Engine:
     """Thin owner of one ng_engine handle."""
 
     def __init__(self, blocks, h, min_delay, max_delay, n_generators=0, precision=NG_FP64, device=0,
-                 tics_per_ms=1000.0, spike_log_capacity=0, start_step=0):
+                 tics_per_ms=1000.0, spike_log_capacity=0, start_step=0, serving=False, max_networks=0,
+                 edge_capacity=0, max_abs_weight=0.0):
         L = load()
         cfg = NGConfig()
         cfg.device = int(device)
@@ -159,6 +246,10 @@ class Engine:
         cfg.n_generators = int(n_generators)
         cfg.spike_log_capacity = int(spike_log_capacity)
         cfg.start_step = int(start_step)
+        cfg.serving = 1 if serving else 0
+        cfg.max_networks = int(max_networks)
+        cfg.edge_capacity = int(edge_capacity)
+        cfg.max_abs_weight = float(max_abs_weight)
         self.handle = ctypes.c_void_p()
         self.L = L
         check(L.ng_create(ctypes.byref(cfg), ctypes.byref(self.handle)))
@@ -272,3 +363,92 @@ class Engine:
         n = ctypes.c_int32(0)
         check(self.L.ng_debug_coefficients(self.handle, int(block), int(index), _p(out), 32, ctypes.byref(n)))
         return out[:n.value]
+
+    # ---- serving
+    def net_add(self, n, steps, seed, var_values, build=None, edges=None, poisson=None, record=True):
+        """Admit a network; returns its id, or None if it does not fit now.
+
+        build: a dict of NGFixedIndegree fields, or an NGPairwiseBernoulli;
+        edges: (source, target, weight, delay_steps) in network-local ids."""
+        names = list(var_values)
+        arrays = [np.ascontiguousarray(np.broadcast_to(np.asarray(var_values[k], dtype=np.float64), (n,)))
+                  for k in names]
+        cnames = (ctypes.c_char_p * max(1, len(names)))(*[k.encode() for k in names])
+        cvals = (ctypes.c_void_p * max(1, len(arrays)))(*[a.ctypes.data for a in arrays])
+        desc = NGNetDesc(n=int(n), steps=int(steps), seed=int(seed) & (2**64 - 1), record=1 if record else 0,
+                         n_vars=len(names), var_names=ctypes.cast(cnames, ctypes.c_void_p),
+                         var_values=ctypes.cast(cvals, ctypes.c_void_p))
+        keep = [arrays, cnames, cvals]
+        if isinstance(build, NGPairwiseBernoulli):
+            keep.append(build)
+            desc.build_pb = ctypes.cast(ctypes.pointer(build), ctypes.c_void_p)
+        elif build is not None:
+            fb = NGFixedIndegree(**build)
+            keep.append(fb)
+            desc.build = ctypes.cast(ctypes.pointer(fb), ctypes.c_void_p)
+        elif edges is not None:
+            src, tgt, w, d = (np.ascontiguousarray(edges[0], dtype=np.int32), np.ascontiguousarray(edges[1], dtype=np.int32),
+                              np.ascontiguousarray(edges[2], dtype=np.float64), np.ascontiguousarray(edges[3], dtype=np.int32))
+            keep += [src, tgt, w, d]
+            desc.nnz = len(src)
+            desc.source, desc.target, desc.weight, desc.delay_steps = (src.ctypes.data, tgt.ctypes.data, w.ctypes.data,
+                                                                      d.ctypes.data)
+        if poisson is not None:
+            r = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson[0], dtype=np.float64), (n,)))
+            pw = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson[1], dtype=np.float64), (n,)))
+            pd = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson[2], dtype=np.int32), (n,)))
+            keep += [r, pw, pd]
+            desc.poisson_rate, desc.poisson_weight, desc.poisson_delay = r.ctypes.data, pw.ctypes.data, pd.ctypes.data
+        nid = ctypes.c_int32(-1)
+        rc = self.L.ng_net_add(self.handle, ctypes.byref(desc), ctypes.byref(nid))
+        del keep
+        if rc == NG_ERR_CAPACITY:
+            return None
+        check(rc)
+        return nid.value
+
+    def net_poll(self, nid):
+        done = ctypes.c_int64(0)
+        fin = ctypes.c_int32(0)
+        check(self.L.ng_net_poll(self.handle, int(nid), ctypes.byref(done), ctypes.byref(fin)))
+        return done.value, bool(fin.value)
+
+    def net_spikes(self, nid, cap=1 << 24):
+        src = np.empty(cap, dtype=np.int32)
+        st = np.empty(cap, dtype=np.int64)
+        got = ctypes.c_int64(0)
+        out_s, out_t = [], []
+        while True:
+            check(self.L.ng_net_spikes(self.handle, int(nid), _p(src), _p(st), cap, ctypes.byref(got)))
+            out_s.append(src[:got.value].copy())
+            out_t.append(st[:got.value].copy())
+            if got.value < cap:
+                break
+        return np.concatenate(out_s), np.concatenate(out_t)
+
+    def net_get_var(self, nid, name, n):
+        out = np.empty(int(n), dtype=np.float64)
+        check(self.L.ng_net_get_var(self.handle, int(nid), name.encode(), _p(out)))
+        return out
+
+    def net_get_connections(self, nid):
+        """(source, target, weight, delay_steps) of the network, local ids."""
+        n = ctypes.c_int64(0)
+        check(self.L.ng_net_get_connections(self.handle, int(nid), None, None, None, None, 0, ctypes.byref(n)))
+        k = n.value
+        s = np.empty(k, dtype=np.int32)
+        t = np.empty(k, dtype=np.int32)
+        w = np.empty(k, dtype=np.float64)
+        d = np.empty(k, dtype=np.int32)
+        if k:
+            check(self.L.ng_net_get_connections(self.handle, int(nid), _p(s), _p(t), _p(w), _p(d), k, ctypes.byref(n)))
+        return s, t, w, d
+
+    def net_remove(self, nid):
+        check(self.L.ng_net_remove(self.handle, int(nid)))
+
+    def net_capacity(self):
+        a = ctypes.c_int64(0)
+        b = ctypes.c_int64(0)
+        check(self.L.ng_net_capacity(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value

@@ -1,0 +1,182 @@
+"""Serving: a request loop that runs many independent network simulations on
+one GPU with continuous batching.
+
+Requests are Brunel-type iaf_psc_exp networks (sizes, coupling and drive
+drawn per request).  The batched server keeps one serving engine
+(``ng_config.serving``): a request is admitted as soon as its neurons and
+edges fit the engine's free pool (admission by device-memory footprint), its
+graph is drawn on the device, it advances together with every other live
+network in the same slice kernels, and it is retired -- its spikes drained,
+its pool space freed -- at the first slice boundary after its duration.  The
+plain server runs the same requests one at a time in the FP64 form.
+
+A network's result does not depend on the mix it runs in: its Philox streams
+(graph and drive) are keyed by its own seed and counted in its own neuron
+numbering and local time, and the FP32 form's int64 ring sums are order
+independent.
+"""
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+
+H = 0.1                      # ms
+DELAY_STEPS = 15             # 1.5 ms
+J_EXC = 87.8                 # pA
+TAU_SYN = 0.5                # ms
+# external rate that brings the mean membrane potential of an iaf_psc_exp
+# neuron (C_m 250 pF, tau_m 10 ms, threshold 15 mV above rest) to threshold:
+# nu_th = 15 mV * C_m / (J * tau_syn * tau_m) [1/ms]
+NU_TH_HZ = 15.0 * 250.0 * 1000.0 / (J_EXC * TAU_SYN * 10.0)
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float           # s after the start of the run
+    n: int
+    n_exc: int
+    k_exc: int
+    k_inh: int
+    g: float
+    eta: float
+    steps: int
+    seed: int
+    admitted: float = math.nan
+    finished: float = math.nan
+    spikes: tuple = field(default=None, repr=False)
+    syn_events: int = 0
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+    def syn_events_from_spikes(self):
+        """Recurrent synaptic events: spikes times the source's out-degree (the
+        graph's expected out-degree equals its in-degree per population)."""
+        src = self.spikes[0]
+        exc = np.count_nonzero(src < self.n_exc)
+        inh = len(src) - exc
+        return exc * (self.n * self.k_exc / max(1, self.n_exc)) + inh * (self.n * self.k_inh / max(1, self.n - self.n_exc))
+
+
+def make_requests(count=256, rate_hz=20.0, seed=2026, n_min=1000, n_max=50000, t_min_ms=500.0, t_max_ms=2000.0):
+    """Request stream of the serving benchmark: Poisson arrivals at `rate_hz`,
+    N ~ log-uniform[n_min, n_max] (80 % excitatory), K_E = min(0.1 N, 1000),
+    K_I = K_E / 4, g ~ U[3, 7], eta ~ U[0.9, 2.0], T ~ U[t_min, t_max] ms."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, count)) if rate_hz > 0 else np.zeros(count)
+    out = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        n_exc = int(round(0.8 * n))
+        k_exc = int(min(round(0.1 * n), 1000))
+        k_inh = max(1, k_exc // 4)
+        t_ms = rng.uniform(t_min_ms, t_max_ms)
+        out.append(Request(rid=i, arrival=float(arrivals[i]), n=n, n_exc=n_exc, k_exc=k_exc, k_inh=k_inh,
+                           g=float(rng.uniform(3.0, 7.0)), eta=float(rng.uniform(0.9, 2.0)),
+                           steps=int(round(t_ms / H)), seed=int(rng.integers(1, 2**62))))
+    return out
+
+
+def _admit(eng, r, record=True):
+    rng = np.random.default_rng(r.seed)
+    V0 = rng.normal(-58.0, 10.0, r.n) + 70.0   # V_m relative to E_L = -70 mV
+    build = dict(n_exc=r.n_exc, k_exc=r.k_exc, k_inh=r.k_inh, w_exc=J_EXC, w_inh=-r.g * J_EXC,
+                 delay_steps=DELAY_STEPS, allow_autapses=0, seed=r.seed ^ 0x5A5A5A5A)
+    rate = r.eta * NU_TH_HZ
+    return eng.net_add(r.n, r.steps, r.seed, {"tau_syn_ex": TAU_SYN, "tau_syn_in": TAU_SYN, "V_m_rel": V0},
+                       build=build, poisson=(rate, J_EXC, DELAY_STEPS), record=record)
+
+
+def footprint(r):
+    """Neurons and edge slots a request needs in the pool."""
+    return r.n, r.n * (r.k_exc + r.k_inh) + 3 * r.n
+
+
+def new_engine(precision="fp32", capacity_neurons=2_000_000, capacity_edges=1_200_000_000, max_networks=512,
+               device=0, graph_slices=64):
+    prec = _abi.NG_FP32 if precision == "fp32" else _abi.NG_FP64
+    eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, capacity_neurons)], H, DELAY_STEPS, DELAY_STEPS, precision=prec,
+                      device=device, serving=True, max_networks=max_networks, edge_capacity=capacity_edges,
+                      max_abs_weight=8.0 * J_EXC)
+    eng.set_graph_slices(graph_slices)
+    return eng
+
+
+def run_batched(requests, eng, max_chunk_slices=64, clock=time.perf_counter, realtime=True):
+    """Continuous batching.  Returns (requests, stats)."""
+    pending = sorted(requests, key=lambda r: r.arrival)
+    waiting = []
+    active = {}
+    t0 = clock()
+    ev0 = eng.stats()["syn_events"]
+    steps_run = 0
+    while pending or waiting or active:
+        now = clock() - t0
+        while pending and (pending[0].arrival <= now or not realtime):
+            waiting.append(pending.pop(0))
+        # admit every waiting request that fits, oldest first
+        still = []
+        for r in waiting:
+            nid = _admit(eng, r)
+            if nid is None:
+                still.append(r)
+            else:
+                r.admitted = clock() - t0
+                active[nid] = r
+        waiting = still
+        if not active:
+            if waiting:
+                raise RuntimeError("a request does not fit the empty pool")
+            if pending:
+                time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
+            continue
+        # advance all live networks to the next retirement (at most a graph chunk)
+        left = min(r.steps - eng.net_poll(nid)[0] for nid, r in active.items())
+        slices = max(1, min(max_chunk_slices, -(-left // DELAY_STEPS)))
+        eng.simulate(slices * DELAY_STEPS)
+        steps_run += slices * DELAY_STEPS
+        for nid in list(active):
+            done, fin = eng.net_poll(nid)
+            if fin:
+                r = active.pop(nid)
+                r.spikes = eng.net_spikes(nid)
+                eng.net_remove(nid)
+                r.finished = clock() - t0
+    makespan = clock() - t0
+    ev = eng.stats()["syn_events"] - ev0
+    return requests, {"makespan_s": makespan, "syn_events": ev, "syn_events_per_s": ev / makespan,
+                      "engine_steps": steps_run}
+
+
+def run_plain(requests, eng, clock=time.perf_counter, realtime=True):
+    """One network at a time (FIFO), each run to completion."""
+    order = sorted(requests, key=lambda r: r.arrival)
+    t0 = clock()
+    ev0 = eng.stats()["syn_events"]
+    for r in order:
+        now = clock() - t0
+        if realtime and r.arrival > now:
+            time.sleep(r.arrival - now)
+        nid = _admit(eng, r)
+        if nid is None:
+            raise RuntimeError("a request does not fit the empty pool")
+        r.admitted = clock() - t0
+        eng.simulate(-(-r.steps // DELAY_STEPS) * DELAY_STEPS)
+        r.spikes = eng.net_spikes(nid)
+        eng.net_remove(nid)
+        r.finished = clock() - t0
+    makespan = clock() - t0
+    ev = eng.stats()["syn_events"] - ev0
+    return order, {"makespan_s": makespan, "syn_events": ev, "syn_events_per_s": ev / makespan}
+
+
+def latency_summary(requests):
+    lat = np.array([r.latency for r in requests])
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "max_s": float(lat.max())}

@@ -8,6 +8,8 @@ c1: Poisson-driven iaf_psc_exp network, 12,500 neurons (10,000 exc, 2,500
     delay 1.5 ms, 8 kHz Poisson drive per neuron, V_m ~ N(-58, 10) mV.
 """
 
+import math
+
 import numpy as np
 
 
@@ -65,3 +67,78 @@ def brunel_exp_batch(nest, copies, n_exc=10000, n_inh=2500, k_exc=1000, k_inh=25
             recs.append(sr)
         pops.append(pop)
     return pops, recs
+
+
+# ---------------------------------------------------------------------------
+# c2: layered 8-population iaf_psc_exp network (microcircuit-shaped, synthetic
+# connection probabilities), 77,169 neurons, pairwise_bernoulli.
+# ---------------------------------------------------------------------------
+LAYERED_SIZES = (20683, 5834, 21915, 5479, 4850, 1065, 14395, 2948)
+LAYERED_EXC = (1, 0, 1, 0, 1, 0, 1, 0)
+
+
+def layered_spec(seed=2024, scale=1.0):
+    """Populations [E, I] x 4 layers; p[i][j] (source population i -> target
+    population j) ~ U[0.01, 0.15]; weights N(87.8, 8.78) pA, inhibitory
+    sources x -4; delays N(1.5, 0.75) ms (exc) / N(0.75, 0.375) ms (inh)
+    clipped to >= dt; per-population Poisson drive 8 Hz x K_ext with
+    K_ext ~ U[1500, 2500]; neurons: C_m 250 pF, tau_m 10 ms, t_ref 2 ms,
+    E_L -65 mV, V_th -50 mV, V_reset -65 mV, tau_syn 0.5 ms, V_m(0) ~
+    N(-58, 10) mV.  `scale` shrinks the populations (connection
+    probabilities kept) for cases the oracle can run."""
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(0.01, 0.15, (8, 8))
+    k_ext = rng.integers(1500, 2501, 8)
+    sizes = [max(1, int(round(s * scale))) for s in LAYERED_SIZES]
+    return {"sizes": sizes, "exc": list(LAYERED_EXC), "p": p, "k_ext": k_ext, "J": 87.8, "J_sd": 8.78, "g": -4.0,
+            "d_exc": (1.5, 0.75), "d_inh": (0.75, 0.375), "nu_ext_hz": 8.0, "tau_syn": 0.5, "E_L": -65.0,
+            "V_th": -50.0, "V_reset": -65.0, "C_m": 250.0, "tau_m": 10.0, "t_ref": 2.0, "d_ext_ms": 1.5,
+            "d_max_ms": 8.0, "seed": seed}
+
+
+def layered_expected_edges(spec):
+    n = np.asarray(spec["sizes"], dtype=np.float64)
+    return float(np.sum(np.outer(n, n) * spec["p"]))
+
+
+def layered_engine(spec, precision="fp64", device=0, graph_slices=64):
+    """A serving engine sized for one layered network (the graph is drawn on
+    the device by the pairwise_bernoulli builder)."""
+    from . import _abi
+
+    n = sum(spec["sizes"])
+    h = 0.1
+    max_steps = int(math.floor(spec["d_max_ms"] / h + 0.5))
+    e_need = layered_expected_edges(spec)
+    cap = int(e_need + 6.0 * math.sqrt(e_need) + 4 * n + 1024)
+    prec = _abi.NG_FP32 if precision == "fp32" else _abi.NG_FP64
+    J = spec["J"]
+    eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, n)], h, 1, max(max_steps, int(round(spec["d_ext_ms"] / h))),
+                      precision=prec, device=device, serving=True, max_networks=1, edge_capacity=cap,
+                      max_abs_weight=abs(spec["g"]) * (J + 12 * spec["J_sd"]) * 2)
+    eng.set_graph_slices(graph_slices)
+    return eng
+
+
+def layered_add(eng, spec, steps, record=True):
+    """Admit the layered network into `eng`; returns its network id."""
+    from . import _abi
+
+    sizes, exc = spec["sizes"], spec["exc"]
+    n = sum(sizes)
+    J, sd, g = spec["J"], spec["J_sd"], spec["g"]
+    pb = _abi.NGPairwiseBernoulli.make(sizes, exc, spec["p"], w_mean=(g * J, J), w_sd=(abs(g) * sd, sd),
+                                       d_mean_ms=(spec["d_inh"][0], spec["d_exc"][0]),
+                                       d_sd_ms=(spec["d_inh"][1], spec["d_exc"][1]), d_max_ms=spec["d_max_ms"],
+                                       allow_autapses=0, seed=spec["seed"] * 7919 + 1)
+    rng = np.random.default_rng(spec["seed"])
+    E_L = spec["E_L"]
+    V0 = rng.normal(-58.0, 10.0, n) - E_L
+    rate = np.repeat(np.asarray(spec["k_ext"], dtype=np.float64) * spec["nu_ext_hz"], sizes)
+    d_ext = int(round(spec["d_ext_ms"] / 0.1))
+    var = {"tau_syn_ex": spec["tau_syn"], "tau_syn_in": spec["tau_syn"], "tau_m": spec["tau_m"], "C_m": spec["C_m"],
+           "t_ref": spec["t_ref"], "V_th_rel": spec["V_th"] - E_L, "V_reset_rel": spec["V_reset"] - E_L, "V_m_rel": V0}
+    nid = eng.net_add(n, steps, spec["seed"], var, build=pb, poisson=(rate, J, d_ext), record=record)
+    if nid is None:
+        raise RuntimeError("the layered network does not fit the engine")
+    return nid
