@@ -54,7 +54,8 @@ typedef struct
   double h;                /* resolution [ms]: Time::get_resolution().get_ms() (nest_time.h:330) */
   double tics_per_ms;      /* Time tics per ms, 1000 by default (nest_time.cpp:43) */
   int32_t min_delay;       /* steps; slice length (connection_manager.cpp:485-530) */
-  int32_t max_delay;       /* steps; ring length is min_delay + max_delay (ring_buffer.cpp:25-46) */
+  int32_t max_delay;       /* steps; the engine's rings hold max_delay slots (ring_buffer.cpp:25-46
+                              holds min_delay + max_delay: the reference delivers before it updates) */
   int32_t n_blocks;
   int32_t block_model[ NG_MAX_BLOCKS ];
   int64_t block_size[ NG_MAX_BLOCKS ];
@@ -82,6 +83,7 @@ typedef struct
   int64_t update_launches;
   int64_t deliver_launches;
   double simulate_ms;        /* host wall time inside ng_simulate */
+  int64_t gather_slices;     /* serving, FP32 form: (network, slice) pairs delivered by the per-target gather */
 } ng_stats;
 
 /* Version of this ABI (NG_ABI_VERSION). */

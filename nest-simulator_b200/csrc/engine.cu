@@ -263,7 +263,7 @@ struct ng_engine
   double log_per_step = 1.0;  // bound on recorded neuron spikes per step (refractoriness)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector< DevBuf* > all;
-  int deliver_ctas = 0;
+  int deliver_ctas = 0, deliver_per_sm = 4;
 
   // ---- serving: networks added to and removed from the running engine
   bool serving = false;
@@ -273,6 +273,7 @@ struct ng_engine
   {
     bool used = false;
     int64_t off = 0, n = 0, e0 = 0, ne = 0, step0 = 0, until = 0;
+    int64_t g0 = -1, gn = 0;  // gather table run
     bool rec = false;
     double log_rate = 0.0;
     std::vector< int32_t > src;
@@ -280,6 +281,12 @@ struct ng_engine
   };
   std::vector< NetInfo > nets;
   std::map< int64_t, int64_t > free_neurons, free_edges;  // run start -> length
+  // per-target gather of fixed_indegree networks (precision form)
+  bool gather_on = false;
+  float gather_frac = 0.15f;
+  DevBuf gmask, gin, net_g, net_mode, net_spk;
+  std::map< int64_t, int64_t > free_gin;
+  std::vector< GatherNet > host_g;
   std::unordered_map< std::string, int32_t > cls_ids;     // engine-wide coefficient classes
   int64_t cls_cap = 0, cdf_cap = 0;
   std::vector< double > cdf_host;
@@ -371,6 +378,26 @@ struct ng_engine
     free_edges.clear();
     free_neurons[ 0 ] = N;
     free_edges[ 0 ] = E;
+    // per-target gather: precision form, current-based models, slices of at most 32 steps
+    gather_on = prec != NG_FP64 && b.model != NG_AEIF_COND_ALPHA && cfg.min_delay <= 32;
+    if ( const char* ge = std::getenv( "NG_GATHER" ) )
+      gather_on = gather_on && std::atoi( ge ) != 0;
+    if ( const char* gf = std::getenv( "NG_GATHER_FRAC" ) )
+      gather_frac = ( float ) std::atof( gf );
+    if ( gather_on )
+    {
+      if ( ( rc = alloc( gmask, ( size_t ) N * 4 ) ) || ( rc = alloc( gin, ( size_t ) E * 2 ) )
+        || ( rc = alloc( net_g, ( size_t ) nmax * sizeof( GatherNet ) ) ) || ( rc = alloc( net_mode, ( size_t ) nmax * 4 ) )
+        || ( rc = alloc( net_spk, ( size_t ) nmax * 4 ) ) )
+        return rc;
+      CU( cudaMemsetAsync( gmask.p, 0, ( size_t ) N * 4, stream ) );
+      CU( cudaMemsetAsync( net_g.p, 0, ( size_t ) nmax * sizeof( GatherNet ), stream ) );
+      CU( cudaMemsetAsync( net_mode.p, 0, ( size_t ) nmax * 4, stream ) );
+      CU( cudaMemsetAsync( net_spk.p, 0, ( size_t ) nmax * 4, stream ) );
+      host_g.assign( ( size_t ) nmax, GatherNet {} );
+      free_gin.clear();
+      free_gin[ 0 ] = E;
+    }
     // one fixed-point scale for every network (FP32 form)
     const double mx = cfg.max_abs_weight > 0 ? cfg.max_abs_weight : 1e4;
     fx_S = ( int ) std::floor( std::log2( 2147483647.0 / mx ) );
@@ -649,6 +676,16 @@ struct ng_engine
     d.net_until = ( const long long* ) d_until.p;
     d.net_off = ( const long long* ) d_off.p;
     d.net_key = ( const uint2* ) d_key.p;
+    if ( gather_on )
+    {
+      d.gmask = ( uint32_t* ) gmask.p;
+      d.gin = ( const uint16_t* ) gin.p;
+      d.net_g = ( const GatherNet* ) net_g.p;
+      d.net_mode = ( int* ) net_mode.p;
+      d.net_spk = ( unsigned* ) net_spk.p;
+      d.n_nets = cfg.max_networks;
+      d.gather_frac = gather_frac;
+    }
     d.sched_step = ( const int64_t* ) sched_step.p;
     d.sched_src = ( const int32_t* ) sched_src.p;
     d.n_sched = n_sched;
@@ -700,12 +737,17 @@ struct ng_engine
   launch_iaf_g( const Net& d, const Block& db, int from_, int to_, int sched )
   {
     const int span = to_ - from_;
-    // one thread per neuron for 1-2 step slices and for networks large enough
-    // to fill the GPU that way; the two-phase kernel otherwise
-    if ( span <= 2 || db.n >= one_thread_min_n || max_lanes == 1 )
+    // one thread per neuron for 1-2 step slices, for networks large enough
+    // to fill the GPU that way and for engines with the per-target gather
+    // (its lag bits are written there); the two-phase kernel otherwise
+    if ( span <= 2 || db.n >= one_thread_min_n || max_lanes == 1 || gather_on )
     {
-      const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 255 ) / 256 );
-      k_update_iaf< Real, FIX, MODEL ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+      // CTAs of 4 warps: a large network's grid is resident in one wave
+      const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 127 ) / 128 );
+      if ( span == 1 )
+        k_update_iaf< Real, FIX, MODEL, 1 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
+      else
+        k_update_iaf< Real, FIX, MODEL, 8 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
     }
     else
     {
@@ -736,6 +778,8 @@ struct ng_engine
   void
   launch_deliver( const Net& d )
   {
+    if ( gather_on )
+      k_gather<<< ( unsigned ) ( ( N + G_TGT - 1 ) / G_TGT ), G_TGT * G_PARTS, 0, stream >>>( d );
     const unsigned grid = ( unsigned ) deliver_ctas;
     if ( prec == NG_FP64 )
       k_deliver< false ><<< grid, 256, 0, stream >>>( d );
@@ -1021,6 +1065,7 @@ struct ng_engine
     stats.spikes = ( int64_t ) c.n_spikes;
     stats.syn_events = ( int64_t ) c.syn_events;
     stats.drive_events = ( int64_t ) c.drive_events;
+    stats.gather_slices = ( int64_t ) c.gathered;
     return NG_OK;
   }
 
@@ -1138,7 +1183,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
   e->h = ( 1 / cfg->tics_per_ms ) * ( double ) e->tics_per_step;
   e->N = N;
   e->n_src = N + cfg->n_generators;
-  e->L = cfg->min_delay + cfg->max_delay;
+  e->L = std::max( cfg->min_delay, cfg->max_delay );  // update-then-deliver order: max_delay slots suffice
   if ( cfg->start_step < 0 )
   {
     delete e;
@@ -1229,7 +1274,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
   if ( ( int64_t ) cfg->max_delay > ( int64_t ) e->dmask )
     return bail( fail( NG_ERR_ARG, "ng_create: max_delay does not fit the packed edge format for this network size" ) );
   if ( e->L >= 65536 )
-    return bail( fail( NG_ERR_ARG, "ng_create: min_delay + max_delay must be below 65536 steps" ) );
+    return bail( fail( NG_ERR_ARG, "ng_create: max_delay must be below 65536 steps" ) );
   e->ent_cap = 1024;
   if ( ( rc = e->alloc( e->ent, ( size_t ) e->ent_cap * sizeof( int4 ) ) ) )
     return bail( rc );
@@ -1250,6 +1295,15 @@ ng_create( const ng_config* cfg, ng_engine** out )
       return bail( fail( NG_ERR_CUDA, "ng_create: control block upload failed" ) );
   }
   e->deliver_ctas = 1;
+  {
+    // resident delivery CTAs per SM (the kernel splits its work over the warps of one wave)
+    int occ = 0;
+    if ( e->prec == NG_FP64 )
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< false >, 256, 0 );
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< true >, 256, 0 );
+    e->deliver_per_sm = std::max( 1, std::min( occ, 8 ) );
+  }
   if ( cfg->serving )
   {
     if ( cfg->n_blocks != 1 || cfg->n_generators != 0 || cfg->edge_capacity < 4 || cfg->max_networks < 1 )
@@ -1257,7 +1311,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
                                      "and network slots" ) );
     if ( ( rc = e->setup_serving() ) )
       return bail( rc );
-    e->deliver_ctas = e->sms * 4;
+    e->deliver_ctas = e->sms * e->deliver_per_sm;
   }
   if ( const char* ml = std::getenv( "NG_MAX_LANES" ) )
   {
@@ -1517,9 +1571,9 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
   }
   if ( ( rc = e->resize_work() ) )
     return rc;
-  // delivery grid: a warp per chunk; up to 4 CTAs of 8 warps per SM, fewer for small graphs
+  // delivery grid: one wave of resident CTAs, fewer for small graphs
   const int64_t want = std::max< int64_t >( 1, e->chunks_all_src / 64 );
-  e->deliver_ctas = ( int ) std::min< int64_t >( want, ( int64_t ) e->sms * 4 );
+  e->deliver_ctas = ( int ) std::min< int64_t >( want, ( int64_t ) e->sms * e->deliver_per_sm );
   CU( cudaStreamSynchronize( e->stream ) );
   ++e->generation;
   return NG_OK;
@@ -1922,9 +1976,12 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     ng_engine::give_run( e->free_neurons, n0, n );
     return fail( NG_ERR_CAPACITY, "ng_net_add: not enough free edges in the pool" );
   }
+  int64_t g0 = -1, gn = 0;  // gather table run, if any
   auto undo = [ & ]( int code ) {
     ng_engine::give_run( e->free_neurons, n0, n );
     ng_engine::give_run( e->free_edges, e0, ne_need );
+    if ( g0 >= 0 )
+      ng_engine::give_run( e->free_gin, g0, gn );
     return code;
   };
   auto& b = e->blk[ 0 ];
@@ -2135,6 +2192,24 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     k_fi_rows<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, n0, e0, ( const int64_t* ) e->sc_beg.p,
       ( const int32_t* ) e->sc_plen.p, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->row_beg.p,
       ( int32_t* ) e->row_len.p, ( int32_t* ) e->real_deg.p );
+    // the in-edge table of the per-target gather (16-bit local ids)
+    if ( e->gather_on && fx && nk > 0 && n <= 65536 && ng_engine::take_run( e->free_gin, nk, &g0 ) )
+    {
+      gn = nk;
+      k_fi_gtab<<< g, 256, 0, e->stream >>>( n, K, ( const int32_t* ) e->sc_src.p, ( uint16_t* ) e->gin.p + g0 );
+      GatherNet gt {};
+      gt.base = g0;
+      gt.off = n0;
+      gt.n = ( int ) n;
+      gt.ke = fb->k_exc;
+      gt.ki = fb->k_inh;
+      gt.d = fb->delay_steps;
+      to_fixed( wex, &gt.we );
+      to_fixed( win, &gt.wi );
+      gt.ce = ( int ) chx;
+      gt.ci = ( int ) chi;
+      e->host_g[ id ] = gt;
+    }
     CU( cudaGetLastError() );
     long long total = 0;
     CU( cudaMemcpyAsync( &total, e->sc_total.p, 8, cudaMemcpyDeviceToHost, e->stream ) );
@@ -2257,6 +2332,19 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   nw.n = n;
   nw.e0 = e0;
   nw.ne = ne_used;
+  nw.g0 = g0;
+  nw.gn = gn;
+  if ( e->gather_on )
+  {
+    if ( g0 < 0 )
+      e->host_g[ id ] = GatherNet {};
+    const int zero = 0;
+    CU( cudaMemcpyAsync( ( GatherNet* ) e->net_g.p + id, &e->host_g[ id ], sizeof( GatherNet ), cudaMemcpyHostToDevice,
+      e->stream ) );
+    CU( cudaMemcpyAsync( ( int* ) e->net_mode.p + id, &zero, 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int* ) e->net_spk.p + id, &zero, 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
   nw.step0 = step0;
   nw.until = until;
   nw.rec = desc->record != 0;
@@ -2384,6 +2472,17 @@ ng_net_remove( ng_engine* e, int32_t id )
   std::fill( e->rec_host.begin() + nw.off, e->rec_host.begin() + nw.off + nw.n, ( uint8_t ) 0 );
   ng_engine::give_run( e->free_neurons, nw.off, nw.n );
   ng_engine::give_run( e->free_edges, nw.e0, nw.ne );
+  if ( e->gather_on )
+  {
+    if ( nw.g0 >= 0 )
+      ng_engine::give_run( e->free_gin, nw.g0, nw.gn );
+    e->host_g[ id ] = GatherNet {};
+    const int zero = 0;
+    CU( cudaMemcpyAsync( ( GatherNet* ) e->net_g.p + id, &e->host_g[ id ], sizeof( GatherNet ), cudaMemcpyHostToDevice,
+      e->stream ) );
+    CU( cudaMemcpyAsync( ( int* ) e->net_mode.p + id, &zero, 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
   e->n_rec -= nw.rec ? nw.n : 0;
   e->log_per_step = std::max( 1.0, e->log_per_step - nw.log_rate );
   nw = ng_engine::NetInfo();

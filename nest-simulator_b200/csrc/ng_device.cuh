@@ -1,6 +1,10 @@
 // ng_device.cuh -- device-side data layout and helpers of the slice engine.
 //
-// HBM layout (one engine = one network, N neurons, L = min_delay + max_delay):
+// HBM layout (one engine = one network, N neurons, ring length L = max_delay:
+// a slice's update reads its min_delay slots before the slice's delivery
+// writes arrivals t_emit + d <= t_end - 1 + max_delay, so max_delay slots
+// hold every pending arrival -- the reference's rings hold min_delay +
+// max_delay because it delivers before it updates):
 //   state     SoA arrays per model block, FP64 (plain) or FP32 (precision form)
 //   classes   per-neuron class id -> row of FP64 coefficients (propagators,
 //             thresholds, refractory counts) computed on the host
@@ -43,6 +47,7 @@ struct Ctl
   long long log_base;   // stamp offset of the log entries
   long long trace_row0; // first trace row index held in the buffer
   long long sched_pos;  // next unconsumed scheduled generator spike
+  unsigned long long gathered;  // (network, slice) pairs delivered by the per-target gather
   int deliver_done;     // finished CTAs of the running delivery launch
   int err;
 };
@@ -56,6 +61,18 @@ struct Block
   void* s[ MAX_STATE ];
   int32_t* r;
   double* istep;
+};
+
+// Per-target gather of one fixed_indegree network of a serving engine
+// (precision form): in-edge table gin[base + j * n + t] (16-bit local source
+// ids, excitatory draws j < ke first, then ki inhibitory ones), uniform
+// weights we / wi (fixed point) into ring channels ce / ci, delay d.
+// ke + ki == 0: no table.
+struct GatherNet
+{
+  long long base, off;
+  int n, ke, ki, d;
+  int we, wi, ce, ci;
 };
 
 struct Net
@@ -95,6 +112,14 @@ struct Net
   const long long* net_until;    // per network: first step it no longer simulates
   const long long* net_off;      // per network: first neuron
   const uint2* net_key;          // per network: Philox key of its drive
+  // per-target gather (serving, precision form); gmask == nullptr: off
+  uint32_t* gmask;               // per neuron: bit k = spike at lag k of the open slice
+  const uint16_t* gin;           // in-edge tables of the gather networks
+  const GatherNet* net_g;        // per network
+  int* net_mode;                 // per network: 1 = gather this slice, 0 = scatter
+  unsigned* net_spk;             // per network: spikes in the open slice
+  int n_nets;
+  float gather_frac;             // gather the next slice when spikes >= gather_frac * n
   const int64_t* sched_step;
   const int32_t* sched_src;
   int64_t n_sched;

@@ -13,6 +13,8 @@
 // the ring sums are order independent.
 #pragma once
 
+#include <type_traits>
+
 #include "ng_device.cuh"
 
 namespace ng
@@ -190,6 +192,113 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
   }
 }
 
+// The same as warp_append_mask, with the reservations of all warps of the
+// CTA combined: one global atomic per counter and CTA (thousands of warps of
+// a large network each reserving on the same control-block line serialise
+// in L2).  A neuron of a network in gather mode queues no edge chunks (its
+// targets gather); spikes are counted per network for the mode choice.
+// Must be called by every thread of the CTA.
+__device__ __forceinline__ void
+cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long t0, int netid, bool gath )
+{
+  __shared__ unsigned long long s_e, s_l, s_r, s_c, g_e, g_l;
+  __shared__ int s_any;
+  const int lane = threadIdx.x & 31;
+  if ( threadIdx.x == 0 )
+  {
+    s_e = s_l = s_r = s_c = 0ull;
+    s_any = 0;
+  }
+  __syncthreads();
+  const int cnt = __popc( mask );
+  const bool any = __ballot_sync( FULL, cnt > 0 ) != 0;
+  long long pdeg = 0, rdeg = 0, row = 0, nch = 0;
+  const bool lg = cnt > 0 && ( d.rec == nullptr || d.rec[ src ] );
+  long long e_incl = 0, l_incl = 0;
+  unsigned long long w_e = 0, w_l = 0;
+  if ( any )
+  {
+    if ( cnt > 0 )
+    {
+      row = d.row_beg[ src ];
+      pdeg = d.row_len[ src ];
+      rdeg = d.real_deg[ src ];
+      nch = gath ? 0 : ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
+      if ( d.net_spk && netid >= 0 )
+      {
+        // one atomic per network present in the warp
+        const unsigned peers = __match_any_sync( __activemask(), netid );
+        const unsigned tot = __reduce_add_sync( peers, ( unsigned ) cnt );
+        if ( lane == __ffs( peers ) - 1 )
+          atomicAdd( d.net_spk + netid, tot );
+      }
+    }
+    e_incl = cnt * nch;
+    l_incl = lg ? cnt : 0;
+#pragma unroll
+    for ( int o = 1; o < 32; o <<= 1 )
+    {
+      const long long b = __shfl_up_sync( FULL, e_incl, o );
+      const long long c = __shfl_up_sync( FULL, l_incl, o );
+      if ( lane >= o )
+      {
+        e_incl += b;
+        l_incl += c;
+      }
+    }
+    const long long tot_e = __shfl_sync( FULL, e_incl, 31 );
+    const long long tot_l = __shfl_sync( FULL, l_incl, 31 );
+    const long long rtot = warp_sum_ll( cnt * rdeg );
+    const long long ctot = warp_sum_ll( cnt );
+    if ( lane == 0 )
+    {
+      w_e = atomicAdd( &s_e, ( unsigned long long ) tot_e );
+      w_l = atomicAdd( &s_l, ( unsigned long long ) tot_l );
+      atomicAdd( &s_r, ( unsigned long long ) rtot );
+      atomicAdd( &s_c, ( unsigned long long ) ctot );
+      s_any = 1;
+    }
+  }
+  __syncthreads();
+  if ( !s_any )
+    return;  // uniform across the CTA
+  if ( threadIdx.x == 0 )
+  {
+    g_e = s_e > 0 ? atomicAdd( &d.ctl->n_ent, s_e ) : 0ull;
+    g_l = s_l > 0 ? atomicAdd( &d.ctl->log_count, s_l ) : 0ull;
+    atomicAdd( &d.ctl->syn_events, s_r );
+    atomicAdd( &d.ctl->n_spikes, s_c );
+  }
+  __syncthreads();
+  const unsigned long long base = g_e + __shfl_sync( FULL, w_e, 0 );
+  const unsigned long long lbase = g_l + __shfl_sync( FULL, w_l, 0 );
+  if ( cnt == 0 )
+    return;
+  long long idx = ( long long ) base + e_incl - cnt * nch;
+  long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
+  const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
+  unsigned m = mask;
+  while ( m )
+  {
+    const int k = __ffs( m ) - 1;
+    m &= m - 1;
+    int slot = slot0 + k;
+    if ( slot >= d.L )
+      slot -= d.L;
+    if ( nch > 0 )
+      put_chunks( d, idx, row, pdeg, slot, 1 );
+    idx += nch;
+    if ( lg )
+    {
+      if ( li < d.log_cap )
+        d.log[ li ] = make_uint2( ( uint32_t ) src, ( uint32_t ) ( t0 + k + 1 - lb0 ) | ( 1u << 24 ) );
+      else
+        atomicOr( &d.ctl->err, ERR_LOG );
+      ++li;
+    }
+  }
+}
+
 // Steps at which neuron i is simulated: [.., until); a free neuron of a
 // serving engine never is.
 __device__ __forceinline__ long long
@@ -249,9 +358,20 @@ drive( const Net& d, int64_t i, long long t, long long& cnt )
   long long k;
   if ( tb.y > 0 )
   {
+    // j = first index with u <= cdf[j] (or the last one); the first 4
+    // entries are loaded together instead of one dependent load per step
     const double* cdf = d.pois_cdf + tb.x;
+    const int n = tb.y;
+    double c[ 4 ];
+#pragma unroll
+    for ( int q = 0; q < 4; ++q )
+      c[ q ] = q < n ? __ldg( cdf + q ) : 1.0;
     int j = 0;
-    while ( j < tb.y - 1 && u > __ldg( cdf + j ) )
+#pragma unroll
+    for ( int q = 0; q < 4; ++q )
+      if ( j == q && q < n - 1 && u > c[ q ] )
+        j = q + 1;
+    while ( j >= 4 && j < n - 1 && u > __ldg( cdf + j ) )
       ++j;
     k = j;
   }
@@ -369,7 +489,7 @@ append_scheduled( const Net& d, long long origin, int from, int to )
 //               state: s0 = V_m - E_L, s1 = i_syn_ex, s2 = i_syn_in,
 //                      s3 = i_0, s4 = i_1, s5 = I_e
 // ---------------------------------------------------------------------
-template < typename Real, bool FIX, int MODEL >
+template < typename Real, bool FIX, int MODEL, int SUB >
 __global__ void __launch_bounds__( 256 )
 k_update_iaf( Net d, Block b, int from, int to, int sched )
 {
@@ -380,6 +500,8 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
   const bool act = li < b.n;
   const int64_t i = b.off + ( act ? li : 0 );
   const long long until = act ? active_until( d, i ) : -1ll;
+  const int netid = ( act && d.nid ) ? d.nid[ i ] : -1;
+  const bool gath = netid >= 0 && d.net_mode && d.net_mode[ netid ] != 0;
   constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
   Real* s0 = ( Real* ) b.s[ 0 ];
   Real* s1 = ( Real* ) b.s[ 1 ];
@@ -426,7 +548,9 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
     r = b.r[ li ];
   }
   long long dcnt = 0;
-  constexpr int SUB = 8;  // lags whose inputs are gathered before the recurrence runs over them
+  // SUB: lags whose inputs are gathered before the recurrence runs over them
+  // (8; 1 for slices of one step, where the unrolled code would only cost
+  // instruction fetch)
   for ( int cb = from; cb < to; cb += 32 )
   {
     const int nl = min( 32, to - cb );
@@ -536,7 +660,15 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
         }
       }
     }
-    warp_append_mask( d, smask, ( int32_t ) i, slot0, t0 );
+    if ( d.gmask && act )
+    {
+      // lag bits of the slice for the gather (min_delay <= 32: one chunk)
+      if ( cb == 0 )
+        d.gmask[ i ] = smask;
+      else
+        d.gmask[ i ] |= smask << cb;
+    }
+    cta_append_mask( d, smask, ( int32_t ) i, slot0, t0, netid, gath );
   }
   flush_drive_count( d, dcnt );
   if ( act )
@@ -1014,15 +1146,99 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
   }
 }
 
+// One lane's share of an edge chunk: 4 edge words and 4 weights.
+template < bool FIX >
+struct ChunkLane
+{
+  uint32_t t[ 4 ];
+  typename std::conditional< FIX, int32_t, double >::type w[ 4 ];
+  int slot0, mult;
+};
+
+template < bool FIX >
+__device__ __forceinline__ void
+load_chunk( const Net& d, const int4 en, const int lane, ChunkLane< FIX >& c )
+{
+  const int j = lane << 2;
+  c.slot0 = en.w & 0xffff;
+  c.mult = en.w >> 16;
+  if ( j < en.z )
+  {
+    const long long edge = ( ( ( long long ) en.y << 32 ) | ( unsigned ) en.x ) + j;
+    const uint4 tdc = __ldg( reinterpret_cast< const uint4* >( d.edge_tdc + edge ) );
+    c.t[ 0 ] = tdc.x;
+    c.t[ 1 ] = tdc.y;
+    c.t[ 2 ] = tdc.z;
+    c.t[ 3 ] = tdc.w;
+    if constexpr ( FIX )
+    {
+      const int4 w4 = __ldg( reinterpret_cast< const int4* >( ( const int32_t* ) d.edge_w + edge ) );
+      c.w[ 0 ] = w4.x;
+      c.w[ 1 ] = w4.y;
+      c.w[ 2 ] = w4.z;
+      c.w[ 3 ] = w4.w;
+    }
+    else
+    {
+      const double2* wp = reinterpret_cast< const double2* >( ( const double* ) d.edge_w + edge );
+      const double2 wa = __ldg( wp ), wb = __ldg( wp + 1 );
+      c.w[ 0 ] = wa.x;
+      c.w[ 1 ] = wa.y;
+      c.w[ 2 ] = wb.x;
+      c.w[ 3 ] = wb.y;
+    }
+  }
+  else
+  {
+#pragma unroll
+    for ( int k = 0; k < 4; ++k )
+    {
+      c.t[ k ] = 0u;
+      c.w[ k ] = 0;
+    }
+  }
+}
+
+template < bool FIX >
+__device__ __forceinline__ void
+apply_chunk( const Net& d, const ChunkLane< FIX >& c )
+{
+#pragma unroll
+  for ( int k = 0; k < 4; ++k )
+  {
+    if ( c.w[ k ] == 0 )
+      continue;
+    const uint32_t tgt = c.t[ k ] & d.tmask;
+    int slot = c.slot0 + ( int ) ( ( c.t[ k ] >> d.tbits ) & d.dmask );
+    if ( slot >= d.L )
+      slot -= d.L;
+    const int64_t idx = ( ( int64_t ) slot * d.C + ( c.t[ k ] >> 31 ) ) * d.N + tgt;
+    if constexpr ( FIX )
+      atomicAdd( ( unsigned long long* ) d.ring + idx,
+        ( unsigned long long ) ( ( long long ) c.w[ k ] * ( long long ) c.mult ) );
+    else
+      atomicAdd( ( double* ) d.ring + idx, c.mult == 1 ? c.w[ k ] : c.w[ k ] * ( double ) c.mult );
+  }
+}
+
+__device__ __forceinline__ int4
+shfl_int4( const int4 v, const int src )
+{
+  return make_int4( __shfl_sync( FULL, v.x, src ), __shfl_sync( FULL, v.y, src ), __shfl_sync( FULL, v.z, src ),
+    __shfl_sync( FULL, v.w, src ) );
+}
+
 // ---------------------------------------------------------------------
 // Delivery: every spike of the closing slice, every out-edge, one red.global
 // add into ring[(t_emit + d) mod L][channel][target]
 // (EventDeliveryManager::deliver_events_ -> Connector::send -> handle,
 // event_delivery_manager.cpp:599-700, connector_base.h:398-434).
 // Work item = one edge chunk (<= 128 edges of one padded CSR row) queued by
-// the update kernel when the spike was emitted; a warp takes a chunk, each
-// lane loads 4 edges (one 16-byte edge-word load, 32 or 16 bytes of
-// weights) and issues their adds.
+// the update kernel when the spike was emitted.  A warp takes a group of up
+// to 4 consecutive chunks (one load of their descriptors), and walks them
+// with the next chunk's edges already in flight while the adds of the
+// current one issue: each lane loads 4 edges (one 16-byte edge-word
+// load, 16 or 32 bytes of weights) and issues their red.global adds.
 // ---------------------------------------------------------------------
 template < bool FIX >
 __global__ void __launch_bounds__( 256 )
@@ -1041,53 +1257,23 @@ k_deliver( Net d )
   const long long nent = ok ? ( long long ) s_nent : 0;
   const int lane = threadIdx.x & 31;
   const long long nwarps = ( ( long long ) gridDim.x * blockDim.x ) >> 5;
-  for ( long long e = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5; e < nent; e += nwarps )
+  const long long gw = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  // chunks per group: at most 4, so the warps sweep the list together (the
+  // chunks of one network, queued together, are delivered together)
+  const long long G = max( 1ll, min( 4ll, nent / nwarps ) );
+  for ( long long base = gw * G; base < nent; base += nwarps * G )
   {
-    const int4 en = d.ent[ e ];  // the same 16 bytes for the whole warp
-    const int j = lane << 2;
-    if ( j >= en.z )
-      continue;
-    const long long edge = ( ( ( long long ) en.y << 32 ) | ( unsigned ) en.x ) + j;
-    const int slot0 = en.w & 0xffff;
-    const int mult = en.w >> 16;
-    const uint4 tdc = __ldg( reinterpret_cast< const uint4* >( d.edge_tdc + edge ) );
-    const uint32_t tw[ 4 ] = { tdc.x, tdc.y, tdc.z, tdc.w };
-    if constexpr ( FIX )
+    const int cnt = ( int ) min( G, nent - base );
+    const int4 my = lane < cnt ? d.ent[ base + lane ] : make_int4( 0, 0, 0, 0 );
+    ChunkLane< FIX > cur, nxt;
+    load_chunk< FIX >( d, shfl_int4( my, 0 ), lane, cur );
+    for ( int k = 0; k < cnt; ++k )
     {
-      const int4 w4 = __ldg( reinterpret_cast< const int4* >( ( const int32_t* ) d.edge_w + edge ) );
-      const int32_t ww[ 4 ] = { w4.x, w4.y, w4.z, w4.w };
-      unsigned long long* ring = ( unsigned long long* ) d.ring;
-#pragma unroll
-      for ( int k = 0; k < 4; ++k )
-      {
-        if ( ww[ k ] == 0 )
-          continue;
-        const uint32_t tgt = tw[ k ] & d.tmask;
-        int slot = slot0 + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
-        if ( slot >= d.L )
-          slot -= d.L;
-        const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
-        atomicAdd( ring + idx, ( unsigned long long ) ( ( long long ) ww[ k ] * ( long long ) mult ) );
-      }
-    }
-    else
-    {
-      const double2* wp = reinterpret_cast< const double2* >( ( const double* ) d.edge_w + edge );
-      const double2 wa = __ldg( wp ), wb = __ldg( wp + 1 );
-      const double ww[ 4 ] = { wa.x, wa.y, wb.x, wb.y };
-      double* ring = ( double* ) d.ring;
-#pragma unroll
-      for ( int k = 0; k < 4; ++k )
-      {
-        if ( ww[ k ] == 0.0 )
-          continue;
-        const uint32_t tgt = tw[ k ] & d.tmask;
-        int slot = slot0 + ( int ) ( ( tw[ k ] >> d.tbits ) & d.dmask );
-        if ( slot >= d.L )
-          slot -= d.L;
-        const int64_t idx = ( ( int64_t ) slot * d.C + ( tw[ k ] >> 31 ) ) * d.N + tgt;
-        atomicAdd( ring + idx, mult == 1 ? ww[ k ] : ww[ k ] * ( double ) mult );
-      }
+      const int4 en = shfl_int4( my, min( k + 1, 31 ) );
+      if ( k + 1 < cnt )
+        load_chunk< FIX >( d, en, lane, nxt );
+      apply_chunk< FIX >( d, cur );
+      cur = nxt;
     }
   }
   // the last CTA to finish closes the slice
@@ -1098,6 +1284,21 @@ k_deliver( Net d )
     s_last = atomicAdd( &d.ctl->deliver_done, 1 ) == ( int ) gridDim.x - 1;
   }
   __syncthreads();
+  if ( s_last && d.net_mode )
+  {
+    // delivery mode of every network for the next slice: gather when this
+    // slice's spikes reached gather_frac of its neurons (the gather reads
+    // every in-edge once, the scatter one edge per spike and out-edge)
+    for ( int id = threadIdx.x; id < d.n_nets; id += blockDim.x )
+    {
+      const unsigned sp = d.net_spk[ id ];
+      d.net_spk[ id ] = 0u;
+      const GatherNet g = d.net_g[ id ];
+      if ( d.net_mode[ id ] )
+        atomicAdd( &d.ctl->gathered, 1ull );
+      d.net_mode[ id ] = ( g.ke + g.ki > 0 && ( float ) sp >= d.gather_frac * ( float ) g.n ) ? 1 : 0;
+    }
+  }
   if ( s_last && threadIdx.x == 0 )
   {
     d.ctl->n_ent = 0ull;

@@ -12,7 +12,7 @@
 // the padded row lengths, scatter).
 #pragma once
 
-#include "ng_device.cuh"
+#include "ng_kernels.cuh"
 
 namespace ng
 {
@@ -102,6 +102,20 @@ k_fi_scatter( int64_t n, int k_exc, int k_inh, const int32_t* tmp_src, const int
   const bool ex = j < k_exc;
   tdc[ e ] = ( uint32_t ) ( n0 + t ) | ( ex ? word_exc : word_inh );
   w[ e ] = ex ? w_exc : w_inh;
+}
+
+// In-edge table of the per-target gather: gin[j * n + t] = local source of
+// draw j of target t (column-major, so consecutive targets read
+// consecutive entries).
+__global__ void
+k_fi_gtab( int64_t n, int K, const int32_t* tmp_src, uint16_t* gin )
+{
+  const int64_t idx = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( idx >= n * K )
+    return;
+  const int64_t t = idx / K;
+  const int j = ( int ) ( idx - t * K );
+  gin[ ( int64_t ) j * n + t ] = ( uint16_t ) tmp_src[ idx ];
 }
 
 // Rows of the region's sources: begin, padded length, real degree.
@@ -298,6 +312,97 @@ k_pb_rowsum( long long n, int nb, const int* cnt_sb, int32_t* cnt )
   for ( int b = 0; b < nb; ++b )
     t += cnt_sb[ s * nb + b ];
   cnt[ s ] = ( int32_t ) t;
+}
+
+}  // namespace ng
+
+namespace ng
+{
+
+// ---------------------------------------------------------------------
+// Per-target gather (precision form of a serving engine): for the networks
+// in gather mode this slice, every target walks its in-edge table and
+// counts, per lag and channel, the in-edges whose source spiked at that lag
+// (the sources' lag bits, gmask, written by the update kernel); the ring
+// then gets count * weight at slot (origin + lag + d) mod L.  The targets'
+// ring cells have no other writer in this slice (their sources queue no
+// edge chunks), so the adds are plain read-modify-writes.  The integer
+// result equals the scatter's, whatever the order.
+// A CTA serves G_TGT targets with G_PARTS threads each (in-edges split in
+// G_PARTS runs, counts combined in shared memory).
+// ---------------------------------------------------------------------
+constexpr int G_TGT = 64;
+constexpr int G_PARTS = 4;
+
+__global__ void __launch_bounds__( G_TGT * G_PARTS )
+k_gather( Net d )
+{
+  __shared__ unsigned s_cnt[ 2 ][ 32 ][ G_TGT ];  // [draw type][lag][target]
+  for ( int k = threadIdx.x; k < 2 * 32 * G_TGT; k += blockDim.x )
+    ( &s_cnt[ 0 ][ 0 ][ 0 ] )[ k ] = 0u;
+  const long long origin = cta_origin( d );  // synchronises the CTA
+  const int ti = threadIdx.x % G_TGT;
+  const int part = threadIdx.x / G_TGT;
+  const int64_t t = ( int64_t ) blockIdx.x * G_TGT + ti;
+  const int id = t < d.N ? d.nid[ t ] : -1;
+  const bool on = id >= 0 && d.net_mode[ id ] != 0;
+  GatherNet g {};
+  if ( on )
+  {
+    g = d.net_g[ id ];
+    const int K = g.ke + g.ki;
+    const int j0 = ( int ) ( ( long long ) K * part / G_PARTS );
+    const int j1 = ( int ) ( ( long long ) K * ( part + 1 ) / G_PARTS );
+    const uint16_t* col = d.gin + g.base + ( t - g.off );
+    const uint32_t* msk = d.gmask + g.off;
+    int j = j0;
+    for ( ; j + 4 <= j1; j += 4 )
+    {
+      uint32_t m[ 4 ];
+#pragma unroll
+      for ( int q = 0; q < 4; ++q )
+        m[ q ] = msk[ col[ ( long long ) ( j + q ) * g.n ] ];
+#pragma unroll
+      for ( int q = 0; q < 4; ++q )
+      {
+        const int ty = ( j + q ) >= g.ke ? 1 : 0;
+        while ( m[ q ] )
+        {
+          const int k = __ffs( m[ q ] ) - 1;
+          m[ q ] &= m[ q ] - 1;
+          atomicAdd( &s_cnt[ ty ][ k ][ ti ], 1u );
+        }
+      }
+    }
+    for ( ; j < j1; ++j )
+    {
+      uint32_t m = msk[ col[ ( long long ) j * g.n ] ];
+      const int ty = j >= g.ke ? 1 : 0;
+      while ( m )
+      {
+        const int k = __ffs( m ) - 1;
+        m &= m - 1;
+        atomicAdd( &s_cnt[ ty ][ k ][ ti ], 1u );
+      }
+    }
+  }
+  __syncthreads();
+  if ( !on )
+    return;
+  long long* ring = ( long long* ) d.ring;
+  for ( int k = part; k < d.min_delay; k += G_PARTS )
+  {
+    const int slot = ( int ) ( ( origin + k + g.d ) % d.L );
+#pragma unroll
+    for ( int ty = 0; ty < 2; ++ty )  // excitatory, inhibitory draws
+    {
+      const unsigned c = s_cnt[ ty ][ k ][ ti ];
+      if ( c == 0u )
+        continue;
+      const int64_t idx = ( ( int64_t ) slot * d.C + ( ty ? g.ci : g.ce ) ) * d.N + t;
+      ring[ idx ] += ( long long ) c * ( long long ) ( ty ? g.wi : g.we );
+    }
+  }
 }
 
 }  // namespace ng

@@ -143,6 +143,7 @@ class NGStats(ctypes.Structure):
         ("update_launches", ctypes.c_int64),
         ("deliver_launches", ctypes.c_int64),
         ("simulate_ms", ctypes.c_double),
+        ("gather_slices", ctypes.c_int64),
     ]
 
 

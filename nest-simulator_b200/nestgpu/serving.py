@@ -176,6 +176,55 @@ def run_plain(requests, eng, clock=time.perf_counter, realtime=True):
     return order, {"makespan_s": makespan, "syn_events": ev, "syn_events_per_s": ev / makespan}
 
 
+def spike_stats(r):
+    """Mean rate [Hz] and mean CV of the inter-spike intervals (neurons with
+    at least 3 spikes) of a finished request."""
+    src, stamp = r.spikes
+    t_s = r.steps * H * 1e-3
+    rate = len(src) / (r.n * t_s)
+    if len(src) < 3:
+        return rate, float("nan")
+    o = np.lexsort((stamp, src))
+    s, t = src[o], stamp[o].astype(np.float64)
+    same = s[1:] == s[:-1]
+    isi = np.diff(t)[same]
+    who = s[1:][same]
+    cnt = np.bincount(who, minlength=r.n)
+    sm = np.bincount(who, weights=isi, minlength=r.n)
+    sq = np.bincount(who, weights=isi * isi, minlength=r.n)
+    ok = cnt >= 2
+    if not ok.any():
+        return rate, float("nan")
+    mu = sm[ok] / cnt[ok]
+    var = np.maximum(sq[ok] / cnt[ok] - mu * mu, 0.0)
+    return rate, float(np.mean(np.sqrt(var) / mu))
+
+
+def accuracy(test, ref):
+    """Rate and CV-ISI error of `test` (e.g. batched FP32) against `ref` (the
+    FP64 form) over the same requests: aggregate rate error (total spikes),
+    the median per-request rate error, and the mean and max absolute CV-ISI
+    difference."""
+    by_id = {r.rid: r for r in ref}
+    rel, dcv = [], []
+    tot_t = tot_r = 0
+    for r in test:
+        q = by_id[r.rid]
+        rt, ct = spike_stats(r)
+        rr, cr = spike_stats(q)
+        tot_t += len(r.spikes[0])
+        tot_r += len(q.spikes[0])
+        if rr > 0:
+            rel.append(abs(rt - rr) / rr)
+        if np.isfinite(ct) and np.isfinite(cr):
+            dcv.append(abs(ct - cr))
+    return {"rate_err_total": abs(tot_t - tot_r) / max(1, tot_r),
+            "rate_err_median": float(np.median(rel)) if rel else None,
+            "cv_isi_err_mean": float(np.mean(dcv)) if dcv else None,
+            "cv_isi_err_max": float(np.max(dcv)) if dcv else None,
+            "requests": len(test)}
+
+
 def latency_summary(requests):
     lat = np.array([r.latency for r in requests])
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),

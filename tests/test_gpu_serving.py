@@ -6,7 +6,8 @@
 - admission by footprint, capacity errors, and slot reuse;
 - device-drawn fixed_indegree graphs have the requested in-degrees;
 - device-drawn pairwise_bernoulli graphs have the requested statistics and
-  are read back through ng_net_get_connections.
+  are read back through ng_net_get_connections;
+- the per-target gather of the precision form equals the scatter.
 """
 
 import numpy as np
@@ -249,3 +250,35 @@ def test_get_connections_of_explicit_graph():
     np.testing.assert_array_equal(t[b], tgt[a])
     np.testing.assert_array_equal(ww[b], w[a])
     np.testing.assert_array_equal(dd[b], d[a])
+
+
+@pytest.mark.parametrize("frac", ["0", "0.03"])
+def test_gather_equals_scatter(monkeypatch, frac):
+    """The per-target gather (always on with fraction 0; switching per slice
+    with 0.03) gives the scatter's spikes and state bit for bit: both add the
+    same integers into the int64 rings."""
+    def run(env):
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        eng = serving.new_engine("fp32", capacity_neurons=100_000, capacity_edges=40_000_000, max_networks=8)
+        ids = [serving._admit(eng, _req(i, n, 1500, seed=500 + i, g=g, eta=eta))
+               for i, (n, g, eta) in enumerate(((4000, 3.5, 1.8), (7000, 5.0, 1.2), (2500, 6.0, 2.0)))]
+        eng.simulate(1500)
+        out = [(eng.net_spikes(i), eng.net_get_var(i, "V_m_rel", n)) for i, n in zip(ids, (4000, 7000, 2500))]
+        st = eng.stats()
+        eng.close()
+        for k in env:
+            monkeypatch.delenv(k)
+        return out, st
+
+    ref, st0 = run({"NG_GATHER": "0"})
+    got, st1 = run({"NG_GATHER_FRAC": frac})
+    assert st0["syn_events"] == st1["syn_events"]
+    assert st0["gather_slices"] == 0
+    assert st1["gather_slices"] > (250 if frac == "0" else 10)
+    for ((s0, t0), v0), ((s1, t1), v1) in zip(ref, got):
+        assert len(s0) > 100
+        o0, o1 = np.lexsort((s0, t0)), np.lexsort((s1, t1))
+        np.testing.assert_array_equal(s0[o0], s1[o1])
+        np.testing.assert_array_equal(t0[o0], t1[o1])
+        np.testing.assert_array_equal(v0, v1)
