@@ -448,6 +448,7 @@ struct ng_engine
     return alloc( ent, ( size_t ) ent_cap * sizeof( int4 ) );
   }
   int max_lanes = 32;             // 1: always one thread per neuron
+  int sub_lags = 8;               // lags whose inputs one thread gathers together (4 or 8)
   int64_t one_thread_min_n = 20000;  // block size from which one thread per neuron fills the GPU
 
   ~ng_engine()
@@ -746,6 +747,8 @@ struct ng_engine
       const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 127 ) / 128 );
       if ( span == 1 )
         k_update_iaf< Real, FIX, MODEL, 1 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
+      else if ( sub_lags == 4 )
+        k_update_iaf< Real, FIX, MODEL, 4 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
       else
         k_update_iaf< Real, FIX, MODEL, 8 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
     }
@@ -1313,6 +1316,8 @@ ng_create( const ng_config* cfg, ng_engine** out )
       return bail( rc );
     e->deliver_ctas = e->sms * e->deliver_per_sm;
   }
+  if ( const char* sl = std::getenv( "NG_UPDATE_SUB" ) )
+    e->sub_lags = std::atoi( sl ) == 4 ? 4 : 8;
   if ( const char* ml = std::getenv( "NG_MAX_LANES" ) )
   {
     const int v = std::atoi( ml );

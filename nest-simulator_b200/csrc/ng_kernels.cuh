@@ -322,56 +322,95 @@ cta_origin( const Net& d )
   return s_origin;
 }
 
-// Poisson drive value for neuron i at step t (generator step t - delay):
-// inversion over the neuron's precomputed CDF table (cdf[k] = P(X <= k)),
-// or, for tables too long to store, the walk from the mode.
-template < typename Real >
-__device__ __forceinline__ Real
-drive( const Net& d, int64_t i, long long t, long long& cnt )
+// Poisson drive of one neuron (generator step t - delay): inversion over
+// the neuron's precomputed CDF table (cdf[k] = P(X <= k)), or, for tables
+// too long to store, the walk from the mode.  The per-neuron constants are
+// loaded once per launch (drive_ctx): inside the lag loop the ring stores
+// would otherwise force every one of them to be re-read at every lag.
+struct DriveCtx
 {
+  const double* cdf;
+  double c[ 4 ];      // the first table entries (1.0 past the table's end)
+  double w;
+  long long t_off;    // global step -> network-local step
+  int n;              // table length; 0: no drive; -1: walk from the mode
+  int pd;             // delay [steps]
+  uint32_t il, k0, k1;
+  long long pair;     // generator-step pair of the cached draw (-1: none)
+  uint32_t o[ 4 ];    // its Philox words: (o0, o1) even step, (o2, o3) odd step
+};
+
+__device__ __forceinline__ void
+drive_ctx( const Net& d, int64_t i, DriveCtx& c )
+{
+  c.n = 0;
+  c.pair = -1;
   if ( !d.has_pois )
-    return Real( 0 );
-  const int2 tb = __ldg( d.pois_cdf_ref + i );
-  if ( tb.y == 0 )
-    return Real( 0 );
+    return;
   // counter = (neuron, generator step) in the network's local numbering,
   // key = the network's seed: a network draws the same drive wherever and
   // whenever it is placed
-  long long tl = t, il = i;
-  uint32_t k0 = d.key0, k1 = d.key1;
+  c.t_off = 0;
+  c.il = ( uint32_t ) i;
+  c.k0 = d.key0;
+  c.k1 = d.key1;
+  int id = 0;
   if ( d.nid )
   {
-    const int id = d.nid[ i ];
-    const uint2 kk = d.net_key[ id ];
-    tl = t - d.net_step0[ id ];
-    il = i - d.net_off[ id ];
-    k0 = kk.x;
-    k1 = kk.y;
+    id = d.nid[ i ];
+    if ( id < 0 )
+      return;  // a free neuron of a serving engine
   }
-  const long long tg = tl - __ldg( d.pois_d + i );
+  const int2 tb = __ldg( d.pois_cdf_ref + i );
+  c.n = tb.y;
+  if ( tb.y == 0 )
+    return;
+  if ( d.nid )
+  {
+    const uint2 kk = d.net_key[ id ];
+    c.t_off = d.net_step0[ id ];
+    c.il = ( uint32_t ) ( i - d.net_off[ id ] );
+    c.k0 = kk.x;
+    c.k1 = kk.y;
+  }
+  c.pd = __ldg( d.pois_d + i );
+  c.w = __ldg( d.pois_w + i );
+  c.cdf = d.pois_cdf + tb.x;
+#pragma unroll
+  for ( int q = 0; q < 4; ++q )
+    c.c[ q ] = q < tb.y ? __ldg( c.cdf + q ) : 1.0;
+}
+
+// One Philox4x32-10 block serves two generator steps: counter (neuron,
+// tg >> 1, DRIVE_STREAM), words (o0, o1) for the even step and (o2, o3) for
+// the odd one, each turned into a 53-bit uniform.
+template < typename Real >
+__device__ __forceinline__ Real
+drive_at( const Net& d, DriveCtx& c, int64_t i, long long t, long long& cnt )
+{
+  if ( c.n == 0 )
+    return Real( 0 );
+  const long long tg = t - c.t_off - c.pd;
   if ( !( d.pois_start < tg && tg <= d.pois_stop ) || tg < 0 )
     return Real( 0 );
-  uint32_t o[ 4 ];
-  philox4x32_10( ( uint32_t ) il, ( uint32_t ) tg, ( uint32_t ) ( ( unsigned long long ) tg >> 32 ), DRIVE_STREAM,
-    k0, k1, o );
-  const double u = u53( o[ 0 ], o[ 1 ] );
-  long long k;
-  if ( tb.y > 0 )
+  const long long tp = tg >> 1;
+  if ( tp != c.pair )
   {
-    // j = first index with u <= cdf[j] (or the last one); the first 4
-    // entries are loaded together instead of one dependent load per step
-    const double* cdf = d.pois_cdf + tb.x;
-    const int n = tb.y;
-    double c[ 4 ];
-#pragma unroll
-    for ( int q = 0; q < 4; ++q )
-      c[ q ] = q < n ? __ldg( cdf + q ) : 1.0;
+    philox4x32_10( c.il, ( uint32_t ) tp, ( uint32_t ) ( ( unsigned long long ) tp >> 32 ), DRIVE_STREAM, c.k0, c.k1,
+      c.o );
+    c.pair = tp;
+  }
+  const double u = ( tg & 1 ) ? u53( c.o[ 2 ], c.o[ 3 ] ) : u53( c.o[ 0 ], c.o[ 1 ] );
+  long long k;
+  if ( c.n > 0 )
+  {
+    // j = first index with u <= cdf[j] (or the last one)
     int j = 0;
 #pragma unroll
     for ( int q = 0; q < 4; ++q )
-      if ( j == q && q < n - 1 && u > c[ q ] )
+      if ( j == q && q < c.n - 1 && u > c.c[ q ] )
         j = q + 1;
-    while ( j >= 4 && j < n - 1 && u > __ldg( cdf + j ) )
+    while ( j >= 4 && j < c.n - 1 && u > __ldg( c.cdf + j ) )
       ++j;
     k = j;
   }
@@ -382,28 +421,44 @@ drive( const Net& d, int64_t i, long long t, long long& cnt )
   cnt += k;
   if ( k <= 0 )
     return Real( 0 );
-  return ( Real ) ( __ldg( d.pois_w + i ) * ( double ) k );
+  return ( Real ) ( c.w * ( double ) k );
+}
+
+// Ring cell of (slot, channel, neuron): read it, then, separately and only
+// after the value has been used, clear it.  A load followed at once by a
+// store to the same address makes the store wait for the load, and the
+// next lag's loads behind it: the reads of a slice's lags would run one
+// round trip at a time.
+template < bool FIX >
+struct RingVal
+{
+  using type = typename std::conditional< FIX, long long, double >::type;
+};
+
+template < bool FIX >
+__device__ __forceinline__ typename RingVal< FIX >::type
+ring_ld( const Net& d, int slot, int ch, int64_t i )
+{
+  const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + i;
+  return reinterpret_cast< const typename RingVal< FIX >::type* >( d.ring )[ idx ];
 }
 
 template < typename Real, bool FIX >
 __device__ __forceinline__ Real
-ring_take( const Net& d, int slot, int ch, int64_t i )
+ring_real( const Net& d, typename RingVal< FIX >::type v )
+{
+  if constexpr ( FIX )
+    return ( Real ) ( ( double ) v * d.fx_inv );
+  else
+    return ( Real ) v;
+}
+
+template < bool FIX >
+__device__ __forceinline__ void
+ring_clear( const Net& d, int slot, int ch, int64_t i )
 {
   const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + i;
-  if constexpr ( FIX )
-  {
-    long long* ring = ( long long* ) d.ring;
-    const long long v = ring[ idx ];
-    ring[ idx ] = 0;
-    return ( Real ) ( ( double ) v * d.fx_inv );
-  }
-  else
-  {
-    double* ring = ( double* ) d.ring;
-    const double v = ring[ idx ];
-    ring[ idx ] = 0.0;
-    return ( Real ) v;
-  }
+  reinterpret_cast< typename RingVal< FIX >::type* >( d.ring )[ idx ] = 0;
 }
 
 // vals[slot] holds the model's state variables in slot order.
@@ -547,6 +602,10 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
     }
     r = b.r[ li ];
   }
+  DriveCtx dc;
+  dc.n = 0;
+  if ( act )
+    drive_ctx( d, i, dc );
   long long dcnt = 0;
   // SUB: lags whose inputs are gathered before the recurrence runs over them
   // (8; 1 for slices of one step, where the unrolled code would only cost
@@ -559,40 +618,26 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
     unsigned smask = 0;
     for ( int sb = 0; sb < nl; sb += SUB )
     {
-      // inputs of up to SUB lags: independent loads and draws, overlapped
-      Real in_ex[ SUB ], in_in[ SUB ];
+      // inputs of up to SUB lags: the ring reads and drive draws of all of
+      // them issued before any is used
+      typename RingVal< FIX >::type raw_ex[ SUB ], raw_in[ SUB ];
+      Real dvs[ SUB ];
 #pragma unroll
       for ( int q = 0; q < SUB; ++q )
       {
-        in_ex[ q ] = Real( 0 );
-        in_in[ q ] = Real( 0 );
+        raw_ex[ q ] = 0;
+        raw_in[ q ] = 0;
+        dvs[ q ] = Real( 0 );
         const int k = sb + q;
         if ( act && k < nl && t0 + k < until )
         {
           int slot = slot0 + k;
           if ( slot >= d.L )
             slot -= d.L;
-          Real ex = ring_take< Real, FIX >( d, slot, 0, i );
-          Real inh = 0;
+          raw_ex[ q ] = ring_ld< FIX >( d, slot, 0, i );
           if constexpr ( EXP )
-            inh = ring_take< Real, FIX >( d, slot, 1, i );
-          const Real dv = drive< Real >( d, i, t0 + k, dcnt );
-          if ( dv != Real( 0 ) )
-          {
-            if constexpr ( EXP )
-            {
-              if ( dv > Real( 0 ) )
-                ex = ex + dv;
-              else
-                inh = inh + dv;
-            }
-            else
-            {
-              ex = ex + dv;
-            }
-          }
-          in_ex[ q ] = ex;
-          in_in[ q ] = inh;
+            raw_in[ q ] = ring_ld< FIX >( d, slot, 1, i );
+          dvs[ q ] = drive_at< Real >( d, dc, i, t0 + k, dcnt );
         }
       }
       // the recurrence over these lags, in order
@@ -602,6 +647,23 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
         const int k = sb + q;
         if ( !act || k >= nl || t0 + k >= until )
           continue;
+        Real ex = ring_real< Real, FIX >( d, raw_ex[ q ] );
+        Real inh = EXP ? ring_real< Real, FIX >( d, raw_in[ q ] ) : Real( 0 );
+        const Real dv = dvs[ q ];
+        if ( dv != Real( 0 ) )
+        {
+          if constexpr ( EXP )
+          {
+            if ( dv > Real( 0 ) )
+              ex = ex + dv;
+            else
+              inh = inh + dv;
+          }
+          else
+          {
+            ex = ex + dv;
+          }
+        }
         bool spk = false;
         if constexpr ( EXP )
         {
@@ -612,8 +674,8 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
           x1 *= c4;
           x2 *= c5;
           x1 += c9 * i1;
-          x1 += in_ex[ q ];
-          x2 += in_in[ q ];
+          x1 += ex;
+          x2 += inh;
           if ( V >= Vth )
           {
             r = refr;
@@ -627,7 +689,7 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
         {
           if ( r == 0 )
           {
-            V = c1 * ( x1 + Ie ) + c0 * V + in_ex[ q ];
+            V = c1 * ( x1 + Ie ) + c0 * V + ex;
             V = ( V < c2 ? c2 : V );
           }
           else
@@ -657,6 +719,21 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
             const double vals[ 3 ] = { ( double ) V, ( double ) x1, ( double ) Ie };
             trace_put( d, i, t0 + k + 1, vals );
           }
+        }
+      }
+      // clear the cells read (their loads have completed)
+#pragma unroll
+      for ( int q = 0; q < SUB; ++q )
+      {
+        const int k = sb + q;
+        if ( act && k < nl && t0 + k < until )
+        {
+          int slot = slot0 + k;
+          if ( slot >= d.L )
+            slot -= d.L;
+          ring_clear< FIX >( d, slot, 0, i );
+          if constexpr ( EXP )
+            ring_clear< FIX >( d, slot, 1, i );
         }
       }
     }
@@ -758,29 +835,65 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
     }
     r = b.r[ li ];
   }
+  // phase 1 items j = threadIdx.x + m * 256 all belong to neuron nb0 + (threadIdx.x & 31)
+  DriveCtx dc;
+  dc.n = 0;
+  if ( nb0 + ( threadIdx.x & 31 ) < b.n )
+    drive_ctx( d, b.off + nb0 + ( threadIdx.x & 31 ), dc );
   long long dcnt = 0;
   for ( int cb = from; cb < to; cb += P2_CH )
   {
     const int nl = min( P2_CH, to - cb );
     const long long t0 = origin + cb;
     const int slot0 = ( int ) ( t0 % d.L );
-    // ---- phase 1: inputs of (neuron q, lag k), item j = k * 32 + q
-    for ( int j = threadIdx.x; j < nl * P2_NB; j += blockDim.x )
+    // ---- phase 1: inputs of (neuron q, lag k), item j = k * 32 + q; a
+    // thread's items j = threadIdx.x + m * 256 (m < 4): all ring reads and
+    // draws first, then their use, then the clears
+    constexpr int P1_MAX = P2_CH * P2_NB / 256;
+    typename RingVal< FIX >::type rex[ P1_MAX ], rin[ P1_MAX ];
+    Real dvs[ P1_MAX ];
+    int slots[ P1_MAX ];
+#pragma unroll
+    for ( int m = 0; m < P1_MAX; ++m )
     {
+      const int j = threadIdx.x + m * 256;
+      rex[ m ] = 0;
+      rin[ m ] = 0;
+      dvs[ m ] = Real( 0 );
+      slots[ m ] = -1;
+      if ( j < nl * P2_NB )
+      {
+        const int k = j >> 5;
+        const int64_t lq = nb0 + ( j & 31 );
+        if ( lq < b.n && t0 + k < active_until( d, b.off + lq ) )
+        {
+          const int64_t iq = b.off + lq;
+          int slot = slot0 + k;
+          if ( slot >= d.L )
+            slot -= d.L;
+          slots[ m ] = slot;
+          rex[ m ] = ring_ld< FIX >( d, slot, 0, iq );
+          if constexpr ( EXP )
+            rin[ m ] = ring_ld< FIX >( d, slot, 1, iq );
+          dvs[ m ] = drive_at< Real >( d, dc, iq, t0 + k, dcnt );
+        }
+      }
+    }
+#pragma unroll
+    for ( int m = 0; m < P1_MAX; ++m )
+    {
+      const int j = threadIdx.x + m * 256;
+      if ( j >= nl * P2_NB )
+        continue;
       const int k = j >> 5;
       const int q = j & 31;
-      const int64_t lq = nb0 + q;
       Real ex = 0, inh = 0;
-      if ( lq < b.n && t0 + k < active_until( d, b.off + lq ) )
+      if ( slots[ m ] >= 0 )
       {
-        const int64_t iq = b.off + lq;
-        int slot = slot0 + k;
-        if ( slot >= d.L )
-          slot -= d.L;
-        ex = ring_take< Real, FIX >( d, slot, 0, iq );
+        ex = ring_real< Real, FIX >( d, rex[ m ] );
         if constexpr ( EXP )
-          inh = ring_take< Real, FIX >( d, slot, 1, iq );
-        const Real dv = drive< Real >( d, iq, t0 + k, dcnt );
+          inh = ring_real< Real, FIX >( d, rin[ m ] );
+        const Real dv = dvs[ m ];
         if ( dv != Real( 0 ) )
         {
           if constexpr ( EXP )
@@ -799,6 +912,16 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
       s_ex[ k ][ q ] = ex;
       if constexpr ( EXP )
         s_in[ k ][ q ] = inh;
+    }
+#pragma unroll
+    for ( int m = 0; m < P1_MAX; ++m )
+    {
+      if ( slots[ m ] < 0 )
+        continue;
+      const int64_t iq = b.off + nb0 + ( ( threadIdx.x + m * 256 ) & 31 );
+      ring_clear< FIX >( d, slots[ m ], 0, iq );
+      if constexpr ( EXP )
+        ring_clear< FIX >( d, slots[ m ], 1, iq );
     }
     __syncthreads();
     // ---- phase 2: the recurrence, one lane per neuron
@@ -1041,6 +1164,10 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
     r = b.r[ li ];
     hs = b.istep[ li ];
   }
+  DriveCtx dc;
+  dc.n = 0;
+  if ( act )
+    drive_ctx( d, i, dc );
   long long t = origin + from;
   int slot = ( int ) ( t % d.L );
   long long dcnt = 0;
@@ -1049,6 +1176,13 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
   {
     int mult = 0;
     const bool live = act && t < until;
+    // this lag's ring cells, read before the integration so the loads overlap it
+    typename RingVal< FIX >::type rex = 0, rin = 0;
+    if ( live && !unstable )
+    {
+      rex = ring_ld< FIX >( d, slot, 0, i );
+      rin = ring_ld< FIX >( d, slot, 1, i );
+    }
     if ( live && !unstable )
     {
       double tt = 0.0;
@@ -1105,9 +1239,11 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
       }
       if ( r > 0 )
         --r;
-      Real ex = ring_take< Real, FIX >( d, slot, 0, i );
-      Real inh = ring_take< Real, FIX >( d, slot, 1, i );
-      const Real dv = drive< Real >( d, i, t, dcnt );
+      Real ex = ring_real< Real, FIX >( d, rex );
+      Real inh = ring_real< Real, FIX >( d, rin );
+      ring_clear< FIX >( d, slot, 0, i );
+      ring_clear< FIX >( d, slot, 1, i );
+      const Real dv = drive_at< Real >( d, dc, i, t, dcnt );
       if ( dv != Real( 0 ) )
       {
         if ( dv > Real( 0 ) )

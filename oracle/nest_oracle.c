@@ -867,7 +867,9 @@ imod( int64_t a, int64_t m )
   return r < 0 ? r + m : r;
 }
 
-/* drive value for neuron i at step t (generator step t - d) */
+/* drive value for neuron i at step t (generator step tg = t - d): one
+ * Philox4x32-10 block per pair of generator steps, counter (i, tg >> 1,
+ * DRIVE_STREAM); words 0-1 serve the even step, words 2-3 the odd one */
 static inline double
 drive( const orc_net* net, int64_t i, int64_t t )
 {
@@ -876,10 +878,12 @@ drive( const orc_net* net, int64_t i, int64_t t )
   const int64_t tg = t - net->pois_d[ i ];
   if ( !( net->pois_start < tg && tg <= net->pois_stop ) || tg < 0 )
     return 0.0;
-  const uint32_t ctr[ 4 ] = { ( uint32_t ) i, ( uint32_t ) tg, ( uint32_t ) ( ( uint64_t ) tg >> 32 ), DRIVE_STREAM };
+  const int64_t tp = tg >> 1;
+  const uint32_t ctr[ 4 ] = { ( uint32_t ) i, ( uint32_t ) tp, ( uint32_t ) ( ( uint64_t ) tp >> 32 ), DRIVE_STREAM };
   uint32_t o[ 4 ];
   orc_philox4x32( ctr, net->key, 10, o );
-  const int64_t k = pois_draw( &net->pois[ i ], u53( o[ 0 ], o[ 1 ] ) );
+  const double u = ( tg & 1 ) ? u53( o[ 2 ], o[ 3 ] ) : u53( o[ 0 ], o[ 1 ] );
+  const int64_t k = pois_draw( &net->pois[ i ], u );
   return k > 0 ? net->pois_w[ i ] * ( double ) k : 0.0;
 }
 
