@@ -84,6 +84,8 @@ typedef struct
   int64_t deliver_launches;
   double simulate_ms;        /* host wall time inside ng_simulate */
   int64_t gather_slices;     /* serving, FP32 form: (network, slice) pairs delivered by the per-target gather */
+  double wait_ms;            /* host time waiting for the device at the end of a group */
+  double drain_ms;           /* host time draining spike logs and trace rows */
 } ng_stats;
 
 /* Version of this ABI (NG_ABI_VERSION). */
@@ -269,7 +271,8 @@ int ng_net_add( ng_engine* eng, const ng_net_desc* desc, int32_t* net_id );
 /* Steps simulated so far and whether the network has reached its duration. */
 int ng_net_poll( ng_engine* eng, int32_t net_id, int64_t* steps_done, int32_t* finished );
 
-/* Drain the network's logged spikes: local neuron index and local stamp. */
+/* Drain the network's logged spikes: local neuron index and local stamp (at
+ * most cap of them; source == NULL: *n_out = the number held, nothing drained). */
 int ng_net_spikes( ng_engine* eng, int32_t net_id, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out );
 
 /* Read a state variable of the network's neurons (length n). */

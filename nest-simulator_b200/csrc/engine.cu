@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <new>
 
 #include "../../include/nestgpu.h"
 #include "ng_kernels.cuh"
@@ -243,7 +244,11 @@ struct ng_engine
   int64_t trace_first_stamp = -1;
   int64_t next_trace_stamp_row = 0;  // absolute row index (stamp / interval) of the next row expected
 
-  Ctl* host_ctl = nullptr;  // pinned
+  Ctl* host_ctl = nullptr;  // pinned, one per log half
+  cudaEvent_t group_done[ 2 ] = { nullptr, nullptr };
+  cudaStream_t copy_stream = nullptr;
+  uint2* pinned_log = nullptr;
+  size_t pinned_log_bytes = 0;
   ng_stats stats {};
   int profiling = 0;
   int graph_slices = 0;
@@ -269,6 +274,48 @@ struct ng_engine
   bool serving = false;
   DevBuf d_nid, d_step0, d_until, d_off, d_key, sc_src, sc_cnt, sc_fill, sc_beg, sc_plen, sc_total, sc_sb;
   std::vector< int32_t > nid_host;
+  // Spikes of a serving network, kept on the host in fixed-size chunks
+  // recycled through a free list (growing one array would copy and
+  // re-fault every page on each reallocation).
+  static constexpr size_t SPIKE_CHUNK = 1 << 18;
+  struct SpikeChunk
+  {
+    int32_t* src = nullptr;
+    int64_t* stamp = nullptr;
+    size_t n = 0;
+  };
+  std::vector< SpikeChunk > free_chunks;
+
+  SpikeChunk
+  new_chunk()
+  {
+    if ( !free_chunks.empty() )
+    {
+      SpikeChunk c = free_chunks.back();
+      free_chunks.pop_back();
+      c.n = 0;
+      return c;
+    }
+    SpikeChunk c;
+    c.src = static_cast< int32_t* >( std::malloc( SPIKE_CHUNK * sizeof( int32_t ) ) );
+    c.stamp = static_cast< int64_t* >( std::malloc( SPIKE_CHUNK * sizeof( int64_t ) ) );
+    if ( !c.src || !c.stamp )
+    {
+      std::free( c.src );
+      std::free( c.stamp );
+      throw std::bad_alloc();
+    }
+    return c;
+  }
+
+  void
+  release_chunks( std::vector< SpikeChunk >& cs )
+  {
+    for ( auto& c : cs )
+      free_chunks.push_back( c );
+    cs.clear();
+  }
+
   struct NetInfo
   {
     bool used = false;
@@ -276,14 +323,15 @@ struct ng_engine
     int64_t g0 = -1, gn = 0;  // gather table run
     bool rec = false;
     double log_rate = 0.0;
-    std::vector< int32_t > src;
-    std::vector< int64_t > stamp;
+    std::vector< SpikeChunk > chunks;  // logged spikes, in order
+    int64_t held = 0;                  // spikes held in the chunks
+    size_t first_off = 0;              // entries of chunks[0] already drained
   };
   std::vector< NetInfo > nets;
   std::map< int64_t, int64_t > free_neurons, free_edges;  // run start -> length
   // per-target gather of fixed_indegree networks (precision form)
   bool gather_on = false;
-  float gather_frac = 0.15f;
+  float gather_frac = 0.08f;
   DevBuf gmask, gin, net_g, net_mode, net_spk;
   std::map< int64_t, int64_t > free_gin;
   std::vector< GatherNet > host_g;
@@ -378,14 +426,16 @@ struct ng_engine
     free_edges.clear();
     free_neurons[ 0 ] = N;
     free_edges[ 0 ] = E;
-    // per-target gather: precision form, current-based models, slices of at most 32 steps
-    gather_on = prec != NG_FP64 && b.model != NG_AEIF_COND_ALPHA && cfg.min_delay <= 32;
+    // per-target gather: precision form, current-based models, slices of at most 16 steps
+    gather_on = prec != NG_FP64 && b.model != NG_AEIF_COND_ALPHA && cfg.min_delay <= 16 && nmax <= 1024;
     if ( const char* ge = std::getenv( "NG_GATHER" ) )
       gather_on = gather_on && std::atoi( ge ) != 0;
     if ( const char* gf = std::getenv( "NG_GATHER_FRAC" ) )
       gather_frac = ( float ) std::atof( gf );
     if ( gather_on )
     {
+      if ( cudaFuncSetAttribute( k_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, ( int ) G_SMEM ) != cudaSuccess )
+        return fail( NG_ERR_CUDA, "serving: cannot reserve shared memory for the per-target gather" );
       if ( ( rc = alloc( gmask, ( size_t ) N * 4 ) ) || ( rc = alloc( gin, ( size_t ) E * 2 ) )
         || ( rc = alloc( net_g, ( size_t ) nmax * sizeof( GatherNet ) ) ) || ( rc = alloc( net_mode, ( size_t ) nmax * 4 ) )
         || ( rc = alloc( net_spk, ( size_t ) nmax * 4 ) ) )
@@ -465,11 +515,27 @@ struct ng_engine
       cudaFree( b.ctab.p );
     }
     DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
-      &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl };
+      &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl, &d_nid, &d_step0, &d_until, &d_off,
+      &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
+      &net_spk };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
       cudaFreeHost( host_ctl );
+    if ( pinned_log )
+      cudaFreeHost( pinned_log );
+    for ( auto& nw : nets )
+      release_chunks( nw.chunks );
+    for ( auto& c : free_chunks )
+    {
+      std::free( c.src );
+      std::free( c.stamp );
+    }
+    for ( auto& ev : group_done )
+      if ( ev )
+        cudaEventDestroy( ev );
+    if ( copy_stream )
+      cudaStreamDestroy( copy_stream );
     if ( ev0 )
       cudaEventDestroy( ev0 );
     if ( ev1 )
@@ -782,7 +848,7 @@ struct ng_engine
   launch_deliver( const Net& d )
   {
     if ( gather_on )
-      k_gather<<< ( unsigned ) ( ( N + G_TGT - 1 ) / G_TGT ), G_TGT * G_PARTS, 0, stream >>>( d );
+      k_gather<<< ( unsigned ) sms, G_THREADS, G_SMEM, stream >>>( d );
     const unsigned grid = ( unsigned ) deliver_ctas;
     if ( prec == NG_FP64 )
       k_deliver< false ><<< grid, 256, 0, stream >>>( d );
@@ -1000,61 +1066,127 @@ struct ng_engine
   bool log_bound_dirty = true;
 
   // one group: set ctl, enqueue, sync, drain
-  int
-  run_group( int64_t n )
+  // A group of steps runs on the device while the host drains the previous
+  // group's spike log: the groups alternate between the two log halves.
+  struct GroupInfo
   {
-    const int64_t clock = origin + from;
-    const int64_t row0 = ( clock + 1 + trace_interval - 1 ) / trace_interval;
-    k_set_ctl<<< 1, 1, 0, stream >>>( ( Ctl* ) ctl.p, clock, row0, 1 );
+    int64_t clock = 0, row0 = 0, end = 0;
+  };
+
+  int
+  launch_group( int64_t n, int sel, GroupInfo& gi )
+  {
+    gi.clock = origin + from;
+    gi.row0 = ( gi.clock + 1 + trace_interval - 1 ) / trace_interval;
+    k_set_ctl<<< 1, 1, 0, stream >>>( ( Ctl* ) ctl.p, gi.clock, gi.row0, 1, sel );
     CU( cudaGetLastError() );
     int rc = enqueue_steps( n );
     if ( rc )
       return rc;
-    CU( cudaMemcpyAsync( host_ctl, ctl.p, sizeof( Ctl ), cudaMemcpyDeviceToHost, stream ) );
-    CU( cudaStreamSynchronize( stream ) );
-    const Ctl& c = *host_ctl;
+    gi.end = origin + from;
+    CU( cudaMemcpyAsync( host_ctl + sel, ctl.p, sizeof( Ctl ), cudaMemcpyDeviceToHost, stream ) );
+    CU( cudaEventRecord( group_done[ sel ], stream ) );
+    return NG_OK;
+  }
+
+  int
+  grow_pinned( size_t bytes )
+  {
+    if ( bytes <= pinned_log_bytes )
+      return NG_OK;
+    if ( pinned_log )
+      cudaFreeHost( pinned_log );
+    pinned_log = nullptr;
+    pinned_log_bytes = 0;
+    if ( cudaMallocHost( &pinned_log, bytes ) != cudaSuccess )
+      return fail( NG_ERR_MEMORY, "cannot allocate pinned host memory for the spike log" );
+    pinned_log_bytes = bytes;
+    return NG_OK;
+  }
+
+  int
+  drain_group( int sel, const GroupInfo& gi )
+  {
+    const auto w0 = std::chrono::steady_clock::now();
+    CU( cudaEventSynchronize( group_done[ sel ] ) );
+    const auto w1 = std::chrono::steady_clock::now();
+    stats.wait_ms += std::chrono::duration< double, std::milli >( w1 - w0 ).count();
+    struct Tally
+    {
+      ng_stats& st;
+      std::chrono::steady_clock::time_point t;
+      ~Tally()
+      {
+        st.drain_ms += std::chrono::duration< double, std::milli >( std::chrono::steady_clock::now() - t ).count();
+      }
+    } tally { stats, w1 };
+    const Ctl& c = host_ctl[ sel ];
     if ( c.err & ERR_NUMERIC )
       return fail( NG_ERR_NUMERIC, "NumericalInstability: aeif_cond_alpha state exploded (V_m < -1e3 or |w| > 1e6)" );
     if ( c.err & ( ERR_SPIKE_LIST | ERR_LOG | ERR_TRACE ) )
       return fail( NG_ERR_CAPACITY, "device spike list, spike log or trace buffer overflowed (err word "
           + std::to_string( c.err ) + ")" );
-    // drain the spike log
     const int64_t nl = ( int64_t ) c.log_count;
     if ( nl > 0 )
     {
-      std::vector< uint2 > tmp( ( size_t ) nl );
-      CU( cudaMemcpy( tmp.data(), log.p, sizeof( uint2 ) * ( size_t ) nl, cudaMemcpyDeviceToHost ) );
-      for ( const uint2& e : tmp )
+      int rc = grow_pinned( ( size_t ) nl * sizeof( uint2 ) );
+      if ( rc )
+        return rc;
+      // the copy engine fetches this half while the next group computes
+      CU( cudaMemcpyAsync( pinned_log, ( uint2* ) log.p + ( sel ? log_cap : 0 ), sizeof( uint2 ) * ( size_t ) nl,
+        cudaMemcpyDeviceToHost, copy_stream ) );
+      CU( cudaStreamSynchronize( copy_stream ) );
+      const uint2* ent = pinned_log;
+      if ( serving )
       {
-        const uint32_t mult = e.y >> 24;
-        const int64_t stamp = clock + ( int64_t ) ( e.y & 0xFFFFFFu );
-        if ( serving )
+        for ( int64_t k = 0; k < nl; ++k )
         {
-          const int32_t id = nid_host[ e.x ];
-          if ( id >= 0 && nets[ id ].used )
+          const uint32_t id = ent[ k ].x >> LOG_ID_SHIFT;
+          if ( id >= nets.size() )
+            return fail( NG_ERR_STATE, "spike log entry " + std::to_string( k ) + " of " + std::to_string( nl )
+                + " names network " + std::to_string( id ) + " (word " + std::to_string( ent[ k ].x ) + ", "
+                + std::to_string( ent[ k ].y ) + ")" );
+          NetInfo& nw = nets[ id ];
+          if ( !nw.used )
+            continue;
+          const int32_t src = ( int32_t ) ( ent[ k ].x & ( ( 1u << LOG_ID_SHIFT ) - 1u ) );
+          const int64_t stamp = gi.clock + ( int64_t ) ( ent[ k ].y & 0xFFFFFFu ) - nw.step0;
+          for ( uint32_t m = ent[ k ].y >> 24; m > 0; --m )
           {
-            NetInfo& nw = nets[ id ];
-            for ( uint32_t m = 0; m < mult; ++m )
-            {
-              nw.src.push_back( ( int32_t ) ( e.x - nw.off ) );
-              nw.stamp.push_back( stamp - nw.step0 );
-            }
+            if ( nw.chunks.empty() || nw.chunks.back().n == SPIKE_CHUNK )
+              nw.chunks.push_back( new_chunk() );
+            SpikeChunk& c = nw.chunks.back();
+            c.src[ c.n ] = src;
+            c.stamp[ c.n ] = stamp;
+            ++c.n;
+            ++nw.held;
           }
-          continue;
         }
-        for ( uint32_t m = 0; m < mult; ++m )
+      }
+      else
+      {
+        int64_t tot = 0;
+        for ( int64_t k = 0; k < nl; ++k )
+          tot += ent[ k ].y >> 24;
+        size_t p = out_src.size();
+        out_src.resize( p + ( size_t ) tot );
+        out_stamp.resize( p + ( size_t ) tot );
+        for ( int64_t k = 0; k < nl; ++k )
         {
-          out_src.push_back( ( int32_t ) e.x );
-          out_stamp.push_back( stamp );
+          const int64_t stamp = gi.clock + ( int64_t ) ( ent[ k ].y & 0xFFFFFFu );
+          for ( uint32_t m = ent[ k ].y >> 24; m > 0; --m, ++p )
+          {
+            out_src[ p ] = ( int32_t ) ent[ k ].x;
+            out_stamp[ p ] = stamp;
+          }
         }
       }
     }
-    // drain the trace rows of this group
+    // the trace rows of this group (tracing runs the groups one at a time)
     if ( n_trace_idx > 0 )
     {
-      const int64_t end = origin + from;
-      const int64_t row_end = end / trace_interval;  // last complete row index
-      const int64_t rows = row_end - row0 + 1;
+      const int64_t row_end = gi.end / trace_interval;  // last complete row index
+      const int64_t rows = row_end - gi.row0 + 1;
       if ( rows > 0 )
       {
         const size_t cnt = ( size_t ) rows * ( size_t ) n_trace_idx * ( size_t ) n_trace_vars;
@@ -1062,7 +1194,7 @@ struct ng_engine
         out_trace.resize( old + cnt );
         CU( cudaMemcpy( out_trace.data() + old, trace.p, cnt * sizeof( double ), cudaMemcpyDeviceToHost ) );
         if ( trace_first_stamp < 0 )
-          trace_first_stamp = row0 * trace_interval;
+          trace_first_stamp = gi.row0 * trace_interval;
       }
     }
     stats.spikes = ( int64_t ) c.n_spikes;
@@ -1093,14 +1225,42 @@ struct ng_engine
     const int64_t chunk = graph_slices > 0 ? ( int64_t ) graph_slices * cfg.min_delay : cfg.min_delay;
     if ( gmax > chunk )
       gmax = ( gmax / chunk ) * chunk;
+    // groups alternate between the log halves; the host drains one group
+    // while the device runs the next (one at a time when tracing).  A call
+    // is cut into at least 4 groups where it is long enough, so only the
+    // last quarter's drain is not hidden behind device work.
+    const bool overlap = n_trace_idx == 0;
+    if ( overlap && graph_slices >= 16 )
+    {
+      const int64_t q = 16 * ( int64_t ) cfg.min_delay;
+      const int64_t quarter = ( ( n / 4 + q - 1 ) / q ) * q;
+      if ( quarter >= q && quarter < gmax )
+        gmax = quarter;
+    }
+    int pending = -1;
+    GroupInfo gi[ 2 ];
     while ( n > 0 )
     {
       const int64_t g = std::min( n, gmax );
-      rc = run_group( g );
+      const int sel = pending == 0 ? 1 : 0;
+      rc = launch_group( g, sel, gi[ sel ] );
+      if ( rc == NG_OK && pending >= 0 )
+        rc = drain_group( pending, gi[ pending ] );
+      pending = sel;
+      if ( rc == NG_OK && !overlap )
+      {
+        rc = drain_group( pending, gi[ pending ] );
+        pending = -1;
+      }
       if ( rc )
+      {
+        cudaStreamSynchronize( stream );
         return rc;
+      }
       n -= g;
     }
+    if ( pending >= 0 && ( rc = drain_group( pending, gi[ pending ] ) ) )
+      return rc;
     stats.clock_steps = origin + from;
     stats.slices = slices;
     stats.simulate_ms += std::chrono::duration< double, std::milli >( std::chrono::steady_clock::now() - t0 ).count();
@@ -1206,9 +1366,13 @@ ng_create( const ng_config* cfg, ng_engine** out )
   e->stream = e->own;
   cudaEventCreate( &e->ev0 );
   cudaEventCreate( &e->ev1 );
-  if ( cudaMallocHost( &e->host_ctl, sizeof( Ctl ) ) != cudaSuccess )
+  if ( cudaMallocHost( &e->host_ctl, 2 * sizeof( Ctl ) ) != cudaSuccess )
     return bail( fail( NG_ERR_MEMORY, "cudaMallocHost failed" ) );
-  std::memset( e->host_ctl, 0, sizeof( Ctl ) );
+  std::memset( e->host_ctl, 0, 2 * sizeof( Ctl ) );
+  if ( cudaEventCreateWithFlags( &e->group_done[ 0 ], cudaEventDisableTiming ) != cudaSuccess
+    || cudaEventCreateWithFlags( &e->group_done[ 1 ], cudaEventDisableTiming ) != cudaSuccess
+    || cudaStreamCreateWithFlags( &e->copy_stream, cudaStreamNonBlocking ) != cudaSuccess )
+    return bail( fail( NG_ERR_CUDA, "ng_create: event or stream creation failed" ) );
   int64_t off = 0;
   for ( int k = 0; k < cfg->n_blocks; ++k )
   {
@@ -1284,7 +1448,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
   e->log_cap = cfg->spike_log_capacity > 0 ? cfg->spike_log_capacity
                                            : std::max< int64_t >( 1 << 22, 64 * e->n_src );
   e->log_cap = std::min< int64_t >( e->log_cap, 1ll << 28 );
-  if ( ( rc = e->alloc( e->log, ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
+  if ( ( rc = e->alloc( e->log, 2 * ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
     return bail( rc );
   if ( ( rc = e->alloc( e->rec, ( size_t ) e->n_src ) ) )
     return bail( rc );
@@ -1309,9 +1473,10 @@ ng_create( const ng_config* cfg, ng_engine** out )
   }
   if ( cfg->serving )
   {
-    if ( cfg->n_blocks != 1 || cfg->n_generators != 0 || cfg->edge_capacity < 4 || cfg->max_networks < 1 )
+    if ( cfg->n_blocks != 1 || cfg->n_generators != 0 || cfg->edge_capacity < 4 || cfg->max_networks < 1
+      || cfg->max_networks > ( 1 << ( 32 - LOG_ID_SHIFT ) ) )
       return bail( fail( NG_ERR_ARG, "ng_create: serving needs one model block, no generators, an edge capacity "
-                                     "and network slots" ) );
+                                     "and 1 to 1024 network slots" ) );
     if ( ( rc = e->setup_serving() ) )
       return bail( rc );
     e->deliver_ctas = e->sms * e->deliver_per_sm;
@@ -1641,7 +1806,7 @@ ng_set_spike_schedule( ng_engine* e, int64_t n, const int64_t* emit_step, const 
   if ( e->log_cap < 2 * n + 4 * e->n_src )
   {
     e->log_cap = 2 * n + 4 * e->n_src;
-    if ( ( rc = e->alloc( e->log, ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
+    if ( ( rc = e->alloc( e->log, 2 * ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
       return rc;
   }
   // consume entries already in the past
@@ -1795,7 +1960,15 @@ ng_simulate( ng_engine* e, int64_t n_steps )
   if ( !e || n_steps < 0 )
     return fail( NG_ERR_ARG, "ng_simulate: bad argument" );
   CU( cudaSetDevice( e->cfg.device ) );
-  return e->simulate( n_steps );
+  try
+  {
+    return e->simulate( n_steps );
+  }
+  catch ( const std::bad_alloc& )
+  {
+    cudaStreamSynchronize( e->stream );
+    return fail( NG_ERR_MEMORY, "ng_simulate: out of host memory for the spike log" );
+  }
 }
 
 int
@@ -1915,7 +2088,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   if ( e->from != 0 )
     return fail( NG_ERR_STATE, "ng_net_add: networks are admitted at slice boundaries" );
   const int64_t n = desc->n;
-  if ( n < 1 || desc->steps < 0 || desc->n_vars < 0 || ( desc->n_vars > 0 && ( !desc->var_names || !desc->var_values ) ) )
+  if ( n < 1 || n >= ( 1ll << LOG_ID_SHIFT ) || desc->steps < 0 || desc->n_vars < 0 || ( desc->n_vars > 0 && ( !desc->var_names || !desc->var_values ) ) )
     return fail( NG_ERR_ARG, "ng_net_add: bad network description" );
   const ng_fixed_indegree* fb = desc->build;
   const ng_pairwise_bernoulli* pb = desc->build_pb;
@@ -2198,9 +2371,13 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       ( const int32_t* ) e->sc_plen.p, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->row_beg.p,
       ( int32_t* ) e->row_len.p, ( int32_t* ) e->real_deg.p );
     // the in-edge table of the per-target gather (16-bit local ids)
-    if ( e->gather_on && fx && nk > 0 && n <= 65536 && ng_engine::take_run( e->free_gin, nk, &g0 ) )
+    const int64_t g_need = ( ( n + 31 ) / 32 * 32 ) * ( int64_t ) ( ( K + 7 ) / 8 * 8 );
+    if ( e->gather_on && fx && nk > 0 && n <= G_MAX_N && K <= G_MAX_K
+      && ng_engine::take_run( e->free_gin, g_need, &g0 ) )
     {
-      gn = nk;
+      gn = g_need;
+      k_fill_u16<<< ( unsigned ) ( ( g_need + 255 ) / 256 ), 256, 0, e->stream >>>( ( uint16_t* ) e->gin.p + g0, g_need,
+        ( uint16_t ) n );
       k_fi_gtab<<< g, 256, 0, e->stream >>>( n, K, ( const int32_t* ) e->sc_src.p, ( uint16_t* ) e->gin.p + g0 );
       GatherNet gt {};
       gt.base = g0;
@@ -2381,14 +2558,39 @@ ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_
   int rc = net_check( e, id );
   if ( rc )
     return rc;
-  if ( !n_out || cap < 0 || ( cap > 0 && ( !source || !stamp ) ) )
+  if ( !n_out || cap < 0 || ( source && !stamp ) )
     return fail( NG_ERR_ARG, "ng_net_spikes: bad argument" );
   auto& nw = e->nets[ id ];
-  const int64_t k = std::min< int64_t >( cap, ( int64_t ) nw.src.size() );
-  std::copy( nw.src.begin(), nw.src.begin() + k, source );
-  std::copy( nw.stamp.begin(), nw.stamp.begin() + k, stamp );
-  nw.src.erase( nw.src.begin(), nw.src.begin() + k );
-  nw.stamp.erase( nw.stamp.begin(), nw.stamp.begin() + k );
+  if ( !source )
+  {
+    *n_out = nw.held;  // count only
+    return NG_OK;
+  }
+  int64_t k = 0;
+  size_t ci = 0;
+  while ( ci < nw.chunks.size() && k < cap )
+  {
+    ng_engine::SpikeChunk& c = nw.chunks[ ci ];
+    const size_t off = ci == 0 ? nw.first_off : 0;
+    const size_t take = ( size_t ) std::min< int64_t >( cap - k, ( int64_t ) ( c.n - off ) );
+    std::memcpy( source + k, c.src + off, take * sizeof( int32_t ) );
+    std::memcpy( stamp + k, c.stamp + off, take * sizeof( int64_t ) );
+    k += ( int64_t ) take;
+    if ( off + take < c.n )
+    {
+      // partially drained chunk: it stays first
+      nw.first_off = off + take;
+      break;
+    }
+    ++ci;
+    nw.first_off = 0;
+  }
+  for ( size_t q = 0; q < ci; ++q )
+    e->free_chunks.push_back( nw.chunks[ q ] );
+  nw.chunks.erase( nw.chunks.begin(), nw.chunks.begin() + ( std::ptrdiff_t ) ci );
+  if ( nw.chunks.empty() )
+    nw.first_off = 0;
+  nw.held -= k;
   *n_out = k;
   return NG_OK;
 }
@@ -2490,6 +2692,7 @@ ng_net_remove( ng_engine* e, int32_t id )
   }
   e->n_rec -= nw.rec ? nw.n : 0;
   e->log_per_step = std::max( 1.0, e->log_per_step - nw.log_rate );
+  e->release_chunks( nw.chunks );
   nw = ng_engine::NetInfo();
   return NG_OK;
 }

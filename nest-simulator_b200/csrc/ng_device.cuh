@@ -50,7 +50,11 @@ struct Ctl
   unsigned long long gathered;  // (network, slice) pairs delivered by the per-target gather
   int deliver_done;     // finished CTAs of the running delivery launch
   int err;
+  int log_sel;          // half of the spike log the running group writes
 };
+
+// Spike-log entry of a serving engine: network-local source | network id << 22.
+constexpr int LOG_ID_SHIFT = 22;
 
 struct Block
 {
@@ -90,7 +94,7 @@ struct Net
   const void* edge_w;
   int4* ent;  // edge chunks: row start (lo, hi), edge count, slot | multiplicity << 16
   int64_t ent_cap;
-  uint2* log;
+  uint2* log;           // two halves of log_cap entries (groups alternate)
   int64_t log_cap;
   const uint8_t* rec;
   const double4* pois;  // lambda, p_m, F_m, m (walk from the mode, long tables)

@@ -40,6 +40,23 @@ warp_sum_ll( long long v )
   return v;
 }
 
+// The half of the spike log the running group writes, and the source
+// field of a log entry (serving: network-local id | network id << 22).
+__device__ __forceinline__ uint2*
+log_half( const Net& d )
+{
+  return d.log + ( ld_volatile( &d.ctl->log_sel ) ? d.log_cap : 0 );
+}
+
+__device__ __forceinline__ uint32_t
+log_source( const Net& d, int32_t src )
+{
+  if ( d.nid == nullptr )
+    return ( uint32_t ) src;
+  const int id = d.nid[ src ];
+  return ( uint32_t ) ( src - d.net_off[ id ] ) | ( ( uint32_t ) id << LOG_ID_SHIFT );
+}
+
 // Queue the edge chunks of one spike: ceil(pdeg / 128) work items.
 __device__ __forceinline__ void
 put_chunks( const Net& d, long long idx, long long row, long long pdeg, int slot, int mult )
@@ -107,7 +124,7 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
     {
       const uint32_t rel = ( uint32_t ) ( stamp - ld_volatile( &d.ctl->log_base ) );
       const uint32_t mu = ( uint32_t ) ( mult < 255 ? mult : 255 );
-      d.log[ li ] = make_uint2( ( uint32_t ) src, rel | ( mu << 24 ) );
+      log_half( d )[ li ] = make_uint2( log_source( d, src ), rel | ( mu << 24 ) );
     }
     else
     {
@@ -170,6 +187,8 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
   long long idx = ( long long ) base + e_incl - cnt * nch;
   long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
   const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
+  uint2* const lg_buf = lg ? log_half( d ) : nullptr;
+  const uint32_t lsrc = lg ? log_source( d, src ) : 0u;
   unsigned m = mask;
   while ( m )
   {
@@ -184,7 +203,7 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
     if ( lg )
     {
       if ( li < d.log_cap )
-        d.log[ li ] = make_uint2( ( uint32_t ) src, ( uint32_t ) ( t0 + k + 1 - lb0 ) | ( 1u << 24 ) );
+        lg_buf[ li ] = make_uint2( lsrc, ( uint32_t ) ( t0 + k + 1 - lb0 ) | ( 1u << 24 ) );
       else
         atomicOr( &d.ctl->err, ERR_LOG );
       ++li;
@@ -277,6 +296,8 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
   long long idx = ( long long ) base + e_incl - cnt * nch;
   long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
   const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
+  uint2* const lg_buf = lg ? log_half( d ) : nullptr;
+  const uint32_t lsrc = lg ? log_source( d, src ) : 0u;
   unsigned m = mask;
   while ( m )
   {
@@ -291,7 +312,7 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
     if ( lg )
     {
       if ( li < d.log_cap )
-        d.log[ li ] = make_uint2( ( uint32_t ) src, ( uint32_t ) ( t0 + k + 1 - lb0 ) | ( 1u << 24 ) );
+        lg_buf[ li ] = make_uint2( lsrc, ( uint32_t ) ( t0 + k + 1 - lb0 ) | ( 1u << 24 ) );
       else
         atomicOr( &d.ctl->err, ERR_LOG );
       ++li;
@@ -1446,10 +1467,11 @@ k_deliver( Net d )
 
 // Host-side ctl edits between groups (log drain, trace window).
 __global__ void
-k_set_ctl( Ctl* ctl, long long log_base, long long trace_row0, int reset_log )
+k_set_ctl( Ctl* ctl, long long log_base, long long trace_row0, int reset_log, int log_sel )
 {
   if ( reset_log )
     ctl->log_count = 0ull;
+  ctl->log_sel = log_sel;
   ctl->log_base = log_base;
   ctl->trace_row0 = trace_row0;
 }

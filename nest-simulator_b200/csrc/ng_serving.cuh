@@ -104,9 +104,9 @@ k_fi_scatter( int64_t n, int k_exc, int k_inh, const int32_t* tmp_src, const int
   w[ e ] = ex ? w_exc : w_inh;
 }
 
-// In-edge table of the per-target gather: gin[j * n + t] = local source of
-// draw j of target t (column-major, so consecutive targets read
-// consecutive entries).
+// In-edge table of the per-target gather (layout at k_gather): draw j of
+// target t, from the drawn sources tmp_src[t * K + j]; the table was
+// filled with the padding id n beforehand.
 __global__ void
 k_fi_gtab( int64_t n, int K, const int32_t* tmp_src, uint16_t* gin )
 {
@@ -115,7 +115,16 @@ k_fi_gtab( int64_t n, int K, const int32_t* tmp_src, uint16_t* gin )
     return;
   const int64_t t = idx / K;
   const int j = ( int ) ( idx - t * K );
-  gin[ ( int64_t ) j * n + t ] = ( uint16_t ) tmp_src[ idx ];
+  const int nb = ( K + 7 ) >> 3;
+  gin[ ( ( ( t >> 5 ) * nb + ( j >> 3 ) ) * 32 + ( t & 31 ) ) * 8 + ( j & 7 ) ] = ( uint16_t ) tmp_src[ idx ];
+}
+
+__global__ void
+k_fill_u16( uint16_t* p, int64_t n, uint16_t v )
+{
+  const int64_t k = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( k < n )
+    p[ k ] = v;
 }
 
 // Rows of the region's sources: begin, padded length, real degree.
@@ -322,86 +331,220 @@ namespace ng
 // ---------------------------------------------------------------------
 // Per-target gather (precision form of a serving engine): for the networks
 // in gather mode this slice, every target walks its in-edge table and
-// counts, per lag and channel, the in-edges whose source spiked at that lag
-// (the sources' lag bits, gmask, written by the update kernel); the ring
-// then gets count * weight at slot (origin + lag + d) mod L.  The targets'
-// ring cells have no other writer in this slice (their sources queue no
-// edge chunks), so the adds are plain read-modify-writes.  The integer
-// result equals the scatter's, whatever the order.
-// A CTA serves G_TGT targets with G_PARTS threads each (in-edges split in
-// G_PARTS runs, counts combined in shared memory).
+// counts, per lag and draw type (excitatory / inhibitory), the in-edges
+// whose source spiked at that lag; the ring then gets count * weight at
+// slot (origin + lag + d) mod L.  The targets' ring cells have no other
+// writer in this slice (their sources queue no edge chunks), so the adds
+// are plain read-modify-writes, and the integer result equals the
+// scatter's whatever the order.
+//
+// One CTA per SM walks a contiguous range of the slice's target tiles
+// (GT targets of one network each).  The network's lag bits (16-bit, one
+// per source, written by the update kernel) are staged in shared memory
+// once per network, so the random source lookups never leave the SM; the
+// in-edge table streams from HBM in 16-byte loads, coalesced per warp
+// (layout below).  Counts are kept as 12 bit planes per thread (bit c of
+// plane p = binary digit p of the count of lag/type c): 8 sources' lag
+// bits at a time go through a Harley-Seal carry-save adder tree (two
+// three-input logic ops per adder), so no counter is indexed dynamically
+// and no lane branches on the data.
+// GP threads share a target (runs of its in-edges); their planes are added
+// in shared memory.
+//
+// In-edge table of a network (16-bit local source ids, Kp = K rounded up
+// to 8, padding = n, whose lag bits are 0): entry (target tl, draw j) at
+// ((tl / 32 * Kp / 8 + j / 8) * 32 + tl % 32) * 8 + j % 8.
 // ---------------------------------------------------------------------
-constexpr int G_TGT = 64;
-constexpr int G_PARTS = 4;
+constexpr int GT = 256;                  // targets per tile
+constexpr int GP = 4;                    // threads per target
+constexpr int G_THREADS = GT * GP;
+constexpr int G_PLANES = 12;             // in-degrees below 4096
+constexpr int G_MAX_N = 65535;           // 16-bit local ids, n itself is the padding id
+constexpr int G_MAX_K = ( 1 << G_PLANES ) - 1;
+constexpr size_t G_SMEM = ( size_t ) ( GP - 1 ) * G_PLANES * GT * 4 + ( size_t ) ( G_MAX_N + 1 ) * 2;
 
-__global__ void __launch_bounds__( G_TGT * G_PARTS )
+// carry-save adder: (acc, a, b) -> acc = acc ^ a ^ b, hi = majority(acc, a, b)
+__device__ __forceinline__ void
+csa( uint32_t& hi, uint32_t& acc, uint32_t a, uint32_t b )
+{
+  const uint32_t u = acc ^ a;
+  hi = ( acc & a ) | ( u & b );
+  acc = u ^ b;
+}
+
+__device__ __forceinline__ unsigned
+plane_count( const uint32_t* P, int bit )
+{
+  unsigned c = 0;
+#pragma unroll
+  for ( int b = 0; b < G_PLANES; ++b )
+    c |= ( ( P[ b ] >> bit ) & 1u ) << b;
+  return c;
+}
+
+__global__ void __launch_bounds__( G_THREADS, 1 )
 k_gather( Net d )
 {
-  __shared__ unsigned s_cnt[ 2 ][ 32 ][ G_TGT ];  // [draw type][lag][target]
-  for ( int k = threadIdx.x; k < 2 * 32 * G_TGT; k += blockDim.x )
-    ( &s_cnt[ 0 ][ 0 ][ 0 ] )[ k ] = 0u;
+  extern __shared__ __align__( 16 ) unsigned char g_smem[];
+  uint32_t* s_pl = reinterpret_cast< uint32_t* >( g_smem );  // [GP - 1][G_PLANES][GT]
+  uint16_t* s_mask = reinterpret_cast< uint16_t* >( g_smem + ( size_t ) ( GP - 1 ) * G_PLANES * GT * 4 );  // [n + 1]
+  __shared__ int s_pref[ 1025 ];
   const long long origin = cta_origin( d );  // synchronises the CTA
-  const int ti = threadIdx.x % G_TGT;
-  const int part = threadIdx.x / G_TGT;
-  const int64_t t = ( int64_t ) blockIdx.x * G_TGT + ti;
-  const int id = t < d.N ? d.nid[ t ] : -1;
-  const bool on = id >= 0 && d.net_mode[ id ] != 0;
-  GatherNet g {};
-  if ( on )
+  const int tid = threadIdx.x;
+  // tiles per network in gather mode, prefix sums (n_nets <= 1024)
+  for ( int id = tid; id < d.n_nets; id += blockDim.x )
   {
-    g = d.net_g[ id ];
-    const int K = g.ke + g.ki;
-    const int j0 = ( int ) ( ( long long ) K * part / G_PARTS );
-    const int j1 = ( int ) ( ( long long ) K * ( part + 1 ) / G_PARTS );
-    const uint16_t* col = d.gin + g.base + ( t - g.off );
-    const uint32_t* msk = d.gmask + g.off;
-    int j = j0;
-    for ( ; j + 4 <= j1; j += 4 )
+    int c = 0;
+    if ( d.net_mode[ id ] )
     {
-      uint32_t m[ 4 ];
+      const GatherNet g = d.net_g[ id ];
+      if ( g.ke + g.ki > 0 )
+        c = ( g.n + GT - 1 ) / GT;
+    }
+    s_pref[ id + 1 ] = c;
+  }
+  if ( tid == 0 )
+    s_pref[ 0 ] = 0;
+  __syncthreads();
+  if ( tid == 0 )
+    for ( int id = 0; id < d.n_nets; ++id )
+      s_pref[ id + 1 ] += s_pref[ id ];
+  __syncthreads();
+  const int total = s_pref[ d.n_nets ];
+  const int w0 = ( int ) ( ( long long ) total * blockIdx.x / gridDim.x );
+  const int w1 = ( int ) ( ( long long ) total * ( blockIdx.x + 1 ) / gridDim.x );
+  const int ti = tid % GT;
+  const int part = tid / GT;
+  long long* ring = ( long long* ) d.ring;
+  int staged = -1;
+  for ( int w = w0; w < w1; ++w )
+  {
+    // the tile's network: last id with s_pref[id] <= w
+    int lo = 0, hi = d.n_nets;
+    while ( hi - lo > 1 )
+    {
+      const int mid = ( lo + hi ) >> 1;
+      if ( s_pref[ mid ] <= w )
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int id = lo;
+    const GatherNet g = d.net_g[ id ];
+    if ( id != staged )
+    {
+      __syncthreads();
+      for ( int q = tid; q <= g.n; q += blockDim.x )
+        s_mask[ q ] = q < g.n ? ( uint16_t ) d.gmask[ g.off + q ] : ( uint16_t ) 0;
+      __syncthreads();
+      staged = id;
+    }
+    const int64_t tl = ( int64_t ) ( w - s_pref[ id ] ) * GT + ti;
+    const int K = g.ke + g.ki;
+    const int nb = ( K + 7 ) >> 3;
+    // bit-parallel counters: bit c of (ones, twos, fours, hi[0..]) holds the
+    // binary digits 1, 2, 4, 8, 16, ... of the count of lag/type c
+    uint32_t P[ G_PLANES ];
 #pragma unroll
-      for ( int q = 0; q < 4; ++q )
-        m[ q ] = msk[ col[ ( long long ) ( j + q ) * g.n ] ];
-#pragma unroll
-      for ( int q = 0; q < 4; ++q )
+    for ( int b = 0; b < G_PLANES; ++b )
+      P[ b ] = 0u;
+    if ( tl < g.n )
+    {
+      const uint4* col = reinterpret_cast< const uint4* >( d.gin + g.base ) + ( ( tl >> 5 ) * nb ) * 32 + ( tl & 31 );
+      const int b0 = nb * part / GP, b1 = nb * ( part + 1 ) / GP;
+      for ( int jb = b0; jb < b1; jb += 2 )
       {
-        const int ty = ( j + q ) >= g.ke ? 1 : 0;
-        while ( m[ q ] )
+        uint4 v[ 2 ];
+        v[ 0 ] = __ldg( col + ( int64_t ) jb * 32 );
+        v[ 1 ] = jb + 1 < b1 ? __ldg( col + ( int64_t ) ( jb + 1 ) * 32 ) : make_uint4( 0, 0, 0, 0 );
+#pragma unroll
+        for ( int h = 0; h < 2; ++h )
         {
-          const int k = __ffs( m[ q ] ) - 1;
-          m[ q ] &= m[ q ] - 1;
-          atomicAdd( &s_cnt[ ty ][ k ][ ti ], 1u );
+          if ( jb + h >= b1 )
+            break;
+          const uint32_t wv[ 4 ] = { v[ h ].x, v[ h ].y, v[ h ].z, v[ h ].w };
+          uint32_t x[ 8 ];
+#pragma unroll
+          for ( int r = 0; r < 8; ++r )
+            x[ r ] = s_mask[ ( wv[ r >> 1 ] >> ( ( r & 1 ) * 16 ) ) & 0xffffu ];
+          // inhibitory draws count in the upper half (uniform across the warp)
+          const int j0 = ( jb + h ) * 8;
+          if ( j0 >= g.ke )
+          {
+#pragma unroll
+            for ( int r = 0; r < 8; ++r )
+              x[ r ] <<= 16;
+          }
+          else if ( j0 + 8 > g.ke )
+          {
+#pragma unroll
+            for ( int r = 0; r < 8; ++r )
+              if ( j0 + r >= g.ke )
+                x[ r ] <<= 16;
+          }
+          // Harley-Seal: 8 inputs through carry-save adders into P[0..2],
+          // the weight-8 carries rippled into P[3..]
+          uint32_t tA, tB, fA, fB, e;
+          csa( tA, P[ 0 ], x[ 0 ], x[ 1 ] );
+          csa( tB, P[ 0 ], x[ 2 ], x[ 3 ] );
+          csa( fA, P[ 1 ], tA, tB );
+          csa( tA, P[ 0 ], x[ 4 ], x[ 5 ] );
+          csa( tB, P[ 0 ], x[ 6 ], x[ 7 ] );
+          csa( fB, P[ 1 ], tA, tB );
+          csa( e, P[ 2 ], fA, fB );
+#pragma unroll
+          for ( int b2 = 3; b2 < G_PLANES; ++b2 )
+          {
+            const uint32_t t = P[ b2 ] & e;
+            P[ b2 ] ^= e;
+            e = t;
+            if ( e == 0u )
+              break;
+          }
         }
       }
     }
-    for ( ; j < j1; ++j )
+    // parts 1.. hand their planes to part 0, which adds them bit-parallel
+    // (a ripple-carry adder over the 12 planes) and writes count * weight
+    // into the ring
+    if ( part > 0 )
     {
-      uint32_t m = msk[ col[ ( long long ) j * g.n ] ];
-      const int ty = j >= g.ke ? 1 : 0;
-      while ( m )
+#pragma unroll
+      for ( int b = 0; b < G_PLANES; ++b )
+        s_pl[ ( ( part - 1 ) * G_PLANES + b ) * GT + ti ] = P[ b ];
+    }
+    __syncthreads();
+    if ( part == 0 && tl < g.n )
+    {
+      for ( int q = 0; q < GP - 1; ++q )
       {
-        const int k = __ffs( m ) - 1;
-        m &= m - 1;
-        atomicAdd( &s_cnt[ ty ][ k ][ ti ], 1u );
+        uint32_t c = 0u;
+#pragma unroll
+        for ( int b = 0; b < G_PLANES; ++b )
+        {
+          const uint32_t y = s_pl[ ( q * G_PLANES + b ) * GT + ti ];
+          const uint32_t u = P[ b ] ^ y;
+          const uint32_t c2 = ( P[ b ] & y ) | ( u & c );
+          P[ b ] = u ^ c;
+          c = c2;
+        }
+      }
+      const int64_t t = g.off + tl;
+      for ( int k = 0; k < d.min_delay; ++k )
+      {
+        const int slot = ( int ) ( ( origin + k + g.d ) % d.L );
+#pragma unroll
+        for ( int ty = 0; ty < 2; ++ty )
+        {
+          const unsigned n = plane_count( P, ty * 16 + k );
+          if ( n == 0u )
+            continue;
+          const int64_t idx = ( ( int64_t ) slot * d.C + ( ty ? g.ci : g.ce ) ) * d.N + t;
+          ring[ idx ] += ( long long ) n * ( long long ) ( ty ? g.wi : g.we );
+        }
       }
     }
-  }
-  __syncthreads();
-  if ( !on )
-    return;
-  long long* ring = ( long long* ) d.ring;
-  for ( int k = part; k < d.min_delay; k += G_PARTS )
-  {
-    const int slot = ( int ) ( ( origin + k + g.d ) % d.L );
-#pragma unroll
-    for ( int ty = 0; ty < 2; ++ty )  // excitatory, inhibitory draws
-    {
-      const unsigned c = s_cnt[ ty ][ k ][ ti ];
-      if ( c == 0u )
-        continue;
-      const int64_t idx = ( ( int64_t ) slot * d.C + ( ty ? g.ci : g.ce ) ) * d.N + t;
-      ring[ idx ] += ( long long ) c * ( long long ) ( ty ? g.wi : g.we );
-    }
+    __syncthreads();
   }
 }
 

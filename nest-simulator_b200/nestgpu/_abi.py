@@ -144,6 +144,8 @@ class NGStats(ctypes.Structure):
         ("deliver_launches", ctypes.c_int64),
         ("simulate_ms", ctypes.c_double),
         ("gather_slices", ctypes.c_int64),
+        ("wait_ms", ctypes.c_double),
+        ("drain_ms", ctypes.c_double),
     ]
 
 
@@ -414,18 +416,16 @@ class Engine:
         check(self.L.ng_net_poll(self.handle, int(nid), ctypes.byref(done), ctypes.byref(fin)))
         return done.value, bool(fin.value)
 
-    def net_spikes(self, nid, cap=1 << 24):
-        src = np.empty(cap, dtype=np.int32)
-        st = np.empty(cap, dtype=np.int64)
+    def net_spikes(self, nid):
+        """Drain the network's spikes: (local source, local stamp)."""
         got = ctypes.c_int64(0)
-        out_s, out_t = [], []
-        while True:
-            check(self.L.ng_net_spikes(self.handle, int(nid), _p(src), _p(st), cap, ctypes.byref(got)))
-            out_s.append(src[:got.value].copy())
-            out_t.append(st[:got.value].copy())
-            if got.value < cap:
-                break
-        return np.concatenate(out_s), np.concatenate(out_t)
+        check(self.L.ng_net_spikes(self.handle, int(nid), None, None, 0, ctypes.byref(got)))
+        k = got.value
+        src = np.empty(k, dtype=np.int32)
+        st = np.empty(k, dtype=np.int64)
+        if k:
+            check(self.L.ng_net_spikes(self.handle, int(nid), _p(src), _p(st), k, ctypes.byref(got)))
+        return src[:got.value], st[:got.value]
 
     def net_get_var(self, nid, name, n):
         out = np.empty(int(n), dtype=np.float64)
