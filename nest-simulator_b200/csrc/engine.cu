@@ -274,46 +274,21 @@ struct ng_engine
   bool serving = false;
   DevBuf d_nid, d_step0, d_until, d_off, d_key, sc_src, sc_cnt, sc_fill, sc_beg, sc_plen, sc_total, sc_sb;
   std::vector< int32_t > nid_host;
-  // Spikes of a serving network, kept on the host in fixed-size chunks
-  // recycled through a free list (growing one array would copy and
-  // re-fault every page on each reallocation).
-  static constexpr size_t SPIKE_CHUNK = 1 << 18;
-  struct SpikeChunk
+  // Spikes of a serving network: the raw log entries of each group, as
+  // grouped by network on the device, decoded only when they are read.
+  struct RawBlock
   {
-    int32_t* src = nullptr;
-    int64_t* stamp = nullptr;
-    size_t n = 0;
+    int64_t clock = 0;  // log base (stamp offset) of the group
+    uint2* e = nullptr;
+    int64_t n = 0;
   };
-  std::vector< SpikeChunk > free_chunks;
 
-  SpikeChunk
-  new_chunk()
+  static void
+  free_blocks( std::vector< RawBlock >& bs )
   {
-    if ( !free_chunks.empty() )
-    {
-      SpikeChunk c = free_chunks.back();
-      free_chunks.pop_back();
-      c.n = 0;
-      return c;
-    }
-    SpikeChunk c;
-    c.src = static_cast< int32_t* >( std::malloc( SPIKE_CHUNK * sizeof( int32_t ) ) );
-    c.stamp = static_cast< int64_t* >( std::malloc( SPIKE_CHUNK * sizeof( int64_t ) ) );
-    if ( !c.src || !c.stamp )
-    {
-      std::free( c.src );
-      std::free( c.stamp );
-      throw std::bad_alloc();
-    }
-    return c;
-  }
-
-  void
-  release_chunks( std::vector< SpikeChunk >& cs )
-  {
-    for ( auto& c : cs )
-      free_chunks.push_back( c );
-    cs.clear();
+    for ( auto& b : bs )
+      std::free( b.e );
+    bs.clear();
   }
 
   struct NetInfo
@@ -323,9 +298,9 @@ struct ng_engine
     int64_t g0 = -1, gn = 0;  // gather table run
     bool rec = false;
     double log_rate = 0.0;
-    std::vector< SpikeChunk > chunks;  // logged spikes, in order
-    int64_t held = 0;                  // spikes held in the chunks
-    size_t first_off = 0;              // entries of chunks[0] already drained
+    std::vector< RawBlock > blocks;  // logged spikes, group by group
+    int64_t held = 0;                // spikes held (multiplicities counted)
+    int64_t first = 0;               // entries of blocks[0] already drained
   };
   std::vector< NetInfo > nets;
   std::map< int64_t, int64_t > free_neurons, free_edges;  // run start -> length
@@ -333,6 +308,8 @@ struct ng_engine
   bool gather_on = false;
   float gather_frac = 0.08f;
   DevBuf gmask, gin, net_g, net_mode, net_spk;
+  DevBuf log_sorted, log_cnt, log_off;  // spike log grouped by network (two halves)
+  long long* host_off = nullptr;        // pinned, 2 x (max_networks + 1)
   std::map< int64_t, int64_t > free_gin;
   std::vector< GatherNet > host_g;
   std::unordered_map< std::string, int32_t > cls_ids;     // engine-wide coefficient classes
@@ -517,7 +494,7 @@ struct ng_engine
     DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
       &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl, &d_nid, &d_step0, &d_until, &d_off,
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
-      &net_spk };
+      &net_spk, &log_sorted, &log_cnt, &log_off };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -525,12 +502,9 @@ struct ng_engine
     if ( pinned_log )
       cudaFreeHost( pinned_log );
     for ( auto& nw : nets )
-      release_chunks( nw.chunks );
-    for ( auto& c : free_chunks )
-    {
-      std::free( c.src );
-      std::free( c.stamp );
-    }
+      free_blocks( nw.blocks );
+    if ( host_off )
+      cudaFreeHost( host_off );
     for ( auto& ev : group_done )
       if ( ev )
         cudaEventDestroy( ev );
@@ -1084,6 +1058,30 @@ struct ng_engine
     if ( rc )
       return rc;
     gi.end = origin + from;
+    if ( serving )
+    {
+      const int nn = cfg.max_networks;
+      if ( log_sorted.bytes < 2 * ( size_t ) log_cap * sizeof( uint2 ) )
+      {
+        if ( ( rc = alloc( log_sorted, 2 * ( size_t ) log_cap * sizeof( uint2 ) ) ) || ( rc = alloc( log_cnt, ( size_t ) nn * 4 ) )
+          || ( rc = alloc( log_off, 2 * ( size_t ) ( nn + 1 ) * 8 ) ) )
+          return rc;
+        if ( !host_off && cudaMallocHost( &host_off, 2 * ( size_t ) ( nn + 1 ) * 8 ) != cudaSuccess )
+          return fail( NG_ERR_MEMORY, "cannot allocate pinned host memory for the spike log offsets" );
+      }
+      // the counters double as the scatter's fill counters: zero them each group
+      CU( cudaMemsetAsync( log_cnt.p, 0, ( size_t ) nn * 4, stream ) );
+      const uint2* half = ( const uint2* ) log.p + ( sel ? log_cap : 0 );
+      long long* off = ( long long* ) log_off.p + ( size_t ) sel * ( nn + 1 );
+      k_log_count<<< ( unsigned ) ( 2 * sms ), 256, 0, stream >>>( ( const Ctl* ) ctl.p, half, log_cap, nn,
+        ( unsigned* ) log_cnt.p );
+      k_log_offsets<<< 1, 1024, 0, stream >>>( ( unsigned* ) log_cnt.p, off, nn );
+      k_log_scatter<<< ( unsigned ) ( 2 * sms ), 256, 0, stream >>>( ( const Ctl* ) ctl.p, half, log_cap, nn, off,
+        ( unsigned* ) log_cnt.p, ( uint2* ) log_sorted.p + ( sel ? log_cap : 0 ) );
+      CU( cudaGetLastError() );
+      CU( cudaMemcpyAsync( host_off + ( size_t ) sel * ( nn + 1 ), off, ( size_t ) ( nn + 1 ) * 8, cudaMemcpyDeviceToHost,
+        stream ) );
+    }
     CU( cudaMemcpyAsync( host_ctl + sel, ctl.p, sizeof( Ctl ), cudaMemcpyDeviceToHost, stream ) );
     CU( cudaEventRecord( group_done[ sel ], stream ) );
     return NG_OK;
@@ -1126,41 +1124,42 @@ struct ng_engine
     if ( c.err & ( ERR_SPIKE_LIST | ERR_LOG | ERR_TRACE ) )
       return fail( NG_ERR_CAPACITY, "device spike list, spike log or trace buffer overflowed (err word "
           + std::to_string( c.err ) + ")" );
-    const int64_t nl = ( int64_t ) c.log_count;
+    // (serving: the entries grouped by network, all with a valid id)
+    const int64_t nl = serving ? std::min< int64_t >( ( int64_t ) c.log_count,
+                                   host_off[ ( size_t ) sel * ( cfg.max_networks + 1 ) + cfg.max_networks ] )
+                               : ( int64_t ) c.log_count;
     if ( nl > 0 )
     {
       int rc = grow_pinned( ( size_t ) nl * sizeof( uint2 ) );
       if ( rc )
         return rc;
       // the copy engine fetches this half while the next group computes
-      CU( cudaMemcpyAsync( pinned_log, ( uint2* ) log.p + ( sel ? log_cap : 0 ), sizeof( uint2 ) * ( size_t ) nl,
-        cudaMemcpyDeviceToHost, copy_stream ) );
+      const uint2* src_half = ( const uint2* ) ( serving ? log_sorted.p : log.p ) + ( sel ? log_cap : 0 );
+      CU( cudaMemcpyAsync( pinned_log, src_half, sizeof( uint2 ) * ( size_t ) nl, cudaMemcpyDeviceToHost, copy_stream ) );
       CU( cudaStreamSynchronize( copy_stream ) );
       const uint2* ent = pinned_log;
       if ( serving )
       {
-        for ( int64_t k = 0; k < nl; ++k )
+        // one block per network: its entries are contiguous
+        const long long* off = host_off + ( size_t ) sel * ( cfg.max_networks + 1 );
+        for ( int id = 0; id < cfg.max_networks; ++id )
         {
-          const uint32_t id = ent[ k ].x >> LOG_ID_SHIFT;
-          if ( id >= nets.size() )
-            return fail( NG_ERR_STATE, "spike log entry " + std::to_string( k ) + " of " + std::to_string( nl )
-                + " names network " + std::to_string( id ) + " (word " + std::to_string( ent[ k ].x ) + ", "
-                + std::to_string( ent[ k ].y ) + ")" );
-          NetInfo& nw = nets[ id ];
-          if ( !nw.used )
+          const int64_t cnt = off[ id + 1 ] - off[ id ];
+          NetInfo& nw = nets[ ( size_t ) id ];
+          if ( cnt <= 0 || !nw.used )
             continue;
-          const int32_t src = ( int32_t ) ( ent[ k ].x & ( ( 1u << LOG_ID_SHIFT ) - 1u ) );
-          const int64_t stamp = gi.clock + ( int64_t ) ( ent[ k ].y & 0xFFFFFFu ) - nw.step0;
-          for ( uint32_t m = ent[ k ].y >> 24; m > 0; --m )
-          {
-            if ( nw.chunks.empty() || nw.chunks.back().n == SPIKE_CHUNK )
-              nw.chunks.push_back( new_chunk() );
-            SpikeChunk& c = nw.chunks.back();
-            c.src[ c.n ] = src;
-            c.stamp[ c.n ] = stamp;
-            ++c.n;
-            ++nw.held;
-          }
+          RawBlock rb;
+          rb.clock = gi.clock;
+          rb.n = cnt;
+          rb.e = static_cast< uint2* >( std::malloc( ( size_t ) cnt * sizeof( uint2 ) ) );
+          if ( !rb.e )
+            return fail( NG_ERR_MEMORY, "out of host memory for the spike log" );
+          std::memcpy( rb.e, ent + off[ id ], ( size_t ) cnt * sizeof( uint2 ) );
+          int64_t m = 0;
+          for ( int64_t k = 0; k < cnt; ++k )
+            m += rb.e[ k ].y >> 24;
+          nw.held += m;
+          nw.blocks.push_back( rb );
         }
       }
       else
@@ -1967,7 +1966,7 @@ ng_simulate( ng_engine* e, int64_t n_steps )
   catch ( const std::bad_alloc& )
   {
     cudaStreamSynchronize( e->stream );
-    return fail( NG_ERR_MEMORY, "ng_simulate: out of host memory for the spike log" );
+    return fail( NG_ERR_MEMORY, "ng_simulate: out of host memory" );
   }
 }
 
@@ -2567,29 +2566,37 @@ ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_
     return NG_OK;
   }
   int64_t k = 0;
-  size_t ci = 0;
-  while ( ci < nw.chunks.size() && k < cap )
+  size_t bi = 0;
+  const uint32_t lmask = ( 1u << LOG_ID_SHIFT ) - 1u;
+  for ( ; bi < nw.blocks.size(); ++bi )
   {
-    ng_engine::SpikeChunk& c = nw.chunks[ ci ];
-    const size_t off = ci == 0 ? nw.first_off : 0;
-    const size_t take = ( size_t ) std::min< int64_t >( cap - k, ( int64_t ) ( c.n - off ) );
-    std::memcpy( source + k, c.src + off, take * sizeof( int32_t ) );
-    std::memcpy( stamp + k, c.stamp + off, take * sizeof( int64_t ) );
-    k += ( int64_t ) take;
-    if ( off + take < c.n )
+    const ng_engine::RawBlock& rb = nw.blocks[ bi ];
+    int64_t q = bi == 0 ? nw.first : 0;
+    for ( ; q < rb.n; ++q )
     {
-      // partially drained chunk: it stays first
-      nw.first_off = off + take;
+      const uint2 en = rb.e[ q ];
+      const uint32_t m = en.y >> 24;
+      if ( k + m > cap )
+        break;
+      const int32_t src = ( int32_t ) ( en.x & lmask );
+      const int64_t st = rb.clock + ( int64_t ) ( en.y & 0xFFFFFFu ) - nw.step0;
+      for ( uint32_t r = 0; r < m; ++r, ++k )
+      {
+        source[ k ] = src;
+        stamp[ k ] = st;
+      }
+    }
+    if ( q < rb.n )
+    {
+      // cap reached inside this block: it stays first
+      nw.first = q;
       break;
     }
-    ++ci;
-    nw.first_off = 0;
+    nw.first = 0;
   }
-  for ( size_t q = 0; q < ci; ++q )
-    e->free_chunks.push_back( nw.chunks[ q ] );
-  nw.chunks.erase( nw.chunks.begin(), nw.chunks.begin() + ( std::ptrdiff_t ) ci );
-  if ( nw.chunks.empty() )
-    nw.first_off = 0;
+  for ( size_t q = 0; q < bi; ++q )
+    std::free( nw.blocks[ q ].e );
+  nw.blocks.erase( nw.blocks.begin(), nw.blocks.begin() + ( std::ptrdiff_t ) bi );
   nw.held -= k;
   *n_out = k;
   return NG_OK;
@@ -2692,7 +2699,7 @@ ng_net_remove( ng_engine* e, int32_t id )
   }
   e->n_rec -= nw.rec ? nw.n : 0;
   e->log_per_step = std::max( 1.0, e->log_per_step - nw.log_rate );
-  e->release_chunks( nw.chunks );
+  ng_engine::free_blocks( nw.blocks );
   nw = ng_engine::NetInfo();
   return NG_OK;
 }

@@ -549,3 +549,73 @@ k_gather( Net d )
 }
 
 }  // namespace ng
+
+namespace ng
+{
+
+// ---------------------------------------------------------------------
+// Spike log of a serving engine grouped by network at the end of a group
+// (counting sort on the network id of each entry), so the host appends
+// each network's spikes with one copy instead of routing them one by one.
+// ---------------------------------------------------------------------
+__global__ void
+k_log_count( const Ctl* ctl, const uint2* half, int64_t cap, int n_nets, unsigned* cnt )
+{
+  __shared__ unsigned s_cnt[ 1024 ];
+  for ( int k = threadIdx.x; k < n_nets; k += blockDim.x )
+    s_cnt[ k ] = 0u;
+  __syncthreads();
+  const int64_t nl = min( ( int64_t ) ctl->log_count, cap );
+  for ( int64_t k = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x; k < nl; k += ( int64_t ) gridDim.x * blockDim.x )
+  {
+    const unsigned id = half[ k ].x >> LOG_ID_SHIFT;
+    if ( id < ( unsigned ) n_nets )
+      atomicAdd( &s_cnt[ id ], 1u );
+  }
+  __syncthreads();
+  for ( int k = threadIdx.x; k < n_nets; k += blockDim.x )
+    if ( s_cnt[ k ] )
+      atomicAdd( &cnt[ k ], s_cnt[ k ] );
+}
+
+// exclusive offsets per network (off[n_nets] = total); the counters are
+// reset here and count again as the scatter's fill positions
+__global__ void __launch_bounds__( 1024 )
+k_log_offsets( unsigned* cnt, long long* off, int n_nets )
+{
+  __shared__ long long s[ 1024 ];
+  const int t = threadIdx.x;
+  const long long v = t < n_nets ? ( long long ) cnt[ t ] : 0ll;
+  s[ t ] = v;
+  __syncthreads();
+  for ( int o = 1; o < 1024; o <<= 1 )
+  {
+    const long long a = t >= o ? s[ t - o ] : 0ll;
+    __syncthreads();
+    s[ t ] += a;
+    __syncthreads();
+  }
+  if ( t < n_nets )
+  {
+    off[ t ] = s[ t ] - v;
+    cnt[ t ] = 0u;
+  }
+  if ( t == 1023 )
+    off[ n_nets ] = s[ 1023 ];
+}
+
+__global__ void
+k_log_scatter( const Ctl* ctl, const uint2* half, int64_t cap, int n_nets, const long long* off, unsigned* fill,
+  uint2* out )
+{
+  const int64_t nl = min( ( int64_t ) ctl->log_count, cap );
+  for ( int64_t k = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x; k < nl; k += ( int64_t ) gridDim.x * blockDim.x )
+  {
+    const uint2 e = half[ k ];
+    const unsigned id = e.x >> LOG_ID_SHIFT;
+    if ( id < ( unsigned ) n_nets )
+      out[ off[ id ] + atomicAdd( &fill[ id ], 1u ) ] = e;
+  }
+}
+
+}  // namespace ng

@@ -46,6 +46,7 @@ class Request:
     eta: float
     steps: int
     seed: int
+    enqueued: float = math.nan   # s: the arrival (real-time runs) or 0 (all queued at the start)
     admitted: float = math.nan
     finished: float = math.nan
     spikes: tuple = field(default=None, repr=False)
@@ -53,7 +54,7 @@ class Request:
 
     @property
     def latency(self):
-        return self.finished - self.arrival
+        return self.finished - self.enqueued
 
     def syn_events_from_spikes(self):
         """Recurrent synaptic events: spikes times the source's out-degree (the
@@ -119,7 +120,9 @@ def run_batched(requests, eng, max_chunk_slices=64, clock=time.perf_counter, rea
     while pending or waiting or active:
         now = clock() - t0
         while pending and (pending[0].arrival <= now or not realtime):
-            waiting.append(pending.pop(0))
+            r = pending.pop(0)
+            r.enqueued = r.arrival if realtime else 0.0
+            waiting.append(r)
         # admit every waiting request that fits, oldest first
         still = []
         for r in waiting:
@@ -163,6 +166,7 @@ def run_plain(requests, eng, clock=time.perf_counter, realtime=True):
         now = clock() - t0
         if realtime and r.arrival > now:
             time.sleep(r.arrival - now)
+        r.enqueued = r.arrival if realtime else 0.0
         nid = _admit(eng, r)
         if nid is None:
             raise RuntimeError("a request does not fit the empty pool")
