@@ -53,7 +53,11 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--batch", type=int, default=8, help="config-1 networks advanced together (batched form)")
+    ap.add_argument("--batch", type=int, default=8, help="Brunel networks advanced together (batched form)")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-layered", action="store_true")
+    ap.add_argument("--no-aeif", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=256)
     return ap.parse_args()
 
 
@@ -363,6 +367,133 @@ def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg):
     return res
 
 
+def timed_sim(eng, steps, dev):
+    """Device time [ms] of `steps` steps on the engine's stream (CUDA events)."""
+    import torch
+
+    st = torch.cuda.current_stream(dev)
+    eng.set_stream(st.cuda_stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    eng.simulate(steps)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1)
+
+
+def kernel_split(eng, steps):
+    """Per-launch device times of the update and delivery kernels over
+    `steps` steps (event records inside the slice graphs)."""
+    eng.set_profiling(True)
+    p0 = eng.stats()
+    eng.simulate(steps)
+    p1 = eng.stats()
+    eng.set_profiling(False)
+    nu = max(1, p1["update_launches"] - p0["update_launches"])
+    nd = max(1, p1["deliver_launches"] - p0["deliver_launches"])
+    return {"update_us": 1e3 * (p1["update_ms"] - p0["update_ms"]) / nu,
+            "deliver_us": 1e3 * (p1["deliver_ms"] - p0["deliver_ms"]) / nd,
+            "update_launches": nu, "deliver_launches": nd}
+
+
+def measure_layered(args, dev, sim_ms=1000.0):
+    """Layered 8-population network (77,169 neurons, pairwise_bernoulli graph
+    drawn on the device): real-time factor in the FP64 and FP32 forms."""
+    from nestgpu import workloads
+
+    spec = workloads.layered_spec()
+    out = {"workload": "layered 8-population iaf_psc_exp network, 77,169 neurons, pairwise_bernoulli "
+                       "p ~ U[0.01, 0.15], 1,000 ms", "neurons": sum(spec["sizes"])}
+    steps = int(round(sim_ms / 0.1))
+    for prec in ("fp64", "fp32"):
+        t0 = time.perf_counter()
+        eng = workloads.layered_engine(spec, prec, device=dev.index)
+        nid = workloads.layered_add(eng, spec, 10 * steps)
+        build = time.perf_counter() - t0
+        eng.simulate(1000)  # 100 ms warm-up (graphs built)
+        s0 = eng.stats()
+        ms = timed_sim(eng, steps, dev)
+        s1 = eng.stats()
+        ks = kernel_split(eng, 200)
+        out["synapses"] = eng.net_connection_count(nid)
+        eng.close()
+        ev = s1["syn_events"] - s0["syn_events"]
+        out[prec] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
+                     "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / out["neurons"] / (sim_ms * 1e-3),
+                     "build_s": build, "kernels": ks}
+    return out
+
+
+def measure_aeif(args, dev, sim_ms=500.0):
+    """50,000 aeif_cond_alpha neurons, K = 1,000: real-time factor, FP64 and
+    FP32 state (FP64 error control in both)."""
+    from nestgpu import workloads
+
+    spec = workloads.aeif_spec()
+    n = spec["n_exc"] + spec["n_inh"]
+    out = {"workload": "50,000 aeif_cond_alpha neurons, fixed_indegree K=1,000, 10 kHz x 0.5 nS drive, 500 ms",
+           "neurons": n}
+    steps = int(round(sim_ms / 0.1))
+    for prec in ("fp64", "fp32"):
+        t0 = time.perf_counter()
+        eng = workloads.aeif_engine(spec, prec, device=dev.index)
+        workloads.aeif_add(eng, spec, 10 * steps)
+        build = time.perf_counter() - t0
+        eng.simulate(1500)  # 150 ms warm-up
+        s0 = eng.stats()
+        ms = timed_sim(eng, steps, dev)
+        s1 = eng.stats()
+        ks = kernel_split(eng, 150)
+        eng.close()
+        ev = s1["syn_events"] - s0["syn_events"]
+        out[prec] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
+                     "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / n / (sim_ms * 1e-3), "build_s": build,
+                     "kernels": ks}
+    return out
+
+
+def measure_serving(args, dev):
+    """Serving sweep: Poisson arrivals (20/s) of Brunel-type requests.  The
+    batched FP32 server (continuous batching) against the plain FP64 server
+    (one request at a time): aggregate synaptic events/s with every request
+    queued at the start (saturation), latency p50/p99 under real-time
+    arrivals, and the rate / CV-ISI error of the batched results against the
+    FP64 results of the same requests."""
+    import copy
+
+    from nestgpu import serving
+
+    reqs = serving.make_requests(count=args.serving_requests, rate_hz=20.0, seed=2026)
+
+    def fresh():
+        return [copy.copy(r) for r in reqs]
+
+    out = {"workload": f"{len(reqs)} iaf_psc_exp Brunel-type requests, Poisson arrivals 20/s, N ~ log-U[1e3, 5e4], "
+                       "T ~ U[500, 2000] ms"}
+    eng = serving.new_engine("fp32", device=dev.index)
+    serving.run_batched(fresh()[:8], eng, realtime=False)  # warm-up: graphs and host buffers
+    b32, st = serving.run_batched(fresh(), eng, realtime=False)
+    gathered = eng.stats()["gather_slices"]
+    rt, st_rt = serving.run_batched(fresh(), eng, realtime=True)
+    eng.close()
+    eng = serving.new_engine("fp64", capacity_neurons=60_000, capacity_edges=80_000_000, max_networks=2,
+                             device=dev.index)
+    serving.run_plain(fresh()[:2], eng, realtime=False)
+    p64, sp = serving.run_plain(fresh(), eng, realtime=False)
+    eng.close()
+    out["batched_fp32"] = {"syn_events_per_s": st["syn_events_per_s"], "makespan_s": st["makespan_s"],
+                           "syn_events": st["syn_events"], "gather_slices": gathered,
+                           "latency_saturated": serving.latency_summary(b32),
+                           "latency_realtime": serving.latency_summary(rt),
+                           "realtime_makespan_s": st_rt["makespan_s"]}
+    out["plain_fp64"] = {"syn_events_per_s": sp["syn_events_per_s"], "makespan_s": sp["makespan_s"],
+                         "syn_events": sp["syn_events"], "latency_saturated": serving.latency_summary(p64)}
+    out["batched_over_plain"] = st["syn_events_per_s"] / sp["syn_events_per_s"]
+    out["accuracy_fp32_vs_fp64"] = serving.accuracy(b32, p64)
+    return out
+
+
 def run_engine(args):
     import torch
 
@@ -377,6 +508,13 @@ def run_engine(args):
     single32 = measure(args, nest, KERNEL, "single", "fp32", 1, seed, local, dev, pg)
     batched = measure(args, nest, KERNEL, "batched", "fp32", args.batch, seed, local, dev, pg) \
         if args.batch > 1 else single32
+    extra = {}
+    if not args.no_layered:
+        extra["layered_8pop"] = measure_layered(args, dev)
+    if not args.no_aeif:
+        extra["aeif_50k"] = measure_aeif(args, dev)
+    if not args.no_serving:
+        extra["serving_sweep"] = measure_serving(args, dev)
     cpu = None
     if rank == 0 and not args.no_cpu:
         from nestgpu import workloads
@@ -404,7 +542,7 @@ def run_engine(args):
                    "parallelism": f"replicas{ws}", "l2": "graph larger than L2 (no flush needed)",
                    "rtf_per_network": r["rtf"],
                    "plain_fp64_single_network": brief(plain), "fp32_single_network": brief(single32),
-                   "batched_over_plain": r["value"] / plain["value"]},
+                   "batched_over_plain": r["value"] / plain["value"], **extra},
         "gpu_launches": int(r["launches"]),
         "clocks": r["clocks"],
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": ach, "peak": peak, "unit": "GB/s",

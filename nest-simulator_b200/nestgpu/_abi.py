@@ -432,6 +432,11 @@ class Engine:
         check(self.L.ng_net_get_var(self.handle, int(nid), name.encode(), _p(out)))
         return out
 
+    def net_connection_count(self, nid):
+        n = ctypes.c_int64(0)
+        check(self.L.ng_net_get_connections(self.handle, int(nid), None, None, None, None, 0, ctypes.byref(n)))
+        return n.value
+
     def net_get_connections(self, nid):
         """(source, target, weight, delay_steps) of the network, local ids."""
         n = ctypes.c_int64(0)

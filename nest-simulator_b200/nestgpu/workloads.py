@@ -142,3 +142,52 @@ def layered_add(eng, spec, steps, record=True):
     if nid is None:
         raise RuntimeError("the layered network does not fit the engine")
     return nid
+
+
+# ---------------------------------------------------------------------------
+# c3: adaptive-integrator network, 50,000 aeif_cond_alpha neurons
+# ---------------------------------------------------------------------------
+def aeif_spec(seed=77, n_exc=40000, n_inh=10000):
+    """aeif_cond_alpha network: fixed_indegree K = 1,000 (800 exc, 200 inh),
+    conductance weights g_E = 1 nS, g_I = -5 nS (inhibitory conductance
+    5 nS), a = 4 nS, b = 80.5 pA, Delta_T = 2 mV, tau_w = 144 ms, delay
+    1.5 ms; Poisson drive 10 kHz x 0.5 nS per neuron; V_m(0) ~ U[E_L, V_th)
+    from seed.  tau_syn_ex = 1 ms (with the model's default 0.2 ms this
+    drive keeps every neuron below threshold: mean conductance 2.7 nS, 6 mV
+    of depolarisation); the other parameters are the model's defaults."""
+    return {"n_exc": n_exc, "n_inh": n_inh, "k_exc": 800, "k_inh": 200, "g_E": 1.0, "g_I": -5.0, "a": 4.0,
+            "b": 80.5, "Delta_T": 2.0, "tau_w": 144.0, "tau_syn_ex": 1.0, "delay_ms": 1.5, "nu_ext_hz": 10000.0,
+            "w_ext": 0.5, "E_L": -70.6, "V_th": -50.4, "seed": seed}
+
+
+def aeif_engine(spec, precision="fp64", device=0, graph_slices=64):
+    """A serving engine sized for one aeif network (fixed_indegree graph
+    drawn on the device)."""
+    from . import _abi
+
+    n = spec["n_exc"] + spec["n_inh"]
+    d = int(round(spec["delay_ms"] / 0.1))
+    K = spec["k_exc"] + spec["k_inh"]
+    prec = _abi.NG_FP32 if precision == "fp32" else _abi.NG_FP64
+    eng = _abi.Engine([(_abi.NG_AEIF_COND_ALPHA, n)], 0.1, d, d, precision=prec, device=device, serving=True,
+                      max_networks=1, edge_capacity=n * (K + 3) + 1024,
+                      max_abs_weight=4 * max(abs(spec["g_E"]), abs(spec["g_I"]), spec["w_ext"]))
+    eng.set_graph_slices(graph_slices)
+    return eng
+
+
+def aeif_add(eng, spec, steps, record=True):
+    """Admit the aeif network into `eng`; returns its network id."""
+    n = spec["n_exc"] + spec["n_inh"]
+    rng = np.random.default_rng(spec["seed"])
+    V0 = rng.uniform(spec["E_L"], spec["V_th"], n)
+    d = int(round(spec["delay_ms"] / 0.1))
+    build = dict(n_exc=spec["n_exc"], k_exc=spec["k_exc"], k_inh=spec["k_inh"], w_exc=spec["g_E"], w_inh=spec["g_I"],
+                 delay_steps=d, allow_autapses=0, seed=spec["seed"] * 104729 + 3)
+    var = {"a": spec["a"], "b": spec["b"], "Delta_T": spec["Delta_T"], "tau_w": spec["tau_w"],
+           "tau_syn_ex": spec["tau_syn_ex"], "V_m": V0}
+    nid = eng.net_add(n, steps, spec["seed"], var, build=build, poisson=(spec["nu_ext_hz"], spec["w_ext"], d),
+                      record=record)
+    if nid is None:
+        raise RuntimeError("the aeif network does not fit the engine")
+    return nid
