@@ -58,7 +58,24 @@ def parse():
     ap.add_argument("--no-layered", action="store_true")
     ap.add_argument("--no-aeif", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--forms", default="plain,fp32,batched",
+                    help="forms of the Brunel network to time (the line's value is the batched one)")
     return ap.parse_args()
+
+
+def load_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` on `workload` from the ncu summary
+    profiles/roofline_traffic.txt (lines: kernel workload bytes_per_launch),
+    or None."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+                return float(parts[2])
+    return None
 
 
 def load_peaks():
@@ -321,7 +338,9 @@ def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg):
         return {"launches": launches, "avg_us": 1e3 * avg, "alg_bytes_per_launch": nbytes,
                 "achieved_gbs": nbytes / (avg * 1e-3) / 1e9 if avg > 0 else None}
 
-    kernels = {"k_update_iaf2": kern(n_upd, upd_ms, upd_bytes), "k_deliver": kern(n_del, del_ms, del_bytes)}
+    # the engine's dispatch: one thread per neuron from 20,000 neurons on, the two-phase kernel below
+    upd_name = "k_update_iaf" if N >= 20000 else "k_update_iaf2"
+    kernels = {upd_name: kern(n_upd, upd_ms, upd_bytes), "k_deliver": kern(n_del, del_ms, del_bytes)}
     res = {"ms": ms_max, "events": ev_all, "clocks": clocks, "kernels": kernels, "copies": copies,
            "launches": (s1["update_launches"] - s0["update_launches"]) +
                        (s1["deliver_launches"] - s0["deliver_launches"]) + 1,
@@ -504,10 +523,11 @@ def run_engine(args):
     from nestgpu.kernel import KERNEL
 
     seed = 4242 + 1000 * rank
-    plain = measure(args, nest, KERNEL, "plain", "fp64", 1, seed, local, dev, pg)
-    single32 = measure(args, nest, KERNEL, "single", "fp32", 1, seed, local, dev, pg)
+    forms = set(args.forms.split(","))
+    plain = measure(args, nest, KERNEL, "plain", "fp64", 1, seed, local, dev, pg) if "plain" in forms else None
+    single32 = measure(args, nest, KERNEL, "single", "fp32", 1, seed, local, dev, pg) if "fp32" in forms else None
     batched = measure(args, nest, KERNEL, "batched", "fp32", args.batch, seed, local, dev, pg) \
-        if args.batch > 1 else single32
+        if args.batch > 1 and "batched" in forms else single32
     extra = {}
     if not args.no_layered:
         extra["layered_8pop"] = measure_layered(args, dev)
@@ -528,6 +548,8 @@ def run_engine(args):
     ach = dom["achieved_gbs"]
 
     def brief(x):
+        if x is None:
+            return None
         return {"value": x["value"], "rtf": x["rtf"], "e2e": x.get("e2e"), "spikes_per_step": x["spikes"] /
                 max(1, args.steps + 1), "kernels": {k: {"avg_us": v["avg_us"], "achieved_gbs": v["achieved_gbs"]}
                                                     for k, v in x["kernels"].items()}}
@@ -542,11 +564,12 @@ def run_engine(args):
                    "parallelism": f"replicas{ws}", "l2": "graph larger than L2 (no flush needed)",
                    "rtf_per_network": r["rtf"],
                    "plain_fp64_single_network": brief(plain), "fp32_single_network": brief(single32),
-                   "batched_over_plain": r["value"] / plain["value"], **extra},
+                   "batched_over_plain": r["value"] / plain["value"] if plain else None, **extra},
         "gpu_launches": int(r["launches"]),
         "clocks": r["clocks"],
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": ach, "peak": peak, "unit": "GB/s",
-                     "frac": (ach / peak) if ach else None, "peak_kind": peak_kind, "traffic": None,
+                     "frac": (ach / peak) if ach else None, "peak_kind": peak_kind,
+                     "traffic": load_traffic(dom_name, f"brunel_x{r['copies']}_{r['precision']}"),
                      "kernels": r["kernels"]},
         "e2e": r.get("e2e"),
         "cpu_baseline": cpu,
