@@ -1648,85 +1648,93 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
     prow[ s + 1 ] = prow[ s ] + ( ( deg + 3 ) & ~3ll );
   }
   const int64_t np = prow[ n_src ];
-  // per-edge channel and effective weight by the target's model
-  std::vector< int > model_of_block;
-  std::vector< int64_t > bend;
-  for ( auto& b : e->blk )
-  {
-    model_of_block.push_back( b.model );
-    bend.push_back( b.off + b.n );
-  }
-  std::vector< uint32_t > tdc( ( size_t ) std::max< int64_t >( np, 4 ), 0u );
-  std::vector< double > weff( ( size_t ) std::max< int64_t >( np, 4 ), 0.0 );
-  double maxabs = 0.0;
-  for ( int64_t s = 0; s < n_src; ++s )
-  {
-    int64_t k = prow[ s ];
-    for ( int64_t j = row_ptr[ s ]; j < row_ptr[ s + 1 ]; ++j, ++k )
-    {
-      const int64_t t = target[ j ];
-      const int32_t d = delay_steps[ j ];
-      if ( t < 0 || t >= e->N )
-        return fail( NG_ERR_ARG, "ng_set_connections: target out of range" );
-      if ( d < e->cfg.min_delay || d > e->cfg.max_delay )
-        return fail( NG_ERR_ARG, "ng_set_connections: delay outside [min_delay, max_delay]" );
-      const double wv = weight[ j ];
-      if ( !std::isfinite( wv ) )
-        return fail( NG_ERR_ARG, "ng_set_connections: weight not finite" );
-      const int bk = ( int ) ( std::upper_bound( bend.begin(), bend.end(), t ) - bend.begin() );
-      const int model = model_of_block[ bk ];
-      uint32_t ch = 0;
-      double we = wv;
-      if ( model == NG_IAF_PSC_EXP )
-        ch = wv > 0 ? 0u : 1u;  // iaf_psc_exp.cpp:351-362
-      else if ( model == NG_AEIF_COND_ALPHA && !( wv > 0.0 ) )
-      {
-        ch = 1u;  // aeif_cond_alpha.cpp:536-550 stores -w in the inhibitory buffer
-        we = -wv;
-      }
-      tdc[ k ] = ( uint32_t ) t | ( ( uint32_t ) d << e->tbits ) | ( ch << 31 );
-      weff[ k ] = we;
-      maxabs = std::max( maxabs, std::fabs( we ) );
-    }
-  }
+  // the edges are packed on the device: copy the caller's arrays as they are
   int rc;
+  DevBuf d_rp, d_prow, d_tgt, d_w, d_d, d_scr;
+  auto free_tmp = [ & ]() {
+    for ( DevBuf* b : { &d_rp, &d_prow, &d_tgt, &d_w, &d_d, &d_scr } )
+      cudaFree( b->p );
+  };
+  PackSpec ps {};
+  ps.n_blocks = ( int ) e->blk.size();
+  for ( int k = 0; k < ps.n_blocks; ++k )
+  {
+    ps.bend[ k ] = e->blk[ k ].off + e->blk[ k ].n;
+    ps.model[ k ] = e->blk[ k ].model;
+  }
+  ps.N = e->N;
+  ps.min_d = e->cfg.min_delay;
+  ps.max_d = e->cfg.max_delay;
+  ps.tbits = e->tbits;
+  if ( ( rc = e->upload( d_rp, row_ptr, ( size_t ) ( n_src + 1 ) * 8 ) ) || ( rc = e->upload( d_prow, prow.data(), prow.size() * 8 ) )
+    || ( rc = e->upload( d_tgt, target, ( size_t ) nnz * 4 ) ) || ( rc = e->upload( d_w, weight, ( size_t ) nnz * 8 ) )
+    || ( rc = e->upload( d_d, delay_steps, ( size_t ) nnz * 4 ) ) || ( rc = e->alloc( d_scr, 16 ) ) )
+  {
+    free_tmp();
+    return rc;
+  }
+  unsigned long long host_scr[ 2 ] = { 0ull, 0ull };
+  if ( nnz > 0 )
+  {
+    const unsigned g = ( unsigned ) std::min< int64_t >( ( nnz + 255 ) / 256, ( int64_t ) e->sms * 16 );
+    k_edge_check<<< g, 256, 0, e->stream >>>( nnz, ( const int32_t* ) d_tgt.p, ( const double* ) d_w.p,
+      ( const int32_t* ) d_d.p, ps, ( unsigned long long* ) d_scr.p, ( int* ) ( ( unsigned long long* ) d_scr.p + 1 ) );
+    CU( cudaGetLastError() );
+    CU( cudaMemcpyAsync( host_scr, d_scr.p, 16, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  const int bad = ( int ) ( host_scr[ 1 ] & 0xffffffffull );
+  if ( bad )
+  {
+    free_tmp();
+    if ( bad & 1 )
+      return fail( NG_ERR_ARG, "ng_set_connections: target out of range" );
+    if ( bad & 2 )
+      return fail( NG_ERR_ARG, "ng_set_connections: delay outside [min_delay, max_delay]" );
+    return fail( NG_ERR_ARG, "ng_set_connections: weight not finite" );
+  }
+  double maxabs = 0.0;
+  std::memcpy( &maxabs, &host_scr[ 0 ], 8 );
   {
     std::vector< int32_t > plen( ( size_t ) n_src );
     for ( int64_t sidx = 0; sidx < n_src; ++sidx )
       plen[ sidx ] = ( int32_t ) ( prow[ sidx + 1 ] - prow[ sidx ] );
-    if ( ( rc = e->upload( e->row_beg, prow.data(), ( size_t ) n_src * sizeof( int64_t ) ) ) )
-      return rc;
-    if ( ( rc = e->upload( e->row_len, plen.data(), plen.size() * sizeof( int32_t ) ) ) )
-      return rc;
-  }
-  if ( ( rc = e->upload( e->real_deg, rdeg.data(), rdeg.size() * sizeof( int32_t ) ) ) )
-    return rc;
-  if ( ( rc = e->upload( e->tdc, tdc.data(), tdc.size() * sizeof( uint32_t ) ) ) )
-    return rc;
-  if ( e->prec == NG_FP64 )
-  {
-    if ( ( rc = e->upload( e->w, weff.data(), weff.size() * sizeof( double ) ) ) )
-      return rc;
-    e->fx_inv = 1.0;
-  }
-  else
-  {
-    // int32 fixed point with a power-of-two scale: |w| * 2^S < 2^31
-    int S = 0;
-    if ( maxabs > 0 )
+    if ( ( rc = e->upload( e->row_beg, prow.data(), ( size_t ) n_src * sizeof( int64_t ) ) )
+      || ( rc = e->upload( e->row_len, plen.data(), plen.size() * sizeof( int32_t ) ) )
+      || ( rc = e->upload( e->real_deg, rdeg.data(), rdeg.size() * sizeof( int32_t ) ) ) )
     {
-      S = ( int ) std::floor( std::log2( 2147483647.0 / maxabs ) );
-      S = std::max( -30, std::min( S, 60 ) );
-      while ( S > -30 && std::ldexp( maxabs, S ) >= 2147483647.0 )
-        --S;
-    }
-    std::vector< int32_t > wf( weff.size(), 0 );
-    for ( size_t k = 0; k < weff.size(); ++k )
-      wf[ k ] = ( int32_t ) std::llrint( std::ldexp( weff[ k ], S ) );
-    if ( ( rc = e->upload( e->w, wf.data(), wf.size() * sizeof( int32_t ) ) ) )
+      free_tmp();
       return rc;
-    e->fx_inv = std::ldexp( 1.0, -S );
+    }
+    CU( cudaStreamSynchronize( e->stream ) );  // the host vectors go out of scope
   }
+  const bool fx = e->prec != NG_FP64;
+  // int32 fixed point with a power-of-two scale: |w| * 2^S < 2^31
+  int S = 0;
+  if ( fx && maxabs > 0 )
+  {
+    S = ( int ) std::floor( std::log2( 2147483647.0 / maxabs ) );
+    S = std::max( -30, std::min( S, 60 ) );
+    while ( S > -30 && std::ldexp( maxabs, S ) >= 2147483647.0 )
+      --S;
+  }
+  const size_t np4 = ( size_t ) std::max< int64_t >( np, 4 );
+  if ( ( rc = e->alloc( e->tdc, np4 * sizeof( uint32_t ) ) ) || ( rc = e->alloc( e->w, np4 * ( fx ? 4 : 8 ) ) ) )
+  {
+    free_tmp();
+    return rc;
+  }
+  if ( n_src > 0 && nnz > 0 )
+  {
+    const unsigned g = ( unsigned ) ( ( n_src * 32 + 255 ) / 256 );
+    k_pack_edges<<< g, 256, 0, e->stream >>>( n_src, ( const long long* ) d_rp.p, ( const long long* ) d_prow.p,
+      ( const int32_t* ) d_tgt.p, ( const double* ) d_w.p, ( const int32_t* ) d_d.p, ps, fx ? 1 : 0, std::ldexp( 1.0, S ),
+      ( uint32_t* ) e->tdc.p, e->w.p );
+    CU( cudaGetLastError() );
+  }
+  CU( cudaStreamSynchronize( e->stream ) );
+  free_tmp();
+  e->fx_inv = fx ? std::ldexp( 1.0, -S ) : 1.0;
   e->nnz_padded = np;
   e->chunks_all_src = 0;
   e->chunks_max_gen = 0;

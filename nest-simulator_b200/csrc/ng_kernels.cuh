@@ -1465,6 +1465,111 @@ k_deliver( Net d )
   }
 }
 
+// ---------------------------------------------------------------------
+// Graph upload (ng_set_connections): the caller's CSR (row pointers,
+// targets, weights, delays) is copied as it is and packed on the device
+// into padded rows of edge words and stored weights -- the channel by the
+// target model's sign rule (iaf_psc_exp.cpp:351-362, aeif_cond_alpha.cpp:
+// 536-550), the aeif inhibitory weight stored as -w, the precision form's
+// weights in int32 fixed point.
+// ---------------------------------------------------------------------
+struct PackSpec
+{
+  int n_blocks;
+  long long bend[ 8 ];  // end of each block's neuron range
+  int model[ 8 ];
+  long long N;
+  int min_d, max_d, tbits;
+};
+
+__device__ __forceinline__ void
+edge_channel( const PackSpec& ps, int32_t t, double wv, uint32_t& ch, double& we )
+{
+  int bk = 0;
+  while ( bk + 1 < ps.n_blocks && t >= ps.bend[ bk ] )
+    ++bk;
+  ch = 0u;
+  we = wv;
+  if ( ps.model[ bk ] == NG_IAF_PSC_EXP_ID )
+    ch = wv > 0 ? 0u : 1u;
+  else if ( ps.model[ bk ] == 2 && !( wv > 0.0 ) )
+  {
+    ch = 1u;
+    we = -wv;
+  }
+}
+
+// validation (error bits: 1 target, 2 delay, 4 weight) and the largest |stored weight|
+__global__ void
+k_edge_check( long long nnz, const int32_t* tgt, const double* w, const int32_t* dl, PackSpec ps,
+  unsigned long long* absmax, int* err )
+{
+  unsigned long long m = 0ull;
+  int e = 0;
+  for ( long long j = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += ( long long ) gridDim.x * blockDim.x )
+  {
+    const int32_t t = tgt[ j ];
+    const int32_t d = dl[ j ];
+    const double wv = w[ j ];
+    if ( t < 0 || t >= ps.N )
+    {
+      e |= 1;
+      continue;
+    }
+    if ( d < ps.min_d || d > ps.max_d )
+      e |= 2;
+    if ( !isfinite( wv ) )
+    {
+      e |= 4;
+      continue;
+    }
+    uint32_t ch;
+    double we;
+    edge_channel( ps, t, wv, ch, we );
+    const unsigned long long b = ( unsigned long long ) __double_as_longlong( fabs( we ) );
+    m = b > m ? b : m;  // the bit patterns of non-negative doubles order like their values
+  }
+#pragma unroll
+  for ( int o = 16; o > 0; o >>= 1 )
+  {
+    const unsigned long long v = __shfl_xor_sync( FULL, m, o );
+    m = v > m ? v : m;
+    e |= __shfl_xor_sync( FULL, e, o );
+  }
+  if ( ( threadIdx.x & 31 ) == 0 )
+  {
+    if ( m )
+      atomicMax( absmax, m );
+    if ( e )
+      atomicOr( err, e );
+  }
+}
+
+// one warp per source row: edge j of the row goes to padded position prow[s] + j
+__global__ void
+k_pack_edges( long long n_src, const long long* row_ptr, const long long* prow, const int32_t* tgt, const double* w,
+  const int32_t* dl, PackSpec ps, int fx, double scale, uint32_t* tdc, void* wout )
+{
+  const long long s = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  const int lane = threadIdx.x & 31;
+  if ( s >= n_src )
+    return;
+  const long long r0 = row_ptr[ s ], r1 = row_ptr[ s + 1 ], p0 = prow[ s ];
+  for ( long long j = r0 + lane; j < r1; j += 32 )
+  {
+    const int32_t t = tgt[ j ];
+    uint32_t ch;
+    double we;
+    edge_channel( ps, t, w[ j ], ch, we );
+    const long long k = p0 + ( j - r0 );
+    tdc[ k ] = ( uint32_t ) t | ( ( uint32_t ) dl[ j ] << ps.tbits ) | ( ch << 31 );
+    if ( fx )
+      reinterpret_cast< int32_t* >( wout )[ k ] = ( int32_t ) llrint( we * scale );
+    else
+      reinterpret_cast< double* >( wout )[ k ] = we;
+  }
+}
+
 // Host-side ctl edits between groups (log drain, trace window).
 __global__ void
 k_set_ctl( Ctl* ctl, long long log_base, long long trace_row0, int reset_log, int log_sel )
