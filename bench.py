@@ -425,9 +425,10 @@ def measure_layered(args, dev, sim_ms=1000.0):
     out = {"workload": "layered 8-population iaf_psc_exp network, 77,169 neurons, pairwise_bernoulli "
                        "p ~ U[0.01, 0.15], 1,000 ms", "neurons": sum(spec["sizes"])}
     steps = int(round(sim_ms / 0.1))
-    for prec in ("fp64", "fp32"):
+    for form in ("fp64", "fp32", "fp32_ring32"):
+        prec = form[:4]
         t0 = time.perf_counter()
-        eng = workloads.layered_engine(spec, prec, device=dev.index)
+        eng = workloads.layered_engine(spec, prec, device=dev.index, ring32=form.endswith("ring32"))
         nid = workloads.layered_add(eng, spec, 10 * steps)
         build = time.perf_counter() - t0
         eng.simulate(1000)  # 100 ms warm-up (graphs built)
@@ -438,9 +439,10 @@ def measure_layered(args, dev, sim_ms=1000.0):
         out["synapses"] = eng.net_connection_count(nid)
         eng.close()
         ev = s1["syn_events"] - s0["syn_events"]
-        out[prec] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
+        out[form] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
                      "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / out["neurons"] / (sim_ms * 1e-3),
                      "build_s": build, "kernels": ks}
+    out["fp32_ring32"]["ring_bound"] = workloads.layered_ring_bound(spec)
     return out
 
 

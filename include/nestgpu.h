@@ -68,6 +68,10 @@ typedef struct
   int32_t max_networks;    /* serving: network slots */
   int64_t edge_capacity;   /* serving: edge pool, padding included */
   double max_abs_weight;   /* serving, FP32 form: largest |weight| (sets the fixed-point scale) */
+  int32_t ring32;          /* serving, FP32 form: 32-bit fixed-point ring cells (half the atomic width)
+                              instead of 64-bit; needs ring_bound */
+  double ring_bound;       /* with ring32: largest sum of |weight| over one neuron's in-edges; sets the
+                              scale so that no ring cell can overflow, checked for every admitted network */
 } ng_config;
 
 /* Counters and timings of an engine. */

@@ -220,6 +220,7 @@ struct ng_engine
   DevBuf ring, row_beg, row_len, real_deg, tdc, w, ent, log, rec, pois, pois_w, pois_d, pois_ref, pois_cdf, trace_col,
     trace, sched_step, sched_src, ctl;
   int32_t tbits = 1;
+  int ring_bytes = 8;  // 4: 32-bit fixed-point ring cells (serving, FP32 form)
   uint32_t tmask = 1, dmask = 0;
   double fx_inv = 1.0;
   int64_t nnz_padded = 0, ent_cap = 0, log_cap = 0, n_sched = 0, n_rec = 0;
@@ -272,7 +273,7 @@ struct ng_engine
 
   // ---- serving: networks added to and removed from the running engine
   bool serving = false;
-  DevBuf d_nid, d_step0, d_until, d_off, d_key, sc_src, sc_cnt, sc_fill, sc_beg, sc_plen, sc_total, sc_sb;
+  DevBuf d_nid, d_step0, d_until, d_off, d_key, sc_src, sc_cnt, sc_fill, sc_beg, sc_plen, sc_total, sc_sb, sc_bound;
   std::vector< int32_t > nid_host;
   // Spikes of a serving network: the raw log entries of each group, as
   // grouped by network on the device, decoded only when they are read.
@@ -426,7 +427,8 @@ struct ng_engine
       free_gin[ 0 ] = E;
     }
     // one fixed-point scale for every network (FP32 form)
-    const double mx = cfg.max_abs_weight > 0 ? cfg.max_abs_weight : 1e4;
+    // 32-bit rings: the scale keeps the largest possible cell sum inside 31 bits
+    const double mx = ring_bytes == 4 ? cfg.ring_bound : cfg.max_abs_weight > 0 ? cfg.max_abs_weight : 1e4;
     fx_S = ( int ) std::floor( std::log2( 2147483647.0 / mx ) );
     fx_S = std::max( -30, std::min( fx_S, 60 ) );
     fx_inv = prec == NG_FP64 ? 1.0 : std::ldexp( 1.0, -fx_S );
@@ -494,7 +496,7 @@ struct ng_engine
     DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
       &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl, &d_nid, &d_step0, &d_until, &d_off,
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
-      &net_spk, &log_sorted, &log_cnt, &log_off };
+      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -683,6 +685,7 @@ struct ng_engine
     d.tmask = tmask;
     d.dmask = dmask;
     d.ring = ring.p;
+    d.ring32 = ring_bytes == 4 ? 1 : 0;
     d.fx_inv = fx_inv;
     d.row_beg = ( const int64_t* ) row_beg.p;
     d.row_len = ( const int32_t* ) row_len.p;
@@ -1418,7 +1421,10 @@ ng_create( const ng_config* cfg, ng_engine** out )
     }
   }
   // ring [L][C][N]
-  if ( ( rc = e->alloc( e->ring, ( size_t ) e->L * e->C * ( size_t ) N * 8 ) ) )
+  if ( cfg->ring32 && !( cfg->serving && cfg->precision == NG_FP32 && cfg->ring_bound > 0 ) )
+    return bail( fail( NG_ERR_ARG, "ng_create: ring32 needs a serving engine in the FP32 form and a ring_bound" ) );
+  e->ring_bytes = cfg->ring32 ? 4 : 8;
+  if ( ( rc = e->alloc( e->ring, ( size_t ) e->L * e->C * ( size_t ) N * e->ring_bytes ) ) )
     return bail( rc );
   // empty CSR: every source has no edges
   if ( ( rc = e->alloc( e->row_beg, ( size_t ) e->n_src * sizeof( int64_t ) ) ) )
@@ -2451,6 +2457,27 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       e->stream ) );
     CU( cudaStreamSynchronize( e->stream ) );
   }
+  // 32-bit rings: no ring cell of this network may exceed 31 bits
+  if ( e->ring_bytes == 4 && ne_used > 0 )
+  {
+    int rc2;
+    if ( ( rc2 = e->grow( e->sc_bound, ( size_t ) n * 8 + 8 ) ) )
+      return undo( rc2 );
+    CU( cudaMemsetAsync( e->sc_bound.p, 0, ( size_t ) n * 8 + 8, e->stream ) );
+    unsigned long long* sums = ( unsigned long long* ) e->sc_bound.p;
+    const unsigned gg = ( unsigned ) std::min< int64_t >( ( ne_used + 255 ) / 256, ( int64_t ) e->sms * 16 );
+    k_in_abs_sum<<< gg, 256, 0, e->stream >>>( e0, ne_used, ( const uint32_t* ) e->tdc.p, ( const int32_t* ) e->w.p,
+      e->tmask, n0, sums );
+    k_max_u64<<< ( unsigned ) std::min< int64_t >( ( n + 255 ) / 256, ( int64_t ) e->sms * 4 ), 256, 0, e->stream >>>(
+      n, sums, sums + n );
+    CU( cudaGetLastError() );
+    unsigned long long mx = 0;
+    CU( cudaMemcpyAsync( &mx, sums + n, 8, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+    if ( mx > 2147483647ull )
+      return undo( fail( NG_ERR_ARG, "ng_net_add: the network's in-edge weight sum exceeds the engine's ring_bound "
+                                     "(32-bit ring cells could overflow)" ) );
+  }
   // give back the unused tail of the edge reservation
   if ( ne_used < ne_need )
     ng_engine::give_run( e->free_edges, e0 + ne_used, ne_need - ne_used );
@@ -2509,7 +2536,8 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   CU( cudaMemcpyAsync( ( long long* ) e->d_off.p + id, &off, 8, cudaMemcpyHostToDevice, e->stream ) );
   CU( cudaMemcpyAsync( ( uint2* ) e->d_key.p + id, &key, 8, cudaMemcpyHostToDevice, e->stream ) );
   k_fill_i32<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( ( int32_t* ) e->d_nid.p + n0, n, id );
-  CU( cudaMemset2DAsync( ( char* ) e->ring.p + n0 * 8, ( size_t ) e->N * 8, 0, ( size_t ) n * 8, ( size_t ) e->L * e->C,
+  CU( cudaMemset2DAsync( ( char* ) e->ring.p + n0 * e->ring_bytes, ( size_t ) e->N * e->ring_bytes, 0,
+    ( size_t ) n * e->ring_bytes, ( size_t ) e->L * e->C,
     e->stream ) );
   CU( cudaGetLastError() );
   CU( cudaStreamSynchronize( e->stream ) );

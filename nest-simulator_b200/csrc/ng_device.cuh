@@ -105,6 +105,7 @@ struct Net
   int64_t pois_start, pois_stop;
   uint32_t key0, key1;
   int has_pois;
+  int ring32;  // precision form with 32-bit ring cells
   const int32_t* trace_col;
   double* trace;
   int32_t n_trace_idx, trace_interval, n_trace_vars;

@@ -461,6 +461,9 @@ __device__ __forceinline__ typename RingVal< FIX >::type
 ring_ld( const Net& d, int slot, int ch, int64_t i )
 {
   const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + i;
+  if constexpr ( FIX )
+    if ( d.ring32 )
+      return reinterpret_cast< const int32_t* >( d.ring )[ idx ];
   return reinterpret_cast< const typename RingVal< FIX >::type* >( d.ring )[ idx ];
 }
 
@@ -479,6 +482,12 @@ __device__ __forceinline__ void
 ring_clear( const Net& d, int slot, int ch, int64_t i )
 {
   const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + i;
+  if constexpr ( FIX )
+    if ( d.ring32 )
+    {
+      reinterpret_cast< int32_t* >( d.ring )[ idx ] = 0;
+      return;
+    }
   reinterpret_cast< typename RingVal< FIX >::type* >( d.ring )[ idx ] = 0;
 }
 
@@ -1371,8 +1380,13 @@ apply_chunk( const Net& d, const ChunkLane< FIX >& c )
       slot -= d.L;
     const int64_t idx = ( ( int64_t ) slot * d.C + ( c.t[ k ] >> 31 ) ) * d.N + tgt;
     if constexpr ( FIX )
-      atomicAdd( ( unsigned long long* ) d.ring + idx,
-        ( unsigned long long ) ( ( long long ) c.w[ k ] * ( long long ) c.mult ) );
+    {
+      if ( d.ring32 )  // the admission bound keeps every cell inside 32 bits
+        atomicAdd( ( int* ) d.ring + idx, c.w[ k ] * c.mult );
+      else
+        atomicAdd( ( unsigned long long* ) d.ring + idx,
+          ( unsigned long long ) ( ( long long ) c.w[ k ] * ( long long ) c.mult ) );
+    }
     else
       atomicAdd( ( double* ) d.ring + idx, c.mult == 1 ? c.w[ k ] : c.w[ k ] * ( double ) c.mult );
   }

@@ -540,7 +540,10 @@ k_gather( Net d )
           if ( n == 0u )
             continue;
           const int64_t idx = ( ( int64_t ) slot * d.C + ( ty ? g.ci : g.ce ) ) * d.N + t;
-          ring[ idx ] += ( long long ) n * ( long long ) ( ty ? g.wi : g.we );
+          if ( d.ring32 )
+            reinterpret_cast< int32_t* >( ring )[ idx ] += ( int32_t ) n * ( ty ? g.wi : g.we );
+          else
+            ring[ idx ] += ( long long ) n * ( long long ) ( ty ? g.wi : g.we );
         }
       }
     }
@@ -616,6 +619,42 @@ k_log_scatter( const Ctl* ctl, const uint2* half, int64_t cap, int n_nets, const
     if ( id < ( unsigned ) n_nets )
       out[ off[ id ] + atomicAdd( &fill[ id ], 1u ) ] = e;
   }
+}
+
+}  // namespace ng
+
+namespace ng
+{
+
+// Largest sum of |stored weight| over one target's in-edges in a region of
+// the edge pool (the ring-cell bound of a 32-bit ring).
+__global__ void
+k_in_abs_sum( long long e0, long long ne, const uint32_t* tdc, const int32_t* w, uint32_t tmask, long long n0,
+  unsigned long long* sum )
+{
+  for ( long long k = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; k < ne; k += ( long long ) gridDim.x * blockDim.x )
+  {
+    const int32_t wv = w[ e0 + k ];
+    if ( wv != 0 )
+      atomicAdd( sum + ( ( long long ) ( tdc[ e0 + k ] & tmask ) - n0 ),
+        ( unsigned long long ) ( wv < 0 ? -( long long ) wv : ( long long ) wv ) );
+  }
+}
+
+__global__ void
+k_max_u64( long long n, const unsigned long long* v, unsigned long long* out )
+{
+  unsigned long long m = 0ull;
+  for ( long long k = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; k < n; k += ( long long ) gridDim.x * blockDim.x )
+    m = v[ k ] > m ? v[ k ] : m;
+#pragma unroll
+  for ( int o = 16; o > 0; o >>= 1 )
+  {
+    const unsigned long long x = __shfl_xor_sync( FULL, m, o );
+    m = x > m ? x : m;
+  }
+  if ( ( threadIdx.x & 31 ) == 0 && m )
+    atomicMax( out, m );
 }
 
 }  // namespace ng

@@ -55,6 +55,8 @@ class NGConfig(ctypes.Structure):
         ("max_networks", ctypes.c_int32),
         ("edge_capacity", ctypes.c_int64),
         ("max_abs_weight", ctypes.c_double),
+        ("ring32", ctypes.c_int32),
+        ("ring_bound", ctypes.c_double),
     ]
 
 
@@ -231,7 +233,7 @@ class Engine:
 
     def __init__(self, blocks, h, min_delay, max_delay, n_generators=0, precision=NG_FP64, device=0,
                  tics_per_ms=1000.0, spike_log_capacity=0, start_step=0, serving=False, max_networks=0,
-                 edge_capacity=0, max_abs_weight=0.0):
+                 edge_capacity=0, max_abs_weight=0.0, ring32=False, ring_bound=0.0):
         L = load()
         cfg = NGConfig()
         cfg.device = int(device)
@@ -253,6 +255,8 @@ class Engine:
         cfg.max_networks = int(max_networks)
         cfg.edge_capacity = int(edge_capacity)
         cfg.max_abs_weight = float(max_abs_weight)
+        cfg.ring32 = 1 if ring32 else 0
+        cfg.ring_bound = float(ring_bound)
         self.handle = ctypes.c_void_p()
         self.L = L
         check(L.ng_create(ctypes.byref(cfg), ctypes.byref(self.handle)))

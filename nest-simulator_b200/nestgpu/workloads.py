@@ -101,9 +101,25 @@ def layered_expected_edges(spec):
     return float(np.sum(np.outer(n, n) * spec["p"]))
 
 
-def layered_engine(spec, precision="fp64", device=0, graph_slices=64):
+def layered_ring_bound(spec):
+    """A bound on the sum of |weight| over one neuron's in-edges: per target
+    population, mean + 8 standard deviations of that sum (binomial
+    in-degrees, normal weights), 5 % margin.  The engine checks the drawn
+    graph against it."""
+    n = np.asarray(spec["sizes"], dtype=np.float64)
+    exc = np.asarray(spec["exc"], dtype=bool)
+    mu_w = np.where(exc, spec["J"], abs(spec["g"]) * spec["J"])
+    sd_w = np.where(exc, spec["J_sd"], abs(spec["g"]) * spec["J_sd"])
+    p = spec["p"]
+    mean = (n[:, None] * p * mu_w[:, None]).sum(axis=0)
+    var = (n[:, None] * p * (1 - p) * (mu_w ** 2)[:, None] + n[:, None] * p * (sd_w ** 2)[:, None]).sum(axis=0)
+    return float(np.max(mean + 8 * np.sqrt(var)) * 1.05)
+
+
+def layered_engine(spec, precision="fp64", device=0, graph_slices=64, ring32=False):
     """A serving engine sized for one layered network (the graph is drawn on
-    the device by the pairwise_bernoulli builder)."""
+    the device by the pairwise_bernoulli builder).  ring32: the FP32 form
+    with 32-bit ring cells, scaled by layered_ring_bound."""
     from . import _abi
 
     n = sum(spec["sizes"])
@@ -115,7 +131,8 @@ def layered_engine(spec, precision="fp64", device=0, graph_slices=64):
     J = spec["J"]
     eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, n)], h, 1, max(max_steps, int(round(spec["d_ext_ms"] / h))),
                       precision=prec, device=device, serving=True, max_networks=1, edge_capacity=cap,
-                      max_abs_weight=abs(spec["g"]) * (J + 12 * spec["J_sd"]) * 2)
+                      max_abs_weight=abs(spec["g"]) * (J + 12 * spec["J_sd"]) * 2, ring32=ring32,
+                      ring_bound=layered_ring_bound(spec) if ring32 else 0.0)
     eng.set_graph_slices(graph_slices)
     return eng
 

@@ -282,3 +282,36 @@ def test_gather_equals_scatter(monkeypatch, frac):
         np.testing.assert_array_equal(s0[o0], s1[o1])
         np.testing.assert_array_equal(t0[o0], t1[o1])
         np.testing.assert_array_equal(v0, v1)
+
+
+def test_ring32_equals_ring64_on_representable_weights():
+    """32-bit ring cells hold the same sums as 64-bit ones when the weights
+    are exact at both scales (multiples of 2^-10): identical spikes and
+    state.  A network whose in-edge weight sums exceed ring_bound is
+    refused at admission."""
+    def run(ring32):
+        eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, 20_000)], 0.1, 15, 15, precision=_abi.NG_FP32, serving=True,
+                          max_networks=4, edge_capacity=20_000_000, max_abs_weight=1000.0, ring32=ring32,
+                          ring_bound=400_000.0 if ring32 else 0.0)
+        r = _req(0, 5000, 2000, seed=31, k=400, g=4.0)
+        build = dict(n_exc=r.n_exc, k_exc=r.k_exc, k_inh=r.k_inh, w_exc=87.75, w_inh=-351.0, delay_steps=15,
+                     allow_autapses=0, seed=77)
+        V0 = np.random.default_rng(3).normal(-58.0, 10.0, r.n) + 70.0
+        nid = eng.net_add(r.n, r.steps, 5, {"tau_syn_ex": 0.5, "tau_syn_in": 0.5, "V_m_rel": V0}, build=build,
+                          poisson=(1.5 * serving.NU_TH_HZ, 87.75, 15))
+        eng.simulate(r.steps)
+        s, t = eng.net_spikes(nid)
+        V = eng.net_get_var(nid, "V_m_rel", r.n)
+        if ring32:
+            with pytest.raises(_abi.EngineError):
+                eng.net_add(r.n, 100, 6, {}, build=dict(build, k_exc=4000, k_inh=1000))
+        eng.close()
+        return s, t, V
+
+    s1, t1, V1 = run(False)
+    s2, t2, V2 = run(True)
+    assert len(s1) > 1000
+    o1, o2 = np.lexsort((s1, t1)), np.lexsort((s2, t2))
+    np.testing.assert_array_equal(s1[o1], s2[o2])
+    np.testing.assert_array_equal(t1[o1], t2[o2])
+    np.testing.assert_array_equal(V1, V2)
