@@ -72,6 +72,11 @@ typedef struct
                               instead of 64-bit; needs ring_bound */
   double ring_bound;       /* with ring32: largest sum of |weight| over one neuron's in-edges; sets the
                               scale so that no ring cell can overflow, checked for every admitted network */
+  int64_t tile_capacity;   /* serving: entries of the segment tables of target-tiled delivery (0: off);
+                              a pairwise_bernoulli network of n neurons needs n * (ceil(n / t) + 1): tiles of
+                              t targets, about a multiple of the SM count S of them, t = min(T, ceil(n / (r S))
+                              rounded up to 32), r = ceil(n / (T S)), T = min(1024, 163840 / (min(max_delay, 32)
+                              * 2 * e) rounded down to 32), e = 4 for 32-bit rings, else 8 */
 } ng_config;
 
 /* Counters and timings of an engine. */

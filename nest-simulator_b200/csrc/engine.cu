@@ -297,6 +297,7 @@ struct ng_engine
     bool used = false;
     int64_t off = 0, n = 0, e0 = 0, ne = 0, step0 = 0, until = 0;
     int64_t g0 = -1, gn = 0;  // gather table run
+    int64_t s0 = -1, sn = 0;  // segment table run (target-tiled delivery)
     bool rec = false;
     double log_rate = 0.0;
     std::vector< RawBlock > blocks;  // logged spikes, group by group
@@ -310,6 +311,13 @@ struct ng_engine
   float gather_frac = 0.08f;
   DevBuf gmask, gin, net_g, net_mode, net_spk;
   DevBuf log_sorted, log_cnt, log_off;  // spike log grouped by network (two halves)
+  // target-tiled delivery of pairwise_bernoulli networks
+  bool tiled_on = false;
+  int tile_t = 0;
+  size_t tile_smem = 0;
+  DevBuf seg, net_t;
+  std::map< int64_t, int64_t > free_seg;
+  std::vector< TileNet > host_t;
   long long* host_off = nullptr;        // pinned, 2 x (max_networks + 1)
   std::map< int64_t, int64_t > free_gin;
   std::vector< GatherNet > host_g;
@@ -426,6 +434,36 @@ struct ng_engine
       free_gin.clear();
       free_gin[ 0 ] = E;
     }
+    // target-tiled delivery: a window of a tile's ring cells in 160 KiB of shared memory
+    if ( cfg.tile_capacity > 0 && b.model != NG_AEIF_COND_ALPHA && nmax <= 1024 )
+    {
+      const size_t esz = ( size_t ) ring_bytes;
+      const size_t W = ( size_t ) std::min( L, TILE_W );
+      tile_t = ( int ) std::min< size_t >( 1024, ( 163840 / ( W * 2 * esz ) ) / 32 * 32 );
+      if ( tile_t >= 32 )
+      {
+        tiled_on = true;
+        tile_smem = W * C * tile_t * esz;
+        cudaError_t ce;
+        if ( prec == NG_FP64 )
+          ce = cudaFuncSetAttribute( k_deliver_tiled< double, false >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ( int ) tile_smem );
+        else if ( ring_bytes == 4 )
+          ce = cudaFuncSetAttribute( k_deliver_tiled< int32_t, true >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ( int ) tile_smem );
+        else
+          ce = cudaFuncSetAttribute( k_deliver_tiled< long long, true >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ( int ) tile_smem );
+        if ( ce != cudaSuccess )
+          return fail( NG_ERR_CUDA, "serving: cannot reserve shared memory for the tiled delivery" );
+        if ( ( rc = alloc( seg, ( size_t ) cfg.tile_capacity * 4 ) )
+          || ( rc = alloc( net_t, ( size_t ) nmax * sizeof( TileNet ) ) ) )
+          return rc;
+        host_t.assign( ( size_t ) nmax, TileNet {} );
+        free_seg.clear();
+        free_seg[ 0 ] = cfg.tile_capacity;
+      }
+    }
     // one fixed-point scale for every network (FP32 form)
     // 32-bit rings: the scale keeps the largest possible cell sum inside 31 bits
     const double mx = ring_bytes == 4 ? cfg.ring_bound : cfg.max_abs_weight > 0 ? cfg.max_abs_weight : 1e4;
@@ -496,7 +534,7 @@ struct ng_engine
     DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
       &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl, &d_nid, &d_step0, &d_until, &d_off,
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
-      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound };
+      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -720,6 +758,14 @@ struct ng_engine
     d.net_until = ( const long long* ) d_until.p;
     d.net_off = ( const long long* ) d_off.p;
     d.net_key = ( const uint2* ) d_key.p;
+    if ( serving )
+      d.n_nets = cfg.max_networks;
+    if ( tiled_on )
+    {
+      d.net_t = ( const TileNet* ) net_t.p;
+      d.seg = ( const int32_t* ) seg.p;
+      d.tile_t = tile_t;
+    }
     if ( gather_on )
     {
       d.gmask = ( uint32_t* ) gmask.p;
@@ -763,11 +809,13 @@ struct ng_engine
       const Block db = dblock( b );
       if ( b.model == NG_AEIF_COND_ALPHA )
       {
-        const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( b.n + 127 ) / 128 );
+        // CTAs of 2 warps, registers capped for 12 warps per SM (the RKF45 state and
+        // tableau need ~170 registers; more warps hide the FP64 latency)
+        const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( b.n + 63 ) / 64 );
         if ( prec == NG_FP64 )
-          k_update_aeif< double, false ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched, h );
+          k_update_aeif< double, false ><<< grid, 64, 0, stream >>>( d, db, from_, to_, sched, h );
         else
-          k_update_aeif< float, true ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched, h );
+          k_update_aeif< float, true ><<< grid, 64, 0, stream >>>( d, db, from_, to_, sched, h );
       }
       else
       {
@@ -784,7 +832,7 @@ struct ng_engine
     // one thread per neuron for 1-2 step slices, for networks large enough
     // to fill the GPU that way and for engines with the per-target gather
     // (its lag bits are written there); the two-phase kernel otherwise
-    if ( span <= 2 || db.n >= one_thread_min_n || max_lanes == 1 || gather_on )
+    if ( span <= 2 || db.n >= one_thread_min_n || max_lanes == 1 || gather_on || tiled_on )
     {
       // CTAs of 4 warps: a large network's grid is resident in one wave
       const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 127 ) / 128 );
@@ -826,6 +874,15 @@ struct ng_engine
   {
     if ( gather_on )
       k_gather<<< ( unsigned ) sms, G_THREADS, G_SMEM, stream >>>( d );
+    if ( tiled_on )
+    {
+      if ( prec == NG_FP64 )
+        k_deliver_tiled< double, false ><<< ( unsigned ) sms, 1024, tile_smem, stream >>>( d );
+      else if ( ring_bytes == 4 )
+        k_deliver_tiled< int32_t, true ><<< ( unsigned ) sms, 1024, tile_smem, stream >>>( d );
+      else
+        k_deliver_tiled< long long, true ><<< ( unsigned ) sms, 1024, tile_smem, stream >>>( d );
+    }
     const unsigned grid = ( unsigned ) deliver_ctas;
     if ( prec == NG_FP64 )
       k_deliver< false ><<< grid, 256, 0, stream >>>( d );
@@ -2168,11 +2225,14 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     return fail( NG_ERR_CAPACITY, "ng_net_add: not enough free edges in the pool" );
   }
   int64_t g0 = -1, gn = 0;  // gather table run, if any
+  int64_t sg0 = -1, sgn = 0;  // segment table run, if any
   auto undo = [ & ]( int code ) {
     ng_engine::give_run( e->free_neurons, n0, n );
     ng_engine::give_run( e->free_edges, e0, ne_need );
     if ( g0 >= 0 )
       ng_engine::give_run( e->free_gin, g0, gn );
+    if ( sg0 >= 0 )
+      ng_engine::give_run( e->free_seg, sg0, sgn );
     return code;
   };
   auto& b = e->blk[ 0 ];
@@ -2333,6 +2393,29 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     k_fi_rows<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, n0, e0, ( const int64_t* ) e->sc_beg.p,
       ( const int32_t* ) e->sc_plen.p, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->row_beg.p,
       ( int32_t* ) e->row_len.p, ( int32_t* ) e->real_deg.p );
+    // the rows are sorted by target: segment table of the target-tiled delivery
+    if ( e->tiled_on )
+    {
+      // tiles: about a multiple of the SM count, at most tile_t targets each
+      const int64_t rounds = ( n + ( int64_t ) e->tile_t * e->sms - 1 ) / ( ( int64_t ) e->tile_t * e->sms );
+      int tt = ( int ) ( ( n + rounds * e->sms - 1 ) / ( rounds * e->sms ) );
+      tt = std::min( e->tile_t, ( tt + 31 ) / 32 * 32 );
+      const int nt = ( int ) ( ( n + tt - 1 ) / tt );
+      const int64_t need = n * ( int64_t ) ( nt + 1 );
+      if ( !ng_engine::take_run( e->free_seg, need, &sg0 ) )
+        return undo( fail( NG_ERR_CAPACITY, "ng_net_add: not enough free segment-table space (tile_capacity)" ) );
+      sgn = need;
+      k_seg_build<<< ( unsigned ) ( ( need + 255 ) / 256 ), 256, 0, e->stream >>>( n, nt, tt, n0,
+        ( const int64_t* ) e->row_beg.p, ( const int32_t* ) e->real_deg.p, ( const uint32_t* ) e->tdc.p, e->tmask,
+        ( int32_t* ) e->seg.p + sg0 );
+      TileNet tn {};
+      tn.seg_base = sg0;
+      tn.off = n0;
+      tn.n = ( int ) n;
+      tn.nt = nt;
+      tn.tt = tt;
+      e->host_t[ id ] = tn;
+    }
     CU( cudaGetLastError() );
     CU( cudaStreamSynchronize( e->stream ) );
   }
@@ -2551,6 +2634,16 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   nw.ne = ne_used;
   nw.g0 = g0;
   nw.gn = gn;
+  nw.s0 = sg0;
+  nw.sn = sgn;
+  if ( e->tiled_on )
+  {
+    if ( sg0 < 0 )
+      e->host_t[ id ] = TileNet {};
+    CU( cudaMemcpyAsync( ( TileNet* ) e->net_t.p + id, &e->host_t[ id ], sizeof( TileNet ), cudaMemcpyHostToDevice,
+      e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
   if ( e->gather_on )
   {
     if ( g0 < 0 )
@@ -2722,6 +2815,15 @@ ng_net_remove( ng_engine* e, int32_t id )
   std::fill( e->rec_host.begin() + nw.off, e->rec_host.begin() + nw.off + nw.n, ( uint8_t ) 0 );
   ng_engine::give_run( e->free_neurons, nw.off, nw.n );
   ng_engine::give_run( e->free_edges, nw.e0, nw.ne );
+  if ( e->tiled_on )
+  {
+    if ( nw.s0 >= 0 )
+      ng_engine::give_run( e->free_seg, nw.s0, nw.sn );
+    e->host_t[ id ] = TileNet {};
+    CU( cudaMemcpyAsync( ( TileNet* ) e->net_t.p + id, &e->host_t[ id ], sizeof( TileNet ), cudaMemcpyHostToDevice,
+      e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
   if ( e->gather_on )
   {
     if ( nw.g0 >= 0 )

@@ -79,6 +79,18 @@ struct GatherNet
   int we, wi, ce, ci;
 };
 
+// Target-tiled delivery of one network of a serving engine: its rows are
+// sorted by target; seg[seg_base + s * (nt + 1) + b] = first position in
+// source s's row whose target lies in tile b,
+// seg[..+ nt] = the row's real length; tiles of tt targets (at most the
+// engine's tile_t).  nt == 0: not tiled.
+struct TileNet
+{
+  long long seg_base, off;
+  int n, nt, tt;  // neurons, tiles, targets per tile
+  int pad;
+};
+
 struct Net
 {
   int64_t N, n_src;
@@ -125,6 +137,10 @@ struct Net
   unsigned* net_spk;             // per network: spikes in the open slice
   int n_nets;
   float gather_frac;             // gather the next slice when spikes >= gather_frac * n
+  // target-tiled delivery; net_t == nullptr: off
+  const TileNet* net_t;
+  const int32_t* seg;
+  int tile_t;
   const int64_t* sched_step;
   const int32_t* sched_src;
   int64_t n_sched;

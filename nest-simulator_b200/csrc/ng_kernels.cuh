@@ -220,6 +220,7 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
 __device__ __forceinline__ void
 cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long t0, int netid, bool gath )
 {
+  const bool tiled = !gath && netid >= 0 && d.net_t != nullptr && d.net_t[ netid ].nt > 0;
   __shared__ unsigned long long s_e, s_l, s_r, s_c, g_e, g_l;
   __shared__ int s_any;
   const int lane = threadIdx.x & 31;
@@ -242,7 +243,9 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
       row = d.row_beg[ src ];
       pdeg = d.row_len[ src ];
       rdeg = d.real_deg[ src ];
-      nch = gath ? 0 : ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
+      // a spike of a tiled network is one work entry (its source), of a
+      // network in gather mode none, else one per 128-edge chunk
+      nch = gath ? 0 : tiled ? 1 : ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
       if ( d.net_spk && netid >= 0 )
       {
         // one atomic per network present in the warp
@@ -306,7 +309,14 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
     int slot = slot0 + k;
     if ( slot >= d.L )
       slot -= d.L;
-    if ( nch > 0 )
+    if ( tiled )
+    {
+      if ( idx < d.ent_cap )
+        d.ent[ idx ] = make_int4( src, 0, -1, slot | ( 1 << 16 ) );  // edge count -1: no scatter chunk
+      else
+        atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+    }
+    else if ( nch > 0 )
       put_chunks( d, idx, row, pdeg, slot, 1 );
     idx += nch;
     if ( lg )
@@ -1147,7 +1157,7 @@ control_yp( double tol, const double* err, const double* f, double& hs )
 }
 
 template < typename Real, bool FIX >
-__global__ void __launch_bounds__( 128 )
+__global__ void __launch_bounds__( 64, 6 )
 k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
 {
   const long long origin = cta_origin( d );

@@ -658,3 +658,246 @@ k_max_u64( long long n, const unsigned long long* v, unsigned long long* out )
 }
 
 }  // namespace ng
+
+namespace ng
+{
+
+// ---------------------------------------------------------------------
+// Target-tiled delivery (owner computes).  For a network whose rows are
+// sorted by target, a CTA owns a tile of tile_t targets at a time: it walks
+// the slice's spikes of the network, takes from each spike's row only the
+// segment that falls into its tile, accumulates the weights in shared
+// memory, and adds the non-zero cells to the ring with plain, coalesced
+// read-modify-writes (the tile has no other writer).  The global atomics of
+// the scatter -- one per synaptic event, which bound it on the L2 atomic
+// units -- become shared-memory atomics.  Shared memory holds a window of
+// TILE_W ring slots from the first slot the slice can reach; the rare events
+// with longer delays go to the ring with global atomics.
+// Work per warp: 8 spikes at a time -- their metadata (network, segment
+// bounds, row) loaded by one lane each, in one round trip -- then their 8
+// segments together, all lanes on consecutive edges of each, the loads of
+// the 8 issued before any is used.  A network's tiles number about a
+// multiple of the SM count (tt at admission), one CTA per SM.
+// A spike of a tiled network is queued as one work entry (source, 0, -1,
+// slot | multiplicity << 16); the scatter kernel skips it.
+// A: accumulator type (int32: 32-bit rings, int64: fixed point, double: FP64).
+// ---------------------------------------------------------------------
+constexpr int TILE_W = 32;
+
+template < typename A, bool FIX >
+__device__ __forceinline__ void
+tile_add( const Net& d, A* acc, int TT, int wbase, int slot, int ch, long long tl, long long gidx, A v )
+{
+  int ws = slot - wbase;
+  if ( ws < 0 )
+    ws += d.L;
+  if ( ws < TILE_W && ws < d.L )
+  {
+    const int q = ( ws * d.C + ch ) * TT + ( int ) tl;
+    if constexpr ( sizeof( A ) == 4 )
+      atomicAdd( reinterpret_cast< int* >( acc ) + q, ( int ) v );
+    else if constexpr ( FIX )
+      atomicAdd( reinterpret_cast< unsigned long long* >( acc ) + q, ( unsigned long long ) v );
+    else
+      atomicAdd( reinterpret_cast< double* >( acc ) + q, ( double ) v );
+  }
+  else
+  {
+    const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + gidx;
+    if constexpr ( sizeof( A ) == 4 )
+      atomicAdd( reinterpret_cast< int* >( d.ring ) + idx, ( int ) v );
+    else if constexpr ( FIX )
+      atomicAdd( reinterpret_cast< unsigned long long* >( d.ring ) + idx, ( unsigned long long ) v );
+    else
+      atomicAdd( reinterpret_cast< double* >( d.ring ) + idx, ( double ) v );
+  }
+}
+
+template < typename A, bool FIX >
+__global__ void __launch_bounds__( 1024, 1 )
+k_deliver_tiled( Net d )
+{
+  extern __shared__ __align__( 16 ) unsigned char t_smem[];
+  A* acc = reinterpret_cast< A* >( t_smem );  // [TILE_W][C][tile_t]
+  __shared__ int s_pref[ 1025 ];
+  __shared__ unsigned long long s_nent;
+  __shared__ int s_err;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  if ( tid == 0 )
+  {
+    s_nent = ld_volatile( &d.ctl->n_ent );
+    s_err = ld_volatile( &d.ctl->err );
+  }
+  const long long origin = cta_origin( d );  // synchronises the CTA
+  for ( int id = tid; id < d.n_nets; id += blockDim.x )
+    s_pref[ id + 1 ] = d.net_t[ id ].nt;
+  if ( tid == 0 )
+    s_pref[ 0 ] = 0;
+  __syncthreads();
+  if ( tid == 0 )
+    for ( int id = 0; id < d.n_nets; ++id )
+      s_pref[ id + 1 ] += s_pref[ id ];
+  __syncthreads();
+  const bool ok = ( long long ) s_nent <= d.ent_cap && ( s_err & ERR_SPIKE_LIST ) == 0;
+  const long long nent = ok ? ( long long ) s_nent : 0;
+  const int total = s_pref[ d.n_nets ];
+  const int w0 = ( int ) ( ( long long ) total * blockIdx.x / gridDim.x );
+  const int w1 = ( int ) ( ( long long ) total * ( blockIdx.x + 1 ) / gridDim.x );
+  const int W = min( TILE_W, d.L );
+  // first slot this slice's spikes can reach: origin + min_delay
+  const int wbase = ( int ) ( ( origin + d.min_delay ) % d.L );
+  for ( int w = w0; w < w1; ++w )
+  {
+    int lo = 0, hi = d.n_nets;
+    while ( hi - lo > 1 )
+    {
+      const int mid = ( lo + hi ) >> 1;
+      if ( s_pref[ mid ] <= w )
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int id = lo;
+    const TileNet g = d.net_t[ id ];
+    const int TT = g.tt;
+    const int cells = W * d.C * TT;
+    const int tile = w - s_pref[ id ];
+    const long long tb = ( long long ) tile * TT;
+    const int tn = ( int ) min( ( long long ) TT, ( long long ) g.n - tb );
+    for ( int q = tid; q < cells; q += blockDim.x )
+      acc[ q ] = A( 0 );
+    __syncthreads();
+    for ( long long e0 = ( long long ) warp * 8; e0 < nent; e0 += ( long long ) nwarps * 8 )
+    {
+      // one spike per lane (lanes 0-7): its segment of this tile
+      long long row = 0;
+      int a = 0, b = 0, sw = 0;
+      const long long e = e0 + lane;
+      if ( lane < 8 && e < nent )
+      {
+        const int4 en = d.ent[ e ];
+        if ( en.z == -1 && d.nid[ en.x ] == id )
+        {
+          const int32_t* sg = d.seg + g.seg_base + ( en.x - g.off ) * ( long long ) ( g.nt + 1 );
+          a = sg[ tile ];
+          b = sg[ tile + 1 ];
+          row = d.row_beg[ en.x ];
+          sw = en.w;
+        }
+      }
+      // up to 8 spikes' segments at a time, their edge loads issued together
+      unsigned live = __ballot_sync( FULL, b > a );
+      while ( live )
+      {
+        long long ru[ 8 ];
+        int au[ 8 ], bu[ 8 ], su[ 8 ];
+        int span = 0;
+#pragma unroll
+        for ( int u = 0; u < 8; ++u )
+        {
+          const int j = live ? __ffs( live ) - 1 : 0;
+          const bool has = live != 0;
+          live &= live - 1;
+          ru[ u ] = __shfl_sync( FULL, row, j );
+          au[ u ] = __shfl_sync( FULL, a, j );
+          bu[ u ] = has ? __shfl_sync( FULL, b, j ) : au[ u ];
+          su[ u ] = __shfl_sync( FULL, sw, j );
+          span = max( span, bu[ u ] - au[ u ] );
+        }
+        for ( int r = 0; r < span; r += 32 )
+        {
+          uint32_t tw[ 8 ];
+          typename std::conditional< FIX, int32_t, double >::type wv[ 8 ];
+#pragma unroll
+          for ( int u = 0; u < 8; ++u )
+          {
+            const int k = au[ u ] + r + lane;
+            tw[ u ] = 0u;
+            wv[ u ] = 0;
+            if ( k < bu[ u ] )
+            {
+              tw[ u ] = __ldg( d.edge_tdc + ru[ u ] + k );
+              if constexpr ( FIX )
+                wv[ u ] = __ldg( ( const int32_t* ) d.edge_w + ru[ u ] + k );
+              else
+                wv[ u ] = __ldg( ( const double* ) d.edge_w + ru[ u ] + k );
+            }
+          }
+#pragma unroll
+          for ( int u = 0; u < 8; ++u )
+          {
+            if ( au[ u ] + r + lane >= bu[ u ] )
+              continue;
+            const long long tl = ( long long ) ( tw[ u ] & d.tmask ) - g.off - tb;
+            if ( tl < 0 || tl >= TT )
+              continue;  // outside the tile: cannot happen for a correct segment table
+            int slot = ( su[ u ] & 0xffff ) + ( int ) ( ( tw[ u ] >> d.tbits ) & d.dmask );
+            if ( slot >= d.L )
+              slot -= d.L;
+            const int mult = su[ u ] >> 16;
+            const int ch = ( int ) ( tw[ u ] >> 31 );
+            if constexpr ( FIX )
+              tile_add< A, FIX >( d, acc, TT, wbase, slot, ch, tl, g.off + tb + tl,
+                ( A ) ( ( long long ) wv[ u ] * mult ) );
+            else
+              tile_add< A, FIX >( d, acc, TT, wbase, slot, ch, tl, g.off + tb + tl,
+                ( A ) ( mult == 1 ? wv[ u ] : wv[ u ] * ( double ) mult ) );
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for ( int q = tid; q < cells; q += blockDim.x )
+    {
+      const int t = q % TT;
+      if ( t >= tn )
+        continue;
+      const A v = acc[ q ];
+      if ( v == A( 0 ) )
+        continue;
+      const int sc = q / TT;  // window slot * C + channel
+      int slot = wbase + sc / d.C;
+      if ( slot >= d.L )
+        slot -= d.L;
+      const int64_t idx = ( ( int64_t ) slot * d.C + sc % d.C ) * d.N + g.off + tb + t;
+      reinterpret_cast< A* >( d.ring )[ idx ] += v;
+    }
+    __syncthreads();
+  }
+}
+
+// Segment table of one network (rows sorted by target): entry (s, b) is
+// the first position in row s whose local target is >= b * tile_t.
+__global__ void
+k_seg_build( long long n, int nt, int tile_t, long long n0, const int64_t* row_beg, const int32_t* real_deg,
+  const uint32_t* tdc, uint32_t tmask, int32_t* seg )
+{
+  const long long idx = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( idx >= n * ( nt + 1 ) )
+    return;
+  const long long s = idx / ( nt + 1 );
+  const int b = ( int ) ( idx - s * ( nt + 1 ) );
+  const int len = real_deg[ n0 + s ];
+  if ( b == nt )
+  {
+    seg[ idx ] = len;
+    return;
+  }
+  const long long row = row_beg[ n0 + s ];
+  const long long bound = n0 + ( long long ) b * tile_t;
+  int lo = 0, hi = len;  // first k with target >= bound
+  while ( lo < hi )
+  {
+    const int mid = ( lo + hi ) >> 1;
+    if ( ( long long ) ( tdc[ row + mid ] & tmask ) < bound )
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  seg[ idx ] = lo;
+}
+
+}  // namespace ng

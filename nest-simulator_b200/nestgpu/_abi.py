@@ -57,6 +57,7 @@ class NGConfig(ctypes.Structure):
         ("max_abs_weight", ctypes.c_double),
         ("ring32", ctypes.c_int32),
         ("ring_bound", ctypes.c_double),
+        ("tile_capacity", ctypes.c_int64),
     ]
 
 
@@ -74,6 +75,29 @@ class NGFixedIndegree(ctypes.Structure):
 
 
 NG_MAX_POPS = 16
+
+
+def tile_targets(max_delay, ring32=False):
+    """Largest number of targets per tile of the target-tiled delivery (as
+    the engine computes it)."""
+    esz = 4 if ring32 else 8
+    return min(1024, (163840 // (min(max_delay, 32) * 2 * esz)) // 32 * 32)
+
+
+def tile_table_entries(n, max_delay, ring32=False, sms=None):
+    """Segment-table entries a tiled network of n neurons takes (the
+    engine's rule: about a multiple of the SM count of tiles)."""
+    if sms is None:
+        try:
+            import torch
+
+            sms = torch.cuda.get_device_properties(0).multi_processor_count
+        except Exception:
+            sms = 148
+    T = tile_targets(max_delay, ring32)
+    rounds = -(-n // (T * sms))
+    tt = min(T, (-(-n // (rounds * sms)) + 31) // 32 * 32)
+    return n * (-(-n // tt) + 1)
 
 
 class NGPairwiseBernoulli(ctypes.Structure):
@@ -233,7 +257,7 @@ class Engine:
 
     def __init__(self, blocks, h, min_delay, max_delay, n_generators=0, precision=NG_FP64, device=0,
                  tics_per_ms=1000.0, spike_log_capacity=0, start_step=0, serving=False, max_networks=0,
-                 edge_capacity=0, max_abs_weight=0.0, ring32=False, ring_bound=0.0):
+                 edge_capacity=0, max_abs_weight=0.0, ring32=False, ring_bound=0.0, tile_capacity=0):
         L = load()
         cfg = NGConfig()
         cfg.device = int(device)
@@ -257,10 +281,12 @@ class Engine:
         cfg.max_abs_weight = float(max_abs_weight)
         cfg.ring32 = 1 if ring32 else 0
         cfg.ring_bound = float(ring_bound)
+        cfg.tile_capacity = int(tile_capacity)
         self.handle = ctypes.c_void_p()
         self.L = L
         check(L.ng_create(ctypes.byref(cfg), ctypes.byref(self.handle)))
         self.blocks = list(blocks)
+        self.max_networks = int(max_networks)
         self.n_trace = 0
         self.n_trace_vars = 0
 

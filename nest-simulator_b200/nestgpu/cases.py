@@ -26,12 +26,14 @@ def main(argv=None):
     ap.add_argument("--capacity-neurons", type=int, default=300_000)
     ap.add_argument("--capacity-edges", type=int, default=200_000_000)
     ap.add_argument("--slices", type=int, default=40, help="serving: min_delay slices simulated")
+    ap.add_argument("--ring32", action="store_true", help="layered: 32-bit ring cells")
+    ap.add_argument("--no-tiled", action="store_true", help="layered: scatter delivery only")
     a = ap.parse_args(argv)
     from . import serving, workloads
 
     if a.case == "layered":
         spec = workloads.layered_spec(scale=a.scale)
-        eng = workloads.layered_engine(spec, a.precision)
+        eng = workloads.layered_engine(spec, a.precision, ring32=a.ring32, tiled=not a.no_tiled)
         steps = int(round(a.ms / 0.1))
         workloads.layered_add(eng, spec, steps + 10)
         eng.simulate(steps)

@@ -109,13 +109,22 @@ def new_engine(precision="fp32", capacity_neurons=2_000_000, capacity_edges=1_20
     return eng
 
 
-def run_batched(requests, eng, max_chunk_slices=64, clock=time.perf_counter, realtime=True):
-    """Continuous batching.  Returns (requests, stats)."""
+def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtime=True):
+    """Continuous batching.  Returns (requests, stats).
+
+    Every live network advances in chunks of `chunk_slices` min_delay slices;
+    between chunks, the networks whose duration has passed are retired (their
+    spikes drained, their pool space freed) and the waiting requests that fit
+    the free pool are admitted, oldest first.  A request is only built (its
+    initial state drawn, its graph requested) when its footprint fits the
+    largest free runs of the pool."""
     pending = sorted(requests, key=lambda r: r.arrival)
     waiting = []
-    active = {}
+    active = {}                       # network id -> (request, engine step at which it ends)
     t0 = clock()
-    ev0 = eng.stats()["syn_events"]
+    st0 = eng.stats()
+    ev0 = st0["syn_events"]
+    now_steps = st0["clock_steps"]
     steps_run = 0
     while pending or waiting or active:
         now = clock() - t0
@@ -123,34 +132,38 @@ def run_batched(requests, eng, max_chunk_slices=64, clock=time.perf_counter, rea
             r = pending.pop(0)
             r.enqueued = r.arrival if realtime else 0.0
             waiting.append(r)
-        # admit every waiting request that fits, oldest first
-        still = []
-        for r in waiting:
-            nid = _admit(eng, r)
-            if nid is None:
-                still.append(r)
-            else:
+        if waiting:
+            free_n, free_e = eng.net_capacity()
+            still = []
+            for r in waiting:
+                fn, fe = footprint(r)
+                nid = None
+                if fn <= free_n and fe <= free_e and len(active) < eng.max_networks:
+                    nid = _admit(eng, r)
+                if nid is None:
+                    still.append(r)
+                    continue
                 r.admitted = clock() - t0
-                active[nid] = r
-        waiting = still
+                active[nid] = (r, now_steps + r.steps)
+                free_n, free_e = eng.net_capacity()
+            waiting = still
         if not active:
             if waiting:
                 raise RuntimeError("a request does not fit the empty pool")
             if pending:
                 time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
             continue
-        # advance all live networks to the next retirement (at most a graph chunk)
-        left = min(r.steps - eng.net_poll(nid)[0] for nid, r in active.items())
-        slices = max(1, min(max_chunk_slices, -(-left // DELAY_STEPS)))
+        # one chunk, or less when every live network ends before its end
+        left = max(end for _, end in active.values()) - now_steps
+        slices = max(1, min(chunk_slices, -(-left // DELAY_STEPS)))
         eng.simulate(slices * DELAY_STEPS)
+        now_steps += slices * DELAY_STEPS
         steps_run += slices * DELAY_STEPS
-        for nid in list(active):
-            done, fin = eng.net_poll(nid)
-            if fin:
-                r = active.pop(nid)
-                r.spikes = eng.net_spikes(nid)
-                eng.net_remove(nid)
-                r.finished = clock() - t0
+        for nid in [k for k, (_, end) in active.items() if now_steps >= end]:
+            r, _ = active.pop(nid)
+            r.spikes = eng.net_spikes(nid)
+            eng.net_remove(nid)
+            r.finished = clock() - t0
     makespan = clock() - t0
     ev = eng.stats()["syn_events"] - ev0
     return requests, {"makespan_s": makespan, "syn_events": ev, "syn_events_per_s": ev / makespan,

@@ -116,10 +116,11 @@ def layered_ring_bound(spec):
     return float(np.max(mean + 8 * np.sqrt(var)) * 1.05)
 
 
-def layered_engine(spec, precision="fp64", device=0, graph_slices=64, ring32=False):
+def layered_engine(spec, precision="fp64", device=0, graph_slices=64, ring32=False, tiled=False):
     """A serving engine sized for one layered network (the graph is drawn on
     the device by the pairwise_bernoulli builder).  ring32: the FP32 form
-    with 32-bit ring cells, scaled by layered_ring_bound."""
+    with 32-bit ring cells, scaled by layered_ring_bound; tiled: target-tiled
+    delivery (segment tables sized here)."""
     from . import _abi
 
     n = sum(spec["sizes"])
@@ -132,7 +133,8 @@ def layered_engine(spec, precision="fp64", device=0, graph_slices=64, ring32=Fal
     eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, n)], h, 1, max(max_steps, int(round(spec["d_ext_ms"] / h))),
                       precision=prec, device=device, serving=True, max_networks=1, edge_capacity=cap,
                       max_abs_weight=abs(spec["g"]) * (J + 12 * spec["J_sd"]) * 2, ring32=ring32,
-                      ring_bound=layered_ring_bound(spec) if ring32 else 0.0)
+                      ring_bound=layered_ring_bound(spec) if ring32 else 0.0,
+                      tile_capacity=_abi.tile_table_entries(n, max(max_steps, 15), ring32) if tiled else 0)
     eng.set_graph_slices(graph_slices)
     return eng
 

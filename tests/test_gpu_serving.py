@@ -315,3 +315,36 @@ def test_ring32_equals_ring64_on_representable_weights():
     np.testing.assert_array_equal(s1[o1], s2[o2])
     np.testing.assert_array_equal(t1[o1], t2[o2])
     np.testing.assert_array_equal(V1, V2)
+
+
+@pytest.mark.parametrize("ring32", [False, True])
+def test_tiled_delivery_equals_scatter(ring32):
+    """Target-tiled delivery (shared-memory accumulation per target tile) of a
+    pairwise_bernoulli network equals the scatter bit for bit in the FP32
+    form (the same integers are added), with 64- and 32-bit ring cells."""
+    n = sum(PB_SIZES)
+
+    def run(tiled):
+        eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, 20_000)], 0.1, 1, 40, precision=_abi.NG_FP32, serving=True,
+                          max_networks=4, edge_capacity=30_000_000, max_abs_weight=1000.0, ring32=ring32,
+                          ring_bound=2.0e6 if ring32 else 0.0,
+                          tile_capacity=_abi.tile_table_entries(n, 40, ring32) if tiled else 0)
+        V0 = np.random.default_rng(8).uniform(0.0, 14.0, n)
+        rate = np.full(n, 9000.0)
+        nid = eng.net_add(n, 3000, 17, {"tau_syn_ex": 0.5, "tau_syn_in": 0.5, "V_m_rel": V0}, build=_pb(seed=21),
+                          poisson=(rate, 87.8, 15))
+        eng.simulate(3000)
+        s, t = eng.net_spikes(nid)
+        V = eng.net_get_var(nid, "V_m_rel", n)
+        st = eng.stats()
+        eng.close()
+        return s, t, V, st
+
+    s0, t0, V0, st0 = run(False)
+    s1, t1, V1, st1 = run(True)
+    assert len(s0) > 1000
+    assert st0["syn_events"] == st1["syn_events"]
+    o0, o1 = np.lexsort((s0, t0)), np.lexsort((s1, t1))
+    np.testing.assert_array_equal(s0[o0], s1[o1])
+    np.testing.assert_array_equal(t0[o0], t1[o1])
+    np.testing.assert_array_equal(V0, V1)
