@@ -432,16 +432,20 @@ def measure_layered(args, dev, sim_ms=1000.0):
         nid = workloads.layered_add(eng, spec, 10 * steps)
         build = time.perf_counter() - t0
         eng.simulate(1000)  # 100 ms warm-up (graphs built)
+        sampler = ClockSampler(dev.index)
+        sampler.start()
         s0 = eng.stats()
         ms = timed_sim(eng, steps, dev)
         s1 = eng.stats()
+        clocks = sampler.stop()
         ks = kernel_split(eng, 200)
         out["synapses"] = eng.net_connection_count(nid)
         eng.close()
         ev = s1["syn_events"] - s0["syn_events"]
         out[form] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
                      "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / out["neurons"] / (sim_ms * 1e-3),
-                     "build_s": build, "kernels": ks}
+                     "build_s": build, "kernels": ks, "clocks": clocks,
+                     "host_ms": {k: s1[k] - s0[k] for k in ("simulate_ms", "wait_ms", "drain_ms")}}
     out["fp32_ring32"]["ring_bound"] = workloads.layered_ring_bound(spec)
     return out
 

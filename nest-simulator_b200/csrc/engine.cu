@@ -1512,6 +1512,9 @@ ng_create( const ng_config* cfg, ng_engine** out )
   e->log_cap = std::min< int64_t >( e->log_cap, 1ll << 28 );
   if ( ( rc = e->alloc( e->log, 2 * ( size_t ) e->log_cap * sizeof( uint2 ) ) ) )
     return bail( rc );
+  // pinned staging for the spike-log drain, sized once for a typical group
+  if ( e->grow_pinned( ( size_t ) std::min< int64_t >( e->log_cap, 1ll << 24 ) * sizeof( uint2 ) ) )
+    return bail( NG_ERR_MEMORY );
   if ( ( rc = e->alloc( e->rec, ( size_t ) e->n_src ) ) )
     return bail( rc );
   if ( ( rc = e->alloc( e->ctl, sizeof( Ctl ) ) ) )
