@@ -230,7 +230,11 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "sample_per_step_ms": sample_ms, "rtf": dt / (args.steps * sample_ms / 1e3)},
+        "config": {"workload": WORKLOAD, "form": "FP64 oracle port (the reference's CPU cycle restated), all host threads",
+                   "networks_per_gpu": args.batch, "sample_per_step_ms": sample_ms,
+                   "sample": f"one of the {args.batch} networks for {sample_ms:.0f} ms of simulated time per step "
+                             "(events/s do not depend on how many identical networks a CPU run holds)",
+                   "rtf": dt / (args.steps * sample_ms / 1e3)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{sample_ms:.0f} ms of simulated time per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
