@@ -481,8 +481,10 @@ template < typename Real, bool FIX >
 __device__ __forceinline__ Real
 ring_real( const Net& d, typename RingVal< FIX >::type v )
 {
+  // fx_inv is a power of two: rounding v to Real and then scaling gives the
+  // same value as scaling in FP64 and then rounding, without the FP64 ops
   if constexpr ( FIX )
-    return ( Real ) ( ( double ) v * d.fx_inv );
+    return ( Real ) v * ( Real ) d.fx_inv;
   else
     return ( Real ) v;
 }
@@ -655,6 +657,8 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
     const int nl = min( 32, to - cb );
     const long long t0 = origin + cb;
     const int slot0 = ( int ) ( t0 % d.L );
+    // lags of this chunk the neuron is simulated at: [0, nact)
+    const int nact = act ? ( int ) max( 0ll, min( ( long long ) nl, until - t0 ) ) : 0;
     unsigned smask = 0;
     for ( int sb = 0; sb < nl; sb += SUB )
     {
@@ -669,7 +673,7 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
         raw_in[ q ] = 0;
         dvs[ q ] = Real( 0 );
         const int k = sb + q;
-        if ( act && k < nl && t0 + k < until )
+        if ( k < nact )
         {
           int slot = slot0 + k;
           if ( slot >= d.L )
@@ -685,7 +689,7 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
       for ( int q = 0; q < SUB; ++q )
       {
         const int k = sb + q;
-        if ( !act || k >= nl || t0 + k >= until )
+        if ( k >= nact )
           continue;
         Real ex = ring_real< Real, FIX >( d, raw_ex[ q ] );
         Real inh = EXP ? ring_real< Real, FIX >( d, raw_in[ q ] ) : Real( 0 );
@@ -766,7 +770,7 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
       for ( int q = 0; q < SUB; ++q )
       {
         const int k = sb + q;
-        if ( act && k < nl && t0 + k < until )
+        if ( k < nact )
         {
           int slot = slot0 + k;
           if ( slot >= d.L )
