@@ -434,8 +434,26 @@ k_gather( Net d )
     if ( id != staged )
     {
       __syncthreads();
-      for ( int q = tid; q <= g.n; q += blockDim.x )
-        s_mask[ q ] = q < g.n ? ( uint16_t ) d.gmask[ g.off + q ] : ( uint16_t ) 0;
+      // 8 independent loads per thread in flight (a load-store loop waits
+      // one round trip per element)
+      const uint32_t* gm = d.gmask + g.off;
+      for ( int q0 = tid; q0 <= g.n; q0 += 8 * blockDim.x )
+      {
+        uint32_t v[ 8 ];
+#pragma unroll
+        for ( int u = 0; u < 8; ++u )
+        {
+          const int q = q0 + u * blockDim.x;
+          v[ u ] = q < g.n ? gm[ q ] : 0u;
+        }
+#pragma unroll
+        for ( int u = 0; u < 8; ++u )
+        {
+          const int q = q0 + u * blockDim.x;
+          if ( q <= g.n )
+            s_mask[ q ] = ( uint16_t ) v[ u ];
+        }
+      }
       __syncthreads();
       staged = id;
     }
@@ -505,8 +523,9 @@ k_gather( Net d )
       }
     }
     // parts 1.. hand their planes to part 0, which adds them bit-parallel
-    // (a ripple-carry adder over the 12 planes) and writes count * weight
-    // into the ring
+    // (a ripple-carry adder over the 12 planes) and hands the sum back; then
+    // every part adds count * weight into the ring for its share of the
+    // (lag, type) pairs, all its ring loads issued before any store
     if ( part > 0 )
     {
 #pragma unroll
@@ -514,7 +533,7 @@ k_gather( Net d )
         s_pl[ ( ( part - 1 ) * G_PLANES + b ) * GT + ti ] = P[ b ];
     }
     __syncthreads();
-    if ( part == 0 && tl < g.n )
+    if ( part == 0 )
     {
       for ( int q = 0; q < GP - 1; ++q )
       {
@@ -529,23 +548,68 @@ k_gather( Net d )
           c = c2;
         }
       }
-      const int64_t t = g.off + tl;
-      for ( int k = 0; k < d.min_delay; ++k )
-      {
-        const int slot = ( int ) ( ( origin + k + g.d ) % d.L );
+    }
+    __syncthreads();
+    if ( part == 0 )
+    {
 #pragma unroll
-        for ( int ty = 0; ty < 2; ++ty )
+      for ( int b = 0; b < G_PLANES; ++b )
+        s_pl[ b * GT + ti ] = P[ b ];
+    }
+    __syncthreads();
+    if ( tl < g.n )
+    {
+      uint32_t S[ G_PLANES ];
+#pragma unroll
+      for ( int b = 0; b < G_PLANES; ++b )
+        S[ b ] = s_pl[ b * GT + ti ];
+      const int64_t t = g.off + tl;
+      // this part owns lags k = part, part + GP, ... (< min_delay <= 16), both
+      // types; with one channel (ce == ci) the two types share a ring cell
+      // and are summed first
+      constexpr int NLAG = 16 / GP;
+      const int64_t dci = ( int64_t ) ( g.ci - g.ce ) * d.N;
+      int64_t idx[ NLAG ];  // ring cell of the excitatory channel; inhibitory at + dci
+      long long v[ 2 * NLAG ];
+      unsigned act = 0u;
+#pragma unroll
+      for ( int j = 0; j < NLAG; ++j )
+      {
+        const int k = part + j * GP;
+        long long ae = 0, ai = 0;
+        if ( k < d.min_delay )
         {
-          const unsigned n = plane_count( P, ty * 16 + k );
-          if ( n == 0u )
-            continue;
-          const int64_t idx = ( ( int64_t ) slot * d.C + ( ty ? g.ci : g.ce ) ) * d.N + t;
-          if ( d.ring32 )
-            reinterpret_cast< int32_t* >( ring )[ idx ] += ( int32_t ) n * ( ty ? g.wi : g.we );
-          else
-            ring[ idx ] += ( long long ) n * ( long long ) ( ty ? g.wi : g.we );
+          ae = ( long long ) plane_count( S, k ) * ( long long ) g.we;
+          ai = ( long long ) plane_count( S, 16 + k ) * ( long long ) g.wi;
         }
+        if ( dci == 0 )
+        {
+          ae += ai;
+          ai = 0;
+        }
+        idx[ j ] = ( ( int64_t ) ( ( origin + k + g.d ) % d.L ) * d.C + g.ce ) * d.N + t;
+        act |= ( ae ? 1u : 0u ) << ( 2 * j );
+        act |= ( ai ? 1u : 0u ) << ( 2 * j + 1 );
+        v[ 2 * j ] = ae;
+        v[ 2 * j + 1 ] = ai;
       }
+#pragma unroll
+      for ( int u = 0; u < 2 * NLAG; ++u )
+        if ( act >> u & 1u )
+        {
+          const int64_t i = idx[ u >> 1 ] + ( u & 1 ? dci : 0 );
+          v[ u ] += d.ring32 ? ( long long ) reinterpret_cast< const int32_t* >( ring )[ i ] : ring[ i ];
+        }
+#pragma unroll
+      for ( int u = 0; u < 2 * NLAG; ++u )
+        if ( act >> u & 1u )
+        {
+          const int64_t i = idx[ u >> 1 ] + ( u & 1 ? dci : 0 );
+          if ( d.ring32 )
+            reinterpret_cast< int32_t* >( ring )[ i ] = ( int32_t ) v[ u ];
+          else
+            ring[ i ] = v[ u ];
+        }
     }
     __syncthreads();
   }
