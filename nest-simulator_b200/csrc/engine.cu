@@ -218,7 +218,7 @@ struct ng_engine
   std::vector< Blk > blk;
 
   DevBuf ring, row_beg, row_len, real_deg, tdc, w, ent, log, rec, pois, pois_w, pois_d, pois_ref, pois_cdf, trace_col,
-    trace, sched_step, sched_src, ctl;
+    trace, sched_step, sched_src, ctl, row_ue, row_ls, ent_late;
   int32_t tbits = 1;
   int ring_bytes = 8;  // 4: 32-bit fixed-point ring cells (serving, FP32 form)
   uint32_t tmask = 1, dmask = 0;
@@ -270,6 +270,68 @@ struct ng_engine
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector< DevBuf* > all;
   int deliver_ctas = 0, deliver_per_sm = 4;
+
+  // ---- late delivery: the edges of delay >= 2 min_delay of a slice's
+  // spikes are delivered on a second stream while the next slice updates
+  // (its update reads no ring slot they reach); the slice after that waits
+  // for them.  Rows hold their shorter-delay edges first (row_ue, row_ls).
+  cudaStream_t late_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_late[ 2 ] = { nullptr, nullptr };
+  bool late_pending[ 2 ] = { false, false };
+  bool late_env = true;
+  int32_t late_min_cur = INT32_MAX;  // in force: 2 min_delay, or INT32_MAX (off)
+  int late_ctas = 1, late_per_sm = 2;
+
+  // rows are split by delay class when the ring can hold such edges and the
+  // target-tiled delivery (which needs target-sorted rows) is off
+  bool
+  late_possible() const
+  {
+    return !tiled_on && cfg.max_delay >= 2 * cfg.min_delay;
+  }
+
+  int32_t
+  late_thr() const
+  {
+    return late_possible() ? 2 * cfg.min_delay : INT32_MAX;
+  }
+
+  // off while a network uses the per-target gather: its plain ring updates
+  // must not meet a late delivery's atomics on the same cells (a network can
+  // turn from scatter to gather between two slices)
+  int32_t
+  late_target() const
+  {
+    if ( !late_possible() || !late_env )
+      return INT32_MAX;
+    if ( gather_on )
+      for ( size_t id = 0; id < nets.size(); ++id )
+        if ( nets[ id ].used && host_g[ id ].ke + host_g[ id ].ki > 0 )
+          return INT32_MAX;
+    return 2 * cfg.min_delay;
+  }
+
+  // a network with a per-target gather table is admitted: the gather kernel
+  // is launched every slice (it needs whole SMs, so it would also wait for
+  // any delivery still running)
+  bool gather_live = false;
+
+  void
+  refresh_late()
+  {
+    const int32_t v = late_target();
+    bool gl = false;
+    if ( gather_on )
+      for ( size_t id = 0; id < nets.size(); ++id )
+        gl = gl || ( nets[ id ].used && host_g[ id ].ke + host_g[ id ].ki > 0 );
+    if ( v != late_min_cur || gl != gather_live )
+    {
+      late_min_cur = v;
+      gather_live = gl;
+      ++generation;
+    }
+    late_ctas = std::max( 1, std::min( deliver_ctas, sms * std::min( late_per_sm, deliver_per_sm ) ) );
+  }
 
   // ---- serving: networks added to and removed from the running engine
   bool serving = false;
@@ -390,9 +452,6 @@ struct ng_engine
       return rc;
     if ( ( rc = alloc( tdc, ( size_t ) E * 4 ) ) || ( rc = alloc( w, ( size_t ) E * ( prec == NG_FP64 ? 8 : 4 ) ) ) )
       return rc;
-    chunks_all_src = E / CHUNK_EDGES + N;
-    if ( ( rc = resize_work() ) )
-      return rc;
     Blk& b = blk[ 0 ];
     cls_cap = 1 << 16;
     if ( ( rc = alloc( b.ctab, ( size_t ) cls_cap * CT_STRIDE * 8 ) ) || ( rc = alloc( b.cls, ( size_t ) N * 4 ) ) )
@@ -464,6 +523,9 @@ struct ng_engine
         free_seg[ 0 ] = cfg.tile_capacity;
       }
     }
+    chunks_all_src = E / CHUNK_EDGES + N;
+    if ( ( rc = resize_work() ) )
+      return rc;
     // one fixed-point scale for every network (FP32 form)
     // 32-bit rings: the scale keeps the largest possible cell sum inside 31 bits
     const double mx = ring_bytes == 4 ? cfg.ring_bound : cfg.max_abs_weight > 0 ? cfg.max_abs_weight : 1e4;
@@ -474,6 +536,53 @@ struct ng_engine
     serving = true;
     ++generation;
     CU( cudaStreamSynchronize( stream ) );
+    return NG_OK;
+  }
+
+  // Rows [n0, n0 + n) of a network drawn on the device, edges [e0, e0 + ne):
+  // each row's edges of delay < 2 min_delay first, through a temporary copy
+  // (without the memory for it, both deliveries walk the whole rows).
+  int
+  split_rows( int64_t n, int64_t n0, int64_t e0, int64_t ne )
+  {
+    if ( n <= 0 )
+      return NG_OK;
+    const size_t wsz = prec == NG_FP64 ? 8 : 4;
+    void* st = nullptr;
+    void* sw = nullptr;
+    const unsigned gn = ( unsigned ) ( ( n + 255 ) / 256 );
+    if ( ne > 0 && cudaMalloc( &st, ( size_t ) ne * 4 ) == cudaSuccess
+      && cudaMalloc( &sw, ( size_t ) ne * wsz ) == cudaSuccess )
+    {
+      const unsigned g = ( unsigned ) ( ( n * 32 + 255 ) / 256 );
+      if ( wsz == 8 )
+        k_row_split< double ><<< g, 256, 0, stream >>>( n, n0, e0, ( const int64_t* ) row_beg.p,
+          ( const int32_t* ) row_len.p, ( const int32_t* ) real_deg.p, ( const uint32_t* ) tdc.p, ( const double* ) w.p,
+          ( uint32_t* ) st, ( double* ) sw, late_thr(), tbits, dmask, ( int32_t* ) row_ue.p, ( int32_t* ) row_ls.p );
+      else
+        k_row_split< int32_t ><<< g, 256, 0, stream >>>( n, n0, e0, ( const int64_t* ) row_beg.p,
+          ( const int32_t* ) row_len.p, ( const int32_t* ) real_deg.p, ( const uint32_t* ) tdc.p, ( const int32_t* ) w.p,
+          ( uint32_t* ) st, ( int32_t* ) sw, late_thr(), tbits, dmask, ( int32_t* ) row_ue.p, ( int32_t* ) row_ls.p );
+      cudaError_t ce = cudaGetLastError();
+      if ( ce == cudaSuccess )
+        ce = cudaMemcpyAsync( ( uint32_t* ) tdc.p + e0, st, ( size_t ) ne * 4, cudaMemcpyDeviceToDevice, stream );
+      if ( ce == cudaSuccess )
+        ce = cudaMemcpyAsync( ( char* ) w.p + ( size_t ) e0 * wsz, sw, ( size_t ) ne * wsz, cudaMemcpyDeviceToDevice,
+          stream );
+      if ( ce == cudaSuccess )
+        ce = cudaStreamSynchronize( stream );
+      cudaFree( st );
+      cudaFree( sw );
+      if ( ce != cudaSuccess )
+        return fail( NG_ERR_CUDA, std::string( "row split: " ) + cudaGetErrorString( ce ) );
+      return NG_OK;
+    }
+    cudaGetLastError();  // a failed allocation leaves no sticky error
+    if ( st )
+      cudaFree( st );
+    k_row_uniform<<< gn, 256, 0, stream >>>( n, n0, ( const int32_t* ) row_len.p, ne > 0 ? 2 : 1,
+      ( int32_t* ) row_ue.p, ( int32_t* ) row_ls.p );
+    CU( cudaGetLastError() );
     return NG_OK;
   }
 
@@ -508,11 +617,14 @@ struct ng_engine
   {
     int64_t need = ( int64_t ) cfg.min_delay * chunks_all_src + n_sched * chunks_max_gen + 1024;
     need = std::min< int64_t >( need, 1ll << 28 );
-    if ( need <= ent_cap )
+    if ( need <= ent_cap && ( !late_possible() || ent_late.bytes >= 2 * ( size_t ) ent_cap * sizeof( int4 ) ) )
       return NG_OK;
-    ent_cap = need;
+    ent_cap = std::max( need, ent_cap );
     ++generation;
-    return alloc( ent, ( size_t ) ent_cap * sizeof( int4 ) );
+    int rc = alloc( ent, ( size_t ) ent_cap * sizeof( int4 ) );
+    if ( rc == NG_OK && late_possible() )
+      rc = alloc( ent_late, 2 * ( size_t ) ent_cap * sizeof( int4 ) );
+    return rc;
   }
   int max_lanes = 32;             // 1: always one thread per neuron
   int sub_lags = 8;               // lags whose inputs one thread gathers together (4 or 8)
@@ -534,7 +646,7 @@ struct ng_engine
     DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
       &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl, &d_nid, &d_step0, &d_until, &d_off,
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
-      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t };
+      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t, &row_ue, &row_ls, &ent_late };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -550,6 +662,11 @@ struct ng_engine
         cudaEventDestroy( ev );
     if ( copy_stream )
       cudaStreamDestroy( copy_stream );
+    if ( late_stream )
+      cudaStreamDestroy( late_stream );
+    for ( cudaEvent_t ev : { ev_fork, ev_late[ 0 ], ev_late[ 1 ] } )
+      if ( ev )
+        cudaEventDestroy( ev );
     if ( ev0 )
       cudaEventDestroy( ev0 );
     if ( ev1 )
@@ -728,6 +845,10 @@ struct ng_engine
     d.row_beg = ( const int64_t* ) row_beg.p;
     d.row_len = ( const int32_t* ) row_len.p;
     d.real_deg = ( const int32_t* ) real_deg.p;
+    d.late_min = late_min_cur;
+    d.row_ue = ( const int32_t* ) row_ue.p;
+    d.row_ls = ( const int32_t* ) row_ls.p;
+    d.ent_late = ( int4* ) ent_late.p;
     d.edge_tdc = ( const uint32_t* ) tdc.p;
     d.edge_w = w.p;
     d.ent = ( int4* ) ent.p;
@@ -872,7 +993,7 @@ struct ng_engine
   void
   launch_deliver( const Net& d )
   {
-    if ( gather_on )
+    if ( gather_live )
       k_gather<<< ( unsigned ) sms, G_THREADS, G_SMEM, stream >>>( d );
     if ( tiled_on )
     {
@@ -885,14 +1006,59 @@ struct ng_engine
     }
     const unsigned grid = ( unsigned ) deliver_ctas;
     if ( prec == NG_FP64 )
-      k_deliver< false ><<< grid, 256, 0, stream >>>( d );
+      k_deliver< false, false ><<< grid, 256, 0, stream >>>( d );
     else
-      k_deliver< true ><<< grid, 256, 0, stream >>>( d );
+      k_deliver< true, false ><<< grid, 256, 0, stream >>>( d );
+  }
+
+  // the late delivery of the slice whose update was launched last
+  void
+  launch_late( const Net& d, cudaStream_t s )
+  {
+    const unsigned grid = ( unsigned ) late_ctas;
+    if ( prec == NG_FP64 )
+      k_deliver< false, true ><<< grid, 256, 0, s >>>( d );
+    else
+      k_deliver< true, true ><<< grid, 256, 0, s >>>( d );
+  }
+
+  // before a slice's update (slice parity j): the late delivery of two
+  // slices back, which read the list this update appends to, has finished
+  void
+  late_wait( int j )
+  {
+    if ( late_pending[ j ] )
+    {
+      cudaStreamWaitEvent( stream, ev_late[ j ], 0 );
+      late_pending[ j ] = false;
+    }
+  }
+
+  // after a slice's update: its late delivery on the second stream
+  void
+  late_fork( const Net& d, int j )
+  {
+    cudaEventRecord( ev_fork, stream );
+    cudaStreamWaitEvent( late_stream, ev_fork, 0 );
+    launch_late( d, late_stream );
+    cudaEventRecord( ev_late[ j ], late_stream );
+    late_pending[ j ] = true;
+  }
+
+  void
+  late_join()
+  {
+    late_wait( 0 );
+    late_wait( 1 );
   }
 
   int
   run_slice_range( const Net& d, int from_, int to_ )
   {
+    const bool late = d.late_min != INT32_MAX;
+    const int par = ( int ) ( slices & 1 );
+    if ( late && from_ == 0 )
+      late_wait( par );
     if ( profiling )
       CU( cudaEventRecord( ev0, stream ) );
     launch_update( d, from_, to_ );
@@ -908,9 +1074,14 @@ struct ng_engine
     stats.update_launches += ( int64_t ) blk.size();
     if ( to_ == cfg.min_delay )
     {
+      // profiling: the late delivery runs after the slice-close one, timed with it
+      if ( late && !profiling )
+        late_fork( d, par );
       if ( profiling )
         CU( cudaEventRecord( ev0, stream ) );
       launch_deliver( d );
+      if ( late && profiling )
+        launch_late( d, stream );
       CU( cudaGetLastError() );
       if ( profiling )
       {
@@ -973,9 +1144,14 @@ struct ng_engine
     }
     cudaGraph_t cg;
     CU( cudaStreamBeginCapture( stream, cudaStreamCaptureModeThreadLocal ) );
-    // event record nodes inside the graph (external events) bracket every kernel
+    // event record nodes inside the graph (external events) bracket every
+    // kernel; late deliveries fork to the second stream and join before the
+    // graph ends (profiling: they run after the slice-close delivery)
+    const bool late = d.late_min != INT32_MAX;
     for ( int sl = 0; sl < k; ++sl )
     {
+      if ( late )
+        late_wait( sl & 1 );
       if ( prof )
         cudaEventRecordWithFlags( g.ev[ 4 * sl + 0 ], stream, cudaEventRecordExternal );
       launch_update( d, 0, cfg.min_delay );
@@ -984,10 +1160,15 @@ struct ng_engine
         cudaEventRecordWithFlags( g.ev[ 4 * sl + 1 ], stream, cudaEventRecordExternal );
         cudaEventRecordWithFlags( g.ev[ 4 * sl + 2 ], stream, cudaEventRecordExternal );
       }
+      if ( late && !prof )
+        late_fork( d, sl & 1 );
       launch_deliver( d );
+      if ( late && prof )
+        launch_late( d, stream );
       if ( prof )
         cudaEventRecordWithFlags( g.ev[ 4 * sl + 3 ], stream, cudaEventRecordExternal );
     }
+    late_join();
     CU( cudaStreamEndCapture( stream, &cg ) );
     cudaError_t e = cudaGraphInstantiate( &g.exec, cg, 0 );
     cudaGraphDestroy( cg );
@@ -1013,6 +1194,7 @@ struct ng_engine
         for ( int cand : { graph_slices, 16, 4 } )
           if ( cand <= graph_slices && cand <= full && cand > k )
             k = cand;
+        late_join();  // a graph starts with no late delivery outstanding
         GraphEntry* g = nullptr;
         int rc = get_graph( d, k, profiling != 0, &g );
         if ( rc )
@@ -1054,6 +1236,7 @@ struct ng_engine
         from = to_;
       }
     }
+    late_join();
     return NG_OK;
   }
 
@@ -1423,6 +1606,20 @@ ng_create( const ng_config* cfg, ng_engine** out )
   if ( cudaStreamCreateWithFlags( &e->own, cudaStreamNonBlocking ) != cudaSuccess )
     return bail( fail( NG_ERR_CUDA, "cudaStreamCreate failed" ) );
   e->stream = e->own;
+  {
+    // the late deliveries yield SM slots to the update kernels
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange( &lo, &hi );
+    if ( cudaStreamCreateWithPriority( &e->late_stream, cudaStreamNonBlocking, lo ) != cudaSuccess
+      || cudaEventCreateWithFlags( &e->ev_fork, cudaEventDisableTiming ) != cudaSuccess
+      || cudaEventCreateWithFlags( &e->ev_late[ 0 ], cudaEventDisableTiming ) != cudaSuccess
+      || cudaEventCreateWithFlags( &e->ev_late[ 1 ], cudaEventDisableTiming ) != cudaSuccess )
+      return bail( fail( NG_ERR_CUDA, "ng_create: late-delivery stream or event creation failed" ) );
+    if ( const char* lt = std::getenv( "NG_LATE" ) )
+      e->late_env = std::atoi( lt ) != 0;
+    if ( const char* lp = std::getenv( "NG_LATE_PER_SM" ) )
+      e->late_per_sm = std::max( 1, std::atoi( lp ) );
+  }
   cudaEventCreate( &e->ev0 );
   cudaEventCreate( &e->ev1 );
   if ( cudaMallocHost( &e->host_ctl, 2 * sizeof( Ctl ) ) != cudaSuccess )
@@ -1490,6 +1687,9 @@ ng_create( const ng_config* cfg, ng_engine** out )
     return bail( rc );
   if ( ( rc = e->alloc( e->real_deg, ( size_t ) e->n_src * sizeof( int32_t ) ) ) )
     return bail( rc );
+  if ( ( rc = e->alloc( e->row_ue, ( size_t ) e->n_src * sizeof( int32_t ) ) )
+    || ( rc = e->alloc( e->row_ls, ( size_t ) e->n_src * sizeof( int32_t ) ) ) )
+    return bail( rc );
   if ( ( rc = e->alloc( e->tdc, 16 ) ) || ( rc = e->alloc( e->w, 32 ) ) )
     return bail( rc );
   e->tbits = 1;
@@ -1531,10 +1731,12 @@ ng_create( const ng_config* cfg, ng_engine** out )
     // resident delivery CTAs per SM (the kernel splits its work over the warps of one wave)
     int occ = 0;
     if ( e->prec == NG_FP64 )
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< false >, 256, 0 );
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< false, false >, 256, 0 );
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< true >, 256, 0 );
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< true, false >, 256, 0 );
     e->deliver_per_sm = std::max( 1, std::min( occ, 8 ) );
+    if ( const char* dp = std::getenv( "NG_DELIVER_PER_SM" ) )
+      e->deliver_per_sm = std::max( 1, std::min( e->deliver_per_sm, std::atoi( dp ) ) );
   }
   if ( cfg->serving )
   {
@@ -1546,6 +1748,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
       return bail( rc );
     e->deliver_ctas = e->sms * e->deliver_per_sm;
   }
+  e->refresh_late();
   if ( const char* sl = std::getenv( "NG_UPDATE_SUB" ) )
     e->sub_lags = std::atoi( sl ) == 4 ? 4 : 8;
   if ( const char* ml = std::getenv( "NG_MAX_LANES" ) )
@@ -1795,8 +1998,13 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
     const unsigned g = ( unsigned ) ( ( n_src * 32 + 255 ) / 256 );
     k_pack_edges<<< g, 256, 0, e->stream >>>( n_src, ( const long long* ) d_rp.p, ( const long long* ) d_prow.p,
       ( const int32_t* ) d_tgt.p, ( const double* ) d_w.p, ( const int32_t* ) d_d.p, ps, fx ? 1 : 0, std::ldexp( 1.0, S ),
-      ( uint32_t* ) e->tdc.p, e->w.p );
+      ( uint32_t* ) e->tdc.p, e->w.p, e->late_thr(), ( int32_t* ) e->row_ue.p, ( int32_t* ) e->row_ls.p );
     CU( cudaGetLastError() );
+  }
+  else
+  {
+    CU( cudaMemsetAsync( e->row_ue.p, 0, e->row_ue.bytes, e->stream ) );
+    CU( cudaMemsetAsync( e->row_ls.p, 0, e->row_ls.bytes, e->stream ) );
   }
   CU( cudaStreamSynchronize( e->stream ) );
   free_tmp();
@@ -1817,6 +2025,7 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
   // delivery grid: one wave of resident CTAs, fewer for small graphs
   const int64_t want = std::max< int64_t >( 1, e->chunks_all_src / 64 );
   e->deliver_ctas = ( int ) std::min< int64_t >( want, ( int64_t ) e->sms * e->deliver_per_sm );
+  e->refresh_late();
   CU( cudaStreamSynchronize( e->stream ) );
   ++e->generation;
   return NG_OK;
@@ -2419,6 +2628,12 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       tn.tt = tt;
       e->host_t[ id ] = tn;
     }
+    if ( e->late_possible() )
+    {
+      int rc3;
+      if ( ( rc3 = e->split_rows( n, n0, e0, total ) ) )
+        return undo( rc3 );
+    }
     CU( cudaGetLastError() );
     CU( cudaStreamSynchronize( e->stream ) );
   }
@@ -2469,6 +2684,9 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     k_fi_rows<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, n0, e0, ( const int64_t* ) e->sc_beg.p,
       ( const int32_t* ) e->sc_plen.p, ( const int32_t* ) e->sc_cnt.p, ( int64_t* ) e->row_beg.p,
       ( int32_t* ) e->row_len.p, ( int32_t* ) e->real_deg.p );
+    // one delay: every row is of one delay class
+    k_row_uniform<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( n, n0, ( const int32_t* ) e->row_len.p,
+      fb->delay_steps < e->late_thr() ? 1 : 0, ( int32_t* ) e->row_ue.p, ( int32_t* ) e->row_ls.p );
     // the in-edge table of the per-target gather (16-bit local ids)
     const int64_t g_need = ( ( n + 31 ) / 32 * 32 ) * ( int64_t ) ( ( K + 7 ) / 8 * 8 );
     if ( e->gather_on && fx && nk > 0 && n <= G_MAX_N && K <= G_MAX_K
@@ -2500,7 +2718,19 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   else
   {
     const int64_t np = prow[ n ];
-    std::vector< int64_t > pos( prow.begin(), prow.end() - 1 );
+    // each row: its edges of delay below the late-delivery threshold first
+    const int32_t thr = e->late_thr();
+    std::vector< int32_t > nu( ( size_t ) n, 0 );
+    for ( int64_t k = 0; k < desc->nnz; ++k )
+      if ( desc->delay_steps[ k ] < thr )
+        ++nu[ desc->source[ k ] ];
+    std::vector< int64_t > pos( prow.begin(), prow.end() - 1 ), pos_l( ( size_t ) n );
+    std::vector< int32_t > ue( ( size_t ) n ), ls( ( size_t ) n );
+    for ( int64_t sidx = 0; sidx < n; ++sidx )
+    {
+      pos_l[ sidx ] = prow[ sidx ] + nu[ sidx ];
+      row_ranges( nu[ sidx ], rdeg[ sidx ], ( int ) ( prow[ sidx + 1 ] - prow[ sidx ] ), ue[ sidx ], ls[ sidx ] );
+    }
     std::vector< uint32_t > tw( ( size_t ) std::max< int64_t >( np, 1 ), 0u );
     std::vector< double > wd( fx ? 0 : ( size_t ) std::max< int64_t >( np, 1 ), 0.0 );
     std::vector< int32_t > wi( fx ? ( size_t ) std::max< int64_t >( np, 1 ) : 0, 0 );
@@ -2512,7 +2742,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       uint32_t ch;
       double we;
       e->edge_word( desc->weight[ k ], &ch, &we );
-      const int64_t j = pos[ desc->source[ k ] ]++;
+      const int64_t j = d < thr ? pos[ desc->source[ k ] ]++ : pos_l[ desc->source[ k ] ]++;
       tw[ j ] = ( uint32_t ) ( n0 + desc->target[ k ] ) | ( ( uint32_t ) d << e->tbits ) | ( ch << 31 );
       if ( fx )
       {
@@ -2541,6 +2771,8 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     CU( cudaMemcpyAsync( ( int32_t* ) e->row_len.p + n0, plen.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
     CU( cudaMemcpyAsync( ( int32_t* ) e->real_deg.p + n0, rdeg.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice,
       e->stream ) );
+    CU( cudaMemcpyAsync( ( int32_t* ) e->row_ue.p + n0, ue.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int32_t* ) e->row_ls.p + n0, ls.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
     CU( cudaStreamSynchronize( e->stream ) );
   }
   // 32-bit rings: no ring cell of this network may exceed 31 bits
@@ -2664,6 +2896,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   nw.log_rate = desc->record ? log_rate : 0.0;
   e->n_rec += desc->record ? n : 0;
   e->log_per_step = std::max( 1.0, e->log_per_step + nw.log_rate );
+  e->refresh_late();
   *net_id = id;
   return NG_OK;
 }
@@ -2842,6 +3075,7 @@ ng_net_remove( ng_engine* e, int32_t id )
   e->log_per_step = std::max( 1.0, e->log_per_step - nw.log_rate );
   ng_engine::free_blocks( nw.blocks );
   nw = ng_engine::NetInfo();
+  e->refresh_late();
   return NG_OK;
 }
 

@@ -51,6 +51,12 @@ struct Ctl
   int deliver_done;     // finished CTAs of the running delivery launch
   int err;
   int log_sel;          // half of the spike log the running group writes
+  // late delivery (edges of delay >= 2 min_delay, delivered while the next
+  // slice updates): two chunk lists used by alternate slices
+  unsigned long long n_late[ 2 ];
+  int late_wr;    // list the open slice's update appends to (flipped when the slice closes)
+  int late_rd;    // list the next late delivery reads (flipped by that delivery)
+  int late_done;  // finished CTAs of the running late delivery
 };
 
 // Spike-log entry of a serving engine: network-local source | network id << 22.
@@ -106,6 +112,15 @@ struct Net
   const void* edge_w;
   int4* ent;  // edge chunks: row start (lo, hi), edge count, slot | multiplicity << 16
   int64_t ent_cap;
+  // late delivery; late_min == INT32_MAX: off (every edge is delivered when
+  // its slice closes).  A row holds its edges of delay < late_min first:
+  // edges [0, row_ue) are covered by the slice-close chunks and [row_ls,
+  // padded length) by the late ones (row_ls <= row_ue: the ranges may share
+  // a 4-edge group; each delivery applies only its own delays)
+  int32_t late_min;
+  const int32_t* row_ue;
+  const int32_t* row_ls;
+  int4* ent_late;  // two lists of ent_cap entries
   uint2* log;           // two halves of log_cap entries (groups alternate)
   int64_t log_cap;
   const uint8_t* rec;

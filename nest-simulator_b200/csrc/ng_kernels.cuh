@@ -57,18 +57,70 @@ log_source( const Net& d, int32_t src )
   return ( uint32_t ) ( src - d.net_off[ id ] ) | ( ( uint32_t ) id << LOG_ID_SHIFT );
 }
 
-// Queue the edge chunks of one spike: ceil(pdeg / 128) work items.
-__device__ __forceinline__ void
-put_chunks( const Net& d, long long idx, long long row, long long pdeg, int slot, int mult )
+// The out-edges of a spiking source as delivery work: chunks of <= 128
+// edges of its padded CSR row.  With late delivery on, the slice-close
+// chunks cover the row's edges [0, ue) and the late chunks [ls, pdeg);
+// otherwise the slice-close chunks cover the whole row.
+struct RowWork
 {
-  for ( long long c = 0; c < pdeg; c += CHUNK_EDGES, ++idx )
+  long long row;
+  int pdeg, ue, ls;
+  int nu, nl;  // chunks: slice close, late
+};
+
+__device__ __forceinline__ RowWork
+row_work( const Net& d, int32_t src )
+{
+  RowWork w;
+  w.row = d.row_beg[ src ];
+  w.pdeg = d.row_len[ src ];
+  w.ue = w.pdeg;
+  w.ls = w.pdeg;
+  if ( d.late_min != INT32_MAX )
   {
-    const long long r = row + c;
-    const int ne = ( int ) ( pdeg - c < CHUNK_EDGES ? pdeg - c : CHUNK_EDGES );
-    if ( idx < d.ent_cap )
-      d.ent[ idx ] = make_int4( ( int ) ( unsigned ) ( r & 0xffffffffll ), ( int ) ( r >> 32 ), ne, slot | ( mult << 16 ) );
-    else
-      atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+    w.ue = d.row_ue[ src ];
+    w.ls = d.row_ls[ src ];
+  }
+  w.nu = ( w.ue + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
+  w.nl = ( w.pdeg - w.ls + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
+  return w;
+}
+
+// The late list the open slice appends to.
+__device__ __forceinline__ int4*
+late_list( const Net& d, int sel )
+{
+  return d.ent_late + ( sel ? d.ent_cap : 0 );
+}
+
+// Work item e of a list: chunk c of the edge range [lo, hi) of a row.
+__device__ __forceinline__ void
+put_chunk( const Net& d, int4* list, long long e, long long row, int lo, int hi, long long c, int slot, int mult )
+{
+  const long long r = row + lo + c * CHUNK_EDGES;
+  const long long left = ( long long ) ( hi - lo ) - c * CHUNK_EDGES;
+  const int ne = ( int ) ( left < CHUNK_EDGES ? left : CHUNK_EDGES );
+  if ( e < d.ent_cap )
+    list[ e ] = make_int4( ( int ) ( unsigned ) ( r & 0xffffffffll ), ( int ) ( r >> 32 ), ne, slot | ( mult << 16 ) );
+  else
+    atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+}
+
+// Inclusive warp prefix sums of two counters.
+__device__ __forceinline__ void
+warp_scan2( long long& a, long long& b )
+{
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for ( int o = 1; o < 32; o <<= 1 )
+  {
+    const long long x = __shfl_up_sync( FULL, a, o );
+    const long long y = __shfl_up_sync( FULL, b, o );
+    if ( lane >= o )
+    {
+      a += x;
+      b += y;
+    }
   }
 }
 
@@ -82,41 +134,48 @@ warp_append( const Net& d, bool spk, int32_t src, int32_t tmod, int32_t mult, lo
     return;
   const int lane = threadIdx.x & 31;
   const unsigned lt = ( 1u << lane ) - 1u;
-  long long pdeg = 0, rdeg = 0, row = 0, nch = 0;
+  RowWork rw {};
+  long long rdeg = 0;
   if ( spk )
   {
-    row = d.row_beg[ src ];
-    pdeg = d.row_len[ src ];
+    rw = row_work( d, src );
     rdeg = ( long long ) d.real_deg[ src ] * mult;
-    nch = ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
   }
-  long long incl = nch;
-#pragma unroll
-  for ( int o = 1; o < 32; o <<= 1 )
-  {
-    const long long v = __shfl_up_sync( FULL, incl, o );
-    if ( lane >= o )
-      incl += v;
-  }
-  const long long tot = __shfl_sync( FULL, incl, 31 );
+  long long inc_u = rw.nu, inc_l = rw.nl;
+  warp_scan2( inc_u, inc_l );
+  const long long tot_u = __shfl_sync( FULL, inc_u, 31 );
+  const long long tot_l = __shfl_sync( FULL, inc_l, 31 );
   const long long rtot = warp_sum_ll( rdeg );
   const long long mtot = warp_sum_ll( spk ? ( long long ) mult : 0ll );
   const bool lg = spk && ( d.rec == nullptr || d.rec[ src ] );
   const unsigned lm = __ballot_sync( FULL, lg );
-  unsigned long long base = 0, lb = 0;
+  unsigned long long base = 0, lb = 0, xb = 0;
+  int sel = 0;
   if ( lane == 0 )
   {
-    if ( tot > 0 )
-      base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot );
+    if ( tot_u > 0 )
+      base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot_u );
+    if ( tot_l > 0 )
+    {
+      sel = ld_volatile( &d.ctl->late_wr );
+      xb = atomicAdd( &d.ctl->n_late[ sel ], ( unsigned long long ) tot_l );
+    }
     if ( lm )
       lb = atomicAdd( &d.ctl->log_count, ( unsigned long long ) __popc( lm ) );
     atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
     atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) mtot );
   }
   base = __shfl_sync( FULL, base, 0 );
+  xb = __shfl_sync( FULL, xb, 0 );
   lb = __shfl_sync( FULL, lb, 0 );
-  if ( spk && nch > 0 )
-    put_chunks( d, ( long long ) base + incl - nch, row, pdeg, tmod, mult );
+  sel = __shfl_sync( FULL, sel, 0 );
+  if ( spk )
+  {
+    for ( int c = 0; c < rw.nu; ++c )
+      put_chunk( d, d.ent, ( long long ) base + inc_u - rw.nu + c, rw.row, 0, rw.ue, c, tmod, mult );
+    for ( int c = 0; c < rw.nl; ++c )
+      put_chunk( d, late_list( d, sel ), ( long long ) xb + inc_l - rw.nl + c, rw.row, rw.ls, rw.pdeg, c, tmod, mult );
+  }
   if ( lg )
   {
     const long long li = ( long long ) lb + __popc( lm & lt );
@@ -145,47 +204,48 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
   if ( __ballot_sync( FULL, cnt > 0 ) == 0 )
     return;
   const int lane = threadIdx.x & 31;
-  long long pdeg = 0, rdeg = 0, row = 0, nch = 0;
+  RowWork rw {};
+  long long rdeg = 0;
   const bool lg = cnt > 0 && ( d.rec == nullptr || d.rec[ src ] );
   if ( cnt > 0 )
   {
-    row = d.row_beg[ src ];
-    pdeg = d.row_len[ src ];
+    rw = row_work( d, src );
     rdeg = d.real_deg[ src ];
-    nch = ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
   }
-  long long e_incl = cnt * nch, l_incl = lg ? cnt : 0;
-#pragma unroll
-  for ( int o = 1; o < 32; o <<= 1 )
-  {
-    const long long b = __shfl_up_sync( FULL, e_incl, o );
-    const long long c = __shfl_up_sync( FULL, l_incl, o );
-    if ( lane >= o )
-    {
-      e_incl += b;
-      l_incl += c;
-    }
-  }
-  const long long tot_e = __shfl_sync( FULL, e_incl, 31 );
-  const long long tot_l = __shfl_sync( FULL, l_incl, 31 );
+  long long inc_u = ( long long ) cnt * rw.nu, inc_l = ( long long ) cnt * rw.nl;
+  warp_scan2( inc_u, inc_l );
+  long long inc_g = lg ? cnt : 0, dummy = 0;
+  warp_scan2( inc_g, dummy );
+  const long long tot_u = __shfl_sync( FULL, inc_u, 31 );
+  const long long tot_l = __shfl_sync( FULL, inc_l, 31 );
+  const long long tot_g = __shfl_sync( FULL, inc_g, 31 );
   const long long rtot = warp_sum_ll( cnt * rdeg );
   const long long ctot = warp_sum_ll( cnt );
-  unsigned long long base = 0, lbase = 0;
+  unsigned long long base = 0, xb = 0, lbase = 0;
+  int sel = 0;
   if ( lane == 0 )
   {
-    if ( tot_e > 0 )
-      base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot_e );
+    if ( tot_u > 0 )
+      base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot_u );
     if ( tot_l > 0 )
-      lbase = atomicAdd( &d.ctl->log_count, ( unsigned long long ) tot_l );
+    {
+      sel = ld_volatile( &d.ctl->late_wr );
+      xb = atomicAdd( &d.ctl->n_late[ sel ], ( unsigned long long ) tot_l );
+    }
+    if ( tot_g > 0 )
+      lbase = atomicAdd( &d.ctl->log_count, ( unsigned long long ) tot_g );
     atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
     atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) ctot );
   }
   base = __shfl_sync( FULL, base, 0 );
+  xb = __shfl_sync( FULL, xb, 0 );
   lbase = __shfl_sync( FULL, lbase, 0 );
+  sel = __shfl_sync( FULL, sel, 0 );
   if ( cnt == 0 )
     return;
-  long long idx = ( long long ) base + e_incl - cnt * nch;
-  long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
+  long long iu = ( long long ) base + inc_u - ( long long ) cnt * rw.nu;
+  long long il = ( long long ) xb + inc_l - ( long long ) cnt * rw.nl;
+  long long li = ( long long ) lbase + inc_g - ( lg ? cnt : 0 );
   const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
   uint2* const lg_buf = lg ? log_half( d ) : nullptr;
   const uint32_t lsrc = lg ? log_source( d, src ) : 0u;
@@ -197,9 +257,12 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
     int slot = slot0 + k;
     if ( slot >= d.L )
       slot -= d.L;
-    if ( nch > 0 )
-      put_chunks( d, idx, row, pdeg, slot, 1 );
-    idx += nch;
+    for ( int c = 0; c < rw.nu; ++c )
+      put_chunk( d, d.ent, iu + c, rw.row, 0, rw.ue, c, slot, 1 );
+    for ( int c = 0; c < rw.nl; ++c )
+      put_chunk( d, late_list( d, sel ), il + c, rw.row, rw.ls, rw.pdeg, c, slot, 1 );
+    iu += rw.nu;
+    il += rw.nl;
     if ( lg )
     {
       if ( li < d.log_cap )
@@ -215,37 +278,47 @@ warp_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long
 // CTA combined: one global atomic per counter and CTA (thousands of warps of
 // a large network each reserving on the same control-block line serialise
 // in L2).  A neuron of a network in gather mode queues no edge chunks (its
-// targets gather); spikes are counted per network for the mode choice.
+// targets gather); spikes are counted per network for the mode choice.  The
+// whole warp writes each spike's chunk entries, consecutive lanes
+// consecutive entries (a source with thousands of out-edges has dozens).
 // Must be called by every thread of the CTA.
 __device__ __forceinline__ void
 cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long t0, int netid, bool gath )
 {
   const bool tiled = !gath && netid >= 0 && d.net_t != nullptr && d.net_t[ netid ].nt > 0;
-  __shared__ unsigned long long s_e, s_l, s_r, s_c, g_e, g_l;
-  __shared__ int s_any;
+  __shared__ unsigned long long s_e, s_x, s_l, s_r, s_c, g_e, g_x, g_l;
+  __shared__ int s_any, s_sel;
   const int lane = threadIdx.x & 31;
   if ( threadIdx.x == 0 )
   {
-    s_e = s_l = s_r = s_c = 0ull;
+    s_e = s_x = s_l = s_r = s_c = 0ull;
     s_any = 0;
   }
   __syncthreads();
   const int cnt = __popc( mask );
   const bool any = __ballot_sync( FULL, cnt > 0 ) != 0;
-  long long pdeg = 0, rdeg = 0, row = 0, nch = 0;
+  RowWork rw {};
+  long long rdeg = 0;
   const bool lg = cnt > 0 && ( d.rec == nullptr || d.rec[ src ] );
-  long long e_incl = 0, l_incl = 0;
-  unsigned long long w_e = 0, w_l = 0;
+  long long inc_u = 0, inc_l = 0, inc_g = 0;
+  unsigned long long w_e = 0, w_x = 0, w_l = 0;
   if ( any )
   {
     if ( cnt > 0 )
     {
-      row = d.row_beg[ src ];
-      pdeg = d.row_len[ src ];
-      rdeg = d.real_deg[ src ];
       // a spike of a tiled network is one work entry (its source), of a
-      // network in gather mode none, else one per 128-edge chunk
-      nch = gath ? 0 : tiled ? 1 : ( pdeg + CHUNK_EDGES - 1 ) / CHUNK_EDGES;
+      // network in gather mode none, else its row's chunks
+      if ( !gath )
+      {
+        if ( tiled )
+        {
+          rw.nu = 1;
+          rw.row = d.row_beg[ src ];
+        }
+        else
+          rw = row_work( d, src );
+      }
+      rdeg = d.real_deg[ src ];
       if ( d.net_spk && netid >= 0 )
       {
         // one atomic per network present in the warp
@@ -255,27 +328,22 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
           atomicAdd( d.net_spk + netid, tot );
       }
     }
-    e_incl = cnt * nch;
-    l_incl = lg ? cnt : 0;
-#pragma unroll
-    for ( int o = 1; o < 32; o <<= 1 )
-    {
-      const long long b = __shfl_up_sync( FULL, e_incl, o );
-      const long long c = __shfl_up_sync( FULL, l_incl, o );
-      if ( lane >= o )
-      {
-        e_incl += b;
-        l_incl += c;
-      }
-    }
-    const long long tot_e = __shfl_sync( FULL, e_incl, 31 );
-    const long long tot_l = __shfl_sync( FULL, l_incl, 31 );
+    inc_u = ( long long ) cnt * rw.nu;
+    inc_l = ( long long ) cnt * rw.nl;
+    warp_scan2( inc_u, inc_l );
+    long long dummy = 0;
+    inc_g = lg ? cnt : 0;
+    warp_scan2( inc_g, dummy );
+    const long long tot_u = __shfl_sync( FULL, inc_u, 31 );
+    const long long tot_l = __shfl_sync( FULL, inc_l, 31 );
+    const long long tot_g = __shfl_sync( FULL, inc_g, 31 );
     const long long rtot = warp_sum_ll( cnt * rdeg );
     const long long ctot = warp_sum_ll( cnt );
     if ( lane == 0 )
     {
-      w_e = atomicAdd( &s_e, ( unsigned long long ) tot_e );
-      w_l = atomicAdd( &s_l, ( unsigned long long ) tot_l );
+      w_e = atomicAdd( &s_e, ( unsigned long long ) tot_u );
+      w_x = atomicAdd( &s_x, ( unsigned long long ) tot_l );
+      w_l = atomicAdd( &s_l, ( unsigned long long ) tot_g );
       atomicAdd( &s_r, ( unsigned long long ) rtot );
       atomicAdd( &s_c, ( unsigned long long ) ctot );
       s_any = 1;
@@ -287,17 +355,56 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
   if ( threadIdx.x == 0 )
   {
     g_e = s_e > 0 ? atomicAdd( &d.ctl->n_ent, s_e ) : 0ull;
+    s_sel = 0;
+    g_x = 0ull;
+    if ( s_x > 0 )
+    {
+      s_sel = ld_volatile( &d.ctl->late_wr );
+      g_x = atomicAdd( &d.ctl->n_late[ s_sel ], s_x );
+    }
     g_l = s_l > 0 ? atomicAdd( &d.ctl->log_count, s_l ) : 0ull;
     atomicAdd( &d.ctl->syn_events, s_r );
     atomicAdd( &d.ctl->n_spikes, s_c );
   }
   __syncthreads();
-  const unsigned long long base = g_e + __shfl_sync( FULL, w_e, 0 );
-  const unsigned long long lbase = g_l + __shfl_sync( FULL, w_l, 0 );
+  // every lane takes part in these shuffles (lanes without a spike leave below)
+  const long long iu0 = ( long long ) ( g_e + __shfl_sync( FULL, w_e, 0 ) ) + inc_u - ( long long ) cnt * rw.nu;
+  const long long il0 = ( long long ) ( g_x + __shfl_sync( FULL, w_x, 0 ) ) + inc_l - ( long long ) cnt * rw.nl;
+  long long li = ( long long ) ( g_l + __shfl_sync( FULL, w_l, 0 ) ) + inc_g - ( lg ? cnt : 0 );
+  int4* const xlist = late_list( d, s_sel );
+  unsigned owners = __ballot_sync( FULL, cnt > 0 && !gath && !tiled && ( rw.nu + rw.nl ) > 0 );
+  while ( owners )
+  {
+    const int ol = __ffs( owners ) - 1;
+    owners &= owners - 1;
+    const long long o_row = __shfl_sync( FULL, rw.row, ol );
+    const int o_pdeg = __shfl_sync( FULL, rw.pdeg, ol );
+    const int o_ue = __shfl_sync( FULL, rw.ue, ol );
+    const int o_ls = __shfl_sync( FULL, rw.ls, ol );
+    const int o_nu = __shfl_sync( FULL, rw.nu, ol );
+    const int o_nl = __shfl_sync( FULL, rw.nl, ol );
+    long long o_iu = __shfl_sync( FULL, iu0, ol );
+    long long o_il = __shfl_sync( FULL, il0, ol );
+    unsigned om = __shfl_sync( FULL, mask, ol );
+    const int o_slot0 = __shfl_sync( FULL, slot0, ol );
+    while ( om )
+    {
+      const int k = __ffs( om ) - 1;
+      om &= om - 1;
+      int slot = o_slot0 + k;
+      if ( slot >= d.L )
+        slot -= d.L;
+      for ( int c = lane; c < o_nu; c += 32 )
+        put_chunk( d, d.ent, o_iu + c, o_row, 0, o_ue, c, slot, 1 );
+      for ( int c = lane; c < o_nl; c += 32 )
+        put_chunk( d, xlist, o_il + c, o_row, o_ls, o_pdeg, c, slot, 1 );
+      o_iu += o_nu;
+      o_il += o_nl;
+    }
+  }
   if ( cnt == 0 )
     return;
-  long long idx = ( long long ) base + e_incl - cnt * nch;
-  long long li = ( long long ) lbase + l_incl - ( lg ? cnt : 0 );
+  long long idx = iu0;
   const long long lb0 = lg ? ld_volatile( &d.ctl->log_base ) : 0;
   uint2* const lg_buf = lg ? log_half( d ) : nullptr;
   const uint32_t lsrc = lg ? log_source( d, src ) : 0u;
@@ -315,10 +422,8 @@ cta_append_mask( const Net& d, unsigned mask, int32_t src, int slot0, long long 
         d.ent[ idx ] = make_int4( src, 0, -1, slot | ( 1 << 16 ) );  // edge count -1: no scatter chunk
       else
         atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+      ++idx;
     }
-    else if ( nch > 0 )
-      put_chunks( d, idx, row, pdeg, slot, 1 );
-    idx += nch;
     if ( lg )
     {
       if ( li < d.log_cap )
@@ -1379,17 +1484,19 @@ load_chunk( const Net& d, const int4 en, const int lane, ChunkLane< FIX >& c )
   }
 }
 
-template < bool FIX >
+template < bool FIX, bool LATE >
 __device__ __forceinline__ void
 apply_chunk( const Net& d, const ChunkLane< FIX >& c )
 {
 #pragma unroll
   for ( int k = 0; k < 4; ++k )
   {
-    if ( c.w[ k ] == 0 )
+    const int dl = ( int ) ( ( c.t[ k ] >> d.tbits ) & d.dmask );
+    // each delivery applies the delays of its own class
+    if ( c.w[ k ] == 0 || ( dl >= d.late_min ) != LATE )
       continue;
     const uint32_t tgt = c.t[ k ] & d.tmask;
-    int slot = c.slot0 + ( int ) ( ( c.t[ k ] >> d.tbits ) & d.dmask );
+    int slot = c.slot0 + dl;
     if ( slot >= d.L )
       slot -= d.L;
     const int64_t idx = ( ( int64_t ) slot * d.C + ( c.t[ k ] >> 31 ) ) * d.N + tgt;
@@ -1425,19 +1532,27 @@ shfl_int4( const int4 v, const int src )
 // current one issue: each lane loads 4 edges (one 16-byte edge-word
 // load, 16 or 32 bytes of weights) and issues their red.global adds.
 // ---------------------------------------------------------------------
-template < bool FIX >
+template < bool FIX, bool LATE >
 __global__ void __launch_bounds__( 256 )
 k_deliver( Net d )
 {
   __shared__ unsigned long long s_nent;
   __shared__ int s_err;
   __shared__ int s_last;
+  __shared__ int s_q;
   if ( threadIdx.x == 0 )
   {
-    s_nent = ld_volatile( &d.ctl->n_ent );
+    if constexpr ( LATE )
+    {
+      s_q = ld_volatile( &d.ctl->late_rd );
+      s_nent = ld_volatile( &d.ctl->n_late[ s_q ] );
+    }
+    else
+      s_nent = ld_volatile( &d.ctl->n_ent );
     s_err = ld_volatile( &d.ctl->err );
   }
   __syncthreads();
+  const int4* const list = LATE ? late_list( d, s_q ) : d.ent;
   const bool ok = ( long long ) s_nent <= d.ent_cap && ( s_err & ERR_SPIKE_LIST ) == 0;
   const long long nent = ok ? ( long long ) s_nent : 0;
   const int lane = threadIdx.x & 31;
@@ -1449,7 +1564,7 @@ k_deliver( Net d )
   for ( long long base = gw * G; base < nent; base += nwarps * G )
   {
     const int cnt = ( int ) min( G, nent - base );
-    const int4 my = lane < cnt ? d.ent[ base + lane ] : make_int4( 0, 0, 0, 0 );
+    const int4 my = lane < cnt ? list[ base + lane ] : make_int4( 0, 0, 0, 0 );
     ChunkLane< FIX > cur, nxt;
     load_chunk< FIX >( d, shfl_int4( my, 0 ), lane, cur );
     for ( int k = 0; k < cnt; ++k )
@@ -1457,18 +1572,29 @@ k_deliver( Net d )
       const int4 en = shfl_int4( my, min( k + 1, 31 ) );
       if ( k + 1 < cnt )
         load_chunk< FIX >( d, en, lane, nxt );
-      apply_chunk< FIX >( d, cur );
+      apply_chunk< FIX, LATE >( d, cur );
       cur = nxt;
     }
   }
-  // the last CTA to finish closes the slice
+  // the last CTA to finish closes the slice (a late delivery: its list)
   __syncthreads();
   if ( threadIdx.x == 0 )
   {
     __threadfence();
-    s_last = atomicAdd( &d.ctl->deliver_done, 1 ) == ( int ) gridDim.x - 1;
+    s_last = atomicAdd( LATE ? &d.ctl->late_done : &d.ctl->deliver_done, 1 ) == ( int ) gridDim.x - 1;
   }
   __syncthreads();
+  if constexpr ( LATE )
+  {
+    if ( s_last && threadIdx.x == 0 )
+    {
+      d.ctl->n_late[ s_q ] = 0ull;
+      d.ctl->late_done = 0;
+      d.ctl->late_rd = s_q ^ 1;
+      __threadfence();
+    }
+    return;
+  }
   if ( s_last && d.net_mode )
   {
     // delivery mode of every network for the next slice: gather when this
@@ -1489,6 +1615,8 @@ k_deliver( Net d )
     d.ctl->n_ent = 0ull;
     d.ctl->deliver_done = 0;
     d.ctl->origin = d.ctl->origin + d.min_delay;
+    if ( d.late_min != INT32_MAX )
+      d.ctl->late_wr ^= 1;
     __threadfence();
   }
 }
@@ -1573,29 +1701,163 @@ k_edge_check( long long nnz, const int32_t* tgt, const double* w, const int32_t*
   }
 }
 
-// one warp per source row: edge j of the row goes to padded position prow[s] + j
+// Slice-close and late edge ranges of a row whose real edges [0, deg) hold
+// its nu edges of delay < late_min first (padded length pdeg): the
+// slice-close chunks cover [0, ue), the late ones [ls, pdeg).
+__host__ __device__ __forceinline__ void
+row_ranges( int nu, int deg, int pdeg, int32_t& ue, int32_t& ls )
+{
+  if ( nu >= deg )
+  {
+    ue = pdeg;
+    ls = pdeg;
+  }
+  else if ( nu == 0 )
+  {
+    ue = 0;
+    ls = 0;
+  }
+  else
+  {
+    ue = ( nu + 3 ) & ~3;
+    ls = nu & ~3;
+  }
+}
+
+// Position of an edge in its row after a stable partition by delay class
+// (delay < thr first), for one 32-edge window of the row: cu / cl count the
+// slice-close / late edges of the earlier windows, nu the row's total of
+// slice-close edges.  All 32 lanes call it.
+__device__ __forceinline__ int
+split_pos( bool in, bool early, int nu, int& cu, int& cl )
+{
+  const unsigned lt = ( 1u << ( threadIdx.x & 31 ) ) - 1u;
+  const unsigned bu = __ballot_sync( FULL, in && early ), bl = __ballot_sync( FULL, in && !early );
+  const int pos = early ? cu + __popc( bu & lt ) : nu + cl + __popc( bl & lt );
+  cu += __popc( bu );
+  cl += __popc( bl );
+  return pos;
+}
+
+__device__ __forceinline__ int
+warp_sum_i( int v )
+{
+#pragma unroll
+  for ( int o = 16; o > 0; o >>= 1 )
+    v += __shfl_xor_sync( FULL, v, o );
+  return v;
+}
+
+// one warp per source row: the row's edges go to its padded positions from
+// prow[s] on, those of delay < late_min first (late_min == INT32_MAX: in
+// the caller's order)
 __global__ void
 k_pack_edges( long long n_src, const long long* row_ptr, const long long* prow, const int32_t* tgt, const double* w,
-  const int32_t* dl, PackSpec ps, int fx, double scale, uint32_t* tdc, void* wout )
+  const int32_t* dl, PackSpec ps, int fx, double scale, uint32_t* tdc, void* wout, int32_t late_min, int32_t* row_ue,
+  int32_t* row_ls )
 {
   const long long s = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
   const int lane = threadIdx.x & 31;
   if ( s >= n_src )
     return;
   const long long r0 = row_ptr[ s ], r1 = row_ptr[ s + 1 ], p0 = prow[ s ];
-  for ( long long j = r0 + lane; j < r1; j += 32 )
+  const int deg = ( int ) ( r1 - r0 );
+  int nu = deg;
+  if ( late_min != INT32_MAX )
   {
+    int c = 0;
+    for ( long long j = r0 + lane; j < r1; j += 32 )
+      c += dl[ j ] < late_min ? 1 : 0;
+    nu = warp_sum_i( c );
+  }
+  int cu = 0, cl = 0;
+  for ( long long j0 = r0; j0 < r1; j0 += 32 )
+  {
+    const long long j = j0 + lane;
+    const bool in = j < r1;
+    const int32_t dj = in ? dl[ j ] : 0;
+    const int pos = split_pos( in, dj < late_min, nu, cu, cl );
+    if ( !in )
+      continue;
     const int32_t t = tgt[ j ];
     uint32_t ch;
     double we;
     edge_channel( ps, t, w[ j ], ch, we );
-    const long long k = p0 + ( j - r0 );
-    tdc[ k ] = ( uint32_t ) t | ( ( uint32_t ) dl[ j ] << ps.tbits ) | ( ch << 31 );
+    const long long k = p0 + pos;
+    tdc[ k ] = ( uint32_t ) t | ( ( uint32_t ) dj << ps.tbits ) | ( ch << 31 );
     if ( fx )
       reinterpret_cast< int32_t* >( wout )[ k ] = ( int32_t ) llrint( we * scale );
     else
       reinterpret_cast< double* >( wout )[ k ] = we;
   }
+  if ( lane == 0 )
+  {
+    int32_t ue, ls;
+    row_ranges( nu, deg, ( deg + 3 ) & ~3, ue, ls );
+    row_ue[ s ] = ue;
+    row_ls[ s ] = ls;
+  }
+}
+
+// Rows [n0, n0 + n) of a network built on the device, edges [e0, e0 + ne):
+// the same stable partition by delay class, out of place into (stdc, sw),
+// padding entries kept at their positions.  One warp per row.
+template < typename W >
+__global__ void
+k_row_split( long long n, long long n0, long long e0, const int64_t* row_beg, const int32_t* row_len,
+  const int32_t* real_deg, const uint32_t* tdc, const W* w, uint32_t* stdc, W* sw, int32_t late_min, int tbits,
+  uint32_t dmask, int32_t* row_ue, int32_t* row_ls )
+{
+  const long long s = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  const int lane = threadIdx.x & 31;
+  if ( s >= n )
+    return;
+  const long long r0 = row_beg[ n0 + s ];
+  const int pdeg = row_len[ n0 + s ], deg = real_deg[ n0 + s ];
+  int c = 0;
+  for ( int j = lane; j < deg; j += 32 )
+    c += ( int ) ( ( tdc[ r0 + j ] >> tbits ) & dmask ) < late_min ? 1 : 0;
+  const int nu = warp_sum_i( c );
+  int cu = 0, cl = 0;
+  const long long o = r0 - e0;
+  for ( int j0 = 0; j0 < deg; j0 += 32 )
+  {
+    const int j = j0 + lane;
+    const bool in = j < deg;
+    const uint32_t t = in ? tdc[ r0 + j ] : 0u;
+    const int pos = split_pos( in, ( int ) ( ( t >> tbits ) & dmask ) < late_min, nu, cu, cl );
+    if ( in )
+    {
+      stdc[ o + pos ] = t;
+      sw[ o + pos ] = w[ r0 + j ];
+    }
+  }
+  for ( int j = deg + lane; j < pdeg; j += 32 )
+  {
+    stdc[ o + j ] = tdc[ r0 + j ];
+    sw[ o + j ] = w[ r0 + j ];
+  }
+  if ( lane == 0 )
+  {
+    int32_t ue, ls;
+    row_ranges( nu, deg, pdeg, ue, ls );
+    row_ue[ n0 + s ] = ue;
+    row_ls[ n0 + s ] = ls;
+  }
+}
+
+// Row ranges without a partition: mode 1, every edge of the row is of the
+// shorter delay class (fixed_indegree networks, one delay); 0, every edge is
+// late; 2, mixed rows in any order (both deliveries walk the whole row).
+__global__ void
+k_row_uniform( long long n, long long n0, const int32_t* row_len, int mode, int32_t* row_ue, int32_t* row_ls )
+{
+  const long long s = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+  if ( s >= n )
+    return;
+  const int32_t p = row_len[ n0 + s ];
+  row_ue[ n0 + s ] = mode != 0 ? p : 0;
+  row_ls[ n0 + s ] = mode == 1 ? p : 0;
 }
 
 // Host-side ctl edits between groups (log drain, trace window).
