@@ -1603,13 +1603,16 @@ ng_create( const ng_config* cfg, ng_engine** out )
     delete e;
     return code;
   };
-  if ( cudaStreamCreateWithFlags( &e->own, cudaStreamNonBlocking ) != cudaSuccess )
+  // the engine's own stream outranks the late deliveries: the update CTAs
+  // are placed first where both wait for SM slots
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange( &lo, &hi );
+  if ( const char* mp = std::getenv( "NG_MAIN_PRIORITY" ) )
+    hi = std::atoi( mp ) ? hi : lo;
+  if ( cudaStreamCreateWithPriority( &e->own, cudaStreamNonBlocking, hi ) != cudaSuccess )
     return bail( fail( NG_ERR_CUDA, "cudaStreamCreate failed" ) );
   e->stream = e->own;
   {
-    // the late deliveries yield SM slots to the update kernels
-    int lo = 0, hi = 0;
-    cudaDeviceGetStreamPriorityRange( &lo, &hi );
     if ( cudaStreamCreateWithPriority( &e->late_stream, cudaStreamNonBlocking, lo ) != cudaSuccess
       || cudaEventCreateWithFlags( &e->ev_fork, cudaEventDisableTiming ) != cudaSuccess
       || cudaEventCreateWithFlags( &e->ev_late[ 0 ], cudaEventDisableTiming ) != cudaSuccess
