@@ -174,6 +174,20 @@ int ng_set_trace( ng_engine* eng, int64_t n_idx, const int32_t* neuron, int32_t 
  * Replaces SimulationManager::run (simulation_manager.cpp:614-671). */
 int ng_simulate( ng_engine* eng, int64_t n_steps );
 
+/* ng_simulate that returns while the last group of steps still runs on the
+ * device; the spikes it logs are drained by the next simulate call (while
+ * that call's first group runs) or by ng_sync.  Every entry point that reads
+ * results or changes the engine drains first, except ng_net_add,
+ * ng_net_poll, ng_net_capacity, and ng_net_spikes / ng_net_remove of a
+ * network that ended before that group began.  The engine-side counterpart
+ * of repeated Run(t) calls between Prepare() and Cleanup()
+ * (pynest/nest/lib/hl_api_simulation.py:66-130), which return when the
+ * steps are done. */
+int ng_simulate_async( ng_engine* eng, int64_t n_steps );
+
+/* Wait for the steps of ng_simulate_async and drain their spikes. */
+int ng_sync( ng_engine* eng );
+
 /* Number of logged spikes waiting to be drained. */
 int ng_spike_count( ng_engine* eng, int64_t* n );
 

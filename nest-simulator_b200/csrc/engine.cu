@@ -1446,8 +1446,25 @@ struct ng_engine
     return NG_OK;
   }
 
+  // a group launched by an asynchronous simulate and not drained yet
+  int pend_sel = -1;
+  GroupInfo pend_gi;
+
   int
-  simulate( int64_t n )
+  sync_pending()
+  {
+    if ( pend_sel < 0 )
+      return NG_OK;
+    const int s = pend_sel;
+    pend_sel = -1;
+    return drain_group( s, pend_gi );
+  }
+
+  // keep: leave the last group running and undrained (asynchronous form);
+  // a group left so by an earlier call is drained while this call's first
+  // group runs
+  int
+  simulate( int64_t n, bool keep = false )
   {
     auto t0 = std::chrono::steady_clock::now();
     int rc = prepare();
@@ -1479,8 +1496,11 @@ struct ng_engine
       if ( quarter >= q && quarter < gmax )
         gmax = quarter;
     }
-    int pending = -1;
+    int pending = pend_sel;
     GroupInfo gi[ 2 ];
+    if ( pending >= 0 )
+      gi[ pending ] = pend_gi;
+    pend_sel = -1;
     while ( n > 0 )
     {
       const int64_t g = std::min( n, gmax );
@@ -1501,8 +1521,16 @@ struct ng_engine
       }
       n -= g;
     }
-    if ( pending >= 0 && ( rc = drain_group( pending, gi[ pending ] ) ) )
-      return rc;
+    if ( pending >= 0 )
+    {
+      if ( keep && overlap )
+      {
+        pend_sel = pending;
+        pend_gi = gi[ pending ];
+      }
+      else if ( ( rc = drain_group( pending, gi[ pending ] ) ) )
+        return rc;
+    }
     stats.clock_steps = origin + from;
     stats.slices = slices;
     stats.simulate_ms += std::chrono::duration< double, std::milli >( std::chrono::steady_clock::now() - t0 ).count();
@@ -1516,6 +1544,19 @@ ng_internal_set_error( const char* msg )
 {
   g_err = msg;
 }
+
+// Entry points that read results or change the engine first drain a group
+// left running by ng_simulate_async.
+#define SETTLE( e )                                                                                                   \
+  do                                                                                                                 \
+  {                                                                                                                  \
+    if ( ( e ) && ( e )->pend_sel >= 0 )                                                                             \
+    {                                                                                                                \
+      const int rc_settle = ( e )->sync_pending();                                                                   \
+      if ( rc_settle )                                                                                               \
+        return rc_settle;                                                                                            \
+    }                                                                                                                \
+  } while ( 0 )
 
 extern "C" {
 
@@ -1794,6 +1835,7 @@ check_range( ng_engine* e, int32_t block, int64_t first, int64_t count )
 int
 ng_set_var( ng_engine* e, int32_t block, const char* name, const double* values, int64_t first, int64_t count )
 {
+  SETTLE( e );
   int rc = check_range( e, block, first, count );
   if ( rc )
     return rc;
@@ -1847,6 +1889,7 @@ ng_set_var( ng_engine* e, int32_t block, const char* name, const double* values,
 int
 ng_get_var( ng_engine* e, int32_t block, const char* name, double* out, int64_t first, int64_t count )
 {
+  SETTLE( e );
   int rc = check_range( e, block, first, count );
   if ( rc )
     return rc;
@@ -1901,6 +1944,7 @@ int
 ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const int32_t* target, const double* weight,
   const int32_t* delay_steps )
 {
+  SETTLE( e );
   if ( !e || !row_ptr )
     return fail( NG_ERR_ARG, "ng_set_connections: null argument" );
   if ( n_src != e->n_src )
@@ -2038,6 +2082,7 @@ int
 ng_set_connections_coo( ng_engine* e, int64_t n_src, int64_t nnz, const int32_t* source, const int32_t* target,
   const double* weight, const int32_t* delay_steps )
 {
+  SETTLE( e );
   if ( !e || nnz < 0 || ( nnz > 0 && ( !source || !target || !weight || !delay_steps ) ) )
     return fail( NG_ERR_ARG, "ng_set_connections_coo: bad argument" );
   if ( n_src != e->n_src )
@@ -2069,6 +2114,7 @@ ng_set_connections_coo( ng_engine* e, int64_t n_src, int64_t nnz, const int32_t*
 int
 ng_set_spike_schedule( ng_engine* e, int64_t n, const int64_t* emit_step, const int32_t* source )
 {
+  SETTLE( e );
   if ( !e || n < 0 || ( n > 0 && ( !emit_step || !source ) ) )
     return fail( NG_ERR_ARG, "ng_set_spike_schedule: bad argument" );
   cudaSetDevice( e->cfg.device );
@@ -2110,6 +2156,7 @@ int
 ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const int32_t* delay_steps,
   int64_t start_step, int64_t stop_step, uint64_t seed )
 {
+  SETTLE( e );
   if ( !e || !rate_hz || !weight || !delay_steps )
     return fail( NG_ERR_ARG, "ng_set_poisson: null argument" );
   cudaSetDevice( e->cfg.device );
@@ -2169,6 +2216,7 @@ ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const
 int
 ng_set_recording( ng_engine* e, const uint8_t* flags )
 {
+  SETTLE( e );
   if ( !e || !flags )
     return fail( NG_ERR_ARG, "ng_set_recording: null argument" );
   cudaSetDevice( e->cfg.device );
@@ -2191,6 +2239,7 @@ int
 ng_set_trace( ng_engine* e, int64_t n_idx, const int32_t* neuron, int32_t n_vars, const char* const* vars,
   int32_t interval_steps )
 {
+  SETTLE( e );
   if ( !e || n_idx < 0 || ( n_idx > 0 && ( !neuron || !vars || n_vars < 1 ) ) || interval_steps < 1
     || n_vars > MAX_STATE || n_vars < 0 )
     return fail( NG_ERR_ARG, "ng_set_trace: bad argument" );
@@ -2257,8 +2306,36 @@ ng_simulate( ng_engine* e, int64_t n_steps )
 }
 
 int
+ng_simulate_async( ng_engine* e, int64_t n_steps )
+{
+  if ( !e || n_steps < 0 )
+    return fail( NG_ERR_ARG, "ng_simulate_async: bad argument" );
+  CU( cudaSetDevice( e->cfg.device ) );
+  try
+  {
+    return e->simulate( n_steps, true );
+  }
+  catch ( const std::bad_alloc& )
+  {
+    cudaStreamSynchronize( e->stream );
+    return fail( NG_ERR_MEMORY, "ng_simulate_async: out of host memory" );
+  }
+}
+
+int
+ng_sync( ng_engine* e )
+{
+  if ( !e )
+    return fail( NG_ERR_ARG, "ng_sync: null engine" );
+  CU( cudaSetDevice( e->cfg.device ) );
+  SETTLE( e );
+  return NG_OK;
+}
+
+int
 ng_spike_count( ng_engine* e, int64_t* n )
 {
+  SETTLE( e );
   if ( !e || !n )
     return fail( NG_ERR_ARG, "ng_spike_count: null argument" );
   *n = ( int64_t ) e->out_src.size();
@@ -2268,6 +2345,7 @@ ng_spike_count( ng_engine* e, int64_t* n )
 int
 ng_get_spikes( ng_engine* e, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out )
 {
+  SETTLE( e );
   if ( !e || !n_out || cap < 0 || ( cap > 0 && ( !source || !stamp ) ) )
     return fail( NG_ERR_ARG, "ng_get_spikes: bad argument" );
   const int64_t k = std::min< int64_t >( cap, ( int64_t ) e->out_src.size() );
@@ -2282,6 +2360,7 @@ ng_get_spikes( ng_engine* e, int32_t* source, int64_t* stamp, int64_t cap, int64
 int
 ng_trace_count( ng_engine* e, int64_t* n_rows, int64_t* first_stamp )
 {
+  SETTLE( e );
   if ( !e || !n_rows || !first_stamp )
     return fail( NG_ERR_ARG, "ng_trace_count: null argument" );
   const int64_t w = ( int64_t ) e->n_trace_idx * e->n_trace_vars;
@@ -2293,6 +2372,7 @@ ng_trace_count( ng_engine* e, int64_t* n_rows, int64_t* first_stamp )
 int
 ng_get_trace( ng_engine* e, double* out, int64_t max_rows, int64_t* n_rows_out )
 {
+  SETTLE( e );
   if ( !e || !n_rows_out || max_rows < 0 || ( max_rows > 0 && !out ) )
     return fail( NG_ERR_ARG, "ng_get_trace: bad argument" );
   if ( e->n_trace_idx == 0 )
@@ -2316,6 +2396,7 @@ ng_get_trace( ng_engine* e, double* out, int64_t max_rows, int64_t* n_rows_out )
 int
 ng_get_stats( ng_engine* e, ng_stats* out )
 {
+  SETTLE( e );
   if ( !e || !out )
     return fail( NG_ERR_ARG, "ng_get_stats: null argument" );
   e->stats.clock_steps = e->origin + e->from;
@@ -2327,6 +2408,7 @@ ng_get_stats( ng_engine* e, ng_stats* out )
 int
 ng_set_profiling( ng_engine* e, int32_t on )
 {
+  SETTLE( e );
   if ( !e )
     return fail( NG_ERR_ARG, "null engine" );
   e->profiling = on ? 1 : 0;
@@ -2336,6 +2418,7 @@ ng_set_profiling( ng_engine* e, int32_t on )
 int
 ng_set_stream( ng_engine* e, void* cuda_stream )
 {
+  SETTLE( e );
   if ( !e )
     return fail( NG_ERR_ARG, "null engine" );
   e->stream = cuda_stream ? ( cudaStream_t ) cuda_stream : e->own;
@@ -2346,6 +2429,7 @@ ng_set_stream( ng_engine* e, void* cuda_stream )
 int
 ng_set_graph_slices( ng_engine* e, int32_t slices_per_graph )
 {
+  SETTLE( e );
   if ( !e || slices_per_graph < 0 || slices_per_graph > 4096 )
     return fail( NG_ERR_ARG, "ng_set_graph_slices: bad argument" );
   e->graph_slices = slices_per_graph;
@@ -2469,10 +2553,16 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     else if ( vs->kind == STATE )
       state_src[ vs->slot ] = desc->var_values[ v ];
   }
+  // host sources of the uploads live until the function returns (after its
+  // last stream synchronisation), so no copy waits for the device here: an
+  // admission's host work overlaps slices still running on the device
+  std::vector< std::vector< char > > st_tmp( ( size_t ) n_states( model ) );
+  std::vector< double > hs;
   {
-    std::vector< char > tmp( ( size_t ) n * e->rsz );
     for ( int sl = 0; sl < n_states( model ); ++sl )
     {
+      std::vector< char >& tmp = st_tmp[ ( size_t ) sl ];
+      tmp.resize( ( size_t ) n * e->rsz );
       for ( int64_t i = 0; i < n; ++i )
       {
         const double v = state_src[ sl ] ? state_src[ sl ][ i ] : default_state( model, sl );
@@ -2483,14 +2573,12 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       }
       CU( cudaMemcpyAsync( ( char* ) b.st[ sl ].p + n0 * e->rsz, tmp.data(), tmp.size(), cudaMemcpyHostToDevice,
         e->stream ) );
-      CU( cudaStreamSynchronize( e->stream ) );
     }
     CU( cudaMemsetAsync( ( int32_t* ) b.r.p + n0, 0, ( size_t ) n * 4, e->stream ) );
     if ( model == NG_AEIF_COND_ALPHA )
     {
-      std::vector< double > hs( ( size_t ) n, e->h );
+      hs.assign( ( size_t ) n, e->h );
       CU( cudaMemcpyAsync( ( double* ) b.istep.p + n0, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice, e->stream ) );
-      CU( cudaStreamSynchronize( e->stream ) );
     }
   }
   // coefficient classes, shared by all networks
@@ -2498,8 +2586,22 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   double log_rate = 0.0;
   const int ri = model == NG_IAF_PSC_DELTA ? 5 : model == NG_IAF_PSC_EXP ? 8 : 18;
   const int64_t first_new = ( int64_t ) e->cls_ids.size();
+  const int np_model = n_params( model );
   for ( int64_t i = n0; i < n0 + n; ++i )
   {
+    // a neuron with its predecessor's parameters has its class
+    if ( i > n0 )
+    {
+      bool same = true;
+      for ( int p2 = 0; p2 < np_model && same; ++p2 )
+        same = b.par[ p2 ][ ( size_t ) i ] == b.par[ p2 ][ ( size_t ) i - 1 ];
+      if ( same )
+      {
+        b.host_cls[ ( size_t ) i ] = b.host_cls[ ( size_t ) i - 1 ];
+        log_rate += 1.0 / ( row[ ri ] + 1.0 );
+        continue;
+      }
+    }
     std::fill( row, row + CT_STRIDE, 0.0 );
     int rc = e->coef_row( b, i, row );
     if ( rc )
@@ -2812,6 +2914,17 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     for ( int64_t i = 0; i < n; ++i )
     {
       const double rate = desc->poisson_rate ? desc->poisson_rate[ i ] : 0.0;
+      // a neuron with its predecessor's drive has its entries
+      if ( i > 0 && desc->poisson_rate && rate == desc->poisson_rate[ i - 1 ]
+        && ( !desc->poisson_weight || desc->poisson_weight[ i ] == desc->poisson_weight[ i - 1 ] )
+        && ( !desc->poisson_delay || desc->poisson_delay[ i ] == desc->poisson_delay[ i - 1 ] ) )
+      {
+        tab[ i ] = tab[ i - 1 ];
+        ref[ i ] = ref[ i - 1 ];
+        pw[ i ] = pw[ i - 1 ];
+        pd[ i ] = pd[ i - 1 ];
+        continue;
+      }
       const double lam = rate > 0 ? e->h * rate * 1e-3 : 0.0;
       tab[ i ] = poisson_table( lam );
       if ( !( lam > 0 ) )
@@ -2928,6 +3041,8 @@ ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_
   if ( !n_out || cap < 0 || ( source && !stamp ) )
     return fail( NG_ERR_ARG, "ng_net_spikes: bad argument" );
   auto& nw = e->nets[ id ];
+  if ( nw.until > e->pend_gi.clock )
+    SETTLE( e );  // the running group may hold spikes of this network
   if ( !source )
   {
     *n_out = nw.held;  // count only
@@ -2984,6 +3099,7 @@ int
 ng_net_get_connections( ng_engine* e, int32_t id, int32_t* source, int32_t* target, double* weight,
   int32_t* delay_steps, int64_t cap, int64_t* n_out )
 {
+  SETTLE( e );
   int rc = net_check( e, id );
   if ( rc )
     return rc;
@@ -3043,6 +3159,8 @@ ng_net_remove( ng_engine* e, int32_t id )
   int rc = net_check( e, id );
   if ( rc )
     return rc;
+  if ( e->nets[ id ].until > e->pend_gi.clock )
+    SETTLE( e );  // the running group may hold spikes of this network
   cudaSetDevice( e->cfg.device );
   auto& nw = e->nets[ id ];
   k_fill_i32<<< ( unsigned ) ( ( nw.n + 255 ) / 256 ), 256, 0, e->stream >>>( ( int32_t* ) e->d_nid.p + nw.off, nw.n, -1 );
@@ -3100,6 +3218,7 @@ ng_net_capacity( ng_engine* e, int64_t* free_neurons, int64_t* free_edges )
 int
 ng_debug_coefficients( ng_engine* e, int32_t block, int64_t index, double* out, int32_t cap, int32_t* n_out )
 {
+  SETTLE( e );
   int rc = check_range( e, block, index, 1 );
   if ( rc )
     return rc;

@@ -30,7 +30,7 @@ NG_MAX_BLOCKS = 8
 EXPORTED = [
     "ng_abi_version", "ng_last_error", "ng_device_count", "ng_create", "ng_destroy", "ng_set_var", "ng_get_var",
     "ng_set_connections", "ng_set_connections_coo", "ng_set_spike_schedule", "ng_set_poisson", "ng_set_recording", "ng_set_trace",
-    "ng_simulate", "ng_spike_count", "ng_get_spikes", "ng_trace_count", "ng_get_trace", "ng_get_stats",
+    "ng_simulate", "ng_simulate_async", "ng_sync", "ng_spike_count", "ng_get_spikes", "ng_trace_count", "ng_get_trace", "ng_get_stats",
     "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients", "ng_net_add", "ng_net_poll",
     "ng_net_spikes", "ng_net_get_var", "ng_net_get_connections", "ng_net_remove", "ng_net_capacity",
     "ng_simulate_noalloc",
@@ -212,6 +212,8 @@ def load():
         "ng_set_recording": ([P, P], ctypes.c_int),
         "ng_set_trace": ([P, i64, P, i32, P, i32], ctypes.c_int),
         "ng_simulate": ([P, i64], ctypes.c_int),
+        "ng_simulate_async": ([P, i64], ctypes.c_int),
+        "ng_sync": ([P], ctypes.c_int),
         "ng_spike_count": ([P, P], ctypes.c_int),
         "ng_get_spikes": ([P, P, P, i64, P], ctypes.c_int),
         "ng_trace_count": ([P, P, P], ctypes.c_int),
@@ -355,6 +357,13 @@ class Engine:
 
     def simulate(self, n_steps):
         check(self.L.ng_simulate(self.handle, int(n_steps)))
+
+    def simulate_async(self, n_steps):
+        """Enqueue n_steps; the last group still runs when this returns."""
+        check(self.L.ng_simulate_async(self.handle, int(n_steps)))
+
+    def sync(self):
+        check(self.L.ng_sync(self.handle))
 
     def spikes(self):
         n = ctypes.c_int64(0)

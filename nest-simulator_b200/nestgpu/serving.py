@@ -117,7 +117,12 @@ def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtim
     spikes drained, their pool space freed) and the waiting requests that fit
     the free pool are admitted, oldest first.  A request is only built (its
     initial state drawn, its graph requested) when its footprint fits the
-    largest free runs of the pool."""
+    largest free runs of the pool.
+
+    The chunks are enqueued with ng_simulate_async: the host reads the spikes
+    of the networks that ended by the start of the running chunk while the
+    device runs it, so a network is retired one chunk after its end (or at
+    once when no live network is left to advance)."""
     pending = sorted(requests, key=lambda r: r.arrival)
     waiting = []
     active = {}                       # network id -> (request, engine step at which it ends)
@@ -155,15 +160,27 @@ def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtim
             continue
         # one chunk, or less when every live network ends before its end
         left = max(end for _, end in active.values()) - now_steps
-        slices = max(1, min(chunk_slices, -(-left // DELAY_STEPS)))
-        eng.simulate(slices * DELAY_STEPS)
-        now_steps += slices * DELAY_STEPS
-        steps_run += slices * DELAY_STEPS
-        for nid in [k for k, (_, end) in active.items() if now_steps >= end]:
-            r, _ = active.pop(nid)
+        if left <= 0:
+            eng.sync()
+            ended = now_steps
+        else:
+            slices = max(1, min(chunk_slices, -(-left // DELAY_STEPS)))
+            ended = now_steps
+            eng.simulate_async(slices * DELAY_STEPS)
+            now_steps += slices * DELAY_STEPS
+            steps_run += slices * DELAY_STEPS
+        # networks that ended by the start of the running chunk: their spikes are
+        # all drained; read them all before the first removal (which waits for
+        # the device)
+        done = [k for k, (_, end) in active.items() if end <= ended]
+        for nid in done:
+            r, _ = active[nid]
             r.spikes = eng.net_spikes(nid)
-            eng.net_remove(nid)
             r.finished = clock() - t0
+        for nid in done:
+            active.pop(nid)
+            eng.net_remove(nid)
+    eng.sync()
     makespan = clock() - t0
     ev = eng.stats()["syn_events"] - ev0
     return requests, {"makespan_s": makespan, "syn_events": ev, "syn_events_per_s": ev / makespan,

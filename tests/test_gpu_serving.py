@@ -348,3 +348,31 @@ def test_tiled_delivery_equals_scatter(ring32):
     np.testing.assert_array_equal(s0[o0], s1[o1])
     np.testing.assert_array_equal(t0[o0], t1[o1])
     np.testing.assert_array_equal(V0, V1)
+
+
+def test_async_simulate_equals_sync():
+    """ng_simulate_async leaves the last group running: the spikes of a network
+    that ended before it are complete without a sync, a network still
+    running is drained on read, and the results equal ng_simulate's."""
+    def run(asynchronous):
+        eng = serving.new_engine("fp32", capacity_neurons=50_000, capacity_edges=20_000_000, max_networks=4)
+        a = serving._admit(eng, _req(0, 4000, 15 * 40, seed=71))
+        b = serving._admit(eng, _req(1, 6000, 15 * 200, seed=72))
+        step = eng.simulate_async if asynchronous else eng.simulate
+        for _ in range(4):
+            step(15 * 32)
+        sa = eng.net_spikes(a)          # ended long before the running group
+        eng.net_remove(a)
+        step(15 * 32)
+        sb = eng.net_spikes(b)          # b ran in the last group: drained on read
+        Vb = eng.net_get_var(b, "V_m_rel", 6000)
+        eng.close()
+        return sa, sb, Vb
+
+    (sa0, sb0, V0), (sa1, sb1, V1) = run(False), run(True)
+    assert len(sa0[0]) > 100 and len(sb0[0]) > 1000
+    for (s0, t0), (s1, t1) in ((sa0, sa1), (sb0, sb1)):
+        o0, o1 = np.lexsort((s0, t0)), np.lexsort((s1, t1))
+        np.testing.assert_array_equal(s0[o0], s1[o1])
+        np.testing.assert_array_equal(t0[o0], t1[o1])
+    np.testing.assert_array_equal(V0, V1)
