@@ -276,6 +276,11 @@ struct ng_engine
   // (its update reads no ring slot they reach); the slice after that waits
   // for them.  Rows hold their shorter-delay edges first (row_ue, row_ls).
   cudaStream_t late_stream = nullptr;
+  // admissions prepare a network's region (state, tables, graph) on their own
+  // stream while the slices already enqueued run; only the activation of the
+  // network is ordered behind them
+  cudaStream_t adm_stream = nullptr;
+  cudaEvent_t ev_adm = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_late[ 2 ] = { nullptr, nullptr };
   bool late_pending[ 2 ] = { false, false };
   bool late_env = true;
@@ -664,6 +669,10 @@ struct ng_engine
       cudaStreamDestroy( copy_stream );
     if ( late_stream )
       cudaStreamDestroy( late_stream );
+    if ( adm_stream )
+      cudaStreamDestroy( adm_stream );
+    if ( ev_adm )
+      cudaEventDestroy( ev_adm );
     for ( cudaEvent_t ev : { ev_fork, ev_late[ 0 ], ev_late[ 1 ] } )
       if ( ev )
         cudaEventDestroy( ev );
@@ -1657,7 +1666,9 @@ ng_create( const ng_config* cfg, ng_engine** out )
     if ( cudaStreamCreateWithPriority( &e->late_stream, cudaStreamNonBlocking, lo ) != cudaSuccess
       || cudaEventCreateWithFlags( &e->ev_fork, cudaEventDisableTiming ) != cudaSuccess
       || cudaEventCreateWithFlags( &e->ev_late[ 0 ], cudaEventDisableTiming ) != cudaSuccess
-      || cudaEventCreateWithFlags( &e->ev_late[ 1 ], cudaEventDisableTiming ) != cudaSuccess )
+      || cudaEventCreateWithFlags( &e->ev_late[ 1 ], cudaEventDisableTiming ) != cudaSuccess
+      || cudaStreamCreateWithFlags( &e->adm_stream, cudaStreamNonBlocking ) != cudaSuccess
+      || cudaEventCreateWithFlags( &e->ev_adm, cudaEventDisableTiming ) != cudaSuccess )
       return bail( fail( NG_ERR_CUDA, "ng_create: late-delivery stream or event creation failed" ) );
     if ( const char* lt = std::getenv( "NG_LATE" ) )
       e->late_env = std::atoi( lt ) != 0;
@@ -2515,6 +2526,15 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       prow[ sidx + 1 ] = prow[ sidx ] + ( ( rdeg[ sidx ] + 3 ) & ~3 );
     ne_need = prow[ n ];
   }
+  // the region's preparation runs on the admission stream (every helper
+  // below works on e->stream); the engine's stream is restored on every exit
+  struct StreamSwap
+  {
+    ng_engine* e;
+    cudaStream_t main;
+    ~StreamSwap() { e->stream = main; }
+  } swap { e, e->stream };
+  e->stream = e->adm_stream;
   int64_t n0 = 0, e0 = 0;
   if ( !ng_engine::take_run( e->free_neurons, n, &n0 ) )
     return fail( NG_ERR_CAPACITY, "ng_net_add: not enough free neurons in the pool" );
@@ -2960,21 +2980,30 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     CU( cudaMemcpyAsync( ( int32_t* ) e->pois_d.p + n0, pd.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
     CU( cudaStreamSynchronize( e->stream ) );
   }
-  // recording, network table, ids, and a clean ring region
+  // activation, in the engine's stream order behind the prepared region and
+  // the slices already enqueued: recording, network table, ids, a clean ring
+  // region (no host memory is read by these, so nothing waits here)
+  CU( cudaEventRecord( e->ev_adm, e->adm_stream ) );
+  e->stream = swap.main;
+  CU( cudaStreamWaitEvent( e->stream, e->ev_adm, 0 ) );
   CU( cudaMemsetAsync( ( uint8_t* ) e->rec.p + n0, desc->record ? 1 : 0, ( size_t ) n, e->stream ) );
   std::fill( e->rec_host.begin() + n0, e->rec_host.begin() + n0 + n, ( uint8_t ) ( desc->record ? 1 : 0 ) );
   const long long step0 = e->origin, until = e->origin + desc->steps, off = n0;
   const uint2 key = make_uint2( ( uint32_t ) desc->seed, ( uint32_t ) ( desc->seed >> 32 ) );
-  CU( cudaMemcpyAsync( ( long long* ) e->d_step0.p + id, &step0, 8, cudaMemcpyHostToDevice, e->stream ) );
-  CU( cudaMemcpyAsync( ( long long* ) e->d_until.p + id, &until, 8, cudaMemcpyHostToDevice, e->stream ) );
-  CU( cudaMemcpyAsync( ( long long* ) e->d_off.p + id, &off, 8, cudaMemcpyHostToDevice, e->stream ) );
-  CU( cudaMemcpyAsync( ( uint2* ) e->d_key.p + id, &key, 8, cudaMemcpyHostToDevice, e->stream ) );
+  if ( e->gather_on && g0 < 0 )
+    e->host_g[ id ] = GatherNet {};
+  if ( e->tiled_on && sg0 < 0 )
+    e->host_t[ id ] = TileNet {};
+  k_net_set<<< 1, 32, 0, e->stream >>>( id, 1, step0, until, off, key, ( long long* ) e->d_step0.p,
+    ( long long* ) e->d_until.p, ( long long* ) e->d_off.p, ( uint2* ) e->d_key.p,
+    e->gather_on ? e->host_g[ id ] : GatherNet {}, e->gather_on ? ( GatherNet* ) e->net_g.p : nullptr,
+    ( int* ) e->net_mode.p, ( unsigned* ) e->net_spk.p, e->tiled_on ? e->host_t[ id ] : TileNet {},
+    e->tiled_on ? ( TileNet* ) e->net_t.p : nullptr );
   k_fill_i32<<< ( unsigned ) ( ( n + 255 ) / 256 ), 256, 0, e->stream >>>( ( int32_t* ) e->d_nid.p + n0, n, id );
   CU( cudaMemset2DAsync( ( char* ) e->ring.p + n0 * e->ring_bytes, ( size_t ) e->N * e->ring_bytes, 0,
     ( size_t ) n * e->ring_bytes, ( size_t ) e->L * e->C,
     e->stream ) );
   CU( cudaGetLastError() );
-  CU( cudaStreamSynchronize( e->stream ) );
   std::fill( e->nid_host.begin() + n0, e->nid_host.begin() + n0 + n, id );
   auto& nw = e->nets[ id ];
   nw = ng_engine::NetInfo();
@@ -2987,25 +3016,6 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   nw.gn = gn;
   nw.s0 = sg0;
   nw.sn = sgn;
-  if ( e->tiled_on )
-  {
-    if ( sg0 < 0 )
-      e->host_t[ id ] = TileNet {};
-    CU( cudaMemcpyAsync( ( TileNet* ) e->net_t.p + id, &e->host_t[ id ], sizeof( TileNet ), cudaMemcpyHostToDevice,
-      e->stream ) );
-    CU( cudaStreamSynchronize( e->stream ) );
-  }
-  if ( e->gather_on )
-  {
-    if ( g0 < 0 )
-      e->host_g[ id ] = GatherNet {};
-    const int zero = 0;
-    CU( cudaMemcpyAsync( ( GatherNet* ) e->net_g.p + id, &e->host_g[ id ], sizeof( GatherNet ), cudaMemcpyHostToDevice,
-      e->stream ) );
-    CU( cudaMemcpyAsync( ( int* ) e->net_mode.p + id, &zero, 4, cudaMemcpyHostToDevice, e->stream ) );
-    CU( cudaMemcpyAsync( ( int* ) e->net_spk.p + id, &zero, 4, cudaMemcpyHostToDevice, e->stream ) );
-    CU( cudaStreamSynchronize( e->stream ) );
-  }
   nw.step0 = step0;
   nw.until = until;
   nw.rec = desc->record != 0;
@@ -3163,11 +3173,16 @@ ng_net_remove( ng_engine* e, int32_t id )
     SETTLE( e );  // the running group may hold spikes of this network
   cudaSetDevice( e->cfg.device );
   auto& nw = e->nets[ id ];
+  // in stream order behind the slices already enqueued; nothing waits here.
+  // The region's rows and state are left as they are (a free neuron never
+  // spikes nor updates), so an admission may prepare the region again on
+  // its own stream while these are still queued.
   k_fill_i32<<< ( unsigned ) ( ( nw.n + 255 ) / 256 ), 256, 0, e->stream >>>( ( int32_t* ) e->d_nid.p + nw.off, nw.n, -1 );
-  CU( cudaMemsetAsync( ( int32_t* ) e->row_len.p + nw.off, 0, ( size_t ) nw.n * 4, e->stream ) );
   CU( cudaMemsetAsync( ( uint8_t* ) e->rec.p + nw.off, 0, ( size_t ) nw.n, e->stream ) );
+  k_net_set<<< 1, 32, 0, e->stream >>>( id, 0, 0, 0, 0, make_uint2( 0u, 0u ), nullptr, nullptr, nullptr, nullptr,
+    GatherNet {}, e->gather_on ? ( GatherNet* ) e->net_g.p : nullptr, ( int* ) e->net_mode.p,
+    ( unsigned* ) e->net_spk.p, TileNet {}, e->tiled_on ? ( TileNet* ) e->net_t.p : nullptr );
   CU( cudaGetLastError() );
-  CU( cudaStreamSynchronize( e->stream ) );
   std::fill( e->nid_host.begin() + nw.off, e->nid_host.begin() + nw.off + nw.n, -1 );
   std::fill( e->rec_host.begin() + nw.off, e->rec_host.begin() + nw.off + nw.n, ( uint8_t ) 0 );
   ng_engine::give_run( e->free_neurons, nw.off, nw.n );
@@ -3177,20 +3192,12 @@ ng_net_remove( ng_engine* e, int32_t id )
     if ( nw.s0 >= 0 )
       ng_engine::give_run( e->free_seg, nw.s0, nw.sn );
     e->host_t[ id ] = TileNet {};
-    CU( cudaMemcpyAsync( ( TileNet* ) e->net_t.p + id, &e->host_t[ id ], sizeof( TileNet ), cudaMemcpyHostToDevice,
-      e->stream ) );
-    CU( cudaStreamSynchronize( e->stream ) );
   }
   if ( e->gather_on )
   {
     if ( nw.g0 >= 0 )
       ng_engine::give_run( e->free_gin, nw.g0, nw.gn );
     e->host_g[ id ] = GatherNet {};
-    const int zero = 0;
-    CU( cudaMemcpyAsync( ( GatherNet* ) e->net_g.p + id, &e->host_g[ id ], sizeof( GatherNet ), cudaMemcpyHostToDevice,
-      e->stream ) );
-    CU( cudaMemcpyAsync( ( int* ) e->net_mode.p + id, &zero, 4, cudaMemcpyHostToDevice, e->stream ) );
-    CU( cudaStreamSynchronize( e->stream ) );
   }
   e->n_rec -= nw.rec ? nw.n : 0;
   e->log_per_step = std::max( 1.0, e->log_per_step - nw.log_rate );

@@ -897,7 +897,9 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
     cta_append_mask( d, smask, ( int32_t ) i, slot0, t0, netid, gath );
   }
   flush_drive_count( d, dcnt );
-  if ( act )
+  // only neurons simulated in this launch write their state back: a free
+  // neuron's state may be in the middle of an admission's upload
+  if ( act && until > origin + from )
   {
     s0[ li ] = V;
     s1[ li ] = x1;
@@ -1149,7 +1151,9 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
     __syncthreads();
   }
   flush_drive_count( d, dcnt );
-  if ( act )
+  // only neurons simulated in this launch write their state back: a free
+  // neuron's state may be in the middle of an admission's upload
+  if ( act && until > origin + from )
   {
     s0[ li ] = V;
     s1[ li ] = x1;
@@ -1421,7 +1425,7 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
   flush_drive_count( d, dcnt );
   if ( unstable )
     atomicOr( &d.ctl->err, ERR_NUMERIC );
-  if ( act )
+  if ( act && until > origin + from )
   {
 #pragma unroll
     for ( int k = 0; k < 6; ++k )
@@ -1858,6 +1862,33 @@ k_row_uniform( long long n, long long n0, const int32_t* row_len, int mode, int3
   const int32_t p = row_len[ n0 + s ];
   row_ue[ n0 + s ] = mode != 0 ? p : 0;
   row_ls[ n0 + s ] = mode == 1 ? p : 0;
+}
+
+// A serving network's per-network entries, written in stream order behind
+// the slices already enqueued (kernel arguments: no host memory that must
+// outlive the call).  on == 0: the network's slot is cleared.
+__global__ void
+k_net_set( int id, int on, long long step0, long long until, long long off, uint2 key, long long* d_step0,
+  long long* d_until, long long* d_off, uint2* d_key, GatherNet g, GatherNet* net_g, int* net_mode,
+  unsigned* net_spk, TileNet tn, TileNet* net_t )
+{
+  if ( threadIdx.x != 0 || blockIdx.x != 0 )
+    return;
+  if ( on )
+  {
+    d_step0[ id ] = step0;
+    d_until[ id ] = until;
+    d_off[ id ] = off;
+    d_key[ id ] = key;
+  }
+  if ( net_g )
+  {
+    net_g[ id ] = g;
+    net_mode[ id ] = 0;
+    net_spk[ id ] = 0u;
+  }
+  if ( net_t )
+    net_t[ id ] = tn;
 }
 
 // Host-side ctl edits between groups (log drain, trace window).
