@@ -632,7 +632,7 @@ struct ng_engine
     return rc;
   }
   int max_lanes = 32;             // 1: always one thread per neuron
-  int sub_lags = 8;               // lags whose inputs one thread gathers together (4 or 8)
+  int sub_lags = 4;               // lags whose inputs one thread gathers together (4 or 8)
   int64_t one_thread_min_n = 20000;  // block size from which one thread per neuron fills the GPU
 
   ~ng_engine()
