@@ -4,9 +4,10 @@ its shorter-delay edges first.  With ring sums that do not depend on the
 order of the adds (dyadic FP64 weights, or the FP32 form's integer rings) the
 result equals the delivery of every edge at the slice's close bit for bit:
 
-- static engine, FP64 and FP32, explicit CSR with delays over [min_delay,
-  max_delay], run in partial slices, slice graphs and a profiled stretch
-  (where the late delivery runs after the slice-close one);
+- static engine, FP64 and FP32, the three update kernels (one thread per
+  neuron, two-phase, aeif RKF45) and both iaf models, explicit CSR with delays
+  over [min_delay, max_delay], run in partial slices, slice graphs and a
+  profiled stretch (where the late delivery runs after the slice-close one);
 - serving engine, a pairwise_bernoulli network drawn on the device (rows
   split after the draw) and an explicit one (rows split on the host).
 """
@@ -19,21 +20,30 @@ from nestgpu import _abi
 pytestmark = pytest.mark.gpu
 
 
-def _static_run(monkeypatch, late, precision):
+def _static_run(monkeypatch, late, precision, model=_abi.NG_IAF_PSC_EXP, md=2):
     monkeypatch.setenv("NG_LATE", "1" if late else "0")
-    n, md, maxd = 3000, 2, 30
+    n, maxd = 3000, 30
     rng = np.random.default_rng(11)
     deg = rng.integers(40, 160, n)
     row = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
     nnz = int(row[-1])
     tgt = rng.integers(0, n, nnz)
-    w = rng.choice([24.0, 12.5, -48.0, -100.0], nnz)
     d = rng.integers(md, maxd + 1, nnz)
-    eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, n)], 0.1, md, maxd, precision=precision)
+    eng = _abi.Engine([(model, n)], 0.1, md, maxd, precision=precision)
+    if model == _abi.NG_AEIF_COND_ALPHA:
+        w = rng.choice([1.0, 0.5, -2.0, -4.0], nnz)                # nS
+        eng.set_var(0, "tau_syn_ex", np.full(n, 1.0))
+        drive = (np.full(n, 15000.0), np.full(n, 1.0))
+        eng.set_var(0, "V_m", rng.uniform(-70.6, -52.0, n))
+    else:
+        w = rng.choice([24.0, 12.5, -48.0, -100.0], nnz)            # pA (iaf_psc_exp) or mV (iaf_psc_delta)
+        if model == _abi.NG_IAF_PSC_DELTA:
+            w = w / 64.0
+        drive = (np.full(n, 12000.0), np.full(n, 16.0 if model == _abi.NG_IAF_PSC_EXP else 0.25))
+        eng.set_var(0, "V_m_rel", rng.uniform(0.0, 15.0, n))
     eng.set_connections(row, tgt, w, d)
     eng.set_recording(np.ones(n, dtype=np.uint8))
-    eng.set_var(0, "V_m_rel", rng.uniform(0.0, 15.0, n))
-    eng.set_poisson(np.full(n, 12000.0), np.full(n, 16.0), np.full(n, md), 0, 10**9, 5)
+    eng.set_poisson(drive[0], drive[1], np.full(n, md), 0, 10**9, 5)
     for k in (7, 13, 3):              # partial slices
         eng.simulate(k)
     eng.simulate(977)                 # slice graphs
@@ -43,18 +53,24 @@ def _static_run(monkeypatch, late, precision):
     eng.set_graph_slices(0)           # slice by slice without graphs
     eng.simulate(301)
     s, t = eng.spikes()
-    V = eng.get_var(0, "V_m_rel")
+    V = eng.get_var(0, "V_m" if model == _abi.NG_AEIF_COND_ALPHA else "V_m_rel")
     st = eng.stats()
     eng.close()
     monkeypatch.delenv("NG_LATE")
     return s, t, V, st
 
 
-@pytest.mark.parametrize("precision", [_abi.NG_FP64, _abi.NG_FP32])
-def test_late_delivery_static_engine(monkeypatch, precision):
-    s0, t0, V0, st0 = _static_run(monkeypatch, False, precision)
-    s1, t1, V1, st1 = _static_run(monkeypatch, True, precision)
-    assert len(s0) > 2000
+@pytest.mark.parametrize("precision,model,md", [
+    (_abi.NG_FP64, _abi.NG_IAF_PSC_EXP, 2),      # one thread per neuron, 4 lags of inputs gathered
+    (_abi.NG_FP32, _abi.NG_IAF_PSC_EXP, 2),
+    (_abi.NG_FP64, _abi.NG_IAF_PSC_EXP, 3),      # two-phase update kernel (slices of 3 steps)
+    (_abi.NG_FP64, _abi.NG_IAF_PSC_DELTA, 3),
+    (_abi.NG_FP64, _abi.NG_AEIF_COND_ALPHA, 2),  # RKF45 kernel, per-spike appends
+])
+def test_late_delivery_static_engine(monkeypatch, precision, model, md):
+    s0, t0, V0, st0 = _static_run(monkeypatch, False, precision, model, md)
+    s1, t1, V1, st1 = _static_run(monkeypatch, True, precision, model, md)
+    assert len(s0) > 500
     assert st0["syn_events"] == st1["syn_events"]
     o0, o1 = np.lexsort((s0, t0)), np.lexsort((s1, t1))
     np.testing.assert_array_equal(s0[o0], s1[o1])
