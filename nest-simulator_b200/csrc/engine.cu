@@ -15,6 +15,7 @@
 #include <chrono>
 #include <string>
 #include <unordered_map>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -349,6 +350,7 @@ struct ng_engine
     int64_t clock = 0;  // log base (stamp offset) of the group
     uint2* e = nullptr;
     int64_t n = 0;
+    int64_t m = 0;      // spikes (multiplicities summed)
   };
 
   static void
@@ -1410,6 +1412,7 @@ struct ng_engine
           int64_t m = 0;
           for ( int64_t k = 0; k < cnt; ++k )
             m += rb.e[ k ].y >> 24;
+          rb.m = m;
           nw.held += m;
           nw.blocks.push_back( rb );
         }
@@ -1498,7 +1501,9 @@ struct ng_engine
     // is cut into at least 4 groups where it is long enough, so only the
     // last quarter's drain is not hidden behind device work.
     const bool overlap = n_trace_idx == 0;
-    if ( overlap && graph_slices >= 16 )
+    // (an asynchronous call needs no split: its group's drain overlaps the
+    // next call's group)
+    if ( overlap && graph_slices >= 16 && !keep )
     {
       const int64_t q = 16 * ( int64_t ) cfg.min_delay;
       const int64_t quarter = ( ( n / 4 + q - 1 ) / q ) * q;
@@ -3058,9 +3063,53 @@ ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_
     *n_out = nw.held;  // count only
     return NG_OK;
   }
+  const uint32_t lmask = ( 1u << LOG_ID_SHIFT ) - 1u;
+  if ( cap >= nw.held && nw.held >= ( 1 << 18 ) )
+  {
+    // the whole store, large: decoded by several host threads, each a share
+    // of every block (entries of multiplicity 1 land at their own index)
+    bool unit = true;
+    for ( size_t q = 0; q < nw.blocks.size() && unit; ++q )
+      unit = nw.blocks[ q ].m == nw.blocks[ q ].n;
+    if ( unit )
+    {
+      const int T = ( int ) std::max( 1u, std::min( 8u, std::thread::hardware_concurrency() ) );
+      std::vector< int64_t > base( nw.blocks.size() + 1, 0 );
+      for ( size_t q = 0; q < nw.blocks.size(); ++q )
+        base[ q + 1 ] = base[ q ] + nw.blocks[ q ].n - ( q == 0 ? nw.first : 0 );
+      auto work = [ & ]( int t ) {
+        for ( size_t q = 0; q < nw.blocks.size(); ++q )
+        {
+          const ng_engine::RawBlock& rb = nw.blocks[ q ];
+          const int64_t f = q == 0 ? nw.first : 0, cnt = rb.n - f;
+          const int64_t lo = f + cnt * t / T, hi = f + cnt * ( t + 1 ) / T;
+          const int64_t sh = rb.clock - nw.step0;
+          int32_t* so = source + base[ q ] - f;
+          int64_t* to = stamp + base[ q ] - f;
+          for ( int64_t j = lo; j < hi; ++j )
+          {
+            const uint2 en = rb.e[ j ];
+            so[ j ] = ( int32_t ) ( en.x & lmask );
+            to[ j ] = sh + ( int64_t ) ( en.y & 0xFFFFFFu );
+          }
+        }
+      };
+      std::vector< std::thread > pool;
+      for ( int t = 1; t < T; ++t )
+        pool.emplace_back( work, t );
+      work( 0 );
+      for ( auto& th : pool )
+        th.join();
+      const int64_t k = base.back();
+      ng_engine::free_blocks( nw.blocks );
+      nw.first = 0;
+      nw.held -= k;
+      *n_out = k;
+      return NG_OK;
+    }
+  }
   int64_t k = 0;
   size_t bi = 0;
-  const uint32_t lmask = ( 1u << LOG_ID_SHIFT ) - 1u;
   for ( ; bi < nw.blocks.size(); ++bi )
   {
     const ng_engine::RawBlock& rb = nw.blocks[ bi ];

@@ -455,6 +455,19 @@ class Kernel:
                 c["recorders"][rid] = mask
                 flags |= mask.astype(np.uint8)
         c["rec_flags"] = flags
+        # recorders over disjoint sources (one population each, the usual case):
+        # a source's recorder index, so a run's spikes are split in one pass
+        c["rec_part"] = None
+        if c["recorders"] and len(c["recorders"]) < 32767:
+            rids = list(c["recorders"])
+            cover = np.zeros(n_src, dtype=np.int32)
+            for rid in rids:
+                cover += c["recorders"][rid]
+            if cover.max() <= 1:
+                of = np.full(n_src, -1, dtype=np.int16)
+                for j, rid in enumerate(rids):
+                    of[c["recorders"][rid]] = j
+                c["rec_part"] = (rids, of)
         # samplers (multimeter / voltmeter)
         c["samplers"] = {}
         if np.any(m_mm):
@@ -612,25 +625,45 @@ class Kernel:
         if len(src) and c["recorders"]:
             senders = c["eng_to_node"][src]
             times = self.stamp_to_ms(stamp)
-            for rid, mask in c["recorders"].items():
-                dev = self.devices[self.node_local[rid - 1]]
-                p = dev.params
-                t_min = self.ms_to_steps_roundup(float(p["origin"]) + float(p["start"]))
-                t_max = INF_STEPS if np.isinf(p["stop"]) else self.ms_to_steps_roundup(float(p["origin"]) +
-                                                                                        float(p["stop"]))
-                sel = mask[src] & (stamp > t_min) & (stamp <= t_max)
-                if np.any(sel):
-                    dev.events["senders"].append(senders[sel])
-                    if p.get("time_in_steps"):
-                        dev.events["times"].append(stamp[sel])
-                    else:
-                        dev.events["times"].append(times[sel])
-                    dev.n_events += int(sel.sum())
+            part = c.get("rec_part")
+            if part is not None:
+                # one stable counting sort by recorder, then each recorder's
+                # spikes are a contiguous run (in emission order)
+                rids, of = part
+                k = of[src]
+                order = np.argsort(k, kind="stable")
+                bounds = np.concatenate([[0], np.cumsum(np.bincount(k.astype(np.int64) + 1,
+                                                                    minlength=len(rids) + 1))])
+                for j, rid in enumerate(rids):
+                    o = order[bounds[j + 1]:bounds[j + 2]]
+                    if len(o):
+                        self._record(rid, senders[o], stamp[o], times[o])
+            else:
+                for rid, mask in c["recorders"].items():
+                    sel = mask[src]
+                    if np.any(sel):
+                        self._record(rid, senders[sel], stamp[sel], times[sel])
         if c["samplers"] and self.trace_neurons is not None:
             first, rows = self.engine.trace()
             if len(rows):
                 self._trace_buf.append((first, rows))
             self._flush_samplers()
+
+    def _record(self, rid, senders, stamp, times):
+        """Spikes of a recorder's sources into its events (start/stop window)."""
+        dev = self.devices[self.node_local[rid - 1]]
+        p = dev.params
+        t_min = self.ms_to_steps_roundup(float(p["origin"]) + float(p["start"]))
+        t_max = INF_STEPS if np.isinf(p["stop"]) else self.ms_to_steps_roundup(float(p["origin"]) +
+                                                                                float(p["stop"]))
+        sel = (stamp > t_min) & (stamp <= t_max)
+        if not np.any(sel):
+            return
+        if not np.all(sel):
+            senders, stamp, times = senders[sel], stamp[sel], times[sel]
+        dev.events["senders"].append(senders)
+        dev.events["times"].append(stamp if p.get("time_in_steps") else times)
+        dev.n_events += len(senders)
 
     def _flush_samplers(self):
         """Hand trace rows to the multimeters when the reference would: data
