@@ -38,7 +38,9 @@ WORKLOAD = ("Poisson-driven iaf_psc_exp network: 12,500 neurons (10,000 exc, 2,5
             "dt=0.1 ms, 1,000 ms per step")
 SIM_MS = 1000.0
 
-# algorithmic bytes (Measurement)
+# algorithmic bytes per unit of work: a synaptic event reads its edge word and
+# weight and read-modify-writes one ring cell; a neuron moves its state once
+# per launch and reads and clears two ring cells per step
 B_EVENT = {"fp64": 4 + 8 + 16, "fp32": 4 + 4 + 16}      # edge word + weight + ring read-modify-write
 B_NEURON_LAUNCH = {"fp64": 144, "fp32": 100}            # state r/w, I_e, class id, drive table per launch
 B_NEURON_LAG = {"fp64": 32, "fp32": 32}                 # 2 ring channels read + cleared per step

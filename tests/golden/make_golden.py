@@ -6,7 +6,7 @@ This script is run once, in a container where the reference NEST
     PYTHONPATH=/tmp/nestinstall/lib/python3.12/site-packages python tests/golden/make_golden.py
 
 (the PyNEST install was built from /root/reference with CMake, GSL off,
-OpenMP on; see DESIGN.md).  It writes small ``.npz`` files that the test
+OpenMP on).  It writes small ``.npz`` files that the test
 suite reads on any machine; the reference is never needed at test time.
 
 Fixtures written
