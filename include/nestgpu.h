@@ -178,8 +178,9 @@ int ng_simulate( ng_engine* eng, int64_t n_steps );
  * device; the spikes it logs are drained by the next simulate call (while
  * that call's first group runs) or by ng_sync.  Every entry point that reads
  * results or changes the engine drains first, except ng_net_add,
- * ng_net_poll, ng_net_capacity, and ng_net_spikes / ng_net_remove of a
- * network that ended before that group began.  The engine-side counterpart
+ * ng_net_poll, ng_net_capacity, ng_spike_count / ng_get_spikes (the spikes
+ * drained so far), and ng_net_spikes / ng_net_remove of a network that ended
+ * before that group began.  The engine-side counterpart
  * of repeated Run(t) calls between Prepare() and Cleanup()
  * (pynest/nest/lib/hl_api_simulation.py:66-130), which return when the
  * steps are done. */

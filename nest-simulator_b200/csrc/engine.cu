@@ -2351,7 +2351,6 @@ ng_sync( ng_engine* e )
 int
 ng_spike_count( ng_engine* e, int64_t* n )
 {
-  SETTLE( e );
   if ( !e || !n )
     return fail( NG_ERR_ARG, "ng_spike_count: null argument" );
   *n = ( int64_t ) e->out_src.size();
@@ -2361,7 +2360,6 @@ ng_spike_count( ng_engine* e, int64_t* n )
 int
 ng_get_spikes( ng_engine* e, int32_t* source, int64_t* stamp, int64_t cap, int64_t* n_out )
 {
-  SETTLE( e );
   if ( !e || !n_out || cap < 0 || ( cap > 0 && ( !source || !stamp ) ) )
     return fail( NG_ERR_ARG, "ng_get_spikes: bad argument" );
   const int64_t k = std::min< int64_t >( cap, ( int64_t ) e->out_src.size() );

@@ -165,6 +165,7 @@ _KERNEL_KEYS = ("resolution", "biological_time", "min_delay", "max_delay", "rng_
 
 def GetKernelStatus(keys=None):
     K = KERNEL
+    K.settle()
     c = K.compiled if not K.structure_changed else None
     if c is None and len(K.node_kind):
         try:
@@ -204,6 +205,7 @@ def GetKernelStatus(keys=None):
 
 def SetKernelStatus(params):
     K = KERNEL
+    K.settle()
     params = dict(params)
     if "tics_per_ms" in params:
         if len(K.node_kind):
@@ -266,6 +268,7 @@ def set_verbosity(level):
 
 def engine_stats():
     """Counters of the last run: spikes, synaptic events, drive events, timings."""
+    KERNEL.settle()
     return dict(KERNEL.stats)
 
 

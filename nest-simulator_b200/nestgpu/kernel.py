@@ -83,6 +83,7 @@ class Kernel:
         self.spike_count = 0
         self.stats = {}
         self._rng = None
+        self._unsettled = False  # a Run's last group still runs on the device
 
     @property
     def h(self):
@@ -102,6 +103,7 @@ class Kernel:
         return self._rng
 
     def set_resolution(self, h):
+        self.settle()
         if len(self.node_kind) > 0:
             raise KernelException("Cannot change time representation after nodes have been created. "
                                   "Please call ResetKernel first.")
@@ -136,6 +138,7 @@ class Kernel:
     # nodes
     # ------------------------------------------------------------------
     def create(self, model, n, params):
+        self.settle()
         if n < 1:
             raise BadProperty("Create: n must be >= 1")
         first_id = len(self.node_kind) + 1
@@ -174,6 +177,7 @@ class Kernel:
         return out
 
     def set_status(self, ids, params):
+        self.settle()
         ids = np.asarray(ids, dtype=np.int64)
         if isinstance(params, (list, tuple)):
             if len(params) != len(ids):
@@ -251,6 +255,7 @@ class Kernel:
 
     def get_status(self, ids, key=None):
         """List of per-node dicts (key None) or list of values."""
+        self.settle()
         ids = np.asarray(ids, dtype=np.int64)
         out = [None] * len(ids)
         for m, pos, loc in self._group(ids):
@@ -308,6 +313,7 @@ class Kernel:
     # connections
     # ------------------------------------------------------------------
     def add_edges(self, src, tgt, w, d_ms):
+        self.settle()
         src = np.asarray(src, dtype=np.int64).ravel()
         tgt = np.asarray(tgt, dtype=np.int64).ravel()
         n = len(src)
@@ -582,7 +588,19 @@ class Kernel:
         self.trace_interval = self.ms_to_steps_exact(
             self.devices[self.node_local[next(iter(c["samplers"])) - 1]].params["interval"], "The sampling interval")
 
+    def settle(self):
+        """Wait for the steps a Run left running on the device and hand their
+        spikes to the recorders (every read or change of the network does
+        this first; Run itself returns while its last group still runs)."""
+        if self._unsettled and self.engine is not None:
+            self._unsettled = False
+            self.engine.sync()
+            self._collect()
+            self.stats = self.engine.stats()
+        self._unsettled = False
+
     def prepare(self):
+        self.settle()
         if self.structure_changed or self.engine is None:
             self._build_engine()
         elif self.engine is not None:
@@ -600,10 +618,19 @@ class Kernel:
         t0 = time.perf_counter()
         if self.engine is not None and steps > 0:
             self._push_dirty()
-            self.engine.simulate(steps)
-            self.clock += steps
-            self._collect()
-            self.stats = self.engine.stats()
+            # the Run in up to four calls of whole slice graphs, each leaving its
+            # last group running: the spikes drained before it (the previous
+            # call's) reach the recorders while it runs
+            unit = max(1, self.graph_slices) * int(self.compiled["min_delay"])
+            part = max(unit, -(-steps // (4 * unit)) * unit)
+            left = steps
+            while left > 0:
+                k = min(part, left)
+                self.engine.simulate_async(k)
+                self.clock += k
+                left -= k
+                self._unsettled = True
+                self._collect()
         else:
             self.clock += steps
         self.time_simulate = time.perf_counter() - t0
@@ -616,6 +643,7 @@ class Kernel:
         self.cleanup()
 
     def cleanup(self):
+        self.settle()
         self.prepared = False
 
     def _collect(self):
@@ -714,6 +742,7 @@ class Kernel:
         return len(src)
 
     def get_connections(self, source=None, target=None):
+        self.settle()
         src, tgt, w, d = self.edges()
         m = np.ones(len(src), dtype=bool)
         if source is not None:
