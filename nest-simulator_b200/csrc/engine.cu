@@ -3093,9 +3093,19 @@ ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_
         }
       };
       std::vector< std::thread > pool;
-      for ( int t = 1; t < T; ++t )
-        pool.emplace_back( work, t );
+      int started = 1;
+      try
+      {
+        for ( ; started < T; ++started )
+          pool.emplace_back( work, started );
+      }
+      catch ( ... )
+      {
+        // no more threads: this one takes the remaining shares
+      }
       work( 0 );
+      for ( int t = started; t < T; ++t )
+        work( t );
       for ( auto& th : pool )
         th.join();
       const int64_t k = base.back();
