@@ -1,14 +1,18 @@
 #!/usr/bin/env python
 """Benchmark of the min_delay-slice engine on the Poisson-driven
 iaf_psc_exp network (12,500 neurons, K_E=1,000, K_I=250, 1.5625e7 synapses,
-8 kHz drive, delay 1.5 ms, h = 0.1 ms).
+8 kHz drive, delay 1.5 ms, h = 0.1 ms), plain FP64 form.
 
 One step = Simulate(1000 ms) of the network (10,000 node-update steps in 667
 min_delay slices).  Metric: recurrent synaptic events per second, i.e.
 (sum over emitted spikes of the source's out-degree) / device time, summed
-over all ranks.  Also reported: real-time factor, the FP32/fixed-point form,
-end-to-end throughput through the C ABI with host buffers, the roofline of
-the dominant kernel, and a CPU baseline (the oracle port on the host cores).
+over all ranks.  The headline is the plain FP64 form on one network -- the
+form and workload the reference arm (the reference's CPU cycle on the host
+cores) runs.  Also reported, under "extra": the FP32/fixed-point form and
+eight networks batched in the FP32 form with their errors against FP64, the
+layered network, the aeif network and the serving sweep; the end-to-end
+throughput through the C ABI with host buffers; the roofline of the
+dominant kernel; and the CPU baseline.
 
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
@@ -17,6 +21,7 @@ no cross-GPU exchange); the time is the max over ranks.
 """
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -38,12 +43,40 @@ WORKLOAD = ("Poisson-driven iaf_psc_exp network: 12,500 neurons (10,000 exc, 2,5
             "dt=0.1 ms, 1,000 ms per step")
 SIM_MS = 1000.0
 
-# algorithmic bytes per unit of work: a synaptic event reads its edge word and
-# weight and read-modify-writes one ring cell; a neuron moves its state once
-# per launch and reads and clears two ring cells per step
-B_EVENT = {"fp64": 4 + 8 + 16, "fp32": 4 + 4 + 16}      # edge word + weight + ring read-modify-write
-B_NEURON_LAUNCH = {"fp64": 144, "fp32": 100}            # state r/w, I_e, class id, drive table per launch
-B_NEURON_LAG = {"fp64": 32, "fp32": 32}                 # 2 ring channels read + cleared per step
+# Algorithmic bytes per unit of work, two models.
+# (1) The per-unit figures of the path's survey (§8(d) of the hot-path scope):
+#     a synaptic event reads its target (4 B), weight (8 / 4 B) and delay
+#     (1 B) and read-modify-writes one ring cell (2 x 8 B); an iaf_psc_exp
+#     neuron-step reads and writes its state (3 values + r), reads and clears
+#     two ring cells and reads I_e.
+B_EVENT_SURVEY = {"fp64": 29, "fp32": 25}
+B_NSTEP_SURVEY = {"fp64": 96, "fp32": 68}
+# (2) The engine's own traffic model: the neuron state moves once per launch
+#     (it stays in registers across the slice's lags), the ring cells per
+#     step; a synaptic event reads its packed edge word (target, delay and
+#     channel in 4 B) and weight and read-modify-writes one ring cell.
+B_EVENT = {"fp64": 4 + 8 + 16, "fp32": 4 + 4 + 16}
+B_NEURON_LAUNCH = {"fp64": 144, "fp32": 100}
+B_NEURON_LAG = {"fp64": 32, "fp32": 32}
+
+
+def headline_config(ws):
+    """The workload both arms run (the reference arm and this engine): the
+    same network, form and simulated time per step."""
+    return {"workload": WORKLOAD, "form": "plain FP64 (state, coefficients and ring buffers in FP64)",
+            "networks_per_gpu": 1, "sim_ms_per_step": SIM_MS, "parallelism": f"replicas{ws}",
+            "l2": "graph (188 MB of edges) larger than L2: no flush needed"}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def parse():
@@ -52,7 +85,6 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--batch", type=int, default=8, help="Brunel networks advanced together (batched form)")
@@ -61,7 +93,8 @@ def parse():
     ap.add_argument("--no-aeif", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--forms", default="plain,fp32,batched",
-                    help="forms of the Brunel network to time (the line's value is the batched one)")
+                    help="forms of the Brunel network to time besides the plain FP64 headline")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the V_m RMS runs of the FP32 form")
     return ap.parse_args()
 
 
@@ -174,13 +207,6 @@ def sum_over_ranks(x, pg, device=None):
     return float(t.item())
 
 
-def build(nest, precision, seed):
-    from nestgpu import workloads
-
-    pop, sr = workloads.c1(nest, precision=precision, seed=seed)
-    return pop, sr
-
-
 def cpu_baseline(K, sample_ms=100.0):
     """The oracle port (C, OpenMP, all host cores) on the same network."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -195,29 +221,31 @@ def cpu_baseline(K, sample_ms=100.0):
     net.run(steps, nthreads=threads)
     dt = time.perf_counter() - t0
     ev = net.syn_events - e0
-    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
             "sample": f"{sample_ms:.0f} ms of simulated time of the same network after 50 ms warm-up "
                       f"({ev} synaptic events in {dt:.2f} s, RTF {dt / (sample_ms / 1000):.2f})"}
 
 
 def run_reference(args):
-    """Reference arm: the oracle port of the reference's CPU path, all host cores."""
+    """Reference arm: the reference's CPU cycle (restated by the oracle port,
+    FP64, OpenMP over all host cores) on the headline workload: the same
+    network, form and 1,000 ms of simulated time per step."""
     # no process group: rank 0 alone does the CPU work, the others exit at once
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    pg = None
     if rank != 0:
         return
     import nestgpu as nest
+    from nestgpu import workloads
     from nestgpu.kernel import KERNEL
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    build(nest, "fp64", 4242)
+    workloads.c1(nest, precision="fp64", seed=4242)
     threads = os.cpu_count() or 1
     net, c = O.net_from_kernel(KERNEL, nthreads=threads)
-    sample_ms = float(os.environ.get("NG_BENCH_SAMPLE_MS", "200"))
-    steps = int(round(sample_ms / KERNEL.h))
+    steps = KERNEL.ms_to_steps_exact(SIM_MS)
     for _ in range(args.warmup):
         net.run(steps, nthreads=threads)
     e0 = net.syn_events
@@ -227,53 +255,22 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     ev = net.syn_events - e0
     value = ev / dt
+    sample = (f"{args.steps} x {SIM_MS:.0f} ms of simulated time of the headline network after {args.warmup} "
+              f"warm-up steps ({ev} synaptic events in {dt:.2f} s)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": WORKLOAD, "form": "FP64 oracle port (the reference's CPU cycle restated), all host threads",
-                   "networks_per_gpu": args.batch, "sample_per_step_ms": sample_ms,
-                   "sample": f"one of the {args.batch} networks for {sample_ms:.0f} ms of simulated time per step "
-                             "(events/s do not depend on how many identical networks a CPU run holds)",
-                   "rtf": dt / (args.steps * sample_ms / 1e3)},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{sample_ms:.0f} ms of simulated time per step"},
+        "impl": "reference", "config": headline_config(ws),
+        "reference_form": "oracle port: the reference's per-min_delay cycle restated in C (FP64, OpenMP, all host "
+                          "threads); the full reference needs its CMake build, which the build rules treat as "
+                          "unbuildable",
+        "rtf": dt / (args.steps * SIM_MS / 1e3),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-def e2e_run(c, K, precision, sim_steps, seed):
-    """One step through the C ABI with host buffers: create the engine,
-    copy graph/state/drive from pinned host memory, simulate, copy the
-    spikes back, destroy."""
-    import torch
-
-    from nestgpu import _abi
-
-    st = K.models[c["blocks"][0]["model"]]
-    prec = _abi.NG_FP32 if precision == "fp32" else _abi.NG_FP64
-    eng = _abi.Engine([(b["engine_model"], b["n"]) for b in c["blocks"]], K.h, c["min_delay"], c["max_delay"],
-                      n_generators=len(c["gen_ids"]), precision=prec, device=torch.cuda.current_device())
-    h2d = 0
-    for k, ev in st.engine_vars.items():
-        eng.set_var(0, ev, c["host_state"][k])
-        h2d += c["host_state"][k].nbytes
-    eng.set_connections(c["row_ptr"], c["tgt_sorted"], c["w_sorted"], c["d_sorted"])
-    h2d += c["row_ptr"].nbytes + c["tgt_sorted"].nbytes + c["w_sorted"].nbytes + c["d_sorted"].nbytes
-    start, stop = c["pois_window"]
-    eng.set_poisson(c["pois_rate"], c["pois_w"], c["pois_d"], start, stop, seed)
-    h2d += c["pois_rate"].nbytes + c["pois_w"].nbytes + c["pois_d"].nbytes
-    eng.set_recording(c["rec_flags"])
-    h2d += c["rec_flags"].nbytes
-    eng.set_graph_slices(K.graph_slices)
-    eng.simulate(sim_steps)
-    src, stamp = eng.spikes()
-    d2h = 8 * len(src)
-    ev = eng.stats()["syn_events"]
-    eng.close()
-    return ev, h2d, d2h
 
 
 def pinned(a):
@@ -284,16 +281,120 @@ def pinned(a):
     return t.numpy()
 
 
-def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg):
+class E2E:
+    """The step through the C ABI with host buffers.  The engine and its graph
+    are set up once (as NEST's Connect builds the connection tables before
+    Simulate); every step copies the network's initial state from pinned host
+    memory (ng_set_var), simulates 1,000 ms (ng_simulate) and copies the
+    recorded spikes back (ng_get_spikes) -- the inputs and the result of the
+    reference's Simulate call."""
+
+    @staticmethod
+    def inputs(K, c):
+        """The caller's host buffers (pinned): CSR, initial state, drive
+        tables and recorder flags, prepared once."""
+        N = c["N"]
+        src = c["src"].astype(np.int64)
+        order = np.argsort(src, kind="stable")
+        row_ptr = np.zeros(c["n_src"] + 1, dtype=np.int64)
+        np.cumsum(np.bincount(src, minlength=c["n_src"]), out=row_ptr[1:])
+        st = K.models[c["blocks"][0]["model"]]
+        return {"state": {ev: pinned(st.data[k][:N].astype(np.float64)) for k, ev in st.engine_vars.items()},
+                "csr": (pinned(row_ptr), pinned(c["tgt"][order].astype(np.int32)),
+                        pinned(c["w"][order].astype(np.float64)), pinned(c["d"][order].astype(np.int32))),
+                "drive": (pinned(c["pois_rate"]), pinned(c["pois_w"]), pinned(c["pois_d"].astype(np.int32))),
+                "rec": pinned(c["rec_flags"])}
+
+    def __init__(self, K, c, precision, seed, inp):
+        import torch
+
+        from nestgpu import _abi
+
+        self.K = K
+        self.state = inp["state"]
+        prec = _abi.NG_FP32 if precision == "fp32" else _abi.NG_FP64
+        eng = _abi.Engine([(b["engine_model"], b["n"]) for b in c["blocks"]], K.h, c["min_delay"], c["max_delay"],
+                          n_generators=len(c["gen_ids"]), precision=prec, device=torch.cuda.current_device())
+        eng.set_connections(*inp["csr"])
+        self.graph_h2d = sum(x.nbytes for x in inp["csr"])
+        start, stop = c["pois_window"]
+        eng.set_poisson(*inp["drive"], start, stop, seed)
+        eng.set_recording(inp["rec"])
+        eng.set_graph_slices(K.graph_slices)
+        self.eng = eng
+        self.steps = K.ms_to_steps_exact(SIM_MS)
+        self.src = pinned(np.zeros(1 << 22, dtype=np.int32))
+        self.stamp = pinned(np.zeros(1 << 22, dtype=np.int64))
+
+    def step(self):
+        from nestgpu import _abi
+
+        h2d = 0
+        for name, arr in self.state.items():
+            self.eng.set_var(0, name, arr)
+            h2d += arr.nbytes
+        s0 = self.eng.stats()["syn_events"]
+        self.eng.simulate(self.steps)
+        n = ctypes.c_int64(0)
+        _abi.check(self.eng.L.ng_spike_count(self.eng.handle, ctypes.byref(n)))
+        if n.value > len(self.src):
+            self.src = pinned(np.zeros(2 * n.value, dtype=np.int32))
+            self.stamp = pinned(np.zeros(2 * n.value, dtype=np.int64))
+        got = ctypes.c_int64(0)
+        _abi.check(self.eng.L.ng_get_spikes(self.eng.handle, self.src.ctypes.data, self.stamp.ctypes.data,
+                                            len(self.src), ctypes.byref(got)))
+        ev = self.eng.stats()["syn_events"] - s0
+        # the device -> host copy of the spike log: 8 bytes per logged spike
+        return ev, h2d, 8 * got.value
+
+    def close(self):
+        self.eng.close()
+
+
+def e2e_with_graph(K, c, precision, seed, steps, inp):
+    """The end-to-end step with the network set up anew each time: engine
+    created, graph, state and drive uploaded from pinned host memory,
+    simulated, spikes read back, engine destroyed (events/s, wall clock)."""
+    import torch
+
+    x = E2E(K, c, precision, seed, inp)  # warm-up (allocations, graphs)
+    x.step()
+    x.close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev_tot = 0
+    h2d = d2h = 0
+    for _ in range(steps):
+        x = E2E(K, c, precision, seed, inp)
+        ev, h, d = x.step()
+        h2d = h + x.graph_h2d
+        d2h = d
+        ev_tot += ev
+        x.close()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    return {"value": ev_tot / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "steps": steps}
+
+
+def raster_of(sr):
+    ev = sr.events
+    s = np.asarray(ev["senders"], dtype=np.int64) - 1
+    st = np.rint(np.asarray(ev["times"]) / 0.1).astype(np.int64)
+    return s, st
+
+
+def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg, e2e=True):
     """Build, warm up, time K steps, profile kernels, and (optionally) run e2e."""
     import torch
 
     from nestgpu import workloads
 
     if copies == 1:
-        workloads.c1(nest, precision=precision, seed=seed)
+        pop, sr = workloads.c1(nest, precision=precision, seed=seed)
+        srs = [sr]
     else:
-        workloads.brunel_exp_batch(nest, copies, precision=precision, seed=seed)
+        pops, srs = workloads.brunel_exp_batch(nest, copies, precision=precision, seed=seed)
     nest.set(device=local)
     nest.Prepare()
     eng = KERNEL.engine
@@ -329,6 +430,7 @@ def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg):
     nest.Run(SIM_MS)
     p1 = eng.stats()
     eng.set_profiling(False)
+    KERNEL.settle()
     upd_ms = p1["update_ms"] - p0["update_ms"]
     del_ms = p1["deliver_ms"] - p0["deliver_ms"]
     n_upd = p1["update_launches"] - p0["update_launches"]
@@ -337,60 +439,90 @@ def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg):
     c = KERNEL.compiled
     md = c["min_delay"]
     N = c["N"]
-    upd_bytes = N * (B_NEURON_LAUNCH[precision] + B_NEURON_LAG[precision] * md)
-    del_bytes = ev_prof / max(1, n_del) * B_EVENT[precision]
+    ev_launch = ev_prof / max(1, n_del)
 
-    def kern(launches, tot_ms, nbytes):
+    def kern(launches, tot_ms, engine_bytes, survey_bytes):
         avg = tot_ms / max(1, launches)
-        return {"launches": launches, "avg_us": 1e3 * avg, "alg_bytes_per_launch": nbytes,
-                "achieved_gbs": nbytes / (avg * 1e-3) / 1e9 if avg > 0 else None}
+        return {"launches": launches, "avg_us": 1e3 * avg, "alg_bytes_per_launch": survey_bytes,
+                "achieved_gbs": survey_bytes / (avg * 1e-3) / 1e9 if avg > 0 else None,
+                "engine_model_bytes_per_launch": engine_bytes,
+                "engine_model_gbs": engine_bytes / (avg * 1e-3) / 1e9 if avg > 0 else None}
 
-    # the engine's dispatch: one thread per neuron from 20,000 neurons on, the two-phase kernel below
-    upd_name = "k_update_iaf" if N >= 20000 else "k_update_iaf2"
-    kernels = {upd_name: kern(n_upd, upd_ms, upd_bytes), "k_deliver": kern(n_del, del_ms, del_bytes)}
+    tuned = eng.tuned()
+    upd_name = tuned.get("update_kernel", "k_update_iaf")
+    kernels = {upd_name: kern(n_upd, upd_ms, N * (B_NEURON_LAUNCH[precision] + B_NEURON_LAG[precision] * md),
+                              N * md * B_NSTEP_SURVEY[precision]),
+               "k_deliver": kern(n_del, del_ms, ev_launch * B_EVENT[precision], ev_launch * B_EVENT_SURVEY[precision])}
+    # statistics of the timed region's raster (network 0)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import spikestats as S
+
+    s_all, st_all = raster_of(srs[0])
+    n0 = 12500
+    t_end = st_all.max() * 0.1 if len(st_all) else 0.0
+    t_beg = max(0.0, t_end - args.steps * SIM_MS)
+    summ = S.summary(s_all, st_all, n0, 0.1, t_beg, t_end, n_pairs=3000, seed=seed) if len(s_all) else None
     res = {"ms": ms_max, "events": ev_all, "clocks": clocks, "kernels": kernels, "copies": copies,
            "launches": (s1["update_launches"] - s0["update_launches"]) +
                        (s1["deliver_launches"] - s0["deliver_launches"]) + 1,
-           "spikes": s1["spikes"] - s0["spikes"], "form": form, "precision": precision}
+           "spikes": s1["spikes"] - s0["spikes"], "form": form, "precision": precision, "tuned": tuned,
+           "summary": summ}
     res["value"] = ev_all / (ms_max * 1e-3)
     res["rtf"] = ms_max / args.steps / SIM_MS
-    # end to end through the C ABI with host buffers
-    if not args.no_e2e:
-        src = c["src"].astype(np.int64)
-        order = np.argsort(src, kind="stable")
-        counts = np.bincount(src, minlength=c["n_src"])
-        row_ptr = np.zeros(c["n_src"] + 1, dtype=np.int64)
-        np.cumsum(counts, out=row_ptr[1:])
-        st = KERNEL.models[c["blocks"][0]["model"]]
-        cc = dict(c)
-        cc["row_ptr"] = pinned(row_ptr)
-        cc["tgt_sorted"] = pinned(c["tgt"][order].astype(np.int32))
-        cc["w_sorted"] = pinned(c["w"][order].astype(np.float64))
-        cc["d_sorted"] = pinned(c["d"][order].astype(np.int32))
-        cc["host_state"] = {k: pinned(st.data[k][:N].astype(np.float64)) for k in st.engine_vars}
-        cc["pois_rate"] = pinned(c["pois_rate"])
-        cc["pois_w"] = pinned(c["pois_w"])
-        cc["pois_d"] = pinned(c["pois_d"].astype(np.int32))
-        cc["rec_flags"] = pinned(c["rec_flags"])
-        del src, order, counts
-        sim_steps = KERNEL.ms_to_steps_exact(SIM_MS)
-        e2e_run(cc, KERNEL, precision, sim_steps, seed)  # warm-up
+    if e2e and not args.no_e2e:
+        inp = E2E.inputs(KERNEL, c)
+        x = E2E(KERNEL, c, precision, seed, inp)
+        x.step()  # warm-up
         if pg is not None:
             pg.barrier()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         tot_ev = 0
+        h2d = d2h = 0
         for _ in range(args.steps):
-            ev_e, h2d, d2h = e2e_run(cc, KERNEL, precision, sim_steps, seed)
+            ev_e, h2d, d2h = x.step()
             tot_ev += ev_e
         torch.cuda.synchronize(dev)
         wall = time.perf_counter() - t0
+        x.close()
         wall_max = max_over_ranks(wall, pg, dev)
         tot_all = sum_over_ranks(tot_ev, pg, dev)
         res["e2e"] = {"value": tot_all / wall_max, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                       "d2h_bytes_per_step": int(d2h)}
+        res["e2e_with_graph_upload"] = e2e_with_graph(KERNEL, c, precision, seed, min(args.steps, 3), inp)
     nest.ResetKernel()
     return res
+
+
+def vm_rms_100ms(nest, seed=4242, n_rec=200):
+    """V_m RMS error [mV] of the FP32 form against the FP64 form over the
+    first 100 ms of the headline network (same graph, drive and initial
+    state): all recorded neurons, and the neurons that have not spiked yet
+    in either form (where the two trajectories can only differ by
+    rounding)."""
+    from nestgpu import workloads
+
+    V, R = {}, {}
+    for prec in ("fp64", "fp32"):
+        pop, sr = workloads.c1(nest, precision=prec, seed=seed)
+        mm = nest.Create("multimeter", params={"interval": 0.1, "record_from": ["V_m"]})
+        nest.Connect(mm, pop[:n_rec])
+        nest.Simulate(100.0)
+        ev = mm.events
+        o = np.lexsort((ev["senders"], ev["times"]))
+        V[prec] = np.asarray(ev["V_m"])[o].reshape(-1, n_rec)
+        s, st = raster_of(sr)
+        first = np.full(n_rec, 10 ** 9)
+        m = s < n_rec
+        np.minimum.at(first, s[m], st[m])
+        R[prec] = first
+        nest.ResetKernel()
+    d = V["fp32"] - V["fp64"]
+    rows = np.arange(d.shape[0])[:, None] + 1  # stamp of each row
+    quiet = rows < np.minimum(R["fp32"], R["fp64"])[None, :]
+    return {"vm_rms_100ms_mV": float(np.sqrt(np.mean(d * d))),
+            "vm_rms_before_first_spike_mV": float(np.sqrt(np.mean(d[quiet] ** 2))) if quiet.any() else None,
+            "neurons": n_rec}
 
 
 def timed_sim(eng, steps, dev):
@@ -438,7 +570,7 @@ def measure_layered(args, dev, sim_ms=1000.0):
         eng = workloads.layered_engine(spec, prec, device=dev.index, ring32=form.endswith("ring32"))
         nid = workloads.layered_add(eng, spec, 10 * steps)
         build = time.perf_counter() - t0
-        eng.simulate(1000)  # 100 ms warm-up (graphs built)
+        eng.simulate(3000)  # 300 ms warm-up (autotuner trials, graphs built)
         sampler = ClockSampler(dev.index)
         sampler.start()
         s0 = eng.stats()
@@ -447,11 +579,12 @@ def measure_layered(args, dev, sim_ms=1000.0):
         clocks = sampler.stop()
         ks = kernel_split(eng, 200)
         out["synapses"] = eng.net_connection_count(nid)
+        tuned = eng.tuned()
         eng.close()
         ev = s1["syn_events"] - s0["syn_events"]
         out[form] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
                      "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / out["neurons"] / (sim_ms * 1e-3),
-                     "build_s": build, "kernels": ks, "clocks": clocks,
+                     "build_s": build, "kernels": ks, "clocks": clocks, "tuned": tuned,
                      "host_ms": {k: s1[k] - s0[k] for k in ("simulate_ms", "wait_ms", "drain_ms")}}
     out["fp32_ring32"]["ring_bound"] = workloads.layered_ring_bound(spec)
     return out
@@ -472,7 +605,7 @@ def measure_aeif(args, dev, sim_ms=500.0):
         eng = workloads.aeif_engine(spec, prec, device=dev.index)
         workloads.aeif_add(eng, spec, 10 * steps)
         build = time.perf_counter() - t0
-        eng.simulate(1500)  # 150 ms warm-up
+        eng.simulate(2000)  # 200 ms warm-up (autotuner trials, graphs built)
         s0 = eng.stats()
         ms = timed_sim(eng, steps, dev)
         s1 = eng.stats()
@@ -535,13 +668,24 @@ def run_engine(args):
     import nestgpu as nest
     from nestgpu.kernel import KERNEL
 
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import spikestats as S
+
     seed = 4242 + 1000 * rank
     forms = set(args.forms.split(","))
-    plain = measure(args, nest, KERNEL, "plain", "fp64", 1, seed, local, dev, pg) if "plain" in forms else None
-    single32 = measure(args, nest, KERNEL, "single", "fp32", 1, seed, local, dev, pg) if "fp32" in forms else None
-    batched = measure(args, nest, KERNEL, "batched", "fp32", args.batch, seed, local, dev, pg) \
-        if args.batch > 1 and "batched" in forms else single32
+    plain = measure(args, nest, KERNEL, "plain", "fp64", 1, seed, local, dev, pg)
+    single32 = measure(args, nest, KERNEL, "single", "fp32", 1, seed, local, dev, pg, e2e=False) \
+        if "fp32" in forms else None
+    batched = measure(args, nest, KERNEL, "batched", "fp32", args.batch, seed, local, dev, pg, e2e=False) \
+        if args.batch > 1 and "batched" in forms else None
     extra = {}
+    if single32 is not None and plain["summary"] and single32["summary"]:
+        acc = S.compare(single32["summary"], plain["summary"])
+        if not args.no_accuracy:
+            acc.update(vm_rms_100ms(nest))
+        extra["accuracy_fp32_vs_fp64"] = acc
+    if batched is not None and plain["summary"] and batched["summary"]:
+        extra["accuracy_batched_fp32_vs_fp64"] = S.compare(batched["summary"], plain["summary"])
     if not args.no_layered:
         extra["layered_8pop"] = measure_layered(args, dev)
     if not args.no_aeif:
@@ -555,7 +699,7 @@ def run_engine(args):
         workloads.c1(nest, precision="fp64", seed=seed)
         cpu = cpu_baseline(KERNEL)
         nest.ResetKernel()
-    r = batched
+    r = plain
     peak, peak_kind = load_peaks()
     dom_name, dom = max(r["kernels"].items(), key=lambda kv: kv[1]["avg_us"] * kv[1]["launches"])
     ach = dom["achieved_gbs"]
@@ -563,29 +707,42 @@ def run_engine(args):
     def brief(x):
         if x is None:
             return None
-        return {"value": x["value"], "rtf": x["rtf"], "e2e": x.get("e2e"), "spikes_per_step": x["spikes"] /
-                max(1, args.steps + 1), "kernels": {k: {"avg_us": v["avg_us"], "achieved_gbs": v["achieved_gbs"]}
-                                                    for k, v in x["kernels"].items()}}
+        out = {"value": x["value"], "rtf": x["rtf"], "networks": x["copies"], "dtype": "f32+i64",
+               "spikes_per_step": x["spikes"] / max(1, args.steps + 1), "tuned": x["tuned"],
+               "kernels": {k: {"avg_us": v["avg_us"], "achieved_gbs": v["achieved_gbs"]}
+                           for k, v in x["kernels"].items()}}
+        if x["summary"]:
+            out["rate_hz"] = x["summary"]["rate_hz"]
+            out["cv_isi_mean"] = x["summary"]["cv_isi_mean"]
+        return out
 
+    extra["fp32_single_network"] = brief(single32)
+    extra["batched_fp32"] = brief(batched)
+    if batched is not None:
+        extra["batched_over_plain"] = batched["value"] / plain["value"]
+    extra["e2e_with_graph_upload"] = r.get("e2e_with_graph_upload")
     line = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+i64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "batched FP32 state + int64 fixed-point rings",
-                   "networks_per_gpu": r["copies"], "global_batch": r["copies"] * ws,
-                   "parallelism": f"replicas{ws}", "l2": "graph larger than L2 (no flush needed)",
-                   "rtf_per_network": r["rtf"],
-                   "plain_fp64_single_network": brief(plain), "fp32_single_network": brief(single32),
-                   "batched_over_plain": r["value"] / plain["value"] if plain else None, **extra},
+        "dtype": "f64", "data": "synthetic",
+        "config": headline_config(ws),
+        "rtf": r["rtf"],
+        "tuned": r["tuned"],
         "gpu_launches": int(r["launches"]),
         "clocks": r["clocks"],
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": (ach / peak) if ach else None, "peak_kind": peak_kind,
-                     "traffic": load_traffic(dom_name, f"brunel_x{r['copies']}_{r['precision']}"),
+                     "bytes_model": "per-unit bytes of the path's survey: 96 B per iaf_psc_exp neuron-step "
+                                    "(FP64), 29 B per synaptic event",
+                     "frac_engine_model": (dom["engine_model_gbs"] / peak) if dom["engine_model_gbs"] else None,
+                     "traffic": load_traffic(dom_name, "brunel_x1_fp64"),
                      "kernels": r["kernels"]},
         "e2e": r.get("e2e"),
         "cpu_baseline": cpu,
+        "rate_hz": r["summary"]["rate_hz"] if r["summary"] else None,
+        "cv_isi_mean": r["summary"]["cv_isi_mean"] if r["summary"] else None,
+        "extra": extra,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -1,14 +1,24 @@
 """Runnable cases of the benchmark workloads at chosen sizes, for profiling
-a kernel on a small instance:
+a kernel on a small instance (run from the repository root):
 
-  python -m nestgpu.cases layered --scale 0.5 --ms 300 --precision fp32
-  python -m nestgpu.cases aeif --neurons 10000 --ms 60
-  python -m nestgpu.cases serving --requests 40 --capacity-neurons 300000 --capacity-edges 200000000 --slices 40
+  python bench_cases.py c1 --precision fp64 --ms 1000 --runs 4
+  python bench_cases.py layered --scale 0.5 --ms 300 --precision fp32
+  python bench_cases.py aeif --neurons 10000 --ms 60
+  python bench_cases.py serving --requests 40 --capacity-neurons 300000 --capacity-edges 200000000 --slices 40
 
-(run from the package directory's parent with it on sys.path, as bench.py
-does).  Each case builds its network on the device, simulates, prints one
-summary line and exits 0.
+Each case builds its network, simulates, prints one summary line and exits 0.
+The c1 case is bench.py's headline network (12,500 iaf_psc_exp neurons,
+K_E = 1,000, K_I = 250, 8 kHz drive) built with the PyNEST-compatible
+front-end and run as `runs` calls of Simulate(ms) -- the first one long
+enough for the autotuner, as in the bench's warm-up.
 """
+
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if os.path.join(ROOT, "nest-simulator_b200") not in sys.path:
+    sys.path.insert(0, os.path.join(ROOT, "nest-simulator_b200"))
 
 import argparse
 import copy
@@ -17,7 +27,7 @@ import sys
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["layered", "aeif", "serving"])
+    ap.add_argument("case", choices=["c1", "layered", "aeif", "serving"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0, help="layered: population size factor")
     ap.add_argument("--neurons", type=int, default=50000, help="aeif: network size (80 % excitatory)")
@@ -26,11 +36,28 @@ def main(argv=None):
     ap.add_argument("--capacity-neurons", type=int, default=300_000)
     ap.add_argument("--capacity-edges", type=int, default=200_000_000)
     ap.add_argument("--slices", type=int, default=40, help="serving: min_delay slices simulated")
+    ap.add_argument("--runs", type=int, default=4, help="c1: Simulate(ms) calls")
+    ap.add_argument("--fixed", default="", help="c1: fixed launch configuration 'variant,ctas_per_sm,chunks_per_warp' "
+                                                  "instead of the autotuner (which measures differently under a profiler)")
     ap.add_argument("--ring32", action="store_true", help="layered: 32-bit ring cells")
     ap.add_argument("--no-tiled", action="store_true", help="layered: scatter delivery only")
     a = ap.parse_args(argv)
-    from . import serving, workloads
+    import nestgpu as nest
+    from nestgpu import serving, workloads
+    from nestgpu.kernel import KERNEL
 
+    if a.case == "c1":
+        workloads.c1(nest, precision=a.precision, seed=4242)
+        if a.fixed:
+            nest.Prepare()
+            KERNEL.engine.set_tuning(0, *[int(x) for x in a.fixed.split(",")])
+        for _ in range(a.runs):
+            nest.Simulate(a.ms)
+        st = nest.engine_stats()
+        print(f"c1: steps {st['clock_steps']} spikes {st['spikes']} syn_events {st['syn_events']} "
+              f"tuned {KERNEL.engine.tuned()['update_kernel']}", flush=True)
+        nest.ResetKernel()
+        return 0
     if a.case == "layered":
         spec = workloads.layered_spec(scale=a.scale)
         eng = workloads.layered_engine(spec, a.precision, ring32=a.ring32, tiled=not a.no_tiled)

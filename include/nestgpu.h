@@ -186,7 +186,18 @@ int ng_simulate( ng_engine* eng, int64_t n_steps );
  * steps are done. */
 int ng_simulate_async( ng_engine* eng, int64_t n_steps );
 
-/* Wait for the steps of ng_simulate_async and drain their spikes. */
+/* Steps [from, to) of the slice that starts at step `origin` -- the call a
+ * NEST node receives once per slice, Node::update(Time const& origin, long
+ * from, long to) (nestkernel/node.h:297, called by SimulationManager::
+ * update_, simulation_manager.cpp:1062-1071).  The engine must stand at
+ * origin + from (NG_ERR_STATE otherwise); a call with to == min_delay
+ * closes the slice (its delivery runs).  Asynchronous: the steps of
+ * successive calls are appended to one group on the device and the host
+ * does not wait; their spikes are drained when the group fills the spike
+ * log, or by ng_sync or any call that reads or changes the engine. */
+int ng_update( ng_engine* eng, int64_t origin, int32_t from, int32_t to );
+
+/* Wait for the steps of ng_simulate_async or ng_update and drain their spikes. */
 int ng_sync( ng_engine* eng );
 
 /* Number of logged spikes waiting to be drained. */
@@ -214,6 +225,58 @@ int ng_set_stream( ng_engine* eng, void* cuda_stream );
 
 /* Capture full slices as CUDA graphs of `slices_per_graph` slices (0: off). */
 int ng_set_graph_slices( ng_engine* eng, int32_t slices_per_graph );
+
+/* ---------------------------------------------------------------------
+ * Launch configuration and the autotuner.  No counterpart in the reference
+ * (its OpenMP loop has no launch shapes to choose).  By default an engine
+ * tunes itself on the first call long enough to afford the trials: it runs
+ * the network's own next slices (real steps of the call) under each
+ * candidate, timed with CUDA events -- the node-update kernel (one thread
+ * per neuron gathering 4 or 8 lags of inputs at a time, or the two-phase
+ * kernel with 256- or 128-thread CTAs), the resident delivery CTAs per SM,
+ * and the edge chunks a delivery warp takes per descriptor load -- and keeps
+ * the fastest.  The choice is cached for the process by network shape and
+ * activity (precision, models, log2 of the neuron count, of the mean
+ * out-degree and of the spikes per neuron-step, min_delay, delivery form),
+ * so an engine of the same kind starts with it.  Every candidate computes
+ * the same result.
+ * --------------------------------------------------------------------- */
+#define NG_TUNE_MAX_CANDIDATES 32
+typedef struct
+{
+  int32_t mode;            /* 0: fixed, 1: autotuned */
+  int32_t state;           /* 0: not tuned yet, 1: measured, 2: from the process cache, 3: fixed */
+  int32_t update_variant;  /* 0/1: one thread per neuron (4/8 lags of inputs at a time), 2/3: two-phase
+                              (256/128-thread CTAs), 4: aeif_cond_alpha's RKF45 kernel */
+  int32_t deliver_per_sm;  /* resident delivery CTAs per SM */
+  int32_t deliver_group;   /* edge chunks per delivery warp and descriptor load */
+  int32_t cache_hit;
+  int32_t rate_bucket;     /* floor(log2(spikes per 1000 neuron-steps)) measured at tuning */
+  int32_t n_candidates;    /* trials below, in the order they ran */
+  int32_t cand_variant[ NG_TUNE_MAX_CANDIDATES ];
+  int32_t cand_per_sm[ NG_TUNE_MAX_CANDIDATES ];
+  int32_t cand_group[ NG_TUNE_MAX_CANDIDATES ];
+  double cand_us_per_slice[ NG_TUNE_MAX_CANDIDATES ]; /* device time per min_delay slice */
+  int64_t trial_steps;     /* steps of one timed trial */
+} ng_tuning;
+
+/* mode 1: autotune at the next long enough call (process cache first);
+ * mode 2: the same, measuring even where the cache has an entry; mode 0:
+ * fixed configuration -- update_variant (0..3, -1: by network size),
+ * delivery CTAs per SM and chunks per warp (-1: defaults). */
+int ng_set_tuning( ng_engine* eng, int32_t mode, int32_t update_variant, int32_t deliver_ctas_per_sm,
+  int32_t deliver_chunks_per_warp );
+
+/* The configuration in force and the autotuner's trials. */
+int ng_get_tuning( ng_engine* eng, ng_tuning* out );
+
+/* Engine options: "late_delivery" (1/0: edges of delay >= 2 min_delay
+ * delivered on a second stream beside the next slice's update),
+ * "late_ctas_per_sm", and for serving engines in the FP32 form, before any
+ * network is admitted, "gather" (1/0: the per-target gather of hot
+ * fixed_indegree networks) and "gather_frac" (the share of a network's
+ * neurons spiking in a slice from which its next slice gathers). */
+int ng_set_option( ng_engine* eng, const char* name, double value );
 
 /* FP64 coefficients the engine computed for a neuron (testing hook):
  * writes up to `cap` values in the model's order, *n_out the count.  For
@@ -332,13 +395,22 @@ int ng_net_capacity( ng_engine* eng, int64_t* free_neurons, int64_t* free_edges 
  * array of NG_NOALLOC_SCRATCH_BYTES that every GPU which loads the library
  * holds until the process exits.  Networks whose scratch
  * ((min_delay + max_delay) * n * 8 + n * min_delay * 8 bytes + 256) does not
- * fit are rejected with NG_ERR_CAPACITY.  Every call starts a fresh run (it
- * zeroes the ring and counters) and shares the one array, so calls that
- * overlap on the GPU race: serialise them (one stream, or events).  The
- * first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  The call
- * is asynchronous on `cuda_stream`; spikes beyond out_cap are counted in
- * *out_count but not written.
+ * fit are rejected with NG_ERR_CAPACITY.  A call with continue_run = 0
+ * starts a fresh run: it zeroes the ring and counters, and start_step must
+ * be a multiple of min_delay.  A call with continue_run = 1 goes on with the
+ * run of the previous call on this device (same n, min_delay, max_delay, and
+ * start_step equal to where that call stopped, which may be inside a
+ * slice): the spikes still pending in the ring and the open slice's spike
+ * list are kept, so a chain of calls gives the same result as one call over
+ * the same steps.  Every call shares the one array, so calls that overlap on
+ * the GPU race: serialise them (one stream, or events).  The first call on a
+ * device looks up the array's device address with that device current; make
+ * that first call before any stream capture.  The call is asynchronous on
+ * `cuda_stream`; spikes beyond out_cap are counted in *out_count but not
+ * written.  The kernels check every edge they walk: an edge whose target is
+ * not in [0, n) or whose delay is not in [min_delay, max_delay] is skipped
+ * and counted in *out_skipped (so no write ever leaves the ring); row_ptr
+ * must be non-decreasing with row_ptr[n] edges in target/weight/delay.
  * --------------------------------------------------------------------- */
 #define NG_NOALLOC_SCRATCH_BYTES ( 16u << 20 )
 
@@ -347,7 +419,8 @@ typedef struct
   int64_t n;                  /* neurons */
   int32_t min_delay;          /* steps */
   int32_t max_delay;          /* steps */
-  int64_t start_step;         /* absolute step of the first slice origin, a multiple of min_delay */
+  int64_t start_step;         /* absolute step of the first step: a multiple of min_delay for a fresh run,
+                                 the previous call's end for a continued one */
   const double* P33;          /* per neuron: exp(-h / tau_m) */
   const double* P30;          /* per neuron: 1 / C_m * (1 - P33) * tau_m */
   const double* V_th_rel;     /* per neuron, relative to E_L */
@@ -364,7 +437,10 @@ typedef struct
   int32_t* out_src;           /* out: spike sources */
   int64_t* out_stamp;         /* out: spike stamps (emission step + 1) */
   int64_t out_cap;            /* capacity of out_src / out_stamp */
-  unsigned long long* out_count; /* out: number of spikes emitted */
+  unsigned long long* out_count; /* out: number of spikes emitted in this call */
+  int32_t continue_run;       /* 0: fresh run; 1: continue the previous call's run on this device */
+  int32_t reserved;           /* must be 0 */
+  unsigned long long* out_skipped; /* out (may be NULL): edges skipped for an out-of-range target or delay */
 } ng_noalloc_net;
 
 /* Simulate n_steps of `net` with no memory allocation (see above). */

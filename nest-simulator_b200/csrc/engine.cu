@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <mutex>
 #include <new>
 
 #include "../../include/nestgpu.h"
@@ -479,11 +480,8 @@ struct ng_engine
     free_neurons[ 0 ] = N;
     free_edges[ 0 ] = E;
     // per-target gather: precision form, current-based models, slices of at most 16 steps
+    // (ng_set_option "gather" turns it off, "gather_frac" sets the switch point)
     gather_on = prec != NG_FP64 && b.model != NG_AEIF_COND_ALPHA && cfg.min_delay <= 16 && nmax <= 1024;
-    if ( const char* ge = std::getenv( "NG_GATHER" ) )
-      gather_on = gather_on && std::atoi( ge ) != 0;
-    if ( const char* gf = std::getenv( "NG_GATHER_FRAC" ) )
-      gather_frac = ( float ) std::atof( gf );
     if ( gather_on )
     {
       if ( cudaFuncSetAttribute( k_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, ( int ) G_SMEM ) != cudaSuccess )
@@ -633,9 +631,40 @@ struct ng_engine
       rc = alloc( ent_late, 2 * ( size_t ) ent_cap * sizeof( int4 ) );
     return rc;
   }
-  int max_lanes = 32;             // 1: always one thread per neuron
-  int sub_lags = 4;               // lags whose inputs one thread gathers together (4 or 8)
-  int64_t one_thread_min_n = 20000;  // block size from which one thread per neuron fills the GPU
+  // ---- launch configuration: chosen by the autotuner (measured on the
+  // network's own first slices, cached per network shape and activity for
+  // the process) or fixed through ng_set_tuning.  Every choice computes the
+  // same result (the kernels share their arithmetic and its order).
+  int tune_mode = 1;         // 0: fixed, 1: autotune (process cache first), 2: autotune, cache ignored
+  int tune_state = 0;        // 0: pending, 1: measured, 2: from the process cache, 3: fixed
+  int upd_variant = -1;      // iaf update kernel: 0/1 one thread per neuron (4/8 lags of inputs at a
+                             // time), 2/3 two-phase (256/128 threads); -1: by network size
+  int occ_deliver = 8;       // resident k_deliver CTAs per SM (occupancy bound)
+  int deliver_group = 4;     // edge chunks one delivery warp takes per descriptor load
+  int64_t deliver_want = 1;  // delivery CTAs the graph can keep busy (its chunks / 64)
+  int rate_bucket = -1;
+  int64_t trial_steps = 0;
+  struct TuneCand
+  {
+    int variant, per_sm, group;
+    double us;
+  };
+  std::vector< TuneCand > tune_log;
+
+  // the update kernel a block of n neurons runs before (or without) tuning
+  static int
+  default_variant( int64_t n )
+  {
+    return n >= 20000 ? 0 : 2;
+  }
+
+  void
+  apply_deliver()
+  {
+    deliver_ctas = ( int ) std::max< int64_t >( 1, std::min< int64_t >( deliver_want, ( int64_t ) sms * deliver_per_sm ) );
+    refresh_late();
+    ++generation;
+  }
 
   ~ng_engine()
   {
@@ -911,6 +940,7 @@ struct ng_engine
     d.sched_step = ( const int64_t* ) sched_step.p;
     d.sched_src = ( const int32_t* ) sched_src.p;
     d.n_sched = n_sched;
+    d.deliver_group = deliver_group;
     d.ctl = ( Ctl* ) ctl.p;
     return d;
   }
@@ -961,16 +991,19 @@ struct ng_engine
   launch_iaf_g( const Net& d, const Block& db, int from_, int to_, int sched )
   {
     const int span = to_ - from_;
-    // one thread per neuron for 1-2 step slices, for networks large enough
-    // to fill the GPU that way and for engines with the per-target gather
-    // (its lag bits are written there); the two-phase kernel otherwise
-    if ( span <= 2 || db.n >= one_thread_min_n || max_lanes == 1 || gather_on || tiled_on )
+    // the tuned (or default) kernel; one thread per neuron for 1-2 step
+    // slices and for engines with the per-target gather or the target-tiled
+    // delivery (the lag bits are written there)
+    int v = upd_variant >= 0 ? upd_variant : default_variant( db.n );
+    if ( span <= 2 || gather_on || tiled_on )
+      v = v == 1 ? 1 : 0;
+    if ( v <= 1 )
     {
       // CTAs of 4 warps: a large network's grid is resident in one wave
       const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 127 ) / 128 );
       if ( span == 1 )
         k_update_iaf< Real, FIX, MODEL, 1 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
-      else if ( sub_lags == 4 )
+      else if ( v == 0 )
         k_update_iaf< Real, FIX, MODEL, 4 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
       else
         k_update_iaf< Real, FIX, MODEL, 8 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
@@ -978,7 +1011,10 @@ struct ng_engine
     else
     {
       const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + P2_NB - 1 ) / P2_NB );
-      k_update_iaf2< Real, FIX, MODEL ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+      if ( v == 2 )
+        k_update_iaf2< Real, FIX, MODEL, 256, 32 ><<< grid, 256, 0, stream >>>( d, db, from_, to_, sched );
+      else
+        k_update_iaf2< Real, FIX, MODEL, 128, 16 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
     }
   }
 
@@ -1302,15 +1338,32 @@ struct ng_engine
   };
 
   int
-  launch_group( int64_t n, int sel, GroupInfo& gi )
+  begin_group( int sel, GroupInfo& gi )
   {
     gi.clock = origin + from;
     gi.row0 = ( gi.clock + 1 + trace_interval - 1 ) / trace_interval;
     k_set_ctl<<< 1, 1, 0, stream >>>( ( Ctl* ) ctl.p, gi.clock, gi.row0, 1, sel );
     CU( cudaGetLastError() );
-    int rc = enqueue_steps( n );
+    return NG_OK;
+  }
+
+  int
+  launch_group( int64_t n, int sel, GroupInfo& gi )
+  {
+    int rc = begin_group( sel, gi );
     if ( rc )
       return rc;
+    if ( ( rc = enqueue_steps( n ) ) )
+      return rc;
+    return end_group( sel, gi );
+  }
+
+  // the group's end: its spike log grouped (serving), the control block
+  // copied back, the event the drain waits for
+  int
+  end_group( int sel, GroupInfo& gi )
+  {
+    int rc = NG_OK;
     gi.end = origin + from;
     if ( serving )
     {
@@ -1462,14 +1515,285 @@ struct ng_engine
   int pend_sel = -1;
   GroupInfo pend_gi;
 
+  // ---- slice-aligned calls (ng_update): the steps of successive calls are
+  // appended to one open group, which is closed (and becomes the pending
+  // group) when it reaches the spike log's capacity or when anything reads
+  // or changes the engine
+  int og_sel = -1;
+  GroupInfo og_gi;
+  int64_t og_steps = 0, og_max = 0;
+
+  int
+  close_group()
+  {
+    if ( og_sel < 0 )
+      return NG_OK;
+    const int sel = og_sel;
+    og_sel = -1;
+    int rc = end_group( sel, og_gi );
+    if ( rc )
+      return rc;
+    if ( pend_sel >= 0 )
+    {
+      const int s = pend_sel;
+      pend_sel = -1;
+      if ( ( rc = drain_group( s, pend_gi ) ) )
+        return rc;
+    }
+    pend_sel = sel;
+    pend_gi = og_gi;
+    return NG_OK;
+  }
+
   int
   sync_pending()
   {
+    if ( og_sel >= 0 )
+    {
+      const int rc = close_group();
+      if ( rc )
+        return rc;
+    }
     if ( pend_sel < 0 )
       return NG_OK;
     const int s = pend_sel;
     pend_sel = -1;
     return drain_group( s, pend_gi );
+  }
+
+  // largest group (in steps) the spike log and the trace buffer hold
+  int
+  group_max( int64_t* gmax_out )
+  {
+    int64_t by_log = ( int64_t ) std::floor( ( double ) ( log_cap - n_sched - n_rec ) / log_per_step );
+    if ( by_log < 1 )
+      return fail( NG_ERR_CAPACITY, "spike log capacity too small for one step" );
+    int64_t gmax = std::min< int64_t >( by_log, ( 1 << 24 ) - 2 );
+    if ( n_trace_idx > 0 )
+      gmax = std::min< int64_t >( gmax, ( trace_rows_cap - 1 ) * trace_interval );
+    if ( gmax < 1 )
+      return fail( NG_ERR_CAPACITY, "trace buffer too small" );
+    *gmax_out = gmax;
+    return NG_OK;
+  }
+
+  // steps [from_, to_) of the open slice (Node::update(origin, from, to)),
+  // enqueued without waiting for the device
+  int
+  update_range( int from_, int to_ )
+  {
+    int rc;
+    if ( og_sel < 0 )
+    {
+      if ( ( rc = prepare() ) || ( rc = group_max( &og_max ) ) )
+        return rc;
+      og_max = std::max< int64_t >( 1, og_max );
+      og_sel = pend_sel == 0 ? 1 : 0;
+      og_steps = 0;
+      if ( ( rc = begin_group( og_sel, og_gi ) ) )
+      {
+        og_sel = -1;
+        return rc;
+      }
+    }
+    if ( ( rc = enqueue_steps( to_ - from_ ) ) )
+      return rc;
+    og_steps += to_ - from_;
+    stats.clock_steps = origin + from;
+    stats.slices = slices;
+    if ( og_steps + cfg.min_delay > og_max )
+      rc = close_group();
+    return rc;
+  }
+
+  // ---- autotuner.  The trials run the network's own next slices (real
+  // steps of the call: every candidate computes the same result), each as
+  // one group timed with CUDA events on the engine's stream: first the
+  // current configuration (which also measures the activity), then the
+  // update kernels, the delivery CTAs per SM and the chunks per delivery
+  // warp, one knob at a time with the others at their best so far.  Each
+  // candidate runs an untimed group first (its slice graphs are captured
+  // there) and a timed one.  The winner is cached for the process by
+  // network shape and activity (precision, models, log2 of N, of the mean
+  // out-degree and of the spikes per neuron-step, min_delay, late
+  // delivery, gather and tiled delivery), so a later engine of the same kind
+  // starts with it.
+  struct TuneKey
+  {
+    std::string k;
+  };
+  static std::mutex& tune_mutex()
+  {
+    static std::mutex m;
+    return m;
+  }
+  static std::map< std::string, TuneCand >& tune_cache()
+  {
+    static std::map< std::string, TuneCand > c;
+    return c;
+  }
+
+  std::string
+  tune_key( int rb ) const
+  {
+    int models = 0;
+    for ( const auto& b : blk )
+      models |= 1 << b.model;
+    int64_t nn = 0, ne = 0;
+    for ( const auto& nw : nets )
+    {
+      nn += nw.used ? nw.n : 0;
+      ne += nw.used ? nw.ne : 0;
+    }
+    const int64_t n_live = serving ? std::max< int64_t >( 1, nn ) : N;
+    const int64_t edges = serving ? ne : nnz_padded;
+    const double deg = ( double ) std::max< int64_t >( 1, edges ) / ( double ) std::max< int64_t >( 1, n_live );
+    char buf[ 160 ];
+    std::snprintf( buf, sizeof( buf ), "p%d m%d n%d k%d r%d md%d L%d late%d g%d t%d s%d", prec, models,
+      ( int ) std::floor( std::log2( ( double ) n_live ) ), ( int ) std::floor( std::log2( deg ) ), rb, cfg.min_delay,
+      L, late_min_cur != INT32_MAX ? 1 : 0, gather_on ? 1 : 0, tiled_on ? 1 : 0, serving ? 1 : 0 );
+    return buf;
+  }
+
+  void
+  apply_cand( const TuneCand& c )
+  {
+    upd_variant = c.variant;
+    deliver_group = c.group;
+    deliver_per_sm = c.per_sm;
+    apply_deliver();
+  }
+
+  // one group of `steps` steps with the current configuration: device time [us]
+  int
+  timed_group( int64_t steps, double* us, int64_t* spikes )
+  {
+    GroupInfo gi;
+    CU( cudaEventRecord( ev0, stream ) );
+    int rc = launch_group( steps, 0, gi );
+    if ( rc )
+      return rc;
+    CU( cudaEventRecord( ev1, stream ) );
+    const int64_t s0 = stats.spikes;
+    if ( ( rc = drain_group( 0, gi ) ) )
+      return rc;
+    float ms = 0;
+    CU( cudaEventElapsedTime( &ms, ev0, ev1 ) );
+    *us = 1e3 * ms;
+    if ( spikes )
+      *spikes = stats.spikes - s0;
+    return NG_OK;
+  }
+
+  int
+  autotune( int64_t& n, int64_t gmax )
+  {
+    const int64_t md = cfg.min_delay;
+    const int64_t S = std::max< int64_t >( 4, ( 64 + md - 1 ) / md );  // slices per trial group
+    const int64_t steps = S * md;
+    if ( steps > gmax )
+      return NG_OK;  // a trial group would not fit the spike log
+    bool iaf = false;
+    for ( const auto& b : blk )
+      iaf = iaf || b.model != NG_AEIF_COND_ALPHA;
+    std::vector< int > variants;
+    if ( iaf )
+    {
+      variants = { 0, 1 };
+      if ( md >= 3 && !gather_on && !tiled_on )
+      {
+        variants.push_back( 2 );
+        variants.push_back( 3 );
+      }
+    }
+    std::vector< int > per_sm;
+    for ( int p : { 1, 2, 4, 8 } )
+      if ( p <= occ_deliver )
+        per_sm.push_back( p );
+    if ( per_sm.back() != occ_deliver )
+      per_sm.push_back( occ_deliver );
+    const std::vector< int > groups = { 1, 2, 4, 8 };
+    if ( variants.empty() )
+      variants.push_back( upd_variant >= 0 ? upd_variant : 0 );
+    const int64_t n_cand = ( int64_t ) ( variants.size() + per_sm.size() + groups.size() );
+    // the probe (3 trial lengths) and the trials must fit the call's steps;
+    // otherwise wait for a longer call
+    if ( n < ( 3 + 2 * n_cand ) * steps || 3 * steps > gmax )
+      return NG_OK;
+    const int v0 = upd_variant >= 0 ? upd_variant : ( iaf ? default_variant( blk[ 0 ].n ) : 0 );
+    TuneCand best { v0, deliver_per_sm, deliver_group, 1e300 };
+    tune_log.clear();
+    int rc;
+    // a group with the current configuration: its spikes give the activity
+    // bucket (its time is not compared: a network's first slices often hold
+    // a transient burst)
+    int64_t spk = 0;
+    double probe_us = 0;
+    if ( ( rc = timed_group( 3 * steps, &probe_us, &spk ) ) )
+      return rc;
+    n -= 3 * steps;
+    trial_steps = steps;
+    int64_t n_live = N;
+    if ( serving )
+    {
+      n_live = 0;
+      for ( const auto& nw : nets )
+        n_live += nw.used ? nw.n : 0;
+      n_live = std::max< int64_t >( 1, n_live );
+    }
+    const double per_kstep = 1e3 * ( double ) spk / ( ( double ) n_live * ( double ) ( 3 * steps ) );
+    rate_bucket = per_kstep > 0 ? ( int ) std::floor( std::log2( per_kstep ) ) : -99;
+    const std::string key = tune_key( rate_bucket );
+    if ( tune_mode == 1 )
+    {
+      std::lock_guard< std::mutex > lock( tune_mutex() );
+      auto it = tune_cache().find( key );
+      if ( it != tune_cache().end() )
+      {
+        apply_cand( it->second );
+        tune_state = 2;
+        return NG_OK;
+      }
+    }
+    auto trial = [ & ]( TuneCand c, double* us ) -> int {
+      apply_cand( c );
+      double warm = 0;
+      int r = timed_group( steps, &warm, nullptr );
+      if ( r == NG_OK )
+        r = timed_group( steps, us, nullptr );
+      n -= 2 * steps;
+      return r;
+    };
+    for ( int pass = 0; pass < 3; ++pass )
+    {
+      const std::vector< int >& opts = pass == 0 ? variants : pass == 1 ? per_sm : groups;
+      TuneCand round_best = best;
+      for ( int o : opts )
+      {
+        TuneCand c = best;
+        if ( pass == 0 )
+          c.variant = o;
+        else if ( pass == 1 )
+          c.per_sm = o;
+        else
+          c.group = o;
+        if ( pass > 0 && c.variant == best.variant && c.per_sm == best.per_sm && c.group == best.group )
+          continue;  // measured in an earlier pass
+        if ( ( rc = trial( c, &c.us ) ) )
+          return rc;
+        tune_log.push_back( c );
+        if ( c.us < round_best.us )
+          round_best = c;
+      }
+      best = round_best;
+    }
+    apply_cand( best );
+    tune_state = 1;
+    {
+      std::lock_guard< std::mutex > lock( tune_mutex() );
+      tune_cache()[ key ] = best;
+    }
+    return NG_OK;
   }
 
   // keep: leave the last group running and undrained (asynchronous form);
@@ -1479,8 +1803,10 @@ struct ng_engine
   simulate( int64_t n, bool keep = false )
   {
     auto t0 = std::chrono::steady_clock::now();
-    int rc = prepare();
+    int rc = close_group();  // steps of slice-aligned calls still open
     if ( rc )
+      return rc;
+    if ( ( rc = prepare() ) )
       return rc;
     // group size: bounded by the spike-log and trace capacities
     // over S steps a recorded neuron logs at most S / (R + 1) + 1 entries
@@ -1509,6 +1835,24 @@ struct ng_engine
       const int64_t quarter = ( ( n / 4 + q - 1 ) / q ) * q;
       if ( quarter >= q && quarter < gmax )
         gmax = quarter;
+    }
+    // the autotuner runs on the first long enough call, at a slice boundary,
+    // with no group in flight and no tracing or profiling
+    bool live = nnz_padded > 0;
+    if ( serving )
+    {
+      live = false;
+      for ( const auto& nw : nets )
+        live = live || ( nw.used && nw.ne > 0 );
+    }
+    if ( tune_mode != 0 && tune_state == 0 && pend_sel < 0 && from == 0 && n_trace_idx == 0 && !profiling && live )
+    {
+      rc = autotune( n, gmax );
+      if ( rc )
+      {
+        cudaStreamSynchronize( stream );
+        return rc;
+      }
     }
     int pending = pend_sel;
     GroupInfo gi[ 2 ];
@@ -1564,7 +1908,7 @@ ng_internal_set_error( const char* msg )
 #define SETTLE( e )                                                                                                   \
   do                                                                                                                 \
   {                                                                                                                  \
-    if ( ( e ) && ( e )->pend_sel >= 0 )                                                                             \
+    if ( ( e ) && ( ( e )->pend_sel >= 0 || ( e )->og_sel >= 0 ) )                                                  \
     {                                                                                                                \
       const int rc_settle = ( e )->sync_pending();                                                                   \
       if ( rc_settle )                                                                                               \
@@ -1662,8 +2006,6 @@ ng_create( const ng_config* cfg, ng_engine** out )
   // are placed first where both wait for SM slots
   int lo = 0, hi = 0;
   cudaDeviceGetStreamPriorityRange( &lo, &hi );
-  if ( const char* mp = std::getenv( "NG_MAIN_PRIORITY" ) )
-    hi = std::atoi( mp ) ? hi : lo;
   if ( cudaStreamCreateWithPriority( &e->own, cudaStreamNonBlocking, hi ) != cudaSuccess )
     return bail( fail( NG_ERR_CUDA, "cudaStreamCreate failed" ) );
   e->stream = e->own;
@@ -1675,10 +2017,6 @@ ng_create( const ng_config* cfg, ng_engine** out )
       || cudaStreamCreateWithFlags( &e->adm_stream, cudaStreamNonBlocking ) != cudaSuccess
       || cudaEventCreateWithFlags( &e->ev_adm, cudaEventDisableTiming ) != cudaSuccess )
       return bail( fail( NG_ERR_CUDA, "ng_create: late-delivery stream or event creation failed" ) );
-    if ( const char* lt = std::getenv( "NG_LATE" ) )
-      e->late_env = std::atoi( lt ) != 0;
-    if ( const char* lp = std::getenv( "NG_LATE_PER_SM" ) )
-      e->late_per_sm = std::max( 1, std::atoi( lp ) );
   }
   cudaEventCreate( &e->ev0 );
   cudaEventCreate( &e->ev1 );
@@ -1794,9 +2132,8 @@ ng_create( const ng_config* cfg, ng_engine** out )
       cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< false, false >, 256, 0 );
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k_deliver< true, false >, 256, 0 );
-    e->deliver_per_sm = std::max( 1, std::min( occ, 8 ) );
-    if ( const char* dp = std::getenv( "NG_DELIVER_PER_SM" ) )
-      e->deliver_per_sm = std::max( 1, std::min( e->deliver_per_sm, std::atoi( dp ) ) );
+    e->occ_deliver = std::max( 1, std::min( occ, 8 ) );
+    e->deliver_per_sm = e->occ_deliver;
   }
   if ( cfg->serving )
   {
@@ -1806,23 +2143,10 @@ ng_create( const ng_config* cfg, ng_engine** out )
                                      "and 1 to 1024 network slots" ) );
     if ( ( rc = e->setup_serving() ) )
       return bail( rc );
+    e->deliver_want = INT64_MAX;
     e->deliver_ctas = e->sms * e->deliver_per_sm;
   }
   e->refresh_late();
-  if ( const char* sl = std::getenv( "NG_UPDATE_SUB" ) )
-    e->sub_lags = std::atoi( sl ) == 4 ? 4 : 8;
-  if ( const char* ml = std::getenv( "NG_MAX_LANES" ) )
-  {
-    const int v = std::atoi( ml );
-    if ( v == 1 || v == 32 )
-      e->max_lanes = v;
-  }
-  if ( const char* tn = std::getenv( "NG_ONE_THREAD_MIN_N" ) )
-  {
-    const long long v = std::atoll( tn );
-    if ( v > 0 )
-      e->one_thread_min_n = v;
-  }
   if ( cudaStreamSynchronize( e->stream ) != cudaSuccess )
     return bail( fail( NG_ERR_CUDA, "ng_create: device initialisation failed" ) );
   *out = e;
@@ -2085,12 +2409,10 @@ ng_set_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const i
   }
   if ( ( rc = e->resize_work() ) )
     return rc;
-  // delivery grid: one wave of resident CTAs, fewer for small graphs
-  const int64_t want = std::max< int64_t >( 1, e->chunks_all_src / 64 );
-  e->deliver_ctas = ( int ) std::min< int64_t >( want, ( int64_t ) e->sms * e->deliver_per_sm );
-  e->refresh_late();
+  // delivery grid: up to one wave of resident CTAs, fewer for small graphs
+  e->deliver_want = std::max< int64_t >( 1, e->chunks_all_src / 64 );
+  e->apply_deliver();
   CU( cudaStreamSynchronize( e->stream ) );
-  ++e->generation;
   return NG_OK;
 }
 
@@ -2339,6 +2661,25 @@ ng_simulate_async( ng_engine* e, int64_t n_steps )
 }
 
 int
+ng_update( ng_engine* e, int64_t origin, int32_t from, int32_t to )
+{
+  if ( !e )
+    return fail( NG_ERR_ARG, "ng_update: null engine" );
+  if ( e->serving )
+    return fail( NG_ERR_STATE, "ng_update: serving engines advance with ng_simulate" );
+  if ( from < 0 || to <= from || to > e->cfg.min_delay )
+    return fail( NG_ERR_ARG, "ng_update: need 0 <= from < to <= min_delay" );
+  if ( origin != e->origin || from != e->from )
+    return fail( NG_ERR_STATE, "ng_update: the engine stands at slice origin " + std::to_string( e->origin ) + ", lag "
+        + std::to_string( e->from ) + " (called with " + std::to_string( origin ) + ", " + std::to_string( from ) + ")" );
+  CU( cudaSetDevice( e->cfg.device ) );
+  const auto t0 = std::chrono::steady_clock::now();
+  const int rc = e->update_range( from, to );
+  e->stats.simulate_ms += std::chrono::duration< double, std::milli >( std::chrono::steady_clock::now() - t0 ).count();
+  return rc;
+}
+
+int
 ng_sync( ng_engine* e )
 {
   if ( !e )
@@ -2448,6 +2789,120 @@ ng_set_graph_slices( ng_engine* e, int32_t slices_per_graph )
     return fail( NG_ERR_ARG, "ng_set_graph_slices: bad argument" );
   e->graph_slices = slices_per_graph;
   ++e->generation;
+  return NG_OK;
+}
+
+int
+ng_set_tuning( ng_engine* e, int32_t mode, int32_t update_variant, int32_t deliver_ctas_per_sm,
+  int32_t deliver_chunks_per_warp )
+{
+  if ( !e )
+    return fail( NG_ERR_ARG, "null engine" );
+  if ( mode < 0 || mode > 2 || update_variant < -1 || update_variant > 3 || deliver_ctas_per_sm < -1
+    || deliver_ctas_per_sm == 0 || deliver_chunks_per_warp < -1 || deliver_chunks_per_warp == 0
+    || deliver_chunks_per_warp > 32 )
+    return fail( NG_ERR_ARG, "ng_set_tuning: mode 0..2, update_variant -1..3, per-SM CTAs and chunks per warp -1 or >= 1" );
+  int rc = e->sync_pending();
+  if ( rc )
+    return rc;
+  cudaSetDevice( e->cfg.device );
+  e->tune_mode = mode;
+  if ( mode == 0 )
+  {
+    e->upd_variant = update_variant;
+    e->deliver_per_sm = deliver_ctas_per_sm > 0 ? std::min( deliver_ctas_per_sm, e->occ_deliver ) : e->occ_deliver;
+    e->deliver_group = deliver_chunks_per_warp > 0 ? deliver_chunks_per_warp : 4;
+    e->tune_state = 3;
+  }
+  else
+  {
+    e->tune_state = 0;  // measured again at the next long enough call
+  }
+  e->tune_log.clear();
+  e->apply_deliver();
+  return NG_OK;
+}
+
+int
+ng_get_tuning( ng_engine* e, ng_tuning* out )
+{
+  if ( !e || !out )
+    return fail( NG_ERR_ARG, "null argument" );
+  std::memset( out, 0, sizeof( *out ) );
+  out->mode = e->tune_mode == 0 ? 0 : 1;
+  out->state = e->tune_state;
+  bool iaf = false;
+  for ( const auto& b : e->blk )
+    iaf = iaf || b.model != NG_AEIF_COND_ALPHA;
+  out->update_variant = !iaf ? 4 : e->upd_variant >= 0 ? e->upd_variant : ng_engine::default_variant( e->blk[ 0 ].n );
+  out->deliver_per_sm = e->deliver_per_sm;
+  out->deliver_group = e->deliver_group;
+  out->cache_hit = e->tune_state == 2 ? 1 : 0;
+  out->rate_bucket = e->rate_bucket;
+  out->trial_steps = e->trial_steps;
+  const int nc = ( int ) std::min< size_t >( e->tune_log.size(), NG_TUNE_MAX_CANDIDATES );
+  out->n_candidates = nc;
+  for ( int k = 0; k < nc; ++k )
+  {
+    const auto& c = e->tune_log[ ( size_t ) k ];
+    out->cand_variant[ k ] = iaf ? c.variant : 4;
+    out->cand_per_sm[ k ] = c.per_sm;
+    out->cand_group[ k ] = c.group;
+    out->cand_us_per_slice[ k ] = e->trial_steps > 0 ? c.us * e->cfg.min_delay / ( double ) e->trial_steps : 0.0;
+  }
+  return NG_OK;
+}
+
+int
+ng_set_option( ng_engine* e, const char* name, double value )
+{
+  if ( !e || !name )
+    return fail( NG_ERR_ARG, "null argument" );
+  int rc = e->sync_pending();
+  if ( rc )
+    return rc;
+  cudaSetDevice( e->cfg.device );
+  const std::string nm( name );
+  if ( nm == "late_delivery" )
+  {
+    e->late_env = value != 0.0;
+    e->refresh_late();
+    ++e->generation;
+  }
+  else if ( nm == "late_ctas_per_sm" )
+  {
+    if ( !( value >= 1 ) )
+      return fail( NG_ERR_ARG, "late_ctas_per_sm must be >= 1" );
+    e->late_per_sm = ( int ) value;
+    e->refresh_late();
+    ++e->generation;
+  }
+  else if ( nm == "gather" || nm == "gather_frac" )
+  {
+    if ( !e->serving )
+      return fail( NG_ERR_STATE, "the per-target gather belongs to serving engines in the FP32 form" );
+    for ( const auto& nw : e->nets )
+      if ( nw.used )
+        return fail( NG_ERR_STATE, "the per-target gather is set before any network is admitted" );
+    if ( nm == "gather" )
+    {
+      if ( value != 0.0 && !e->gather_on )
+        return fail( NG_ERR_STATE, "this engine has no per-target gather (FP32 serving form, min_delay <= 16)" );
+      e->gather_on = e->gather_on && value != 0.0;
+    }
+    else
+    {
+      if ( !( value >= 0 ) )
+        return fail( NG_ERR_ARG, "gather_frac must be >= 0" );
+      e->gather_frac = ( float ) value;
+    }
+    e->refresh_late();
+    ++e->generation;
+  }
+  else
+  {
+    return fail( NG_ERR_UNKNOWN_NAME, "unknown option: " + nm + " (late_delivery, late_ctas_per_sm, gather, gather_frac)" );
+  }
   return NG_OK;
 }
 
@@ -3054,7 +3509,7 @@ ng_net_spikes( ng_engine* e, int32_t id, int32_t* source, int64_t* stamp, int64_
   if ( !n_out || cap < 0 || ( source && !stamp ) )
     return fail( NG_ERR_ARG, "ng_net_spikes: bad argument" );
   auto& nw = e->nets[ id ];
-  if ( nw.until > e->pend_gi.clock )
+  if ( e->og_sel >= 0 || nw.until > e->pend_gi.clock )
     SETTLE( e );  // the running group may hold spikes of this network
   if ( !source )
   {
@@ -3226,7 +3681,7 @@ ng_net_remove( ng_engine* e, int32_t id )
   int rc = net_check( e, id );
   if ( rc )
     return rc;
-  if ( e->nets[ id ].until > e->pend_gi.clock )
+  if ( e->og_sel >= 0 || e->nets[ id ].until > e->pend_gi.clock )
     SETTLE( e );  // the running group may hold spikes of this network
   cudaSetDevice( e->cfg.device );
   auto& nw = e->nets[ id ];

@@ -159,6 +159,7 @@ struct Net
   const int64_t* sched_step;
   const int32_t* sched_src;
   int64_t n_sched;
+  int32_t deliver_group;  // most edge chunks one delivery warp takes per descriptor load (autotuned)
   Ctl* ctl;
 };
 

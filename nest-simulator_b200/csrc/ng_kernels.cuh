@@ -923,13 +923,18 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
 // ballot.  Same arithmetic, in the same order, as k_update_iaf.
 // ---------------------------------------------------------------------
 constexpr int P2_NB = 32;  // neurons per CTA
-constexpr int P2_CH = 32;  // lags per chunk
 
-template < typename Real, bool FIX, int MODEL >
-__global__ void __launch_bounds__( 256 )
+// TPB threads per CTA, CH lags per chunk (the autotuner picks between
+// 256 threads with chunks of 32 lags and 128 threads with chunks of 16:
+// the same phase-1 items per thread, half the CTA -- more CTAs resident
+// per SM where the registers of the 256-thread form allow only one)
+template < typename Real, bool FIX, int MODEL, int TPB, int CH >
+__global__ void __launch_bounds__( TPB )
 k_update_iaf2( Net d, Block b, int from, int to, int sched )
 {
   constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
+  constexpr int P2_CH = CH;
+  static_assert( TPB % 32 == 0 && CH <= 32 && ( CH * P2_NB ) % TPB == 0, "two-phase update shape" );
   __shared__ Real s_ex[ P2_CH ][ P2_NB ];
   __shared__ Real s_in[ EXP ? P2_CH : 1 ][ P2_NB ];
   const long long origin = cta_origin( d );
@@ -986,7 +991,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
     }
     r = b.r[ li ];
   }
-  // phase 1 items j = threadIdx.x + m * 256 all belong to neuron nb0 + (threadIdx.x & 31)
+  // phase 1 items j = threadIdx.x + m * TPB all belong to neuron nb0 + (threadIdx.x & 31)
   DriveCtx dc;
   dc.n = 0;
   if ( nb0 + ( threadIdx.x & 31 ) < b.n )
@@ -998,16 +1003,16 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
     const long long t0 = origin + cb;
     const int slot0 = ( int ) ( t0 % d.L );
     // ---- phase 1: inputs of (neuron q, lag k), item j = k * 32 + q; a
-    // thread's items j = threadIdx.x + m * 256 (m < 4): all ring reads and
-    // draws first, then their use, then the clears
-    constexpr int P1_MAX = P2_CH * P2_NB / 256;
+    // thread's items j = threadIdx.x + m * TPB (m < P1_MAX): all ring reads
+    // and draws first, then their use, then the clears
+    constexpr int P1_MAX = P2_CH * P2_NB / TPB;
     typename RingVal< FIX >::type rex[ P1_MAX ], rin[ P1_MAX ];
     Real dvs[ P1_MAX ];
     int slots[ P1_MAX ];
 #pragma unroll
     for ( int m = 0; m < P1_MAX; ++m )
     {
-      const int j = threadIdx.x + m * 256;
+      const int j = threadIdx.x + m * TPB;
       rex[ m ] = 0;
       rin[ m ] = 0;
       dvs[ m ] = Real( 0 );
@@ -1033,7 +1038,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
 #pragma unroll
     for ( int m = 0; m < P1_MAX; ++m )
     {
-      const int j = threadIdx.x + m * 256;
+      const int j = threadIdx.x + m * TPB;
       if ( j >= nl * P2_NB )
         continue;
       const int k = j >> 5;
@@ -1069,7 +1074,7 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
     {
       if ( slots[ m ] < 0 )
         continue;
-      const int64_t iq = b.off + nb0 + ( ( threadIdx.x + m * 256 ) & 31 );
+      const int64_t iq = b.off + nb0 + ( ( threadIdx.x + m * TPB ) & 31 );
       ring_clear< FIX >( d, slots[ m ], 0, iq );
       if constexpr ( EXP )
         ring_clear< FIX >( d, slots[ m ], 1, iq );
@@ -1562,9 +1567,10 @@ k_deliver( Net d )
   const int lane = threadIdx.x & 31;
   const long long nwarps = ( ( long long ) gridDim.x * blockDim.x ) >> 5;
   const long long gw = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
-  // chunks per group: at most 4, so the warps sweep the list together (the
-  // chunks of one network, queued together, are delivered together)
-  const long long G = max( 1ll, min( 4ll, nent / nwarps ) );
+  // chunks per group: at most deliver_group (autotuned, 1 to 8), so the
+  // warps sweep the list together (the chunks of one network, queued
+  // together, are delivered together)
+  const long long G = max( 1ll, min( ( long long ) d.deliver_group, nent / nwarps ) );
   for ( long long base = gw * G; base < nent; base += nwarps * G )
   {
     const int cnt = ( int ) min( G, nent - base );

@@ -14,9 +14,15 @@
 //
 // The kernels are variants of the engine's node-update and delivery kernels
 // (ng_kernels.cuh) for unpadded CSR input: same arithmetic in the same order,
-// so a run matches ng_simulate on the same network.
+// so a run matches ng_simulate on the same network.  A controller that steps
+// the network a few steps per tick sets continue_run: the ring buffer and
+// the open slice's spikes stay in the scratch array between its calls, and
+// a chain of calls equals one call over the same steps.  The edges come from
+// caller memory and are range-checked on the device before they index the
+// ring.
 #include <cstddef>
 #include <cstdint>
+#include <algorithm>
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -33,14 +39,25 @@ __device__ __align__( 256 ) unsigned char g_noalloc_scratch[ NG_NOALLOC_SCRATCH_
 // counters at the start of the scratch array
 struct NaCtl
 {
-  unsigned long long n_spk;  // spikes of the open slice
-  unsigned long long n_out;  // spikes written to the caller's output
+  unsigned long long n_spk;   // spikes of the open slice
+  unsigned long long n_out;   // spikes of this call (written to the caller's output up to out_cap)
+  unsigned long long n_skip;  // edges of this call skipped for an out-of-range target or delay
+};
+
+// Where the previous call on a device stopped, for continue_run: the
+// scratch array holds that run's ring and open-slice spike list.
+struct NaRun
+{
+  bool valid = false;
+  int64_t n = 0;
+  int32_t min_delay = 0, max_delay = 0;
+  int64_t next_step = 0;
 };
 
 struct NaNet
 {
   int64_t n;
-  int32_t L, min_delay;
+  int32_t L, min_delay, max_delay;
   const double *P33, *P30, *V_th, *V_reset, *V_min, *I_e;
   const int32_t* refr_counts;
   double* V;
@@ -53,6 +70,7 @@ struct NaNet
   int64_t* out_stamp;
   int64_t out_cap;
   unsigned long long* out_count;
+  unsigned long long* out_skipped;
   // scratch
   NaCtl* ctl;
   double* ring;     // [L][n]
@@ -109,7 +127,9 @@ k_na_update( NaNet d, long long origin, int from, int to )
 }
 
 // Delivery of the closing slice: one warp per spike walks its CSR row and
-// adds the weights into ring[(t_emit + d) mod L][target].
+// adds the weights into ring[(t_emit + d) mod L][target].  The edges come
+// from caller memory: one whose target or delay is out of range would index
+// outside the ring, so it is skipped and counted instead.
 __global__ void
 k_na_deliver( NaNet d )
 {
@@ -124,10 +144,17 @@ k_na_deliver( NaNet d )
     const int64_t e0 = d.row_ptr[ sp.x ], e1 = d.row_ptr[ sp.x + 1 ];
     for ( int64_t e = e0 + lane; e < e1; e += 32 )
     {
-      int slot = sp.y + d.delay[ e ];
+      const int32_t tg = d.target[ e ];
+      const int32_t dl = d.delay[ e ];
+      if ( tg < 0 || ( int64_t ) tg >= d.n || dl < d.min_delay || dl > d.max_delay )
+      {
+        atomicAdd( &d.ctl->n_skip, 1ull );
+        continue;
+      }
+      int slot = sp.y + dl;  // sp.y < L and dl <= max_delay < L
       if ( slot >= d.L )
         slot -= d.L;
-      atomicAdd( d.ring + ( int64_t ) slot * d.n + d.target[ e ], d.weight[ e ] );
+      atomicAdd( d.ring + ( int64_t ) slot * d.n + tg, d.weight[ e ] );
     }
   }
 }
@@ -138,14 +165,26 @@ k_na_close_slice( NaNet d )
   d.ctl->n_spk = 0ull;
 }
 
+// A continued run keeps the ring and the open slice's spikes; only the
+// per-call counters start from zero.
+__global__ void
+k_na_begin_call( NaNet d )
+{
+  d.ctl->n_out = 0ull;
+  d.ctl->n_skip = 0ull;
+}
+
 __global__ void
 k_na_finish( NaNet d )
 {
   *d.out_count = d.ctl->n_out;
+  if ( d.out_skipped )
+    *d.out_skipped = d.ctl->n_skip;
 }
 
 std::mutex g_na_mutex;
 void* g_na_addr[ NA_MAX_DEVICES ] = {};
+NaRun g_na_run[ NA_MAX_DEVICES ];
 
 }  // namespace
 
@@ -161,16 +200,23 @@ ng_simulate_noalloc( const ng_noalloc_net* net, int64_t n_steps, void* cuda_stre
     ng_internal_set_error( "ng_simulate_noalloc: null network or negative step count" );
     return NG_ERR_ARG;
   }
-  if ( net->n < 1 || net->min_delay < 1 || net->max_delay < net->min_delay || net->start_step < 0
-    || net->start_step % net->min_delay != 0 || net->out_cap < 0 )
+  if ( net->n < 1 || net->n > INT32_MAX || net->min_delay < 1 || net->max_delay < net->min_delay
+    || net->start_step < 0 || net->out_cap < 0 || ( net->continue_run != 0 && net->continue_run != 1 )
+    || net->reserved != 0 )
   {
-    ng_internal_set_error( "ng_simulate_noalloc: need n >= 1, 1 <= min_delay <= max_delay, start_step a "
-                           "non-negative multiple of min_delay" );
+    ng_internal_set_error( "ng_simulate_noalloc: need 1 <= n < 2^31, 1 <= min_delay <= max_delay, start_step >= 0, "
+                           "out_cap >= 0, continue_run 0 or 1, reserved 0" );
+    return NG_ERR_ARG;
+  }
+  if ( !net->continue_run && net->start_step % net->min_delay != 0 )
+  {
+    ng_internal_set_error( "ng_simulate_noalloc: a fresh run starts at a slice boundary (start_step a multiple of "
+                           "min_delay)" );
     return NG_ERR_ARG;
   }
   if ( !net->P33 || !net->P30 || !net->V_th_rel || !net->V_reset_rel || !net->V_min_rel || !net->I_e
-    || !net->refr_counts || !net->V_m_rel || !net->r || !net->row_ptr || !net->out_src || !net->out_stamp
-    || !net->out_count )
+    || !net->refr_counts || !net->V_m_rel || !net->r || !net->row_ptr || !net->target || !net->weight || !net->delay
+    || !net->out_src || !net->out_stamp || !net->out_count )
   {
     ng_internal_set_error( "ng_simulate_noalloc: a required device pointer is null" );
     return NG_ERR_ARG;
@@ -187,33 +233,40 @@ ng_simulate_noalloc( const ng_noalloc_net* net, int64_t n_steps, void* cuda_stre
   const size_t ring_bytes = ( size_t ) L * ( size_t ) net->n * sizeof( double );
   const size_t spk_cap = ( size_t ) net->n * ( size_t ) net->min_delay;
   const size_t need = ctl_bytes + ( ( ring_bytes + 255 ) & ~( size_t ) 255 ) + spk_cap * sizeof( int2 );
-  if ( need > NG_NOALLOC_SCRATCH_BYTES )
+  if ( L > INT32_MAX / 2 || need > NG_NOALLOC_SCRATCH_BYTES )
   {
     ng_internal_set_error( "ng_simulate_noalloc: the network's ring buffer and spike list need more than the "
                            "16 MiB static scratch array (NG_NOALLOC_SCRATCH_BYTES)" );
     return NG_ERR_CAPACITY;
   }
-  void* base = nullptr;
+  std::lock_guard< std::mutex > lock( g_na_mutex );
+  // once per device, with that device current: the scratch array's device
+  // address (the symbol itself names a host-side stand-in)
+  if ( !g_na_addr[ dev ] )
   {
-    // once per device, with that device current: the scratch array's device
-    // address (the symbol itself names a host-side stand-in)
-    std::lock_guard< std::mutex > lock( g_na_mutex );
-    if ( !g_na_addr[ dev ] )
+    if ( cudaGetSymbolAddress( &g_na_addr[ dev ], g_noalloc_scratch ) != cudaSuccess )
     {
-      if ( cudaGetSymbolAddress( &g_na_addr[ dev ], g_noalloc_scratch ) != cudaSuccess )
-      {
-        g_na_addr[ dev ] = nullptr;
-        ng_internal_set_error( "ng_simulate_noalloc: cudaGetSymbolAddress of the scratch array failed" );
-        return NG_ERR_CUDA;
-      }
+      g_na_addr[ dev ] = nullptr;
+      ng_internal_set_error( "ng_simulate_noalloc: cudaGetSymbolAddress of the scratch array failed" );
+      return NG_ERR_CUDA;
     }
-    base = g_na_addr[ dev ];
+  }
+  void* const base = g_na_addr[ dev ];
+  NaRun& run = g_na_run[ dev ];
+  if ( net->continue_run
+    && !( run.valid && run.n == net->n && run.min_delay == net->min_delay && run.max_delay == net->max_delay
+      && run.next_step == net->start_step ) )
+  {
+    ng_internal_set_error( "ng_simulate_noalloc: continue_run needs the previous call on this device to have run the "
+                           "same network (n, min_delay, max_delay) up to start_step" );
+    return NG_ERR_STATE;
   }
   cudaStream_t st = ( cudaStream_t ) cuda_stream;
   NaNet d {};
   d.n = net->n;
   d.L = ( int32_t ) L;
   d.min_delay = net->min_delay;
+  d.max_delay = net->max_delay;
   d.P33 = net->P33;
   d.P30 = net->P30;
   d.V_th = net->V_th_rel;
@@ -231,31 +284,53 @@ ng_simulate_noalloc( const ng_noalloc_net* net, int64_t n_steps, void* cuda_stre
   d.out_stamp = net->out_stamp;
   d.out_cap = net->out_cap;
   d.out_count = net->out_count;
+  d.out_skipped = net->out_skipped;
   d.ctl = ( NaCtl* ) base;
   d.ring = ( double* ) ( ( unsigned char* ) base + ctl_bytes );
   d.spk = ( int2* ) ( ( unsigned char* ) base + ctl_bytes + ( ( ring_bytes + 255 ) & ~( size_t ) 255 ) );
   d.spk_cap = ( int64_t ) spk_cap;
-  // every call starts a fresh run: counters and ring buffer to zero
-  if ( cudaMemsetAsync( base, 0, ctl_bytes + ring_bytes, st ) != cudaSuccess )
+  // until this call has been enqueued, no later call may continue its run
+  run.valid = false;
+  cudaError_t ce;
+  if ( net->continue_run )
+  {
+    k_na_begin_call<<< 1, 1, 0, st >>>( d );
+    ce = cudaGetLastError();
+  }
+  else
+  {
+    // a fresh run: counters and ring buffer to zero
+    ce = cudaMemsetAsync( base, 0, ctl_bytes + ring_bytes, st );
+  }
+  if ( ce != cudaSuccess )
   {
     ng_internal_set_error( "ng_simulate_noalloc: clearing the scratch array failed" );
     return NG_ERR_CUDA;
   }
   const unsigned ugrid = ( unsigned ) ( ( net->n + 255 ) / 256 );
   const unsigned dgrid = 64;
-  long long origin = net->start_step;
+  // slice origin and the lag the run stands at (a continued run may stop
+  // and resume inside a slice; fresh runs start at a slice boundary)
+  const int64_t lag0 = net->start_step % net->min_delay;
+  long long origin = net->start_step - lag0;
+  int from = ( int ) lag0;
   int64_t left = n_steps;
   while ( left > 0 )
   {
-    const int to = ( int ) ( left < net->min_delay ? left : net->min_delay );
-    k_na_update<<< ugrid, 256, 0, st >>>( d, origin, 0, to );
+    const int to = ( int ) std::min< int64_t >( ( int64_t ) from + left, net->min_delay );
+    k_na_update<<< ugrid, 256, 0, st >>>( d, origin, from, to );
+    left -= to - from;
     if ( to == net->min_delay )
     {
       k_na_deliver<<< dgrid, 256, 0, st >>>( d );
       k_na_close_slice<<< 1, 1, 0, st >>>( d );
+      origin += net->min_delay;
+      from = 0;
     }
-    origin += to;
-    left -= to;
+    else
+    {
+      from = to;
+    }
   }
   k_na_finish<<< 1, 1, 0, st >>>( d );
   if ( cudaGetLastError() != cudaSuccess )
@@ -263,6 +338,11 @@ ng_simulate_noalloc( const ng_noalloc_net* net, int64_t n_steps, void* cuda_stre
     ng_internal_set_error( "ng_simulate_noalloc: kernel launch failed" );
     return NG_ERR_CUDA;
   }
+  run.valid = true;
+  run.n = net->n;
+  run.min_delay = net->min_delay;
+  run.max_delay = net->max_delay;
+  run.next_step = net->start_step + n_steps;
   return NG_OK;
 }
 

@@ -33,7 +33,7 @@ EXPORTED = [
     "ng_simulate", "ng_simulate_async", "ng_sync", "ng_spike_count", "ng_get_spikes", "ng_trace_count", "ng_get_trace", "ng_get_stats",
     "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients", "ng_net_add", "ng_net_poll",
     "ng_net_spikes", "ng_net_get_var", "ng_net_get_connections", "ng_net_remove", "ng_net_capacity",
-    "ng_simulate_noalloc",
+    "ng_simulate_noalloc", "ng_set_tuning", "ng_get_tuning", "ng_set_option", "ng_update",
 ]
 
 
@@ -230,6 +230,10 @@ def load():
         "ng_net_get_connections": ([P, i32, P, P, P, P, i64, P], ctypes.c_int),
         "ng_net_remove": ([P, i32], ctypes.c_int),
         "ng_net_capacity": ([P, P, P], ctypes.c_int),
+        "ng_set_tuning": ([P, i32, i32, i32, i32], ctypes.c_int),
+        "ng_get_tuning": ([P, P], ctypes.c_int),
+        "ng_set_option": ([P, ctypes.c_char_p, dbl], ctypes.c_int),
+        "ng_update": ([P, i64, i32, i32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -252,6 +256,45 @@ def device_count():
     n = ctypes.c_int32(0)
     rc = load().ng_device_count(ctypes.byref(n))
     return n.value if rc == NG_OK else 0
+
+
+class NGTuning(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32),
+        ("state", ctypes.c_int32),
+        ("update_variant", ctypes.c_int32),
+        ("deliver_per_sm", ctypes.c_int32),
+        ("deliver_group", ctypes.c_int32),
+        ("cache_hit", ctypes.c_int32),
+        ("rate_bucket", ctypes.c_int32),
+        ("n_candidates", ctypes.c_int32),
+        ("cand_variant", ctypes.c_int32 * 32),
+        ("cand_per_sm", ctypes.c_int32 * 32),
+        ("cand_group", ctypes.c_int32 * 32),
+        ("cand_us_per_slice", ctypes.c_double * 32),
+        ("trial_steps", ctypes.c_int64),
+    ]
+
+
+UPDATE_VARIANTS = {0: "k_update_iaf (one thread per neuron, 4 lags of inputs at a time)",
+                   1: "k_update_iaf (one thread per neuron, 8 lags of inputs at a time)",
+                   2: "k_update_iaf2 (two-phase, 32 neurons per 256-thread CTA)",
+                   3: "k_update_iaf2 (two-phase, 32 neurons per 128-thread CTA)",
+                   4: "k_update_aeif"}
+UPDATE_KERNELS = {0: "k_update_iaf", 1: "k_update_iaf", 2: "k_update_iaf2", 3: "k_update_iaf2", 4: "k_update_aeif"}
+
+
+def tuning_dict(t):
+    n = t.n_candidates
+    return {"mode": ["fixed", "auto"][t.mode] if t.mode in (0, 1) else t.mode,
+            "state": ["pending", "tuned", "cached", "fixed"][t.state] if 0 <= t.state < 4 else t.state,
+            "update_variant": t.update_variant, "update_kernel": UPDATE_KERNELS.get(t.update_variant, "?"),
+            "update_variant_name": UPDATE_VARIANTS.get(t.update_variant, "?"),
+            "deliver_ctas_per_sm": t.deliver_per_sm, "deliver_chunks_per_warp": t.deliver_group,
+            "rate_bucket": t.rate_bucket, "trial_steps": t.trial_steps,
+            "candidates": [{"update_variant": t.cand_variant[k], "deliver_ctas_per_sm": t.cand_per_sm[k],
+                            "deliver_chunks_per_warp": t.cand_group[k], "us_per_slice": t.cand_us_per_slice[k]}
+                           for k in range(n)]}
 
 
 class Engine:
@@ -362,6 +405,10 @@ class Engine:
         """Enqueue n_steps; the last group still runs when this returns."""
         check(self.L.ng_simulate_async(self.handle, int(n_steps)))
 
+    def update(self, origin, frm, to):
+        """Steps [frm, to) of the slice at `origin` (Node::update), enqueued."""
+        check(self.L.ng_update(self.handle, int(origin), int(frm), int(to)))
+
     def sync(self):
         check(self.L.ng_sync(self.handle))
 
@@ -390,6 +437,22 @@ class Engine:
         s = NGStats()
         check(self.L.ng_get_stats(self.handle, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in NGStats._fields_}
+
+    def tuned(self):
+        """The launch configuration the engine runs with (and, once the
+        autotuner has run, what it measured)."""
+        t = NGTuning()
+        check(self.L.ng_get_tuning(self.handle, ctypes.byref(t)))
+        return tuning_dict(t)
+
+    def set_tuning(self, mode=1, update_variant=-1, deliver_ctas_per_sm=-1, deliver_chunks_per_warp=-1):
+        """mode 1: autotune (process cache first), 2: autotune ignoring the
+        cache, 0: fixed configuration (-1: the defaults)."""
+        check(self.L.ng_set_tuning(self.handle, int(mode), int(update_variant), int(deliver_ctas_per_sm),
+                                   int(deliver_chunks_per_warp)))
+
+    def set_option(self, name, value):
+        check(self.L.ng_set_option(self.handle, name.encode(), float(value)))
 
     def set_profiling(self, on):
         check(self.L.ng_set_profiling(self.handle, 1 if on else 0))

@@ -4,12 +4,20 @@
 # for pinning the oracle's and the engine's FP64 coefficients.  The
 # reference's build system is not used; its generated config.h is replaced by
 # an empty header (these two files need none of its macros).
-# Usage: oracle/build_ref.sh [reference root, default /root/reference]
+# Usage: oracle/build_ref.sh [--if-present] [reference root]
+# The reference root defaults to $NEST_REFERENCE_ROOT, else /root/reference.
+# With --if-present a missing source tree is not an error (nothing is built).
 set -e
-REF=${1:-/root/reference}
+IF_PRESENT=0
+if [ "$1" = "--if-present" ]; then IF_PRESENT=1; shift; fi
+REF=${1:-${NEST_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
-[ -f "$REF/libnestutil/iaf_propagator.cpp" ] || { echo "reference sources not found under $REF" >&2; exit 1; }
+if [ ! -f "$REF/libnestutil/iaf_propagator.cpp" ]; then
+  [ "$IF_PRESENT" = 1 ] && exit 0
+  echo "reference sources not found under $REF" >&2
+  exit 1
+fi
 mkdir -p "$OUT/include"
 : > "$OUT/include/config.h"
 CXX=${CXX:-/usr/bin/g++}

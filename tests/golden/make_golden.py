@@ -3,9 +3,10 @@
 This script is run once, in a container where the reference NEST
 (nest-simulator 3.10.0-post0.dev0) is importable as PyNEST, e.g.
 
-    PYTHONPATH=/tmp/nestinstall/lib/python3.12/site-packages python tests/golden/make_golden.py
+    NEST_REFERENCE_ROOT=<reference source tree> \
+    PYTHONPATH=<install prefix>/lib/python3.12/site-packages python tests/golden/make_golden.py [fixture ...]
 
-(the PyNEST install was built from /root/reference with CMake, GSL off,
+(the PyNEST install was built from the reference's sources with CMake, GSL off,
 OpenMP on).  It writes small ``.npz`` files that the test
 suite reads on any machine; the reference is never needed at test time.
 
@@ -46,7 +47,8 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+# the reference's source tree (its test-suite data files are read from it)
+REF = os.environ.get("NEST_REFERENCE_ROOT", "")
 
 
 def _nest():

@@ -20,8 +20,7 @@ from nestgpu import _abi
 pytestmark = pytest.mark.gpu
 
 
-def _static_run(monkeypatch, late, precision, model=_abi.NG_IAF_PSC_EXP, md=2):
-    monkeypatch.setenv("NG_LATE", "1" if late else "0")
+def _static_run(late, precision, model=_abi.NG_IAF_PSC_EXP, md=2):
     n, maxd = 3000, 30
     rng = np.random.default_rng(11)
     deg = rng.integers(40, 160, n)
@@ -30,6 +29,7 @@ def _static_run(monkeypatch, late, precision, model=_abi.NG_IAF_PSC_EXP, md=2):
     tgt = rng.integers(0, n, nnz)
     d = rng.integers(md, maxd + 1, nnz)
     eng = _abi.Engine([(model, n)], 0.1, md, maxd, precision=precision)
+    eng.set_option("late_delivery", 1 if late else 0)
     if model == _abi.NG_AEIF_COND_ALPHA:
         w = rng.choice([1.0, 0.5, -2.0, -4.0], nnz)                # nS
         eng.set_var(0, "tau_syn_ex", np.full(n, 1.0))
@@ -56,7 +56,6 @@ def _static_run(monkeypatch, late, precision, model=_abi.NG_IAF_PSC_EXP, md=2):
     V = eng.get_var(0, "V_m" if model == _abi.NG_AEIF_COND_ALPHA else "V_m_rel")
     st = eng.stats()
     eng.close()
-    monkeypatch.delenv("NG_LATE")
     return s, t, V, st
 
 
@@ -67,9 +66,9 @@ def _static_run(monkeypatch, late, precision, model=_abi.NG_IAF_PSC_EXP, md=2):
     (_abi.NG_FP64, _abi.NG_IAF_PSC_DELTA, 3),
     (_abi.NG_FP64, _abi.NG_AEIF_COND_ALPHA, 2),  # RKF45 kernel, per-spike appends
 ])
-def test_late_delivery_static_engine(monkeypatch, precision, model, md):
-    s0, t0, V0, st0 = _static_run(monkeypatch, False, precision, model, md)
-    s1, t1, V1, st1 = _static_run(monkeypatch, True, precision, model, md)
+def test_late_delivery_static_engine(precision, model, md):
+    s0, t0, V0, st0 = _static_run(False, precision, model, md)
+    s1, t1, V1, st1 = _static_run(True, precision, model, md)
     assert len(s0) > 500
     assert st0["syn_events"] == st1["syn_events"]
     o0, o1 = np.lexsort((s0, t0)), np.lexsort((s1, t1))
@@ -84,11 +83,11 @@ PB_P = np.array([[0.05, 0.10, 0.02],
                  [0.01, 0.30, 0.08]])
 
 
-def _serving_run(monkeypatch, late):
-    monkeypatch.setenv("NG_LATE", "1" if late else "0")
+def _serving_run(late):
     n = sum(PB_SIZES)
     eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, 20_000)], 0.1, 1, 40, precision=_abi.NG_FP32, serving=True,
                       max_networks=4, edge_capacity=30_000_000, max_abs_weight=1000.0)
+    eng.set_option("late_delivery", 1 if late else 0)
     pb = _abi.NGPairwiseBernoulli.make(PB_SIZES, (1, 0, 1), PB_P, w_mean=(-351.2, 87.8), w_sd=(35.12, 8.78),
                                        d_mean_ms=(0.75, 1.5), d_sd_ms=(0.375, 0.75), d_max_ms=3.95, seed=21)
     V0 = np.random.default_rng(8).uniform(0.0, 14.0, n)
@@ -107,13 +106,12 @@ def _serving_run(monkeypatch, late):
     conn = eng.net_get_connections(a)
     st = eng.stats()
     eng.close()
-    monkeypatch.delenv("NG_LATE")
     return out, conn, st
 
 
-def test_late_delivery_serving_engine(monkeypatch):
-    ref, c0, st0 = _serving_run(monkeypatch, False)
-    got, c1, st1 = _serving_run(monkeypatch, True)
+def test_late_delivery_serving_engine():
+    ref, c0, st0 = _serving_run(False)
+    got, c1, st1 = _serving_run(True)
     assert st0["syn_events"] == st1["syn_events"]
     for ((s0, t0), v0), ((s1, t1), v1) in zip(ref, got):
         assert len(s0) > 500

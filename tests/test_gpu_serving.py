@@ -252,30 +252,28 @@ def test_get_connections_of_explicit_graph():
     np.testing.assert_array_equal(dd[b], d[a])
 
 
-@pytest.mark.parametrize("frac", ["0", "0.03"])
-def test_gather_equals_scatter(monkeypatch, frac):
+@pytest.mark.parametrize("frac", [0.0, 0.03])
+def test_gather_equals_scatter(frac):
     """The per-target gather (always on with fraction 0; switching per slice
     with 0.03) gives the scatter's spikes and state bit for bit: both add the
     same integers into the int64 rings."""
-    def run(env):
-        for k, v in env.items():
-            monkeypatch.setenv(k, v)
+    def run(opts):
         eng = serving.new_engine("fp32", capacity_neurons=100_000, capacity_edges=40_000_000, max_networks=8)
+        for k, v in opts.items():
+            eng.set_option(k, v)
         ids = [serving._admit(eng, _req(i, n, 1500, seed=500 + i, g=g, eta=eta))
                for i, (n, g, eta) in enumerate(((4000, 3.5, 1.8), (7000, 5.0, 1.2), (2500, 6.0, 2.0)))]
         eng.simulate(1500)
         out = [(eng.net_spikes(i), eng.net_get_var(i, "V_m_rel", n)) for i, n in zip(ids, (4000, 7000, 2500))]
         st = eng.stats()
         eng.close()
-        for k in env:
-            monkeypatch.delenv(k)
         return out, st
 
-    ref, st0 = run({"NG_GATHER": "0"})
-    got, st1 = run({"NG_GATHER_FRAC": frac})
+    ref, st0 = run({"gather": 0})
+    got, st1 = run({"gather_frac": frac})
     assert st0["syn_events"] == st1["syn_events"]
     assert st0["gather_slices"] == 0
-    assert st1["gather_slices"] > (250 if frac == "0" else 10)
+    assert st1["gather_slices"] > (250 if frac == 0.0 else 10)
     for ((s0, t0), v0), ((s1, t1), v1) in zip(ref, got):
         assert len(s0) > 100
         o0, o1 = np.lexsort((s0, t0)), np.lexsort((s1, t1))
