@@ -91,6 +91,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-layered", action="store_true")
     ap.add_argument("--no-aeif", action="store_true")
+    ap.add_argument("--no-slice-calls", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--forms", default="plain,fp32,batched",
                     help="forms of the Brunel network to time besides the plain FP64 headline")
@@ -618,6 +619,76 @@ def measure_aeif(args, dev, sim_ms=500.0):
     return out
 
 
+def measure_slice_calls(args, dev):
+    """The network driven the way NEST's node loop drives an engine node
+    (gpu_engine::update): one ng_update per min_delay slice, enqueued without
+    waiting, against one ng_simulate over the same steps on the same engine.
+    Config 1 (15-step slices, 667 calls per simulated second) and the layered
+    network at a quarter of its size (1-step slices, 10,000 calls per
+    simulated second; graph drawn on the device, exported and loaded into a
+    static engine)."""
+    import torch
+
+    import nestgpu as nest
+    from nestgpu import _abi, workloads
+    from nestgpu.kernel import KERNEL
+
+    def drive(eng, steps, md):
+        st = torch.cuda.current_stream(dev)
+        eng.set_stream(st.cuda_stream)
+        eng.simulate(steps)                     # warm-up (autotuner, graphs)
+        eng.sync()
+        out = {}
+        for how in ("update", "simulate"):
+            origin = eng.stats()["clock_steps"]
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            if how == "update":
+                for k in range(steps // md):
+                    eng.update(origin + k * md, 0, md)
+            else:
+                eng.simulate(steps)
+            eng.sync()
+            torch.cuda.synchronize(dev)
+            out[how + "_rtf"] = (time.perf_counter() - t0) / (steps * 1e-4)
+        out["calls_per_sim_s"] = 10000 // md
+        return out
+
+    res = {}
+    workloads.c1(nest, precision="fp64", seed=4242)
+    c = KERNEL.compile()
+    inp = E2E.inputs(KERNEL, c)
+    x = E2E(KERNEL, c, "fp64", 4242, inp)
+    for name, arr in x.state.items():
+        x.eng.set_var(0, name, arr)
+    res["c1_fp64"] = drive(x.eng, 10000, int(c["min_delay"]))
+    x.close()
+    nest.ResetKernel()
+    spec = workloads.layered_spec(scale=0.25)
+    n = sum(spec["sizes"])
+    srv = workloads.layered_engine(spec, "fp64", device=dev.index)
+    nid = workloads.layered_add(srv, spec, 10 ** 7)
+    src, tgt, w, d = srv.net_get_connections(nid)
+    srv.close()
+    eng = _abi.Engine([(_abi.NG_IAF_PSC_EXP, n)], 0.1, 1, int(d.max()), device=dev.index)
+    E_L = spec["E_L"]
+    V0 = np.random.default_rng(spec["seed"]).normal(-58.0, 10.0, n) - E_L
+    for k, v in {"tau_syn_ex": spec["tau_syn"], "tau_syn_in": spec["tau_syn"], "tau_m": spec["tau_m"],
+                 "C_m": spec["C_m"], "t_ref": spec["t_ref"], "V_th_rel": spec["V_th"] - E_L,
+                 "V_reset_rel": spec["V_reset"] - E_L, "V_m_rel": V0}.items():
+        eng.set_var(0, k, np.broadcast_to(np.asarray(v, dtype=np.float64), (n,)).copy())
+    eng.set_connections_coo(src, tgt, w, d, n)
+    rate = np.repeat(np.asarray(spec["k_ext"], dtype=np.float64) * spec["nu_ext_hz"], spec["sizes"])
+    eng.set_poisson(rate, np.full(n, spec["J"]), np.full(n, int(round(spec["d_ext_ms"] / 0.1)), dtype=np.int32),
+                    0, 10 ** 12, spec["seed"])
+    eng.set_recording(np.ones(n, dtype=np.uint8))
+    eng.set_graph_slices(64)
+    res["layered_quarter_fp64"] = drive(eng, 5000, 1)
+    res["layered_quarter_fp64"]["synapses"] = int(len(src))
+    eng.close()
+    return res
+
+
 def measure_serving(args, dev):
     """Serving sweep: Poisson arrivals (20/s) of Brunel-type requests.  The
     batched FP32 server (continuous batching) against the plain FP64 server
@@ -692,6 +763,8 @@ def run_engine(args):
         extra["aeif_50k"] = measure_aeif(args, dev)
     if not args.no_serving:
         extra["serving_sweep"] = measure_serving(args, dev)
+    if not args.no_slice_calls:
+        extra["slice_calls"] = measure_slice_calls(args, dev)
     cpu = None
     if rank == 0 and not args.no_cpu:
         from nestgpu import workloads

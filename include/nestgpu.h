@@ -36,6 +36,7 @@ extern "C" {
 #define NG_IAF_PSC_DELTA 0   /* models/iaf_psc_delta.{h,cpp} */
 #define NG_IAF_PSC_EXP 1     /* models/iaf_psc_exp.{h,cpp} */
 #define NG_AEIF_COND_ALPHA 2 /* models/aeif_cond_alpha.{h,cpp} */
+#define NG_IAF_PSC_ALPHA 3   /* models/iaf_psc_alpha.{h,cpp} */
 
 /* arithmetic forms */
 #define NG_FP64 0 /* plain: FP64 state and FP64 ring buffers (red.global.add.f64) */
@@ -281,7 +282,10 @@ int ng_set_option( ng_engine* eng, const char* name, double value );
 /* FP64 coefficients the engine computed for a neuron (testing hook):
  * writes up to `cap` values in the model's order, *n_out the count.  For
  * iaf_psc_delta: P33, P30, RefractoryCounts; iaf_psc_exp: P11ex, P11in, P22,
- * P21ex, P21in, P20, RefractoryCounts (models/iaf_psc_exp.cpp:244-285). */
+ * P21ex, P21in, P20, RefractoryCounts (models/iaf_psc_exp.cpp:244-285);
+ * iaf_psc_alpha: P11ex, P11in, P21ex, P21in, P30, P31ex, P32ex, P31in, P32in,
+ * expm1(-h/tau_m), EPSC and IPSC initial values, RefractoryCounts
+ * (models/iaf_psc_alpha.cpp, pre_run_hook). */
 int ng_debug_coefficients( ng_engine* eng, int32_t block, int64_t index, double* out, int32_t cap, int32_t* n_out );
 
 /* ---------------------------------------------------------------------

@@ -81,20 +81,42 @@ const VarSpec AEIF_VARS[] = { { "V_peak", PARAM, 0 }, { "V_reset", PARAM, 1 }, {
   { "dg_ex", STATE, 1 }, { "g_ex", STATE, 2 }, { "dg_in", STATE, 3 }, { "g_in", STATE, 4 }, { "w", STATE, 5 },
   { "I_e", STATE, 6 }, { "r", REFR, 0 }, { "integration_step", ISTEP, 0 }, { nullptr, 0, 0 } };
 
+// iaf_psc_alpha: the state in iaf_psc_exp's slot layout (V_m, I_syn_ex,
+// I_syn_in, then the derivatives dI_ex, dI_in of the alpha currents, I_e)
+const VarSpec ALPHA_VARS[] = { { "tau_m", PARAM, 0 }, { "C_m", PARAM, 1 }, { "t_ref", PARAM, 2 },
+  { "V_th_rel", PARAM, 3 }, { "V_reset_rel", PARAM, 4 }, { "tau_syn_ex", PARAM, 5 }, { "tau_syn_in", PARAM, 6 },
+  { "V_min_rel", PARAM, 7 }, { "V_m_rel", STATE, 0 }, { "I_syn_ex", STATE, 1 }, { "I_syn_in", STATE, 2 },
+  { "dI_syn_ex", STATE, 3 }, { "dI_syn_in", STATE, 4 }, { "I_e", STATE, 5 }, { "r", REFR, 0 }, { nullptr, 0, 0 } };
+
 const VarSpec*
 vars_of( int model )
 {
-  return model == NG_IAF_PSC_DELTA ? DELTA_VARS : model == NG_IAF_PSC_EXP ? EXP_VARS : AEIF_VARS;
+  return model == NG_IAF_PSC_DELTA ? DELTA_VARS
+    : model == NG_IAF_PSC_EXP      ? EXP_VARS
+    : model == NG_IAF_PSC_ALPHA    ? ALPHA_VARS
+                                   : AEIF_VARS;
 }
 int
 n_params( int model )
 {
-  return model == NG_IAF_PSC_DELTA ? 6 : model == NG_IAF_PSC_EXP ? 7 : 16;
+  return model == NG_IAF_PSC_DELTA ? 6 : model == NG_IAF_PSC_EXP ? 7 : model == NG_IAF_PSC_ALPHA ? 8 : 16;
 }
 int
 n_states( int model )
 {
-  return model == NG_IAF_PSC_DELTA ? 3 : model == NG_IAF_PSC_EXP ? 6 : 7;
+  return model == NG_IAF_PSC_DELTA ? 3 : model == NG_IAF_PSC_EXP ? 6 : model == NG_IAF_PSC_ALPHA ? 6 : 7;
+}
+// the coefficient row index of RefractoryCounts
+int
+refr_index( int model )
+{
+  return model == NG_IAF_PSC_DELTA ? 5 : model == NG_IAF_PSC_EXP ? 8 : model == NG_IAF_PSC_ALPHA ? 15 : 18;
+}
+// models whose input splits into excitatory/inhibitory channels by the weight's sign
+bool
+sign_channels( int model )
+{
+  return model == NG_IAF_PSC_EXP || model == NG_IAF_PSC_ALPHA;
 }
 const VarSpec*
 find_var( int model, const char* name )
@@ -113,6 +135,8 @@ default_params( int model, std::vector< double >& p )
     p = { 10.0, 250.0, 2.0, -55.0 - ( -70.0 ), -70.0 - ( -70.0 ), -1.7976931348623157e308 };
   else if ( model == NG_IAF_PSC_EXP )
     p = { 10.0, 250.0, 2.0, -55.0 - ( -70.0 ), -70.0 - ( -70.0 ), 2.0, 2.0 };
+  else if ( model == NG_IAF_PSC_ALPHA )
+    p = { 10.0, 250.0, 2.0, -55.0 - ( -70.0 ), -70.0 - ( -70.0 ), 2.0, 2.0, -HUGE_VAL };
   else
     p = { 0.0, -60.0, 0.0, 30.0, 281.0, 0.0, -85.0, -70.6, 2.0, 144.0, 4.0, 80.5, -50.4, 0.2, 2.0, 1e-6 };
 }
@@ -142,6 +166,40 @@ propagator_exp( double tau_syn, double tau_m, double c_m, double h )
     return P32;
   const double exp_h_tau = std::exp( -h * inv_tau_m );
   return h * inv_c_m * exp_h_tau;
+}
+
+// IAFPropagatorAlpha::evaluate (libnestutil/iaf_propagator.cpp:95-118, with
+// the P32 of :56-75 and NUMERICAL_STABILITY_FACTOR_ = 1e-7,
+// iaf_propagator.h:66): (P31, P32), each with its singular tau_m ~ tau_syn
+// form.  The same formulas and operation order (bit-equal coefficients).
+void
+propagator_alpha( double tau_syn, double tau_m, double c_m, double h, double* P31, double* P32 )
+{
+  const double h_min_regular = 1e-7 * tau_m * tau_m / std::abs( tau_m - tau_syn );
+  const double beta = tau_syn * tau_m / ( tau_m - tau_syn );
+  const double gamma = beta / c_m;
+  const double inv_tau_syn = 1 / tau_syn;
+  const double inv_tau_m = 1 / tau_m;
+  const double inv_c_m = 1 / c_m;
+  const double inv_beta = ( tau_m - tau_syn ) / ( tau_syn * tau_m );
+  const double exp_h_tau_syn = std::exp( -h * inv_tau_syn );
+  const double expm1_h_tau = std::expm1( h * inv_beta );
+  double p32 = gamma * exp_h_tau_syn * expm1_h_tau;
+  double exp_h_tau = std::nan( "" );
+  if ( !( std::isnormal( p32 ) and p32 > 0 ) )
+  {
+    exp_h_tau = std::exp( -h * inv_tau_m );
+    p32 = h * inv_c_m * exp_h_tau;
+  }
+  *P32 = p32;
+  if ( h > h_min_regular )
+  {
+    *P31 = gamma * exp_h_tau_syn * ( beta * expm1_h_tau - h );
+    return;
+  }
+  if ( std::isnan( exp_h_tau ) )
+    exp_h_tau = std::exp( -h * inv_tau_m );
+  *P31 = 0.5 * h * h * inv_c_m * exp_h_tau;
 }
 
 // Poisson table (lambda, p_m, F_m, m) for inversion from the mode.
@@ -598,7 +656,7 @@ struct ng_engine
     const int model = blk[ 0 ].model;
     *ch = 0;
     *we = wv;
-    if ( model == NG_IAF_PSC_EXP )
+    if ( sign_channels( model ) )
       *ch = wv > 0 ? 0u : 1u;
     else if ( model == NG_AEIF_COND_ALPHA && !( wv > 0.0 ) )
     {
@@ -777,6 +835,35 @@ struct ng_engine
     row[ 3 ] = P[ 4 ][ i ];
     row[ 4 ] = P[ 5 ][ i ];
     row[ 5 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
+  }
+  else if ( b.model == NG_IAF_PSC_ALPHA )
+  {
+    // iaf_psc_alpha::pre_run_hook (models/iaf_psc_alpha.cpp), same order
+    const double tau_m = P[ 0 ][ i ], c_m = P[ 1 ][ i ], tex = P[ 5 ][ i ], tin = P[ 6 ][ i ];
+    if ( !( c_m > 0 ) )
+      return fail( NG_ERR_ARG, "Capacitance must be > 0." );
+    if ( !( tau_m > 0 ) )
+      return fail( NG_ERR_ARG, "Membrane time constant must be > 0." );
+    if ( !( tex > 0 ) || !( tin > 0 ) )
+      return fail( NG_ERR_ARG, "All synaptic time constants must be > 0." );
+    if ( P[ 2 ][ i ] < 0 )
+      return fail( NG_ERR_ARG, "Refractory time must not be negative." );
+    if ( P[ 4 ][ i ] >= P[ 3 ][ i ] )
+      return fail( NG_ERR_ARG, "Reset potential must be smaller than threshold." );
+    row[ 0 ] = std::exp( -h / tex );  // P11ex = P22ex
+    row[ 1 ] = std::exp( -h / tin );  // P11in = P22in
+    row[ 9 ] = std::expm1( -h / tau_m );
+    row[ 4 ] = -tau_m / c_m * std::expm1( -h / tau_m );  // P30
+    row[ 2 ] = h * row[ 0 ];                               // P21ex
+    row[ 3 ] = h * row[ 1 ];                               // P21in
+    propagator_alpha( tex, tau_m, c_m, h, &row[ 5 ], &row[ 6 ] );
+    propagator_alpha( tin, tau_m, c_m, h, &row[ 7 ], &row[ 8 ] );
+    row[ 10 ] = 1.0 * M_E / tex;
+    row[ 11 ] = 1.0 * M_E / tin;
+    row[ 12 ] = P[ 3 ][ i ];
+    row[ 13 ] = P[ 4 ][ i ];
+    row[ 14 ] = P[ 7 ][ i ];
+    row[ 15 ] = ( double ) ms_to_steps( P[ 2 ][ i ] );
   }
   else if ( b.model == NG_IAF_PSC_EXP )
   {
@@ -1027,6 +1114,13 @@ struct ng_engine
         launch_iaf_g< double, false, NG_IAF_PSC_DELTA >( d, db, from_, to_, sched );
       else
         launch_iaf_g< float, true, NG_IAF_PSC_DELTA >( d, db, from_, to_, sched );
+    }
+    else if ( model == NG_IAF_PSC_ALPHA )
+    {
+      if ( prec == NG_FP64 )
+        launch_iaf_g< double, false, NG_IAF_PSC_ALPHA >( d, db, from_, to_, sched );
+      else
+        launch_iaf_g< float, true, NG_IAF_PSC_ALPHA >( d, db, from_, to_, sched );
     }
     else
     {
@@ -1295,7 +1389,7 @@ struct ng_engine
     double bound = 0.0;
     for ( const auto& b : blk )
     {
-      const int ri = b.model == NG_IAF_PSC_DELTA ? 5 : b.model == NG_IAF_PSC_EXP ? 8 : 18;
+      const int ri = refr_index( b.model );
       for ( int64_t j = 0; j < b.n; ++j )
       {
         const int64_t i = b.off + j;
@@ -1718,7 +1812,7 @@ struct ng_engine
     const int64_t n_cand = ( int64_t ) ( variants.size() + per_sm.size() + groups.size() );
     // the probe (3 trial lengths) and the trials must fit the call's steps;
     // otherwise wait for a longer call
-    if ( n < ( 3 + 2 * n_cand ) * steps || 3 * steps > gmax )
+    if ( n < ( 3 + 2 * n_cand ) * steps )
       return NG_OK;
     const int v0 = upd_variant >= 0 ? upd_variant : ( iaf ? default_variant( blk[ 0 ].n ) : 0 );
     TuneCand best { v0, deliver_per_sm, deliver_group, 1e300 };
@@ -1728,10 +1822,15 @@ struct ng_engine
     // bucket (its time is not compared: a network's first slices often hold
     // a transient burst)
     int64_t spk = 0;
-    double probe_us = 0;
-    if ( ( rc = timed_group( 3 * steps, &probe_us, &spk ) ) )
-      return rc;
-    n -= 3 * steps;
+    for ( int k = 0; k < 3; ++k )
+    {
+      double probe_us = 0;
+      int64_t sk = 0;
+      if ( ( rc = timed_group( steps, &probe_us, &sk ) ) )
+        return rc;
+      spk += sk;
+      n -= steps;
+    }
     trial_steps = steps;
     int64_t n_live = N;
     if ( serving )
@@ -1961,7 +2060,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
   int64_t N = 0;
   for ( int k = 0; k < cfg->n_blocks; ++k )
   {
-    if ( cfg->block_model[ k ] < 0 || cfg->block_model[ k ] > 2 || cfg->block_size[ k ] < 0 )
+    if ( cfg->block_model[ k ] < 0 || cfg->block_model[ k ] > 3 || cfg->block_size[ k ] < 0 )
       return fail( NG_ERR_ARG, "ng_create: bad block model or size" );
     N += cfg->block_size[ k ];
   }
@@ -3062,7 +3161,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   // coefficient classes, shared by all networks
   double row[ CT_STRIDE ];
   double log_rate = 0.0;
-  const int ri = model == NG_IAF_PSC_DELTA ? 5 : model == NG_IAF_PSC_EXP ? 8 : 18;
+  const int ri = refr_index( model );
   const int64_t first_new = ( int64_t ) e->cls_ids.size();
   const int np_model = n_params( model );
   for ( int64_t i = n0; i < n0 + n; ++i )
@@ -3162,7 +3261,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       || ( rc = e->grow( e->sc_plen, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_total, 8 ) ) )
       return undo( rc );
     const unsigned g = ( unsigned ) std::max< int64_t >( 1, ( items + 255 ) / 256 );
-    const bool ex_m = model == NG_IAF_PSC_EXP, ae_m = model == NG_AEIF_COND_ALPHA;
+    const bool ex_m = sign_channels( model ), ae_m = model == NG_AEIF_COND_ALPHA;
     const double fxs = std::ldexp( 1.0, e->fx_S );
     k_pb_pass< double ><<< g, 256, 0, e->stream >>>( sp, n, false, ( int* ) e->sc_sb.p, nullptr, 0, 0, e->tbits, ex_m,
       ae_m, 1.0, nullptr, nullptr );
@@ -3750,6 +3849,9 @@ ng_debug_coefficients( ng_engine* e, int32_t block, int64_t index, double* out, 
     v = { row[ 0 ], row[ 1 ], row[ 5 ] };
   else if ( b.model == NG_IAF_PSC_EXP )
     v = { row[ 4 ], row[ 5 ], row[ 0 ], row[ 1 ], row[ 2 ], row[ 3 ], row[ 8 ] };
+  else if ( b.model == NG_IAF_PSC_ALPHA )
+    v = { row[ 0 ], row[ 1 ], row[ 2 ], row[ 3 ], row[ 4 ], row[ 5 ], row[ 6 ], row[ 7 ], row[ 8 ], row[ 9 ], row[ 10 ],
+      row[ 11 ], row[ 15 ] };
   else
     v = { row[ 15 ], row[ 16 ], row[ 17 ], row[ 18 ] };
   const int32_t k = std::min< int32_t >( cap, ( int32_t ) v.size() );

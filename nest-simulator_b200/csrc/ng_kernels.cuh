@@ -23,6 +23,7 @@ namespace ng
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int NG_IAF_PSC_DELTA_ID = 0;
 constexpr int NG_IAF_PSC_EXP_ID = 1;
+constexpr int NG_IAF_PSC_ALPHA_ID = 3;
 
 template < typename T >
 __device__ __forceinline__ T
@@ -676,6 +677,76 @@ append_scheduled( const Net& d, long long origin, int from, int to )
 }
 
 // ---------------------------------------------------------------------
+// iaf_psc_alpha (models/iaf_psc_alpha.cpp, update): exact integration of
+// alpha-shaped currents.  ctab: P11ex (= P22ex), P11in, P21ex, P21in, P30,
+// P31ex, P32ex, P31in, P32in, expm1(-h/tau_m), EPSC and IPSC initial values
+// (e / tau_syn), Theta, V_reset, LowerBound, RefractoryCounts; state in the
+// slots of iaf_psc_exp's layout: V_m - E_L, I_syn_ex, I_syn_in, dI_syn_ex,
+// dI_syn_in, I_e.  The operations and their order are the reference's
+// (every product and sum rounds on its own: -fmad=false); the model's
+// current input y0 is 0 on this path (no CurrentEvent sources).
+// ---------------------------------------------------------------------
+template < typename Real >
+struct AlphaCoef
+{
+  Real P11e, P11i, P21e, P21i, P30, P31e, P32e, P31i, P32i, em1, Ee, Ei, Vth, Vreset, Vmin;
+  int refr;
+};
+
+template < typename Real >
+__device__ __forceinline__ void
+alpha_coef( const double* ct, AlphaCoef< Real >& c )
+{
+  c.P11e = ( Real ) ct[ 0 ];
+  c.P11i = ( Real ) ct[ 1 ];
+  c.P21e = ( Real ) ct[ 2 ];
+  c.P21i = ( Real ) ct[ 3 ];
+  c.P30 = ( Real ) ct[ 4 ];
+  c.P31e = ( Real ) ct[ 5 ];
+  c.P32e = ( Real ) ct[ 6 ];
+  c.P31i = ( Real ) ct[ 7 ];
+  c.P32i = ( Real ) ct[ 8 ];
+  c.em1 = ( Real ) ct[ 9 ];
+  c.Ee = ( Real ) ct[ 10 ];
+  c.Ei = ( Real ) ct[ 11 ];
+  c.Vth = ( Real ) ct[ 12 ];
+  c.Vreset = ( Real ) ct[ 13 ];
+  c.Vmin = ( Real ) ct[ 14 ];
+  c.refr = ( int ) ct[ 15 ];
+}
+
+// one step; ex / inh: this step's ring input per channel (SYN_EX, SYN_IN)
+template < typename Real >
+__device__ __forceinline__ bool
+alpha_step( const AlphaCoef< Real >& c, Real& V, Real& Iex, Real& Iin, Real& dIex, Real& dIin, int& r, const Real Ie,
+  const Real ex, const Real inh )
+{
+  const Real y0 = Real( 0 );
+  if ( r == 0 )
+  {
+    V = c.P30 * ( y0 + Ie ) + c.P31e * dIex + c.P32e * Iex + c.P31i * dIin + c.P32i * Iin + c.em1 * V + V;
+    V = ( V < c.Vmin ? c.Vmin : V );
+  }
+  else
+  {
+    --r;
+  }
+  Iex = c.P21e * dIex + c.P11e * Iex;
+  dIex *= c.P11e;
+  dIex += c.Ee * ex;
+  Iin = c.P21i * dIin + c.P11i * Iin;
+  dIin *= c.P11i;
+  dIin += c.Ei * inh;
+  if ( V >= c.Vth )
+  {
+    r = c.refr;
+    V = c.Vreset;
+    return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------
 // iaf_psc_delta (models/iaf_psc_delta.cpp:272-329) and iaf_psc_exp
 // (models/iaf_psc_exp.cpp:288-348), one thread per neuron.
 //
@@ -704,7 +775,9 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
   const long long until = act ? active_until( d, i ) : -1ll;
   const int netid = ( act && d.nid ) ? d.nid[ i ] : -1;
   const bool gath = netid >= 0 && d.net_mode && d.net_mode[ netid ] != 0;
-  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
+  // iaf_psc_alpha keeps iaf_psc_exp's two channels and state layout
+  constexpr bool ALPHA = MODEL == NG_IAF_PSC_ALPHA_ID;
+  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID || ALPHA;
   Real* s0 = ( Real* ) b.s[ 0 ];
   Real* s1 = ( Real* ) b.s[ 1 ];
   Real* s2 = ( Real* ) b.s[ 2 ];
@@ -712,11 +785,14 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
   Real* s4 = ( Real* ) b.s[ 4 ];
   Real V = 0, x1 = 0, x2 = 0, i0 = 0, i1 = 0, Ie = 0;
   Real c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, Vth = 0, Vreset = 0, c9 = 0;
+  AlphaCoef< Real > ac {};
   int r = 0, refr = 0;
   if ( act )
   {
     const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
-    if constexpr ( EXP )
+    if constexpr ( ALPHA )
+      alpha_coef< Real >( ct, ac );
+    if constexpr ( EXP && !ALPHA )
     {
       c0 = ( Real ) ct[ 0 ];
       c1 = ( Real ) ct[ 1 ];
@@ -728,6 +804,9 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
       Vreset = ( Real ) ct[ 7 ];
       refr = ( int ) ct[ 8 ];
       c9 = ( Real ) ct[ 9 ];
+    }
+    if constexpr ( EXP )
+    {
       V = s0[ li ];
       x1 = s1[ li ];
       x2 = s2[ li ];
@@ -814,7 +893,11 @@ k_update_iaf( Net d, Block b, int from, int to, int sched )
           }
         }
         bool spk = false;
-        if constexpr ( EXP )
+        if constexpr ( ALPHA )
+        {
+          spk = alpha_step< Real >( ac, V, x1, x2, i0, i1, r, Ie, ex, inh );
+        }
+        else if constexpr ( EXP )
         {
           if ( r == 0 )
             V = V * c0 + x1 * c1 + x2 * c2 + ( Ie + i0 ) * c3;
@@ -932,7 +1015,9 @@ template < typename Real, bool FIX, int MODEL, int TPB, int CH >
 __global__ void __launch_bounds__( TPB )
 k_update_iaf2( Net d, Block b, int from, int to, int sched )
 {
-  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID;
+  // iaf_psc_alpha keeps iaf_psc_exp's two channels and state layout
+  constexpr bool ALPHA = MODEL == NG_IAF_PSC_ALPHA_ID;
+  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID || ALPHA;
   constexpr int P2_CH = CH;
   static_assert( TPB % 32 == 0 && CH <= 32 && ( CH * P2_NB ) % TPB == 0, "two-phase update shape" );
   __shared__ Real s_ex[ P2_CH ][ P2_NB ];
@@ -954,11 +1039,14 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
   Real* s4 = ( Real* ) b.s[ 4 ];
   Real V = 0, x1 = 0, x2 = 0, i0 = 0, i1 = 0, Ie = 0;
   Real c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, Vth = 0, Vreset = 0, c9 = 0;
+  AlphaCoef< Real > ac {};
   int r = 0, refr = 0;
   if ( act )
   {
     const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
-    if constexpr ( EXP )
+    if constexpr ( ALPHA )
+      alpha_coef< Real >( ct, ac );
+    if constexpr ( EXP && !ALPHA )
     {
       c0 = ( Real ) ct[ 0 ];
       c1 = ( Real ) ct[ 1 ];
@@ -970,6 +1058,9 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
       Vreset = ( Real ) ct[ 7 ];
       refr = ( int ) ct[ 8 ];
       c9 = ( Real ) ct[ 9 ];
+    }
+    if constexpr ( EXP )
+    {
       V = s0[ li ];
       x1 = s1[ li ];
       x2 = s2[ li ];
@@ -1091,7 +1182,11 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
         if ( act && t0 + k < until )
         {
           const Real in_ex = s_ex[ k ][ lane ];
-          if constexpr ( EXP )
+          if constexpr ( ALPHA )
+          {
+            spk = alpha_step< Real >( ac, V, x1, x2, i0, i1, r, Ie, in_ex, s_in[ k ][ lane ] );
+          }
+          else if constexpr ( EXP )
           {
             const Real in_in = s_in[ k ][ lane ];
             if ( r == 0 )
@@ -1656,7 +1751,7 @@ edge_channel( const PackSpec& ps, int32_t t, double wv, uint32_t& ch, double& we
     ++bk;
   ch = 0u;
   we = wv;
-  if ( ps.model[ bk ] == NG_IAF_PSC_EXP_ID )
+  if ( ps.model[ bk ] == NG_IAF_PSC_EXP_ID || ps.model[ bk ] == NG_IAF_PSC_ALPHA_ID )
     ch = wv > 0 ? 0u : 1u;
   else if ( ps.model[ bk ] == 2 && !( wv > 0.0 ) )
   {

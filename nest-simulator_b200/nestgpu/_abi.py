@@ -22,7 +22,7 @@ NG_ERR_MEMORY = -5
 NG_ERR_CAPACITY = -6
 NG_ERR_UNKNOWN_NAME = -7
 
-NG_IAF_PSC_DELTA, NG_IAF_PSC_EXP, NG_AEIF_COND_ALPHA = 0, 1, 2
+NG_IAF_PSC_DELTA, NG_IAF_PSC_EXP, NG_AEIF_COND_ALPHA, NG_IAF_PSC_ALPHA = 0, 1, 2, 3
 NG_FP64, NG_FP32 = 0, 1
 NG_MAX_BLOCKS = 8
 

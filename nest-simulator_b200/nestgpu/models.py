@@ -8,6 +8,7 @@ shift them when E_L changes):
 
 - iaf_psc_delta: models/iaf_psc_delta.cpp:94-200
 - iaf_psc_exp:   models/iaf_psc_exp.cpp:100-195
+- iaf_psc_alpha: models/iaf_psc_alpha.cpp (Parameters_::set, State_::set)
 - aeif_cond_alpha: models/aeif_cond_alpha.cpp:130-300
 """
 
@@ -207,6 +208,67 @@ class IafPscExp(NeuronModel):
         return v + self.data["E_L"][idx] if key == "V_m" else v
 
 
+class IafPscAlpha(NeuronModel):
+    """iaf_psc_alpha: alpha-shaped synaptic currents (I_syn and its
+    derivative per channel); V_m, V_th, V_reset, V_min relative to E_L."""
+    name = "iaf_psc_alpha"
+    engine_model = _abi.NG_IAF_PSC_ALPHA
+    storage = {"tau_m": 10.0, "C_m": 250.0, "t_ref": 2.0, "E_L": -70.0, "I_e": 0.0,
+               "V_th_rel": -55.0 - (-70.0), "V_reset_rel": -70.0 - (-70.0), "tau_syn_ex": 2.0,
+               "tau_syn_in": 2.0, "V_min_rel": -np.inf, "V_m_rel": 0.0, "I_syn_ex": 0.0, "I_syn_in": 0.0,
+               "dI_syn_ex": 0.0, "dI_syn_in": 0.0}
+    engine_vars = {"tau_m": "tau_m", "C_m": "C_m", "t_ref": "t_ref", "V_th_rel": "V_th_rel",
+                   "V_reset_rel": "V_reset_rel", "tau_syn_ex": "tau_syn_ex", "tau_syn_in": "tau_syn_in",
+                   "V_min_rel": "V_min_rel", "V_m_rel": "V_m_rel", "I_syn_ex": "I_syn_ex", "I_syn_in": "I_syn_in",
+                   "dI_syn_ex": "dI_syn_ex", "dI_syn_in": "dI_syn_in", "I_e": "I_e"}
+    state_vars = ("V_m_rel", "I_syn_ex", "I_syn_in", "dI_syn_ex", "dI_syn_in")
+    recordables = ("I_syn_ex", "I_syn_in", "V_m")
+    public = ("C_m", "E_L", "I_e", "V_m", "V_min", "V_reset", "V_th", "t_ref", "tau_m", "tau_syn_ex", "tau_syn_in",
+              "I_syn_ex", "I_syn_in", "dI_syn_ex", "dI_syn_in")
+
+    def set(self, idx, d):
+        D = self.data
+        n = len(idx)
+        EL_old = D["E_L"][idx].copy()
+        EL = _as(d["E_L"], n) if "E_L" in d else EL_old
+        dEL = EL - EL_old
+        Vreset = _as(d["V_reset"], n) - EL if "V_reset" in d else D["V_reset_rel"][idx] - dEL
+        Vth = _as(d["V_th"], n) - EL if "V_th" in d else D["V_th_rel"][idx] - dEL
+        Vmin = _as(d["V_min"], n) - EL if "V_min" in d else D["V_min_rel"][idx] - dEL
+        vals = {}
+        for k in ("I_e", "C_m", "tau_m", "tau_syn_ex", "tau_syn_in", "t_ref", "I_syn_ex", "I_syn_in", "dI_syn_ex",
+                  "dI_syn_in"):
+            vals[k] = _as(d[k], n) if k in d else D[k][idx]
+        if np.any(Vreset >= Vth):
+            raise BadProperty("Reset potential must be smaller than threshold.")
+        if np.any(vals["C_m"] <= 0):
+            raise BadProperty("Capacitance must be > 0.")
+        if np.any(vals["tau_m"] <= 0):
+            raise BadProperty("Membrane time constant must be > 0.")
+        if np.any(vals["tau_syn_ex"] <= 0) or np.any(vals["tau_syn_in"] <= 0):
+            raise BadProperty("All synaptic time constants must be > 0.")
+        if np.any(vals["t_ref"] < 0):
+            raise BadProperty("Refractory time must not be negative.")
+        V = _as(d["V_m"], n) - EL if "V_m" in d else D["V_m_rel"][idx] - dEL
+        D["E_L"][idx] = EL
+        D["V_reset_rel"][idx] = Vreset
+        D["V_th_rel"][idx] = Vth
+        D["V_min_rel"][idx] = Vmin
+        for k, v in vals.items():
+            D[k][idx] = v
+        D["V_m_rel"][idx] = V
+        self._touch(*self.storage)
+
+    def get(self, idx, key):
+        D = self.data
+        if key in ("V_m", "V_th", "V_reset", "V_min"):
+            return D[key + "_rel"][idx] + D["E_L"][idx]
+        return D[key][idx]
+
+    def recordable_value(self, key, v, idx):
+        return v + self.data["E_L"][idx] if key == "V_m" else v
+
+
 class AeifCondAlpha(NeuronModel):
     name = "aeif_cond_alpha"
     engine_model = _abi.NG_AEIF_COND_ALPHA
@@ -253,7 +315,8 @@ class AeifCondAlpha(NeuronModel):
         return self.data[key][idx]
 
 
-NEURON_MODELS = {"iaf_psc_delta": IafPscDelta, "iaf_psc_exp": IafPscExp, "aeif_cond_alpha": AeifCondAlpha}
+NEURON_MODELS = {"iaf_psc_delta": IafPscDelta, "iaf_psc_exp": IafPscExp, "iaf_psc_alpha": IafPscAlpha,
+                 "aeif_cond_alpha": AeifCondAlpha}
 
 #: device models and their parameter defaults
 DEVICE_MODELS = {

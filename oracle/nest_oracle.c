@@ -221,6 +221,39 @@ orc_iaf_propagator_exp( double tau_syn, double tau_m, double c_m, double h )
   return h * inv_c_m * exp_h_tau;
 }
 
+/* IAFPropagatorAlpha::evaluate (libnestutil/iaf_propagator.cpp:95-118) with
+ * the base class's P32 (:56-75) and h_min_regular from
+ * NUMERICAL_STABILITY_FACTOR_ = 1e-7 (iaf_propagator.h:66). */
+void
+orc_iaf_propagator_alpha( double tau_syn, double tau_m, double c_m, double h, double* out )
+{
+  const double h_min_regular = 1e-7 * tau_m * tau_m / fabs( tau_m - tau_syn );
+  const double beta = tau_syn * tau_m / ( tau_m - tau_syn );
+  const double gamma = beta / c_m;
+  const double inv_tau_syn = 1 / tau_syn;
+  const double inv_tau_m = 1 / tau_m;
+  const double inv_c_m = 1 / c_m;
+  const double inv_beta = ( tau_m - tau_syn ) / ( tau_syn * tau_m );
+  const double exp_h_tau_syn = exp( -h * inv_tau_syn );
+  const double expm1_h_tau = expm1( h * inv_beta );
+  double P32 = gamma * exp_h_tau_syn * expm1_h_tau;
+  double exp_h_tau = NAN;
+  if ( !( isnormal( P32 ) && P32 > 0 ) )
+  {
+    exp_h_tau = exp( -h * inv_tau_m );
+    P32 = h * inv_c_m * exp_h_tau;
+  }
+  out[ 1 ] = P32;
+  if ( h > h_min_regular )
+  {
+    out[ 0 ] = gamma * exp_h_tau_syn * ( beta * expm1_h_tau - h );
+    return;
+  }
+  if ( isnan( exp_h_tau ) )
+    exp_h_tau = exp( -h * inv_tau_m );
+  out[ 0 ] = 0.5 * h * h * inv_c_m * exp_h_tau;
+}
+
 /* Time(ms(t)).get_steps() with the default 1000 tics/ms
  * (nestkernel/nest_time.h:306-311, 508-521). */
 static int64_t
@@ -247,6 +280,10 @@ static const var_name DELTA_VARS[] = { { "tau_m", 0 }, { "C_m", 1 }, { "t_ref", 
 static const var_name EXP_VARS[] = { { "tau_m", 0 }, { "C_m", 1 }, { "t_ref", 2 }, { "I_e", 3 }, { "V_th_rel", 4 },
   { "V_reset_rel", 5 }, { "tau_syn_ex", 6 }, { "tau_syn_in", 7 }, { "V_m_rel", 8 }, { "I_syn_ex", 9 },
   { "I_syn_in", 10 }, { "i_0", 11 }, { "i_1", 12 }, { "r", 13 }, { NULL, 0 } };
+/* iaf_psc_alpha: y3 = V_m_rel, I_ex, I_in, dI_ex, dI_in (models/iaf_psc_alpha.h State_) */
+static const var_name ALPHA_VARS[] = { { "tau_m", 0 }, { "C_m", 1 }, { "t_ref", 2 }, { "I_e", 3 }, { "V_th_rel", 4 },
+  { "V_reset_rel", 5 }, { "tau_syn_ex", 6 }, { "tau_syn_in", 7 }, { "V_min_rel", 8 }, { "V_m_rel", 9 },
+  { "I_syn_ex", 10 }, { "I_syn_in", 11 }, { "dI_syn_ex", 12 }, { "dI_syn_in", 13 }, { "r", 14 }, { NULL, 0 } };
 static const var_name AEIF_VARS[] = { { "V_peak", 0 }, { "V_reset", 1 }, { "t_ref", 2 }, { "g_L", 3 }, { "C_m", 4 },
   { "E_ex", 5 }, { "E_in", 6 }, { "E_L", 7 }, { "Delta_T", 8 }, { "tau_w", 9 }, { "a", 10 }, { "b", 11 },
   { "V_th", 12 }, { "tau_syn_ex", 13 }, { "tau_syn_in", 14 }, { "I_e", 15 }, { "gsl_error_tol", 16 },
@@ -302,13 +339,17 @@ struct orc_net
   int prepared;
   /* derived coefficients */
   double *P33, *P30, *P22, *P11ex, *P11in, *P21ex, *P21in, *P20, *g0ex, *g0in;
+  double *P31ex, *P32ex, *P31in, *P32in, *em1; /* iaf_psc_alpha (P11, P21, P30, g0 above too) */
   int32_t* refr;
 };
 
 static const var_name*
 vars_of( int model )
 {
-  return model == ORC_IAF_PSC_DELTA ? DELTA_VARS : model == ORC_IAF_PSC_EXP ? EXP_VARS : AEIF_VARS;
+  return model == ORC_IAF_PSC_DELTA ? DELTA_VARS
+    : model == ORC_IAF_PSC_EXP      ? EXP_VARS
+    : model == ORC_IAF_PSC_ALPHA    ? ALPHA_VARS
+                                    : AEIF_VARS;
 }
 
 static int
@@ -334,7 +375,7 @@ nvars( int model )
 orc_net*
 orc_create( int model, int64_t n, double h, int32_t min_delay, int32_t max_delay )
 {
-  if ( model < 0 || model > 2 || n < 0 || min_delay < 1 || max_delay < min_delay || !( h > 0 ) )
+  if ( model < 0 || model > 3 || n < 0 || min_delay < 1 || max_delay < min_delay || !( h > 0 ) )
   {
     set_err( "orc_create: bad arguments" );
     return NULL;
@@ -362,6 +403,19 @@ orc_create( int model, int64_t n, double h, int32_t min_delay, int32_t max_delay
       v[ 4 ][ i ] = -55.0 - ( -70.0 );
       v[ 5 ][ i ] = -70.0 - ( -70.0 );
       v[ 6 ][ i ] = -DBL_MAX;
+    }
+    else if ( model == ORC_IAF_PSC_ALPHA )
+    {
+      double* const* v = net->v;
+      v[ 0 ][ i ] = 10.0;
+      v[ 1 ][ i ] = 250.0;
+      v[ 2 ][ i ] = 2.0;
+      v[ 3 ][ i ] = 0.0;
+      v[ 4 ][ i ] = -55.0 - ( -70.0 );
+      v[ 5 ][ i ] = -70.0 - ( -70.0 );
+      v[ 6 ][ i ] = 2.0;
+      v[ 7 ][ i ] = 2.0;
+      v[ 8 ][ i ] = -INFINITY;
     }
     else if ( model == ORC_IAF_PSC_EXP )
     {
@@ -442,6 +496,11 @@ orc_destroy( orc_net* net )
   free( net->P21ex );
   free( net->P21in );
   free( net->P20 );
+  free( net->P31ex );
+  free( net->P32ex );
+  free( net->P31in );
+  free( net->P32in );
+  free( net->em1 );
   free( net->g0ex );
   free( net->g0in );
   free( net->refr );
@@ -669,7 +728,7 @@ prepare( orc_net* net )
   const int64_t n = net->n;
   const double h = net->h;
   double** pa[] = { &net->P33, &net->P30, &net->P22, &net->P11ex, &net->P11in, &net->P21ex, &net->P21in, &net->P20,
-    &net->g0ex, &net->g0in };
+    &net->g0ex, &net->g0in, &net->P31ex, &net->P32ex, &net->P31in, &net->P32in, &net->em1 };
   for ( size_t k = 0; k < sizeof( pa ) / sizeof( pa[ 0 ] ); ++k )
   {
     free( *pa[ k ] );
@@ -687,6 +746,28 @@ prepare( orc_net* net )
       const double tau_m = net->v[ 0 ][ i ], c_m = net->v[ 1 ][ i ];
       net->P33[ i ] = exp( -h / tau_m );
       net->P30[ i ] = 1 / c_m * ( 1 - net->P33[ i ] ) * tau_m;
+      net->refr[ i ] = ( int32_t ) ms_to_steps_roundup( net->v[ 2 ][ i ], tics_per_ms, tps );
+    }
+    else if ( net->model == ORC_IAF_PSC_ALPHA )
+    {
+      /* iaf_psc_alpha::pre_run_hook (models/iaf_psc_alpha.cpp), same order */
+      const double tau_m = net->v[ 0 ][ i ], c_m = net->v[ 1 ][ i ];
+      const double tex = net->v[ 6 ][ i ], tin = net->v[ 7 ][ i ];
+      double pp[ 2 ];
+      net->P11ex[ i ] = exp( -h / tex );
+      net->P11in[ i ] = exp( -h / tin );
+      net->em1[ i ] = expm1( -h / tau_m );
+      net->P30[ i ] = -tau_m / c_m * expm1( -h / tau_m );
+      net->P21ex[ i ] = h * net->P11ex[ i ];
+      net->P21in[ i ] = h * net->P11in[ i ];
+      orc_iaf_propagator_alpha( tex, tau_m, c_m, h, pp );
+      net->P31ex[ i ] = pp[ 0 ];
+      net->P32ex[ i ] = pp[ 1 ];
+      orc_iaf_propagator_alpha( tin, tau_m, c_m, h, pp );
+      net->P31in[ i ] = pp[ 0 ];
+      net->P32in[ i ] = pp[ 1 ];
+      net->g0ex[ i ] = 1.0 * M_E / tex;
+      net->g0in[ i ] = 1.0 * M_E / tin;
       net->refr[ i ] = ( int32_t ) ms_to_steps_roundup( net->v[ 2 ][ i ], tics_per_ms, tps );
     }
     else if ( net->model == ORC_IAF_PSC_EXP )
@@ -985,6 +1066,45 @@ update_neuron( orc_net* net, int64_t i, int64_t origin, int32_t from, int32_t to
       }
       v[ 8 ][ i ] = 0.0; /* currents ring: no current inputs on this path */
     }
+    else if ( net->model == ORC_IAF_PSC_ALPHA )
+    {
+      /* iaf_psc_alpha::update (models/iaf_psc_alpha.cpp): y0 = 0 (no
+       * current input on this path) */
+      double ex = *r0, inh = *r1;
+      const double dv = drive( net, i, t );
+      if ( dv != 0.0 )
+      {
+        if ( dv > 0 )
+          ex = ex + dv;
+        else
+          inh = inh + dv;
+      }
+      *r0 = 0.0;
+      *r1 = 0.0;
+      const double y0 = 0.0;
+      if ( v[ 14 ][ i ] == 0 )
+      {
+        v[ 9 ][ i ] = net->P30[ i ] * ( y0 + v[ 3 ][ i ] ) + net->P31ex[ i ] * v[ 12 ][ i ] + net->P32ex[ i ] * v[ 10 ][ i ]
+          + net->P31in[ i ] * v[ 13 ][ i ] + net->P32in[ i ] * v[ 11 ][ i ] + net->em1[ i ] * v[ 9 ][ i ] + v[ 9 ][ i ];
+        v[ 9 ][ i ] = ( v[ 9 ][ i ] < v[ 8 ][ i ] ? v[ 8 ][ i ] : v[ 9 ][ i ] );
+      }
+      else
+      {
+        v[ 14 ][ i ] = v[ 14 ][ i ] - 1;
+      }
+      v[ 10 ][ i ] = net->P21ex[ i ] * v[ 12 ][ i ] + net->P11ex[ i ] * v[ 10 ][ i ];
+      v[ 12 ][ i ] *= net->P11ex[ i ];
+      v[ 12 ][ i ] += net->g0ex[ i ] * ex;
+      v[ 11 ][ i ] = net->P21in[ i ] * v[ 13 ][ i ] + net->P11in[ i ] * v[ 11 ][ i ];
+      v[ 13 ][ i ] *= net->P11in[ i ];
+      v[ 13 ][ i ] += net->g0in[ i ] * inh;
+      if ( v[ 9 ][ i ] >= v[ 4 ][ i ] )
+      {
+        v[ 14 ][ i ] = net->refr[ i ];
+        v[ 9 ][ i ] = v[ 5 ][ i ];
+        mult = 1;
+      }
+    }
     else if ( net->model == ORC_IAF_PSC_EXP )
     {
       /* models/iaf_psc_exp.cpp:288-348 */
@@ -1125,7 +1245,7 @@ deliver( orc_net* net, int nthreads )
         const double wv = ww[ e ] * m;
         if ( net->model == ORC_IAF_PSC_DELTA )
           net->ring[ ( slot * 2 + 0 ) * n + tg[ e ] ] += wv;
-        else if ( net->model == ORC_IAF_PSC_EXP )
+        else if ( net->model == ORC_IAF_PSC_EXP || net->model == ORC_IAF_PSC_ALPHA )
           net->ring[ ( slot * 2 + ( wv > 0 ? 0 : 1 ) ) * n + tg[ e ] ] += wv;
         else if ( ww[ e ] > 0.0 )
           net->ring[ ( slot * 2 + 0 ) * n + tg[ e ] ] += wv;

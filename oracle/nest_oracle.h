@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-enum { ORC_IAF_PSC_DELTA = 0, ORC_IAF_PSC_EXP = 1, ORC_AEIF_COND_ALPHA = 2 };
+enum { ORC_IAF_PSC_DELTA = 0, ORC_IAF_PSC_EXP = 1, ORC_AEIF_COND_ALPHA = 2, ORC_IAF_PSC_ALPHA = 3 };
 
 typedef struct orc_net orc_net;
 
@@ -88,6 +88,8 @@ int64_t orc_syn_events( orc_net* net );
 
 /* Propagator restatement (libnestutil/iaf_propagator.cpp) for pinning. */
 double orc_iaf_propagator_exp( double tau_syn, double tau_m, double c_m, double h );
+/* IAFPropagatorAlpha::evaluate (libnestutil/iaf_propagator.cpp:95-118): out[0] = P31, out[1] = P32 */
+void orc_iaf_propagator_alpha( double tau_syn, double tau_m, double c_m, double h, double* out );
 
 /* Philox4x32-10 block (Salmon et al., SC'11) for known-answer tests. */
 void orc_philox4x32( const uint32_t ctr[ 4 ], const uint32_t key[ 2 ], int rounds, uint32_t out[ 4 ] );

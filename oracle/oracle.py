@@ -14,8 +14,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
-IAF_PSC_DELTA, IAF_PSC_EXP, AEIF_COND_ALPHA = 0, 1, 2
-MODEL_IDS = {"iaf_psc_delta": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2}
+IAF_PSC_DELTA, IAF_PSC_EXP, AEIF_COND_ALPHA, IAF_PSC_ALPHA = 0, 1, 2, 3
+MODEL_IDS = {"iaf_psc_delta": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2, "iaf_psc_alpha": 3}
 
 _lib = None
 
@@ -55,6 +55,8 @@ def lib():
         L.orc_get_trace.argtypes = [P, P, i64]
         L.orc_iaf_propagator_exp.restype = dbl
         L.orc_iaf_propagator_exp.argtypes = [dbl, dbl, dbl, dbl]
+        L.orc_iaf_propagator_alpha.restype = None
+        L.orc_iaf_propagator_alpha.argtypes = [dbl, dbl, dbl, dbl, P]
         L.orc_philox4x32.argtypes = [P, P, ctypes.c_int, P]
         L.orc_poisson_draw.restype = i64
         L.orc_poisson_draw.argtypes = [dbl, dbl]

@@ -31,6 +31,12 @@ c1_exp_poisson_stats.npz
     K_E=1,000, K_I=250, J=87.8 pA, g=5, 8 kHz drive): per-neuron spike
     counts and CV-ISI and binned population counts, for the statistical
     (KS) oracle.
+iaf_psc_alpha_kat.npz
+    The expected V_m traces and spike times that the reference test suite
+    holds for iaf_psc_alpha with an internal DC current
+    (testsuite/pytests/neurons/test_iaf_psc_alpha.py: test_iaf_psc_alpha_i0,
+    and test_iaf_psc_alpha_i0_refractory at resolutions 0.1, 0.2, 0.5, 1.0
+    ms), read from the test file's array literals with the ast module.
 aeif_lsodar.npz
     The LSODAR reference solution the reference test suite pins
     aeif_cond_alpha to (testsuite/pytests/neurons/test_aeif_data_lsodar.dat,
@@ -329,6 +335,31 @@ def make_aeif_lsodar():
     print("aeif lsodar rows", data.shape)
 
 
+def _array_literals(path, func):
+    """The np.array([...]) literals inside function `func` of a test file,
+    in source order (evaluated as plain Python lists)."""
+    import ast
+
+    tree = ast.parse(open(path).read())
+    out = []
+    for node in ast.walk(tree):
+        if isinstance(node, ast.FunctionDef) and node.name == func:
+            for sub in ast.walk(node):
+                if (isinstance(sub, ast.Call) and isinstance(sub.func, ast.Attribute) and sub.func.attr == "array"
+                        and sub.args and isinstance(sub.args[0], ast.List)):
+                    out.append((sub.lineno, np.array(ast.literal_eval(sub.args[0]), dtype=np.float64)))
+    return [a for _, a in sorted(out, key=lambda x: x[0])]
+
+
+def make_alpha_kat():
+    path = os.path.join(REF, "testsuite/pytests/neurons/test_iaf_psc_alpha.py")
+    i0 = _array_literals(path, "test_iaf_psc_alpha_i0")
+    refr = _array_literals(path, "test_iaf_psc_alpha_i0_refractory")
+    np.savez_compressed(os.path.join(HERE, "iaf_psc_alpha_kat.npz"), i0_vm=i0[0], i0_spikes=i0[1],
+                        i0_refractory_vm=refr[0])
+    print("iaf_psc_alpha KAT rows", i0[0].shape, i0[1].shape, refr[0].shape)
+
+
 def make_philox_kat():
     path = os.path.join(REF, "thirdparty/Random123/tests/kat_vectors")
     rounds, ctr, key, out = [], [], [], []
@@ -348,9 +379,11 @@ def make_philox_kat():
 
 
 if __name__ == "__main__":
-    which = set(sys.argv[1:]) or {"c0", "exp", "single", "c1", "aeif", "philox"}
+    which = set(sys.argv[1:]) or {"c0", "exp", "single", "c1", "aeif", "philox", "alpha"}
     if "aeif" in which:
         make_aeif_lsodar()
+    if "alpha" in which:
+        make_alpha_kat()
     if "philox" in which:
         make_philox_kat()
     if which & {"c0", "exp", "single", "c1"}:

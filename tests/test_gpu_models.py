@@ -100,41 +100,6 @@ def test_c1_engine_vs_oracle_same_network(nest):
     assert ev == net.syn_events or abs(ev / net.syn_events - 1) < 0.02
 
 
-def test_fp32_form_error_against_fp64(nest):
-    """Precision form (FP32 state, int64 fixed-point rings) vs the plain FP64
-    form on the same networks and drive: rate error <= 2 %, CV-ISI error
-    <= 0.05, and V_m RMS error over the first 100 ms reported.  The two
-    forms' trajectories decorrelate after the first spikes (the network is
-    chaotic), so the comparison is over 4 realizations (seeds) of 2 s each:
-    the rate of a single 1 s realization varies by ~3 % across seeds in the
-    reference itself."""
-    from nestgpu import workloads
-
-    tot = {"fp64": [0, []], "fp32": [0, []]}
-    Vs = {}
-    for seed in (4242, 11, 23, 37):
-        for prec in ("fp64", "fp32"):
-            pop, sr = workloads.c1(nest, precision=prec, seed=seed)
-            if seed == 4242:
-                mm = nest.Create("multimeter", params={"interval": 0.1, "record_from": ["V_m"]})
-                nest.Connect(mm, pop[:50])
-            nest.Simulate(2000.0)
-            s, st = _engine_raster(nest, sr)
-            tot[prec][0] += len(s)
-            tot[prec][1].append(np.nanmean(_cv_isi(s, st, 12500, 0.1)))
-            if seed == 4242:
-                ev = mm.events
-                o = np.lexsort((ev["senders"], ev["times"]))
-                Vs[prec] = np.asarray(ev["V_m"])[o].reshape(-1, 50)[:1000]
-    n64, n32 = tot["fp64"][0], tot["fp32"][0]
-    cv64, cv32 = np.mean(tot["fp64"][1]), np.mean(tot["fp32"][1])
-    assert abs(n32 / n64 - 1) <= 0.02
-    assert abs(cv32 - cv64) <= 0.05
-    rms = np.sqrt(np.mean((Vs["fp32"] - Vs["fp64"]) ** 2))
-    assert rms < 5.0  # mV; trajectories decorrelate after the first spikes
-    print(f"fp32 vs fp64: spikes {n32}/{n64}, CV {cv32:.4f}/{cv64:.4f}, V_m RMS(100 ms) {rms:.3e} mV")
-
-
 def test_aeif_against_lsodar_on_gpu(nest, golden):
     """neurons/test_aeif_lsodar.py on the engine: mean relative difference
     to the LSODAR reference < 5e-4 (V_m) and < 1e-4 (w)."""
