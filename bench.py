@@ -451,9 +451,20 @@ def measure(args, nest, KERNEL, form, precision, copies, seed, local, dev, pg, e
 
     tuned = eng.tuned()
     upd_name = tuned.get("update_kernel", "k_update_iaf")
-    kernels = {upd_name: kern(n_upd, upd_ms, N * (B_NEURON_LAUNCH[precision] + B_NEURON_LAG[precision] * md),
-                              N * md * B_NSTEP_SURVEY[precision]),
-               "k_deliver": kern(n_del, del_ms, ev_launch * B_EVENT[precision], ev_launch * B_EVENT_SURVEY[precision])}
+    if upd_name == "k_run_slices":
+        # one launch runs node update and delivery of many slices: its bytes are
+        # both phases' for every slice it covers
+        sl = (p1["slices"] - p0["slices"]) / max(1, n_upd)
+        ev_l = ev_prof / max(1, n_upd)
+        kernels = {upd_name: kern(n_upd, upd_ms, sl * N * (B_NEURON_LAUNCH[precision] / max(1.0, sl) +
+                                                          B_NEURON_LAG[precision] * md) + ev_l * B_EVENT[precision],
+                                  sl * N * md * B_NSTEP_SURVEY[precision] + ev_l * B_EVENT_SURVEY[precision])}
+        kernels[upd_name]["slices_per_launch"] = sl
+    else:
+        kernels = {upd_name: kern(n_upd, upd_ms, N * (B_NEURON_LAUNCH[precision] + B_NEURON_LAG[precision] * md),
+                                  N * md * B_NSTEP_SURVEY[precision]),
+                   "k_deliver": kern(n_del, del_ms, ev_launch * B_EVENT[precision],
+                                     ev_launch * B_EVENT_SURVEY[precision])}
     # statistics of the timed region's raster (network 0)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import spikestats as S
@@ -611,11 +622,13 @@ def measure_aeif(args, dev, sim_ms=500.0):
         ms = timed_sim(eng, steps, dev)
         s1 = eng.stats()
         ks = kernel_split(eng, 150)
+        tuned = eng.tuned()
         eng.close()
         ev = s1["syn_events"] - s0["syn_events"]
         out[prec] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
                      "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / n / (sim_ms * 1e-3), "build_s": build,
-                     "kernels": ks}
+                     "kernels": ks, "tuned": {k: tuned[k] for k in ("state", "deliver_ctas_per_sm",
+                                                                  "deliver_chunks_per_warp")}}
     return out
 
 
@@ -636,6 +649,7 @@ def measure_slice_calls(args, dev):
     def drive(eng, steps, md):
         st = torch.cuda.current_stream(dev)
         eng.set_stream(st.cuda_stream)
+        steps -= steps % md                     # whole slices: the update loop starts at a slice origin
         eng.simulate(steps)                     # warm-up (autotuner, graphs)
         eng.sync()
         out = {}
@@ -757,14 +771,22 @@ def run_engine(args):
         extra["accuracy_fp32_vs_fp64"] = acc
     if batched is not None and plain["summary"] and batched["summary"]:
         extra["accuracy_batched_fp32_vs_fp64"] = S.compare(batched["summary"], plain["summary"])
+    def guarded(name, fn):
+        # a failing secondary measurement is reported in the line, not fatal
+        try:
+            extra[name] = fn(args, dev)
+        except Exception as err:  # noqa: BLE001
+            extra[name] = {"error": f"{type(err).__name__}: {err}"}
+            print(f"bench: {name} failed: {err}", file=sys.stderr, flush=True)
+
     if not args.no_layered:
-        extra["layered_8pop"] = measure_layered(args, dev)
+        guarded("layered_8pop", measure_layered)
     if not args.no_aeif:
-        extra["aeif_50k"] = measure_aeif(args, dev)
+        guarded("aeif_50k", measure_aeif)
     if not args.no_serving:
-        extra["serving_sweep"] = measure_serving(args, dev)
+        guarded("serving_sweep", measure_serving)
     if not args.no_slice_calls:
-        extra["slice_calls"] = measure_slice_calls(args, dev)
+        guarded("slice_calls", measure_slice_calls)
     cpu = None
     if rank == 0 and not args.no_cpu:
         from nestgpu import workloads

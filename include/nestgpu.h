@@ -144,6 +144,24 @@ int ng_set_connections( ng_engine* eng, int64_t n_src, const int64_t* row_ptr, c
 int ng_set_connections_coo( ng_engine* eng, int64_t n_src, int64_t nnz, const int32_t* source, const int32_t* target,
   const double* weight, const int32_t* delay_steps );
 
+/* stdp_pl_synapse_hom connections (models/stdp_pl_synapse_hom.h) as a CSR
+ * over neuron sources 0..n_src-1: targets, initial weights (>= 0), delays
+ * in steps, and the common properties lambda, alpha, mu, tau_plus.  Each
+ * presynaptic spike updates its connections' weights -- facilitation by
+ * the target's spikes since the source's previous spike, depression by the
+ * target's trace -- before it reaches the ring buffer
+ * (stdp_pl_synapse_hom::send, :255-298); targets keep the spike history
+ * and trace of ArchivingNode (nestkernel/archiving_node.cpp, their
+ * "tau_minus" set with ng_set_var, default 20 ms).  Static engines with
+ * iaf_psc_delta / iaf_psc_exp / iaf_psc_alpha targets and min_delay <= 32
+ * steps; a history holds 64 spikes per neuron (NG_ERR_CAPACITY if a
+ * presynaptic neuron stays silent for longer than its targets' last 64). */
+int ng_set_plastic_connections( ng_engine* eng, int64_t n_src, const int64_t* row_ptr, const int32_t* target,
+  const double* weight, const int32_t* delay_steps, double lambda, double alpha, double mu, double tau_plus );
+
+/* Current weights of the plastic connections, in their CSR order (n = their count). */
+int ng_get_plastic_weights( ng_engine* eng, double* out, int64_t n );
+
 /* Spikes of generator ports: emission step t_e (spike stamp minus one) and
  * source index (>= n_neurons), sorted by step.  Replaces
  * spike_generator::update (models/spike_generator.cpp:320-388). */
@@ -273,7 +291,9 @@ int ng_get_tuning( ng_engine* eng, ng_tuning* out );
 
 /* Engine options: "late_delivery" (1/0: edges of delay >= 2 min_delay
  * delivered on a second stream beside the next slice's update),
- * "late_ctas_per_sm", and for serving engines in the FP32 form, before any
+ * "late_ctas_per_sm", "aeif_binning" (1/0: aeif_cond_alpha neurons ordered
+ * by their last RKF45 step size before each slice, so a warp's neurons need
+ * similar numbers of sub-steps), and for serving engines in the FP32 form, before any
  * network is admitted, "gather" (1/0: the per-target gather of hot
  * fixed_indegree networks) and "gather_frac" (the share of a network's
  * neurons spiking in a slice from which its next slice gathers). */

@@ -26,7 +26,9 @@
 
 #include "../../include/nestgpu.h"
 #include "ng_kernels.cuh"
+#include "ng_persistent.cuh"
 #include "ng_serving.cuh"
+#include "ng_stdp.cuh"
 
 using namespace ng;
 
@@ -271,6 +273,7 @@ struct ng_engine
     std::vector< std::vector< double > > par;  // [param][neuron]
     bool dirty = true;
     DevBuf st[ MAX_STATE ], r, istep, cls, ctab;
+    DevBuf perm, bins;  // aeif: substep-binned thread order and its counting-sort counters
     int64_t n_classes = 0;
     std::vector< double > host_ctab;
     std::vector< int32_t > host_cls;
@@ -696,12 +699,23 @@ struct ng_engine
   int tune_mode = 1;         // 0: fixed, 1: autotune (process cache first), 2: autotune, cache ignored
   int tune_state = 0;        // 0: pending, 1: measured, 2: from the process cache, 3: fixed
   int upd_variant = -1;      // iaf update kernel: 0/1 one thread per neuron (4/8 lags of inputs at a
-                             // time), 2/3 two-phase (256/128 threads); -1: by network size
+                             // time), 2/3 two-phase (256/128 threads), 5 the persistent slice kernel
+                             // (update and delivery of many slices in one launch); -1: by network size
+  DevBuf pk;                 // grid-barrier state of the persistent slice kernel
+  // ---- stdp_pl_synapse_hom connections (ng_set_plastic_connections)
+  bool plastic_on = false;
+  DevBuf pl_row, pl_tgt, pl_dly, pl_w, pl_Kplus, pl_tlast, pl_ninc, pl_tauinv, pl_Kminus, pl_last, pl_hist_t, pl_hist_K,
+    pl_hist_n;
+  int64_t pl_nnz = 0, pl_nsrc = 0;
+  double pl_lambda = 0.1, pl_alpha = 1.0, pl_mu = 0.4, pl_tau_plus = 20.0;
+  std::vector< double > tau_minus_host;  // per neuron, the postsynaptic trace's time constant (ArchivingNode)
+  int pk_occ = -1;           // its resident CTAs per SM (-1: not known yet)
   int occ_deliver = 8;       // resident k_deliver CTAs per SM (occupancy bound)
   int deliver_group = 4;     // edge chunks one delivery warp takes per descriptor load
   int64_t deliver_want = 1;  // delivery CTAs the graph can keep busy (its chunks / 64)
   int rate_bucket = -1;
   int64_t trial_steps = 0;
+  bool aeif_binning = true;  // order aeif threads by RKF45 step size (ng_set_option "aeif_binning")
   struct TuneCand
   {
     int variant, per_sm, group;
@@ -736,11 +750,15 @@ struct ng_engine
       cudaFree( b.istep.p );
       cudaFree( b.cls.p );
       cudaFree( b.ctab.p );
+      cudaFree( b.perm.p );
+      cudaFree( b.bins.p );
     }
     DevBuf* bufs[] = { &ring, &row_beg, &row_len, &real_deg, &tdc, &w, &ent, &log, &rec, &pois, &pois_w, &pois_d,
       &pois_ref, &pois_cdf, &trace_col, &trace, &sched_step, &sched_src, &ctl, &d_nid, &d_step0, &d_until, &d_off,
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
-      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t, &row_ue, &row_ls, &ent_late };
+      &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t, &row_ue, &row_ls, &ent_late, &pk, &pl_row,
+      &pl_tgt, &pl_dly, &pl_w, &pl_Kplus, &pl_tlast, &pl_ninc, &pl_tauinv, &pl_Kminus, &pl_last, &pl_hist_t, &pl_hist_K,
+      &pl_hist_n };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -1014,6 +1032,8 @@ struct ng_engine
       d.seg = ( const int32_t* ) seg.p;
       d.tile_t = tile_t;
     }
+    if ( plastic_on )
+      d.gmask = ( uint32_t* ) gmask.p;  // the update writes each neuron's lag bits of the slice
     if ( gather_on )
     {
       d.gmask = ( uint32_t* ) gmask.p;
@@ -1045,6 +1065,7 @@ struct ng_engine
       k.s[ s ] = b.st[ s ].p;
     k.r = ( int32_t* ) b.r.p;
     k.istep = ( double* ) b.istep.p;
+    k.perm = ( aeif_binning && b.perm.p ) ? ( const int32_t* ) b.perm.p : nullptr;
     return k;
   }
 
@@ -1058,6 +1079,15 @@ struct ng_engine
       const Block db = dblock( b );
       if ( b.model == NG_AEIF_COND_ALPHA )
       {
+        if ( db.perm )
+        {
+          // threads ordered by the neurons' last RKF45 step size (k_aeif_bin_*)
+          const unsigned gb = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( b.n + 255 ) / 256, 2 * sms ) );
+          cudaMemsetAsync( b.bins.p, 0, 2 * AEIF_BINS * sizeof( unsigned ), stream );
+          k_aeif_bin_count<<< gb, 256, 0, stream >>>( ( const double* ) b.istep.p, b.n, h, ( unsigned* ) b.bins.p );
+          k_aeif_bin_scatter<<< gb, 256, 0, stream >>>( ( const double* ) b.istep.p, b.n, h, ( unsigned* ) b.bins.p,
+            ( int32_t* ) b.perm.p );
+        }
         // CTAs of 2 warps, registers capped for 12 warps per SM (the RKF45 state and
         // tableau need ~170 registers; more warps hide the FP64 latency)
         const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( b.n + 63 ) / 64 );
@@ -1082,7 +1112,7 @@ struct ng_engine
     // slices and for engines with the per-target gather or the target-tiled
     // delivery (the lag bits are written there)
     int v = upd_variant >= 0 ? upd_variant : default_variant( db.n );
-    if ( span <= 2 || gather_on || tiled_on )
+    if ( span <= 2 || gather_on || tiled_on || plastic_on )
       v = v == 1 ? 1 : 0;
     if ( v <= 1 )
     {
@@ -1131,9 +1161,126 @@ struct ng_engine
     }
   }
 
+  template < typename Real, bool FIX, int MODEL >
+  const void*
+  pk_func() const
+  {
+    return reinterpret_cast< const void* >( &k_run_slices< Real, FIX, MODEL > );
+  }
+
+  const void*
+  pk_kernel() const
+  {
+    const int m = blk[ 0 ].model;
+    if ( prec == NG_FP64 )
+      return m == NG_IAF_PSC_DELTA ? pk_func< double, false, NG_IAF_PSC_DELTA >()
+        : m == NG_IAF_PSC_EXP      ? pk_func< double, false, NG_IAF_PSC_EXP >()
+                                   : pk_func< double, false, NG_IAF_PSC_ALPHA >();
+    return m == NG_IAF_PSC_DELTA ? pk_func< float, true, NG_IAF_PSC_DELTA >()
+      : m == NG_IAF_PSC_EXP      ? pk_func< float, true, NG_IAF_PSC_EXP >()
+                                 : pk_func< float, true, NG_IAF_PSC_ALPHA >();
+  }
+
+  // the persistent slice kernel applies: one iaf block of a static engine
+  // that fits one resident wave of its CTAs, no traces or scheduled
+  // generator spikes (whose bookkeeping is per launch), a device that
+  // supports cooperative launches
+  bool
+  persistent_ok()
+  {
+    if ( serving || blk.size() != 1 || blk[ 0 ].model == NG_AEIF_COND_ALPHA || n_sched > 0 || n_trace_idx > 0
+      || gather_on || tiled_on || plastic_on || nnz_padded <= 0 )
+      return false;
+    if ( pk_occ < 0 )
+    {
+      int coop = 0, occ = 0;
+      cudaDeviceGetAttribute( &coop, cudaDevAttrCooperativeLaunch, cfg.device );
+      if ( !coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, pk_kernel(), PK_THREADS, 0 ) != cudaSuccess )
+        occ = 0;
+      cudaGetLastError();
+      pk_occ = occ;
+      if ( occ > 0 && !pk.p && alloc( pk, sizeof( PkCtl ) ) != NG_OK )
+        pk_occ = 0;
+    }
+    return pk_occ > 0 && N <= ( int64_t ) pk_occ * sms * PK_NB;
+  }
+
+  // k full slices in one cooperative launch; the grid covers the neurons
+  // (32 per CTA) and at least one CTA per SM (every CTA takes part in the
+  // delivery)
+  int
+  launch_persistent( const Net& d, int k )
+  {
+    Net dd = d;
+    dd.late_min = INT32_MAX;  // every edge at its slice's close
+    Block db = dblock( blk[ 0 ] );
+    const int64_t need = ( N + PK_NB - 1 ) / PK_NB;
+    const int64_t cap = ( int64_t ) pk_occ * sms;
+    const unsigned grid = ( unsigned ) std::min< int64_t >( cap, std::max< int64_t >( need, sms ) );
+    PkCtl* pkc = ( PkCtl* ) pk.p;
+    CU( cudaMemsetAsync( pk.p, 0, sizeof( PkCtl ), stream ) );
+    void* args[] = { &dd, &db, &k, &pkc };
+    CU( cudaLaunchCooperativeKernel( pk_kernel(), dim3( grid ), dim3( PK_THREADS ), args, 0, stream ) );
+    return NG_OK;
+  }
+
+  int
+  upload_tau_minus()
+  {
+    if ( !plastic_on )
+      return NG_OK;  // uploaded with the plastic connections
+    cudaSetDevice( cfg.device );
+    std::vector< double > inv( ( size_t ) N );
+    for ( int64_t i = 0; i < N; ++i )
+      inv[ ( size_t ) i ] = 1. / tau_minus_host[ ( size_t ) i ];
+    CU( cudaMemcpyAsync( pl_tauinv.p, inv.data(), inv.size() * 8, cudaMemcpyHostToDevice, stream ) );
+    CU( cudaStreamSynchronize( stream ) );
+    return NG_OK;
+  }
+
+  StdpNet
+  stdp() const
+  {
+    StdpNet p {};
+    p.row = ( const int64_t* ) pl_row.p;
+    p.tgt = ( const int32_t* ) pl_tgt.p;
+    p.dly = ( const int32_t* ) pl_dly.p;
+    p.w = ( double* ) pl_w.p;
+    p.Kplus = ( double* ) pl_Kplus.p;
+    p.tlast = ( double* ) pl_tlast.p;
+    p.n_src = pl_nsrc;
+    p.n_inc = ( const uint8_t* ) pl_ninc.p;
+    p.tau_minus_inv = ( const double* ) pl_tauinv.p;
+    p.Kminus = ( double* ) pl_Kminus.p;
+    p.last_spike = ( double* ) pl_last.p;
+    p.hist_t = ( double* ) pl_hist_t.p;
+    p.hist_K = ( double* ) pl_hist_K.p;
+    p.hist_n = ( int64_t* ) pl_hist_n.p;
+    p.lambda = pl_lambda;
+    p.alpha = pl_alpha;
+    p.mu = pl_mu;
+    p.tau_plus_inv = 1. / pl_tau_plus;
+    p.ms_per_tic = 1. / cfg.tics_per_ms;
+    p.tics_per_step = tics_per_step;
+    p.sign_channels = sign_channels( blk[ 0 ].model ) ? 1 : 0;
+    return p;
+  }
+
   void
   launch_deliver( const Net& d )
   {
+    if ( plastic_on )
+    {
+      // plastic connections of the closing slice: postsynaptic histories first
+      const StdpNet p = stdp();
+      const unsigned ga = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( N + 255 ) / 256, 4 * sms ) );
+      const unsigned gd = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( pl_nsrc * 32 + 255 ) / 256, 8 * sms ) );
+      k_stdp_archive<<< ga, 256, 0, stream >>>( d, p );
+      if ( prec == NG_FP64 )
+        k_stdp_deliver< false ><<< gd, 256, 0, stream >>>( d, p );
+      else
+        k_stdp_deliver< true ><<< gd, 256, 0, stream >>>( d, p );
+    }
     if ( gather_live )
       k_gather<<< ( unsigned ) sms, G_THREADS, G_SMEM, stream >>>( d );
     if ( tiled_on )
@@ -1327,6 +1474,31 @@ struct ng_engine
     const Net d = net();
     while ( n > 0 )
     {
+      if ( from == 0 && upd_variant == 5 && n >= cfg.min_delay && persistent_ok() )
+      {
+        const int k = ( int ) std::min< int64_t >( n / cfg.min_delay, 1 << 20 );
+        late_join();
+        if ( profiling )
+          CU( cudaEventRecord( ev0, stream ) );
+        int rc = launch_persistent( d, k );
+        if ( rc )
+          return rc;
+        if ( profiling )
+        {
+          // the fused kernel's time is counted as node update
+          CU( cudaEventRecord( ev1, stream ) );
+          CU( cudaEventSynchronize( ev1 ) );
+          float ms = 0;
+          CU( cudaEventElapsedTime( &ms, ev0, ev1 ) );
+          stats.update_ms += ms;
+        }
+        const int64_t st = ( int64_t ) k * cfg.min_delay;
+        origin += st;
+        slices += k;
+        n -= st;
+        stats.update_launches += 1;
+        continue;
+      }
       if ( from == 0 && graph_slices > 0 && n >= cfg.min_delay )
       {
         // largest graph chunk that fits: graph_slices, 16, 4 or 1 slices
@@ -1522,6 +1694,11 @@ struct ng_engine
     const Ctl& c = host_ctl[ sel ];
     if ( c.err & ERR_NUMERIC )
       return fail( NG_ERR_NUMERIC, "NumericalInstability: aeif_cond_alpha state exploded (V_m < -1e3 or |w| > 1e6)" );
+    if ( c.err & ERR_STDP_HISTORY )
+      return fail( NG_ERR_CAPACITY, "stdp_pl_synapse_hom: a postsynaptic spike history of " + std::to_string( STDP_HIST )
+          + " entries did not reach back to a presynaptic neuron's previous spike" );
+    if ( c.err & ERR_BARRIER )
+      return fail( NG_ERR_CUDA, "persistent slice kernel: a grid barrier gave up waiting (a CTA did not arrive)" );
     if ( c.err & ( ERR_SPIKE_LIST | ERR_LOG | ERR_TRACE ) )
       return fail( NG_ERR_CAPACITY, "device spike list, spike log or trace buffer overflowed (err word "
           + std::to_string( c.err ) + ")" );
@@ -1783,10 +1960,12 @@ struct ng_engine
   autotune( int64_t& n, int64_t gmax )
   {
     const int64_t md = cfg.min_delay;
-    const int64_t S = std::max< int64_t >( 4, ( 64 + md - 1 ) / md );  // slices per trial group
-    const int64_t steps = S * md;
-    if ( steps > gmax )
+    // slices per trial group: ~256 steps (a few hundred microseconds of
+    // device time, long enough for event timing), within the spike log
+    const int64_t S = std::min< int64_t >( std::max< int64_t >( 4, ( 256 + md - 1 ) / md ), gmax / md );
+    if ( S < 2 )
       return NG_OK;  // a trial group would not fit the spike log
+    const int64_t steps = S * md;
     bool iaf = false;
     for ( const auto& b : blk )
       iaf = iaf || b.model != NG_AEIF_COND_ALPHA;
@@ -1794,11 +1973,13 @@ struct ng_engine
     if ( iaf )
     {
       variants = { 0, 1 };
-      if ( md >= 3 && !gather_on && !tiled_on )
+      if ( md >= 3 && !gather_on && !tiled_on && !plastic_on )
       {
         variants.push_back( 2 );
         variants.push_back( 3 );
       }
+      if ( persistent_ok() )
+        variants.push_back( 5 );
     }
     std::vector< int > per_sm;
     for ( int p : { 1, 2, 4, 8 } )
@@ -1865,6 +2046,8 @@ struct ng_engine
     };
     for ( int pass = 0; pass < 3; ++pass )
     {
+      if ( pass > 0 && best.variant == 5 )
+        break;  // the persistent kernel delivers inside itself: the delivery launch shape is unused
       const std::vector< int >& opts = pass == 0 ? variants : pass == 1 ? per_sm : groups;
       TuneCand round_best = best;
       for ( int o : opts )
@@ -2086,6 +2269,7 @@ ng_create( const ng_config* cfg, ng_engine** out )
   e->h = ( 1 / cfg->tics_per_ms ) * ( double ) e->tics_per_step;
   e->N = N;
   e->n_src = N + cfg->n_generators;
+  e->tau_minus_host.assign( ( size_t ) N, 20.0 );  // ArchivingNode default
   e->L = std::max( cfg->min_delay, cfg->max_delay );  // update-then-deliver order: max_delay slots suffice
   if ( cfg->start_step < 0 )
   {
@@ -2168,6 +2352,9 @@ ng_create( const ng_config* cfg, ng_engine** out )
     {
       std::vector< double > hs( ( size_t ) b.n, e->h );
       if ( ( rc = e->upload( b.istep, hs.data(), hs.size() * sizeof( double ) ) ) )
+        return bail( rc );
+      if ( ( rc = e->alloc( b.perm, ( size_t ) std::max< int64_t >( b.n, 1 ) * sizeof( int32_t ) ) )
+        || ( rc = e->alloc( b.bins, 2 * AEIF_BINS * sizeof( unsigned ) ) ) )
         return bail( rc );
     }
   }
@@ -2281,6 +2468,15 @@ ng_set_var( ng_engine* e, int32_t block, const char* name, const double* values,
   if ( !name || ( count > 0 && !values ) )
     return fail( NG_ERR_ARG, "ng_set_var: null argument" );
   auto& b = e->blk[ block ];
+  if ( std::strcmp( name, "tau_minus" ) == 0 )
+  {
+    // ArchivingNode's tau_minus (archiving_node.cpp:232-245), for postsynaptic traces of STDP
+    for ( int64_t k = 0; k < count; ++k )
+      if ( !( values[ k ] > 0.0 ) )
+        return fail( NG_ERR_ARG, "All time constants must be strictly positive." );
+    std::copy( values, values + count, e->tau_minus_host.begin() + b.off + first );
+    return e->upload_tau_minus();
+  }
   const VarSpec* v = find_var( b.model, name );
   if ( !v )
     return fail( NG_ERR_UNKNOWN_NAME, std::string( "unknown variable '" ) + name + "' for this model" );
@@ -2335,6 +2531,11 @@ ng_get_var( ng_engine* e, int32_t block, const char* name, double* out, int64_t 
   if ( !name || ( count > 0 && !out ) )
     return fail( NG_ERR_ARG, "ng_get_var: null argument" );
   auto& b = e->blk[ block ];
+  if ( std::strcmp( name, "tau_minus" ) == 0 )
+  {
+    std::copy( e->tau_minus_host.begin() + b.off + first, e->tau_minus_host.begin() + b.off + first + count, out );
+    return NG_OK;
+  }
   const VarSpec* v = find_var( b.model, name );
   if ( !v )
     return fail( NG_ERR_UNKNOWN_NAME, std::string( "unknown variable '" ) + name + "' for this model" );
@@ -2546,6 +2747,88 @@ ng_set_connections_coo( ng_engine* e, int64_t n_src, int64_t nnz, const int32_t*
     dd[ j ] = delay_steps[ k ];
   }
   return ng_set_connections( e, n_src, row.data(), tg.data(), ww.data(), dd.data() );
+}
+
+int
+ng_set_plastic_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr, const int32_t* target,
+  const double* weight, const int32_t* delay_steps, double lambda, double alpha, double mu, double tau_plus )
+{
+  SETTLE( e );
+  if ( !e || !row_ptr || n_src < 0 || n_src > ( e ? e->N : 0 ) )
+    return fail( NG_ERR_ARG, "ng_set_plastic_connections: sources are neurons 0..n_src-1, n_src <= neurons" );
+  if ( e->serving )
+    return fail( NG_ERR_STATE, "ng_set_plastic_connections: plastic connections run in a static engine" );
+  for ( const auto& b : e->blk )
+    if ( b.model == NG_AEIF_COND_ALPHA || sign_channels( b.model ) != sign_channels( e->blk[ 0 ].model ) )
+      return fail( NG_ERR_ARG, "ng_set_plastic_connections: targets are iaf_psc_delta, iaf_psc_exp or iaf_psc_alpha "
+                               "neurons with one input rule" );
+  if ( e->cfg.min_delay > 32 )
+    return fail( NG_ERR_ARG, "ng_set_plastic_connections: needs min_delay <= 32 steps" );
+  if ( !( tau_plus > 0 ) )
+    return fail( NG_ERR_ARG, "tau_plus must be > 0" );
+  const int64_t nnz = row_ptr[ n_src ];
+  if ( row_ptr[ 0 ] != 0 || nnz < 0 || ( nnz > 0 && ( !target || !weight || !delay_steps ) ) )
+    return fail( NG_ERR_ARG, "ng_set_plastic_connections: bad CSR" );
+  std::vector< uint8_t > ninc( ( size_t ) e->N, 0 );
+  for ( int64_t s2 = 0; s2 < n_src; ++s2 )
+    if ( row_ptr[ s2 + 1 ] < row_ptr[ s2 ] )
+      return fail( NG_ERR_ARG, "ng_set_plastic_connections: row pointers must not decrease" );
+  for ( int64_t k = 0; k < nnz; ++k )
+  {
+    if ( target[ k ] < 0 || target[ k ] >= e->N )
+      return fail( NG_ERR_ARG, "ng_set_plastic_connections: target out of range" );
+    if ( delay_steps[ k ] < e->cfg.min_delay || delay_steps[ k ] > e->cfg.max_delay )
+      return fail( NG_ERR_ARG, "ng_set_plastic_connections: delay outside [min_delay, max_delay]" );
+    if ( !( weight[ k ] >= 0.0 ) )
+      return fail( NG_ERR_ARG, "stdp_pl_synapse_hom: weights must be >= 0 (the power law of the facilitation)" );
+    ninc[ ( size_t ) target[ k ] ] = 1;
+  }
+  cudaSetDevice( e->cfg.device );
+  int rc;
+  const size_t N = ( size_t ) e->N;
+  std::vector< double > inv( N );
+  for ( size_t i = 0; i < N; ++i )
+    inv[ i ] = 1. / e->tau_minus_host[ i ];
+  if ( ( rc = e->upload( e->pl_row, row_ptr, ( size_t ) ( n_src + 1 ) * 8 ) )
+    || ( rc = e->upload( e->pl_tgt, target, ( size_t ) std::max< int64_t >( nnz, 1 ) * 4 ) )
+    || ( rc = e->upload( e->pl_dly, delay_steps, ( size_t ) std::max< int64_t >( nnz, 1 ) * 4 ) )
+    || ( rc = e->upload( e->pl_w, weight, ( size_t ) std::max< int64_t >( nnz, 1 ) * 8 ) )
+    || ( rc = e->alloc( e->pl_Kplus, ( size_t ) std::max< int64_t >( n_src, 1 ) * 8 ) )
+    || ( rc = e->alloc( e->pl_tlast, ( size_t ) std::max< int64_t >( n_src, 1 ) * 8 ) )
+    || ( rc = e->upload( e->pl_ninc, ninc.data(), N ) ) || ( rc = e->upload( e->pl_tauinv, inv.data(), N * 8 ) )
+    || ( rc = e->alloc( e->pl_Kminus, N * 8 ) ) || ( rc = e->alloc( e->pl_last, N * 8 ) )
+    || ( rc = e->alloc( e->pl_hist_t, N * STDP_HIST * 8 ) ) || ( rc = e->alloc( e->pl_hist_K, N * STDP_HIST * 8 ) )
+    || ( rc = e->alloc( e->pl_hist_n, N * 8 ) ) )
+    return rc;
+  if ( !e->gmask.p && ( rc = e->alloc( e->gmask, N * 4 ) ) )
+    return rc;
+  e->pl_nnz = nnz;
+  e->pl_nsrc = n_src;
+  e->pl_lambda = lambda;
+  e->pl_alpha = alpha;
+  e->pl_mu = mu;
+  e->pl_tau_plus = tau_plus;
+  e->plastic_on = true;
+  ++e->generation;
+  CU( cudaStreamSynchronize( e->stream ) );
+  return NG_OK;
+}
+
+int
+ng_get_plastic_weights( ng_engine* e, double* out, int64_t n )
+{
+  SETTLE( e );
+  if ( !e || ( n > 0 && !out ) )
+    return fail( NG_ERR_ARG, "ng_get_plastic_weights: null argument" );
+  if ( n != e->pl_nnz )
+    return fail( NG_ERR_ARG, "ng_get_plastic_weights: n must be the number of plastic connections" );
+  cudaSetDevice( e->cfg.device );
+  if ( n > 0 )
+  {
+    CU( cudaMemcpyAsync( out, e->pl_w.p, ( size_t ) n * 8, cudaMemcpyDeviceToHost, e->stream ) );
+    CU( cudaStreamSynchronize( e->stream ) );
+  }
+  return NG_OK;
 }
 
 int
@@ -2897,10 +3180,11 @@ ng_set_tuning( ng_engine* e, int32_t mode, int32_t update_variant, int32_t deliv
 {
   if ( !e )
     return fail( NG_ERR_ARG, "null engine" );
-  if ( mode < 0 || mode > 2 || update_variant < -1 || update_variant > 3 || deliver_ctas_per_sm < -1
+  if ( mode < 0 || mode > 2 || update_variant < -1 || update_variant > 5 || update_variant == 4 || deliver_ctas_per_sm < -1
     || deliver_ctas_per_sm == 0 || deliver_chunks_per_warp < -1 || deliver_chunks_per_warp == 0
     || deliver_chunks_per_warp > 32 )
-    return fail( NG_ERR_ARG, "ng_set_tuning: mode 0..2, update_variant -1..3, per-SM CTAs and chunks per warp -1 or >= 1" );
+    return fail( NG_ERR_ARG, "ng_set_tuning: mode 0..2, update_variant -1, 0..3 or 5, per-SM CTAs and chunks per warp -1 "
+                             "or >= 1" );
   int rc = e->sync_pending();
   if ( rc )
     return rc;
@@ -2976,6 +3260,11 @@ ng_set_option( ng_engine* e, const char* name, double value )
     e->refresh_late();
     ++e->generation;
   }
+  else if ( nm == "aeif_binning" )
+  {
+    e->aeif_binning = value != 0.0;
+    ++e->generation;
+  }
   else if ( nm == "gather" || nm == "gather_frac" )
   {
     if ( !e->serving )
@@ -3000,7 +3289,8 @@ ng_set_option( ng_engine* e, const char* name, double value )
   }
   else
   {
-    return fail( NG_ERR_UNKNOWN_NAME, "unknown option: " + nm + " (late_delivery, late_ctas_per_sm, gather, gather_frac)" );
+    return fail( NG_ERR_UNKNOWN_NAME,
+      "unknown option: " + nm + " (late_delivery, late_ctas_per_sm, aeif_binning, gather, gather_frac)" );
   }
   return NG_OK;
 }

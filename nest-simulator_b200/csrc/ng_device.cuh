@@ -71,6 +71,7 @@ struct Block
   void* s[ MAX_STATE ];
   int32_t* r;
   double* istep;
+  const int32_t* perm;  // aeif: thread -> neuron order grouping equal RKF45 step sizes (nullptr: identity)
 };
 
 // Per-target gather of one fixed_indegree network of a serving engine

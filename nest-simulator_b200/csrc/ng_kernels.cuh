@@ -1369,6 +1369,61 @@ control_yp( double tol, const double* err, const double* f, double& hs )
   return 0;
 }
 
+// Substep binning of aeif_cond_alpha: a neuron near a spike takes many
+// adaptive RKF45 sub-steps per step, a quiet one a single step, and a warp
+// runs as long as its slowest lane.  Before each slice the neurons are
+// ordered by their last step size (bucket k: h / 2^k > hs >= h / 2^(k+1),
+// a counting sort), and the update kernel's thread j simulates neuron
+// perm[j], so the neurons of a warp need similar numbers of sub-steps.  The
+// order changes only which thread computes a neuron, not any arithmetic.
+constexpr int AEIF_BINS = 16;
+
+__device__ __forceinline__ int
+aeif_bin( double hs, double h )
+{
+  if ( !( hs < h ) )
+    return 0;
+  const int k = 1 + ( int ) floor( log2( h / hs ) );
+  return k < AEIF_BINS - 1 ? k : AEIF_BINS - 1;
+}
+
+// counts[0..BINS) histogram, counts[BINS..2 BINS) fill positions (zeroed here)
+__global__ void
+k_aeif_bin_count( const double* istep, int64_t n, double h, unsigned* counts )
+{
+  __shared__ unsigned s_h[ AEIF_BINS ];
+  if ( threadIdx.x < AEIF_BINS )
+    s_h[ threadIdx.x ] = 0u;
+  __syncthreads();
+  for ( int64_t i = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += ( int64_t ) gridDim.x * blockDim.x )
+    atomicAdd( &s_h[ aeif_bin( istep[ i ], h ) ], 1u );
+  __syncthreads();
+  if ( threadIdx.x < AEIF_BINS && s_h[ threadIdx.x ] )
+    atomicAdd( &counts[ threadIdx.x ], s_h[ threadIdx.x ] );
+}
+
+__global__ void
+k_aeif_bin_scatter( const double* istep, int64_t n, double h, unsigned* counts, int32_t* perm )
+{
+  __shared__ unsigned s_off[ AEIF_BINS ];
+  if ( threadIdx.x == 0 )
+  {
+    unsigned acc = 0;
+    for ( int k = 0; k < AEIF_BINS; ++k )
+    {
+      s_off[ k ] = acc;
+      acc += counts[ k ];
+    }
+  }
+  __syncthreads();
+  for ( int64_t i = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += ( int64_t ) gridDim.x * blockDim.x )
+  {
+    const int k = aeif_bin( istep[ i ], h );
+    const unsigned pos = s_off[ k ] + atomicAdd( &counts[ AEIF_BINS + k ], 1u );
+    perm[ pos ] = ( int32_t ) i;
+  }
+}
+
 template < typename Real, bool FIX >
 __global__ void __launch_bounds__( 64, 6 )
 k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
@@ -1376,8 +1431,9 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
   const long long origin = cta_origin( d );
   if ( sched && blockIdx.x == 0 && threadIdx.x < 32 )
     append_scheduled( d, origin, from, to );
-  const int64_t li = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = li < b.n;
+  const int64_t gj = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = gj < b.n;
+  const int64_t li = ( act && b.perm ) ? ( int64_t ) b.perm[ gj ] : gj;
   const int64_t i = b.off + ( act ? li : 0 );
   const long long until = act ? active_until( d, i ) : -1ll;
   Real* sy[ 6 ];

@@ -1,9 +1,9 @@
 """nestgpu -- PyNEST-compatible front-end of the B200 slice engine.
 
 A script written for the reference's PyNEST runs unchanged on the engine
-for the models on its path (iaf_psc_delta, iaf_psc_exp, aeif_cond_alpha,
-static_synapse, poisson_generator, spike_generator, spike_recorder,
-multimeter, voltmeter):
+for the models on its path (iaf_psc_delta, iaf_psc_exp, iaf_psc_alpha,
+aeif_cond_alpha, static_synapse, stdp_pl_synapse_hom, poisson_generator,
+spike_generator, spike_recorder, multimeter, voltmeter):
 
     import nestgpu as nest
     nest.ResetKernel()
@@ -38,7 +38,8 @@ __version__ = "3.10.0-b200"
 
 __all__ = ["ResetKernel", "Create", "Connect", "Simulate", "Run", "Prepare", "Cleanup", "RunManager", "GetStatus",
            "SetStatus", "GetConnections", "GetKernelStatus", "SetKernelStatus", "SetDefaults", "GetDefaults",
-           "NodeCollection", "SynapseCollection", "Models", "BadProperty", "KernelException", "set", "get",
+           "NodeCollection", "SynapseCollection", "Models", "CopyModel", "BadProperty", "KernelException", "set",
+           "get",
            "random", "math", "engine_stats"]
 
 
@@ -113,15 +114,27 @@ def SetStatus(nodes, params, val=None):
     KERNEL.set_status(nodes.ids, params)
 
 
+def _set_syn_defaults(model, params):
+    d = KERNEL.syn_defaults[model]
+    for k, v in params.items():
+        if k not in d:
+            raise BadProperty(f"Unaccessed dictionary entries for {model}: ['{k}']")
+        if k == "tau_plus" and not float(v) > 0:
+            raise BadProperty("tau_plus must be > 0.")
+        if k == "weight" and KERNEL.syn_kind[model] == "stdp_pl" and float(v) < 0:
+            raise BadProperty("Weight of stdp_pl_synapse_hom must be non-negative")
+    for k, v in params.items():
+        d[k] = float(v)
+    if KERNEL.syn_kind[model] == "stdp_pl" and model in KERNEL.pl_models:
+        KERNEL.structure_changed = True    # common properties of existing connections changed
+
+
 def SetDefaults(model, params, val=None):
     if isinstance(params, str):
         params = {params: val}
-    if model in ("static_synapse", "static_synapse_hom_w"):
-        d = KERNEL.syn_defaults["static_synapse"]
-        for k, v in params.items():
-            if k not in d:
-                raise BadProperty(f"Unaccessed dictionary entries for {model}: ['{k}']")
-            d[k] = float(v)
+    if model in KERNEL.syn_defaults:
+        KERNEL.settle()
+        _set_syn_defaults(model, params)
         return
     if model in KERNEL.models:
         KERNEL.models[model].set_defaults(params)
@@ -133,8 +146,9 @@ def SetDefaults(model, params, val=None):
 
 
 def GetDefaults(model, keys=None):
-    if model in ("static_synapse", "static_synapse_hom_w"):
-        d = dict(KERNEL.syn_defaults["static_synapse"])
+    if model in KERNEL.syn_defaults:
+        d = dict(KERNEL.syn_defaults[model])
+        d["synapse_model"] = model
     elif model in KERNEL.models:
         d = KERNEL.models[model].get_defaults()
         d["model"] = model
@@ -150,9 +164,29 @@ def GetDefaults(model, keys=None):
     return tuple(d[k] for k in keys)
 
 
+def CopyModel(existing, new, params=None):
+    """Copy a synapse model under a new name with changed defaults
+    (hl_api_models.py CopyModel); copies of neuron and device models are not
+    on the engine's path."""
+    if new in KERNEL.syn_defaults or new in KERNEL.models or new in KERNEL.model_defaults:
+        raise KernelException(f"NewModelNameExists: {new}")
+    if existing not in KERNEL.syn_defaults:
+        if existing in KERNEL.models or existing in KERNEL.model_defaults:
+            raise NotImplementedError("CopyModel of neuron and device models is not on the engine's path")
+        raise KernelException(f"UnknownSynapseType: {existing}")
+    KERNEL.syn_defaults[new] = dict(KERNEL.syn_defaults[existing])
+    KERNEL.syn_kind[new] = KERNEL.syn_kind[existing]
+    if params:
+        try:
+            _set_syn_defaults(new, dict(params))
+        except Exception:
+            del KERNEL.syn_defaults[new], KERNEL.syn_kind[new]
+            raise
+
+
 def Models(mtype="all", sel=None):
     nodes = sorted(list(NEURON_MODELS) + list(DEVICE_MODELS))
-    syn = ["static_synapse", "static_synapse_hom_w"]
+    syn = sorted(KERNEL.syn_defaults)
     out = nodes if mtype == "nodes" else syn if mtype == "synapses" else nodes + syn
     return tuple(m for m in out if sel is None or sel in m)
 

@@ -34,6 +34,7 @@ EXPORTED = [
     "ng_set_profiling", "ng_set_stream", "ng_set_graph_slices", "ng_debug_coefficients", "ng_net_add", "ng_net_poll",
     "ng_net_spikes", "ng_net_get_var", "ng_net_get_connections", "ng_net_remove", "ng_net_capacity",
     "ng_simulate_noalloc", "ng_set_tuning", "ng_get_tuning", "ng_set_option", "ng_update",
+    "ng_set_plastic_connections", "ng_get_plastic_weights",
 ]
 
 
@@ -234,6 +235,8 @@ def load():
         "ng_get_tuning": ([P, P], ctypes.c_int),
         "ng_set_option": ([P, ctypes.c_char_p, dbl], ctypes.c_int),
         "ng_update": ([P, i64, i32, i32], ctypes.c_int),
+        "ng_set_plastic_connections": ([P, i64, P, P, P, P, dbl, dbl, dbl, dbl], ctypes.c_int),
+        "ng_get_plastic_weights": ([P, P, i64], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -280,8 +283,10 @@ UPDATE_VARIANTS = {0: "k_update_iaf (one thread per neuron, 4 lags of inputs at 
                    1: "k_update_iaf (one thread per neuron, 8 lags of inputs at a time)",
                    2: "k_update_iaf2 (two-phase, 32 neurons per 256-thread CTA)",
                    3: "k_update_iaf2 (two-phase, 32 neurons per 128-thread CTA)",
-                   4: "k_update_aeif"}
-UPDATE_KERNELS = {0: "k_update_iaf", 1: "k_update_iaf", 2: "k_update_iaf2", 3: "k_update_iaf2", 4: "k_update_aeif"}
+                   4: "k_update_aeif",
+                   5: "k_run_slices (persistent: node update and delivery of many slices in one cooperative launch)"}
+UPDATE_KERNELS = {0: "k_update_iaf", 1: "k_update_iaf", 2: "k_update_iaf2", 3: "k_update_iaf2", 4: "k_update_aeif",
+                  5: "k_run_slices"}
 
 
 def tuning_dict(t):
@@ -372,6 +377,22 @@ class Engine:
         delay_steps = np.ascontiguousarray(delay_steps, dtype=np.int32)
         check(self.L.ng_set_connections_coo(self.handle, int(n_src), len(source), _p(source), _p(target),
                                             _p(weight), _p(delay_steps)))
+
+    def set_plastic(self, row_ptr, target, weight, delay_steps, lam=0.1, alpha=1.0, mu=0.4, tau_plus=20.0):
+        """stdp_pl_synapse_hom connections as a CSR over neuron sources."""
+        row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        target = np.ascontiguousarray(target, dtype=np.int32)
+        weight = np.ascontiguousarray(weight, dtype=np.float64)
+        delay_steps = np.ascontiguousarray(delay_steps, dtype=np.int32)
+        check(self.L.ng_set_plastic_connections(self.handle, len(row_ptr) - 1, _p(row_ptr), _p(target), _p(weight),
+                                                _p(delay_steps), float(lam), float(alpha), float(mu),
+                                                float(tau_plus)))
+        self._n_plastic = len(target)
+
+    def plastic_weights(self):
+        out = np.empty(getattr(self, "_n_plastic", 0), dtype=np.float64)
+        check(self.L.ng_get_plastic_weights(self.handle, _p(out), len(out)))
+        return out
 
     def set_spike_schedule(self, emit_step, source):
         emit_step = np.ascontiguousarray(emit_step, dtype=np.int64)

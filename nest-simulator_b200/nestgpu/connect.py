@@ -10,7 +10,7 @@ connect-arrays path of ``nest.Connect``).
 
 import numpy as np
 
-from .kernel import KERNEL, KernelException
+from .kernel import KERNEL, STDP_COMMON, KernelException
 from .models import BadProperty
 from .nodes import NodeCollection
 from .random import Parameter
@@ -81,9 +81,15 @@ def connect(pre, post, conn_spec=None, syn_spec=None, return_synapsecollection=F
         syn_spec = {"synapse_model": syn_spec}
     syn_spec = dict(syn_spec)
     model = syn_spec.pop("synapse_model", "static_synapse")
-    if model not in ("static_synapse", "static_synapse_hom_w"):
-        raise BadProperty(f"synapse model '{model}' is not on the engine's path (static_synapse only)")
-    defaults = K.syn_defaults["static_synapse"]
+    if model not in K.syn_defaults:
+        raise BadProperty(f"synapse model '{model}' is not on the engine's path (static_synapse and "
+                          "stdp_pl_synapse_hom and their copies)")
+    defaults = K.syn_defaults[model]
+    plastic = K.syn_kind[model] == "stdp_pl"
+    common = [k for k in STDP_COMMON if k in syn_spec]
+    if plastic and common:
+        # stdp_pl_synapse_hom's STDPPLHomCommonProperties are per model
+        raise BadProperty(f"{common} are common properties of {model}: set them with SetDefaults or CopyModel")
     allow_autapses = bool(conn_spec.pop("allow_autapses", True))
     allow_multapses = bool(conn_spec.pop("allow_multapses", True))
     npre, npost = len(spre), len(spost)
@@ -170,37 +176,51 @@ def connect(pre, post, conn_spec=None, syn_spec=None, return_synapsecollection=F
         d = np.asarray(d, dtype=np.float64).ravel()
     wv = _values(w, n, rng)
     dv = _values(d, n, rng)
-    K.add_edges(s, t, wv, dv)
+    if plastic:
+        K.add_plastic_edges(s, t, wv, dv, model)
+    else:
+        K.add_edges(s, t, wv, dv)
     if return_synapsecollection:
-        return get_connections(NodeCollection(np.unique(s)), NodeCollection(np.unique(t)))
+        return get_connections(NodeCollection(np.unique(s)), NodeCollection(np.unique(t)), model)
     return None
 
 
 class SynapseCollection:
-    """Connections selected by GetConnections (indices into the kernel's
-    edge table, sorted by source then target)."""
+    """Connections selected by GetConnections: indices into the kernel's
+    static edge table and into its plastic (stdp_pl_synapse_hom) table, each
+    sorted by source then target."""
 
-    def __init__(self, idx):
+    def __init__(self, idx, pidx=None):
         self._idx = np.asarray(idx, dtype=np.int64)
+        self._pidx = np.zeros(0, dtype=np.int64) if pidx is None else np.asarray(pidx, dtype=np.int64)
 
     def __len__(self):
-        return len(self._idx)
+        return len(self._idx) + len(self._pidx)
 
     def _col(self, key):
+        i, j = self._idx, self._pidx
         src, tgt, w, d = KERNEL.edges()
-        i = self._idx
+        if len(j):
+            ps, pt, pw, pd, pm = KERNEL.plastic_edges()
+        else:
+            ps = pt = pd = np.zeros(0, dtype=np.int32)
+            pw, pm = np.zeros(0), np.zeros(0, dtype=np.int16)
         if key == "source":
-            return src[i].astype(np.int64)
+            return np.concatenate([src[i], ps[j]]).astype(np.int64)
         if key == "target":
-            return tgt[i].astype(np.int64)
+            return np.concatenate([tgt[i], pt[j]]).astype(np.int64)
         if key == "weight":
-            return w[i]
+            return np.concatenate([w[i], pw[j]])
         if key == "delay":
-            return d[i].astype(np.int64) * KERNEL.ms_per_step
+            return np.concatenate([d[i], pd[j]]).astype(np.int64) * KERNEL.ms_per_step
         if key == "synapse_model":
-            return np.array(["static_synapse"] * len(i), dtype=object)
+            names = np.array(KERNEL.pl_models or [""], dtype=object)
+            return np.concatenate([np.array(["static_synapse"] * len(i), dtype=object), names[pm[j]]])
         if key in ("receptor", "port", "target_thread", "synapse_id"):
-            return np.zeros(len(i), dtype=np.int64)
+            return np.zeros(len(self), dtype=np.int64)
+        if key in STDP_COMMON and len(i) == 0:
+            names = [KERNEL.pl_models[k] for k in pm[j]]
+            return np.array([KERNEL.syn_defaults[m][key] for m in names], dtype=np.float64)
         raise KeyError(key)
 
     def get(self, keys=None, output=""):
@@ -221,18 +241,30 @@ class SynapseCollection:
 
     def set(self, params=None, **kw):
         params = dict(params or {}, **kw)
+        ni = len(self._idx)
         src, tgt, w, d = KERNEL.edges()
+        if len(self._pidx):
+            _, _, pw, pd, _ = KERNEL.plastic_edges()
         for k, v in params.items():
-            vals = np.broadcast_to(np.asarray(v, dtype=np.float64), (len(self._idx),))
+            vals = np.broadcast_to(np.asarray(v, dtype=np.float64), (len(self),))
             if k == "weight":
-                w[self._idx] = vals
+                if len(self._pidx) and np.any(vals[ni:] < 0):
+                    raise BadProperty("Weight of stdp_pl_synapse_hom must be non-negative")
+                w[self._idx] = vals[:ni]
+                if len(self._pidx):
+                    pw[self._pidx] = vals[ni:]
             elif k == "delay":
                 steps = KERNEL.delay_ms_to_steps(vals)
                 if np.any(steps < 1):
                     raise BadProperty("Delay must be greater than or equal to resolution")
-                d[self._idx] = steps
+                d[self._idx] = steps[:ni]
+                if len(self._pidx):
+                    pd[self._pidx] = steps[ni:]
+            elif k in STDP_COMMON:
+                raise BadProperty(f"'{k}' is a common property of stdp_pl_synapse_hom: set it with SetDefaults")
             else:
-                raise BadProperty(f"cannot set '{k}' on static_synapse connections")
+                raise BadProperty(f"cannot set '{k}' on these connections")
+        # the engine is rebuilt at the next run (the plastic traces start over)
         KERNEL.structure_changed = True
 
     def __getattr__(self, name):
@@ -250,7 +282,17 @@ class SynapseCollection:
 
 
 def get_connections(source=None, target=None, synapse_model=None, synapse_label=None):
-    if synapse_model not in (None, "static_synapse"):
-        return SynapseCollection([])
-    return SynapseCollection(KERNEL.get_connections(None if source is None else _ids(source),
-                                                    None if target is None else _ids(target)))
+    """Static connections are reported as static_synapse; the plastic ones
+    under the synapse model they were made with."""
+    kind = None if synapse_model is None else KERNEL.syn_kind.get(synapse_model)
+    s = None if source is None else _ids(source)
+    t = None if target is None else _ids(target)
+    idx = KERNEL.get_connections(s, t) if kind in (None, "static") else []
+    pidx = KERNEL.get_connections(s, t, plastic=True) if kind in (None, "stdp_pl") else []
+    if synapse_model is not None and kind == "stdp_pl" and len(pidx):
+        _, _, _, _, pm = KERNEL.plastic_edges()
+        names = np.array(KERNEL.pl_models, dtype=object)
+        pidx = pidx[names[pm[pidx]] == synapse_model]
+    if synapse_model is not None and kind is None:
+        idx, pidx = [], []
+    return SynapseCollection(idx, pidx)

@@ -24,6 +24,11 @@ from .random import Parameter
 INF_STEPS = 2**62
 
 
+STATIC_SYNAPSES = ("static_synapse", "static_synapse_hom_w", "static_synapse_hpc")
+STDP_SYNAPSES = ("stdp_pl_synapse_hom", "stdp_pl_synapse_hom_hpc")
+STDP_COMMON = ("lambda", "alpha", "mu", "tau_plus")
+
+
 class KernelException(RuntimeError):
     """Invalid kernel operation (the reference's KernelException)."""
 
@@ -67,7 +72,16 @@ class Kernel:
         self.user_max_delay = None
         self.models = {name: cls() for name, cls in NEURON_MODELS.items()}
         self.model_defaults = {m: dict(p) for m, p in DEVICE_MODELS.items()}
-        self.syn_defaults = {"static_synapse": {"weight": 1.0, "delay": 1.0}}
+        # synapse models: defaults and kind ("static" or "stdp_pl"); the _hpc
+        # variants are the reference's thread-indexed copies of the same rules
+        stdp = {"weight": 1.0, "delay": 1.0, "lambda": 0.1, "alpha": 1.0, "mu": 0.4, "tau_plus": 20.0}
+        self.syn_defaults = {m: {"weight": 1.0, "delay": 1.0} for m in STATIC_SYNAPSES}
+        self.syn_defaults.update({m: dict(stdp) for m in STDP_SYNAPSES})
+        self.syn_kind = {m: "static" for m in STATIC_SYNAPSES}
+        self.syn_kind.update({m: "stdp_pl" for m in STDP_SYNAPSES})
+        self.pl_src, self.pl_tgt, self.pl_w, self.pl_d, self.pl_model = [], [], [], [], []
+        self.pl_models = []     # synapse model names of the plastic connections (index in pl_model)
+        self._pl_fresh = True   # the host copy of the plastic weights is the engine's
         self.node_kind = np.zeros(0, dtype=np.int8)     # 0 neuron, 1 device
         self.node_model = []                             # model name per node
         self.node_local = np.zeros(0, dtype=np.int64)    # index in model storage / device list
@@ -333,6 +347,66 @@ class Kernel:
         self.n_conns += n
         self.structure_changed = True
 
+    def add_plastic_edges(self, src, tgt, w, d_ms, model):
+        """stdp_pl_synapse_hom connections (neuron -> neuron)."""
+        self.settle()
+        self._pull_plastic()
+        src = np.asarray(src, dtype=np.int64).ravel()
+        tgt = np.asarray(tgt, dtype=np.int64).ravel()
+        n = len(src)
+        if n == 0:
+            return
+        w = np.broadcast_to(np.asarray(w, dtype=np.float64), (n,)).copy()
+        steps = self.delay_ms_to_steps(np.broadcast_to(np.asarray(d_ms, dtype=np.float64), (n,)))
+        if np.any(steps < 1):
+            raise BadProperty("Delay must be greater than or equal to resolution")
+        if src.max() > len(self.node_kind) or tgt.max() > len(self.node_kind) or src.min() < 1 or tgt.min() < 1:
+            raise KernelException("Connect: unknown node id")
+        if np.any(self.node_kind[src - 1] != 0) or np.any(self.node_kind[tgt - 1] != 0):
+            raise KernelException(f"{model} connects neurons to neurons")
+        if np.any(w < 0):
+            raise BadProperty("Weight of stdp_pl_synapse_hom must be non-negative (power-law facilitation)")
+        if model not in self.pl_models:
+            self.pl_models.append(model)
+        self.pl_src.append(src.astype(np.int32))
+        self.pl_tgt.append(tgt.astype(np.int32))
+        self.pl_w.append(w)
+        self.pl_d.append(steps.astype(np.int32))
+        self.pl_model.append(np.full(n, self.pl_models.index(model), dtype=np.int16))
+        self.structure_changed = True
+
+    def plastic_edges(self):
+        """(src, tgt, weight, delay steps, model index) of the plastic
+        connections; weights as the engine has them after the last run."""
+        self._pull_plastic()
+        if not self.pl_src:
+            z = np.zeros(0, dtype=np.int32)
+            return z, z, np.zeros(0), z, np.zeros(0, dtype=np.int16)
+        if len(self.pl_src) > 1:
+            for a in ("pl_src", "pl_tgt", "pl_w", "pl_d", "pl_model"):
+                setattr(self, a, [np.concatenate(getattr(self, a))])
+        return self.pl_src[0], self.pl_tgt[0], self.pl_w[0], self.pl_d[0], self.pl_model[0]
+
+    def _pull_plastic(self):
+        c = self.compiled
+        if self.engine is None or c is None or c.get("pl") is None or self._pl_fresh:
+            return
+        self.settle()
+        self._pl_fresh = True
+        w = self.engine.plastic_weights()
+        self.pl_w[0][c["pl"]["order"]] = w
+
+    def stdp_common(self):
+        """The common properties of the network's plastic connections (one
+        set per network on the engine)."""
+        if not self.pl_models:
+            return None
+        sets = {tuple(float(self.syn_defaults[m][k]) for k in STDP_COMMON) for m in self.pl_models}
+        if len(sets) > 1:
+            raise NotImplementedError("stdp_pl_synapse_hom models with different common properties in one network "
+                                      "are not supported by the engine")
+        return dict(zip(STDP_COMMON, sets.pop()))
+
     def edges(self):
         if not self.conn_src:
             z = np.zeros(0, dtype=np.int32)
@@ -387,13 +461,15 @@ class Kernel:
         if np.any(bad):
             k = int(np.nonzero(bad)[0][0])
             raise KernelException(f"Connection {s_mod[k]} -> {t_mod[k]} is not supported by the engine")
+        psrc, ptgt, pw, pdl, _ = self.plastic_edges()
+        alld = np.concatenate([dsteps, pdl]) if len(pdl) else dsteps
         # delay extrema over all connections, devices included
         if self.user_min_delay is not None:
             min_d, max_d = self.user_min_delay, self.user_max_delay
-            if len(dsteps) and (dsteps.min() < min_d or dsteps.max() > max_d):
+            if len(alld) and (alld.min() < min_d or alld.max() > max_d):
                 raise BadProperty("Connection delays lie outside the user-set min_delay/max_delay")
-        elif len(dsteps):
-            min_d, max_d = int(dsteps.min()), int(dsteps.max())
+        elif len(alld):
+            min_d, max_d = int(alld.min()), int(alld.max())
         else:
             min_d = max_d = 1
         c = {"blocks": blocks, "N": N, "n_src": n_src, "min_delay": min_d, "max_delay": max_d,
@@ -403,6 +479,15 @@ class Kernel:
         c["tgt"] = node_to_eng[tgt[m_syn]].astype(np.int32)
         c["w"] = w[m_syn]
         c["d"] = dsteps[m_syn].astype(np.int32)
+        # plastic connections: a CSR over neuron sources (stable order by source)
+        c["pl"] = None
+        if len(psrc):
+            es, et = node_to_eng[psrc], node_to_eng[ptgt]
+            order = np.argsort(es, kind="stable")
+            row = np.zeros(N + 1, dtype=np.int64)
+            np.cumsum(np.bincount(es, minlength=N), out=row[1:])
+            c["pl"] = {"row": row, "tgt": et[order].astype(np.int32), "w": pw[order], "d": pdl[order],
+                       "order": order, "common": self.stdp_common()}
         # Poisson drive, fused per target neuron
         rate = np.zeros(N)
         pw = np.zeros(N)
@@ -493,6 +578,7 @@ class Kernel:
         """Copy engine state back into the front-end storage."""
         if self.engine is None or self.compiled is None:
             return
+        self._pull_plastic()
         for bi, b in enumerate(self.compiled["blocks"]):
             st = self.models[b["model"]]
             for k in st.state_vars:
@@ -542,6 +628,12 @@ class Kernel:
                 if istep is not None:
                     eng.set_var(bi, "integration_step", istep)
         eng.set_connections_coo(c["src"], c["tgt"], c["w"], c["d"], c["n_src"])
+        if c["pl"] is not None:
+            p = c["pl"]
+            cm = p["common"]
+            eng.set_plastic(p["row"], p["tgt"], p["w"], p["d"], lam=cm["lambda"], alpha=cm["alpha"], mu=cm["mu"],
+                            tau_plus=cm["tau_plus"])
+        self._pl_fresh = True
         if len(c["sched_step"]):
             eng.set_spike_schedule(c["sched_step"], c["sched_src"])
         if np.any(c["pois_rate"] > 0):
@@ -627,6 +719,7 @@ class Kernel:
             while left > 0:
                 k = min(part, left)
                 self.engine.simulate_async(k)
+                self._pl_fresh = False
                 self.clock += k
                 left -= k
                 self._unsettled = True
@@ -739,11 +832,14 @@ class Kernel:
 
     def num_connections(self):
         src, tgt, _, _ = self.edges()
-        return len(src)
+        return len(src) + sum(len(a) for a in self.pl_src)
 
-    def get_connections(self, source=None, target=None):
+    def get_connections(self, source=None, target=None, plastic=False):
         self.settle()
-        src, tgt, w, d = self.edges()
+        if plastic:
+            src, tgt = self.plastic_edges()[:2]
+        else:
+            src, tgt, w, d = self.edges()
         m = np.ones(len(src), dtype=bool)
         if source is not None:
             m &= np.isin(src, np.asarray(source))

@@ -315,6 +315,33 @@ class AeifCondAlpha(NeuronModel):
         return self.data[key][idx]
 
 
+def _archiving(cls):
+    """Give an iaf model ArchivingNode's tau_minus (nestkernel/archiving_node.cpp:232-245):
+    the time constant of the postsynaptic trace that STDP connections onto the
+    neuron read (default 20 ms; every value must be > 0)."""
+    model_set = cls.set
+
+    def set(self, idx, d):
+        tm = None
+        if "tau_minus" in d:
+            d = dict(d)
+            tm = _as(d.pop("tau_minus"), len(idx))
+            if np.any(tm <= 0):
+                raise BadProperty("All time constants must be strictly positive.")
+        model_set(self, idx, d)
+        if tm is not None:
+            self.data["tau_minus"][idx] = tm
+            self._touch("tau_minus")
+
+    cls.set = set
+    cls.storage = dict(cls.storage, tau_minus=20.0)
+    cls.engine_vars = dict(cls.engine_vars, tau_minus="tau_minus")
+    cls.public = tuple(sorted(cls.public + ("tau_minus",)))
+
+
+for _m in (IafPscDelta, IafPscExp, IafPscAlpha):
+    _archiving(_m)
+
 NEURON_MODELS = {"iaf_psc_delta": IafPscDelta, "iaf_psc_exp": IafPscExp, "iaf_psc_alpha": IafPscAlpha,
                  "aeif_cond_alpha": AeifCondAlpha}
 

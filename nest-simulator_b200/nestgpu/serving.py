@@ -17,6 +17,7 @@ independent.
 """
 
 import math
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -263,3 +264,136 @@ def latency_summary(requests):
     lat = np.array([r.latency for r in requests])
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "max_s": float(lat.max())}
+
+
+class OnlineBatcher:
+    """Continuous batching of requests that arrive while the engine runs (the
+    serving routes of nestgpu.server): one worker thread owns the FP32
+    serving engine; ``submit`` queues a Brunel-type network and returns its
+    id at once; the worker admits queued networks as pool space frees up,
+    advances every live network in chunks of ``chunk_slices`` slices, and
+    retires a network (spikes read, pool space freed) after its duration,
+    as run_batched does for a stream known in advance."""
+
+    def __init__(self, precision="fp32", capacity_neurons=2_000_000, capacity_edges=1_200_000_000, max_networks=512,
+                 device=0, chunk_slices=32, clock=time.perf_counter):
+        self.clock = clock
+        self.t0 = clock()
+        self.cv = threading.Condition()
+        self.waiting = []
+        self.requests = {}
+        self.active = {}
+        self.next_id = 0
+        self.closed = False
+        self.error = None
+        self.cached_stats = {}
+        self.chunk = chunk_slices
+        self._args = (precision, capacity_neurons, capacity_edges, max_networks, device)
+        self.ready = threading.Event()
+        self.thread = threading.Thread(target=self._loop, daemon=True)
+        self.thread.start()
+        self.ready.wait(timeout=120)
+        if self.error:
+            raise RuntimeError(self.error)
+
+    def submit(self, n, g=5.0, eta=2.0, t_ms=1000.0, seed=1):
+        n = int(n)
+        if n < 2:
+            raise ValueError("a network needs at least 2 neurons")
+        k_exc = int(min(round(0.1 * n), 1000))
+        with self.cv:
+            rid = self.next_id
+            self.next_id += 1
+            r = Request(rid=rid, arrival=self.clock() - self.t0, n=n, n_exc=int(round(0.8 * n)), k_exc=max(1, k_exc),
+                        k_inh=max(1, k_exc // 4), g=float(g), eta=float(eta), steps=int(round(t_ms / H)),
+                        seed=int(seed))
+            r.enqueued = r.arrival
+            self.requests[rid] = r
+            self.waiting.append(r)
+            self.cv.notify_all()
+        return rid
+
+    def result(self, rid, spikes=False):
+        with self.cv:
+            r = self.requests.get(rid)
+            if r is None:
+                return None
+            if r.spikes is None:
+                return {"request": rid, "status": "running" if not math.isnan(r.admitted) else "queued"}
+        rate, cv = spike_stats(r)
+        out = {"request": rid, "status": "done", "n": r.n, "steps": r.steps, "spikes": int(len(r.spikes[0])),
+               "rate_hz": rate, "cv_isi": cv, "latency_s": r.latency, "admitted_after_s": r.admitted - r.enqueued}
+        if spikes:
+            out["senders"] = r.spikes[0]
+            out["times_ms"] = r.spikes[1] * H
+        return out
+
+    def stats(self):
+        with self.cv:
+            return dict(self.cached_stats, queued=len(self.waiting), live=len(self.active),
+                        done=sum(1 for r in self.requests.values() if r.spikes is not None))
+
+    def close(self):
+        with self.cv:
+            self.closed = True
+            self.cv.notify_all()
+        self.thread.join(timeout=60)
+
+    def _loop(self):
+        try:
+            eng = new_engine(self._args[0], capacity_neurons=self._args[1], capacity_edges=self._args[2],
+                             max_networks=self._args[3], device=self._args[4])
+        except Exception as err:  # surfaced by the constructor
+            self.error = f"serving engine: {err}"
+            self.ready.set()
+            return
+        self.ready.set()
+        now_steps = eng.stats()["clock_steps"]
+        try:
+            while True:
+                with self.cv:
+                    if self.closed:
+                        break
+                    if not self.waiting and not self.active:
+                        self.cv.wait(timeout=0.5)
+                        continue
+                    waiting = list(self.waiting)
+                # admissions (engine calls outside the lock: submit never waits for the device)
+                if waiting:
+                    free_n, free_e = eng.net_capacity()
+                    admitted = []
+                    for r in waiting:
+                        fn, fe = footprint(r)
+                        if fn <= free_n and fe <= free_e and len(self.active) < eng.max_networks:
+                            nid = _admit(eng, r)
+                            if nid is not None:
+                                r.admitted = self.clock() - self.t0
+                                self.active[nid] = (r, now_steps + r.steps)
+                                admitted.append(r)
+                                free_n, free_e = eng.net_capacity()
+                    with self.cv:
+                        self.waiting = [r for r in self.waiting if r not in admitted]
+                if not self.active:
+                    time.sleep(0.01)
+                    continue
+                left = max(end for _, end in self.active.values()) - now_steps
+                ended = now_steps
+                if left <= 0:
+                    eng.sync()
+                else:
+                    slices = max(1, min(self.chunk, -(-left // DELAY_STEPS)))
+                    eng.simulate_async(slices * DELAY_STEPS)
+                    now_steps += slices * DELAY_STEPS
+                done = [k for k, (_, end) in self.active.items() if end <= ended]
+                results = {nid: eng.net_spikes(nid) for nid in done}
+                for nid in done:
+                    r, _ = self.active.pop(nid)
+                    eng.net_remove(nid)
+                    with self.cv:
+                        r.spikes = results[nid]
+                        r.finished = self.clock() - self.t0
+                st = eng.stats()
+                with self.cv:
+                    self.cached_stats = {k: st[k] for k in ("clock_steps", "spikes", "syn_events", "gather_slices")}
+        finally:
+            eng.close()

@@ -6,6 +6,7 @@ data is not used (synthetic stand-ins with the stated shapes).
 c1: Poisson-driven iaf_psc_exp network, 12,500 neurons (10,000 exc, 2,500
     inh), tau_syn 0.5 ms, fixed_indegree K_E=1,000, K_I=250, J=87.8 pA, g=5,
     delay 1.5 ms, 8 kHz Poisson drive per neuron, V_m ~ N(-58, 10) mV.
+hpc_benchmark: the reference's HPC benchmark (iaf_psc_alpha, STDP E->E).
 """
 
 import math
@@ -67,6 +68,69 @@ def brunel_exp_batch(nest, copies, n_exc=10000, n_inh=2500, k_exc=1000, k_inh=25
             recs.append(sr)
         pops.append(pop)
     return pops, recs
+
+
+# ---------------------------------------------------------------------------
+# hpc_benchmark: the reference's HPC benchmark network (pynest/examples/
+# hpc_benchmark.py): iaf_psc_alpha, NE = 9000 scale, NI = 2250 scale,
+# fixed in-degrees CE = 9000, CI = 2250 (independent of scale), E->E
+# connections stdp_pl_synapse_hom, the rest static, delays 1.5 ms, one
+# Poisson drive at 1.685 times the threshold rate.
+# ---------------------------------------------------------------------------
+HPC_TAU_SYN = 0.32582722403722841
+
+
+def alpha_pa_per_mv(tau_m, tau_syn, C_m):
+    """Current amplitude (pA) of an alpha-shaped PSC whose PSP peaks at 1 mV
+    in a leaky membrane: the PSP's maximum lies where its derivative
+    vanishes, t* = (W_-1(-exp(-1/a)/a) stretched) with a = tau_m / tau_syn,
+    from the Lambert W function's -1 branch."""
+    from scipy.special import lambertw
+
+    a = tau_m / tau_syn
+    b = 1.0 / tau_syn - 1.0 / tau_m
+    t_peak = (1.0 / b) * (-lambertw(-math.exp(-1.0 / a) / a, k=-1).real - 1.0 / a)
+    v_max = (math.e / (tau_syn * C_m * b)) * ((math.exp(-t_peak / tau_m) - math.exp(-t_peak / tau_syn)) / b
+                                              - t_peak * math.exp(-t_peak / tau_syn))
+    return 1.0 / v_max
+
+
+def hpc_benchmark(nest, scale=1.0, indegree_scale=1.0, precision="fp64", seed=4242, record=True, plastic=True):
+    """Build the HPC benchmark network; returns (E, I, recorder).
+    indegree_scale < 1 thins every in-degree (for CPU-sized checks)."""
+    nest.ResetKernel()
+    nest.set(resolution=0.1, rng_seed=seed, precision=precision)
+    NE, NI = int(9000 * scale), int(2250 * scale)
+    tau_m, C_m, V_th = 10.0, 250.0, 20.0
+    params = {"E_L": 0.0, "C_m": C_m, "tau_m": tau_m, "t_ref": 0.5, "V_th": V_th, "V_reset": 0.0,
+              "tau_syn_ex": HPC_TAU_SYN, "tau_syn_in": HPC_TAU_SYN, "tau_minus": 30.0, "V_m": 5.7}
+    E = nest.Create("iaf_psc_alpha", NE, params=params)
+    I = nest.Create("iaf_psc_alpha", NI, params=params)
+    rng = np.random.default_rng(seed)
+    E.set(V_m=rng.normal(5.7, 7.2, NE))
+    I.set(V_m=rng.normal(5.7, 7.2, NI))
+    CE, CI = int(9000 * indegree_scale), int(2250 * indegree_scale)
+    JE = alpha_pa_per_mv(tau_m, HPC_TAU_SYN, C_m) * 0.14          # 0.14 mV peak EPSP
+    nu_th = V_th / (9000 * tau_m / C_m * JE * math.e * HPC_TAU_SYN)
+    pg = nest.Create("poisson_generator", params={"rate": 1.685 * nu_th * 9000 * 1000.0})
+    nest.SetDefaults("static_synapse_hpc", {"delay": 1.5})
+    nest.CopyModel("static_synapse_hpc", "syn_ex", {"weight": JE})
+    nest.CopyModel("static_synapse_hpc", "syn_in", {"weight": -5.0 * JE})
+    ee = "stdp_pl_synapse_hom_hpc" if plastic else "syn_ex"
+    nest.SetDefaults("stdp_pl_synapse_hom_hpc", {"delay": 1.5, "alpha": 0.0513, "lambda": 0.1, "mu": 0.4,
+                                                 "tau_plus": 15.0, "weight": JE})
+    nest.Connect(pg, E, {"rule": "all_to_all"}, {"synapse_model": "syn_ex"})
+    nest.Connect(pg, I, {"rule": "all_to_all"}, {"synapse_model": "syn_ex"})
+    kin = {"allow_autapses": False, "allow_multapses": True}
+    nest.Connect(E, E, dict(rule="fixed_indegree", indegree=CE, **kin), {"synapse_model": ee})
+    nest.Connect(I, E, dict(rule="fixed_indegree", indegree=CI, **kin), {"synapse_model": "syn_in"})
+    nest.Connect(E, I, dict(rule="fixed_indegree", indegree=CE, **kin), {"synapse_model": "syn_ex"})
+    nest.Connect(I, I, dict(rule="fixed_indegree", indegree=CI, **kin), {"synapse_model": "syn_in"})
+    sr = None
+    if record:
+        sr = nest.Create("spike_recorder")
+        nest.Connect(E + I, sr, syn_spec={"delay": 1.5})
+    return E, I, sr
 
 
 # ---------------------------------------------------------------------------

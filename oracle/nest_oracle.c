@@ -337,11 +337,29 @@ struct orc_net
   int64_t sp_len, sp_cap;
   int64_t syn_events;
   int prepared;
+  /* stdp_pl_synapse_hom connections (models/stdp_pl_synapse_hom.h) in a CSR
+   * of their own: per-edge weight_, Kplus_ and t_lastspike_ as the
+   * reference's Connection holds them, and the common properties */
+  int64_t pl_nsrc, pl_nnz;
+  int64_t* pl_row;
+  int32_t *pl_tgt, *pl_d;
+  double *pl_w, *pl_Kplus, *pl_tlast;
+  double pl_lambda, pl_alpha, pl_mu, pl_tau_plus_inv;
+  /* ArchivingNode (nestkernel/archiving_node.cpp) of each neuron: tau_minus,
+   * the Kminus trace at the last spike, the spike history (t, Kminus) and
+   * whether it has incoming STDP connections */
+  double *tau_minus, *Kminus, *last_spike;
+  int32_t* n_incoming;
+  double **hist_t, **hist_K;
+  int64_t *hist_len, *hist_cap;
   /* derived coefficients */
   double *P33, *P30, *P22, *P11ex, *P11in, *P21ex, *P21in, *P20, *g0ex, *g0in;
   double *P31ex, *P32ex, *P31in, *P32in, *em1; /* iaf_psc_alpha (P11, P21, P30, g0 above too) */
   int32_t* refr;
 };
+
+static inline double stamp_ms( const orc_net* net, int64_t stamp );
+static void archive_spike( orc_net* net, int64_t i, double t_ms );
 
 static const var_name*
 vars_of( int model )
@@ -440,6 +458,16 @@ orc_create( int model, int64_t n, double h, int32_t min_delay, int32_t max_delay
   }
   net->istep = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double ) );
   net->I_stim = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double ) );
+  net->tau_minus = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double ) );
+  net->Kminus = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double ) );
+  net->last_spike = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double ) );
+  net->n_incoming = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( int32_t ) );
+  net->hist_t = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double* ) );
+  net->hist_K = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( double* ) );
+  net->hist_len = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( int64_t ) );
+  net->hist_cap = calloc( ( size_t ) ( n > 0 ? n : 1 ), sizeof( int64_t ) );
+  for ( int64_t i = 0; i < n; ++i )
+    net->tau_minus[ i ] = 20.0; /* ArchivingNode default */
   for ( int64_t i = 0; i < n; ++i )
     net->istep[ i ] = h;
   net->ring = calloc( ( size_t ) net->L * 2 * ( size_t ) ( n > 0 ? n : 1 ), sizeof( double ) );
@@ -459,6 +487,25 @@ orc_destroy( orc_net* net )
     free( net->v[ i ] );
   free( net->istep );
   free( net->I_stim );
+  for ( int64_t i = 0; i < net->n; ++i )
+  {
+    free( net->hist_t[ i ] );
+    free( net->hist_K[ i ] );
+  }
+  free( net->hist_t );
+  free( net->hist_K );
+  free( net->hist_len );
+  free( net->hist_cap );
+  free( net->tau_minus );
+  free( net->Kminus );
+  free( net->last_spike );
+  free( net->n_incoming );
+  free( net->pl_row );
+  free( net->pl_tgt );
+  free( net->pl_d );
+  free( net->pl_w );
+  free( net->pl_Kplus );
+  free( net->pl_tlast );
   free( net->ring );
   for ( int p = 0; p < net->nparts; ++p )
   {
@@ -513,6 +560,11 @@ orc_set( orc_net* net, const char* name, const double* values )
   if ( strcmp( name, "integration_step" ) == 0 )
   {
     memcpy( net->istep, values, sizeof( double ) * ( size_t ) net->n );
+    return 0;
+  }
+  if ( strcmp( name, "tau_minus" ) == 0 )
+  {
+    memcpy( net->tau_minus, values, sizeof( double ) * ( size_t ) net->n );
     return 0;
   }
   const int s = slot_of( net->model, name );
@@ -1204,10 +1256,169 @@ update_neuron( orc_net* net, int64_t i, int64_t origin, int32_t from, int32_t to
       v[ 23 ][ i ] = ( double ) r;
     }
     if ( mult > 0 )
+    {
       tb_push( tb, ( int32_t ) i, t, mult );
+      archive_spike( net, i, stamp_ms( net, t + 1 ) );
+    }
     if ( trace_row )
       trace_row[ ( int64_t ) lag * net->n_trace_idx + trace_col ] = v[ net->trace_slot ][ i ];
   }
+}
+
+/* ---------------------------------------------------------------------
+ * stdp_pl_synapse_hom (models/stdp_pl_synapse_hom.h) and the spike history
+ * of ArchivingNode (nestkernel/archiving_node.cpp)
+ * ------------------------------------------------------------------- */
+static const double STDP_EPS = 1.0e-6; /* ConnectionManager stdp_eps default */
+
+int
+orc_set_plastic( orc_net* net, int64_t n_src, const int64_t* row_ptr, const int32_t* tgt, const double* w,
+  const int32_t* d, double lambda, double alpha, double mu, double tau_plus )
+{
+  if ( n_src < 0 || n_src > net->n || !( tau_plus > 0 ) )
+  {
+    set_err( "orc_set_plastic: plastic sources are neurons; tau_plus > 0" );
+    return -1;
+  }
+  const int64_t nnz = row_ptr[ n_src ];
+  free( net->pl_row );
+  free( net->pl_tgt );
+  free( net->pl_d );
+  free( net->pl_w );
+  free( net->pl_Kplus );
+  free( net->pl_tlast );
+  net->pl_nsrc = n_src;
+  net->pl_nnz = nnz;
+  net->pl_row = malloc( sizeof( int64_t ) * ( size_t ) ( n_src + 1 ) );
+  memcpy( net->pl_row, row_ptr, sizeof( int64_t ) * ( size_t ) ( n_src + 1 ) );
+  net->pl_tgt = malloc( sizeof( int32_t ) * ( size_t ) ( nnz > 0 ? nnz : 1 ) );
+  net->pl_d = malloc( sizeof( int32_t ) * ( size_t ) ( nnz > 0 ? nnz : 1 ) );
+  net->pl_w = malloc( sizeof( double ) * ( size_t ) ( nnz > 0 ? nnz : 1 ) );
+  net->pl_Kplus = calloc( ( size_t ) ( nnz > 0 ? nnz : 1 ), sizeof( double ) );
+  net->pl_tlast = calloc( ( size_t ) ( nnz > 0 ? nnz : 1 ), sizeof( double ) );
+  memcpy( net->pl_tgt, tgt, sizeof( int32_t ) * ( size_t ) nnz );
+  memcpy( net->pl_d, d, sizeof( int32_t ) * ( size_t ) nnz );
+  memcpy( net->pl_w, w, sizeof( double ) * ( size_t ) nnz );
+  for ( int64_t e = 0; e < nnz; ++e )
+  {
+    if ( tgt[ e ] < 0 || tgt[ e ] >= net->n || d[ e ] < net->min_delay || d[ e ] > net->max_delay )
+    {
+      set_err( "orc_set_plastic: target or delay out of range" );
+      return -1;
+    }
+    net->n_incoming[ tgt[ e ] ] += 1;
+  }
+  net->pl_lambda = lambda;
+  net->pl_alpha = alpha;
+  net->pl_mu = mu;
+  net->pl_tau_plus_inv = 1. / tau_plus;
+  return 0;
+}
+
+int
+orc_get_plastic( orc_net* net, double* w )
+{
+  memcpy( w, net->pl_w, sizeof( double ) * ( size_t ) net->pl_nnz );
+  return 0;
+}
+
+/* Time::get_ms of a stamp and Time::delay_steps_to_ms of a delay: MS_PER_TIC
+ * times the tics, with 1000 tics per ms (nestkernel/nest_time.h) */
+static inline double
+stamp_ms( const orc_net* net, int64_t stamp )
+{
+  const int64_t tps = ( int64_t ) floor( 1000.0 * net->h + 0.5 );
+  return ( 1.0 / 1000.0 ) * ( double ) ( stamp * tps );
+}
+
+static inline double
+delay_ms( const orc_net* net, int32_t d )
+{
+  const int64_t tps = ( int64_t ) floor( 1000.0 * net->h + 0.5 );
+  return ( double ) d * ( ( double ) tps * ( 1.0 / 1000.0 ) );
+}
+
+/* ArchivingNode::set_spiketime (archiving_node.cpp:182-220): the Kminus
+ * trace and the history entry of a neuron with incoming STDP connections
+ * (pruning only frees memory and is left out) */
+static void
+archive_spike( orc_net* net, int64_t i, double t_ms )
+{
+  if ( !net->n_incoming[ i ] )
+  {
+    net->last_spike[ i ] = t_ms;
+    return;
+  }
+  net->Kminus[ i ] = net->Kminus[ i ] * exp( ( net->last_spike[ i ] - t_ms ) * ( 1. / net->tau_minus[ i ] ) ) + 1.0;
+  net->last_spike[ i ] = t_ms;
+  if ( net->hist_len[ i ] == net->hist_cap[ i ] )
+  {
+    net->hist_cap[ i ] = net->hist_cap[ i ] ? 2 * net->hist_cap[ i ] : 16;
+    net->hist_t[ i ] = realloc( net->hist_t[ i ], sizeof( double ) * ( size_t ) net->hist_cap[ i ] );
+    net->hist_K[ i ] = realloc( net->hist_K[ i ], sizeof( double ) * ( size_t ) net->hist_cap[ i ] );
+  }
+  net->hist_t[ i ][ net->hist_len[ i ] ] = t_ms;
+  net->hist_K[ i ][ net->hist_len[ i ] ] = net->Kminus[ i ];
+  ++net->hist_len[ i ];
+}
+
+/* ArchivingNode::get_K_value (archiving_node.cpp:87-113) */
+static double
+k_value( const orc_net* net, int64_t i, double t )
+{
+  for ( int64_t k = net->hist_len[ i ] - 1; k >= 0; --k )
+    if ( t - net->hist_t[ i ][ k ] > STDP_EPS )
+      return net->hist_K[ i ][ k ] * exp( ( net->hist_t[ i ][ k ] - t ) * ( 1. / net->tau_minus[ i ] ) );
+  return 0.;
+}
+
+/* stdp_pl_synapse_hom::send for every plastic out-edge of one spike, then
+ * handle(SpikeEvent&) into the ring (stdp_pl_synapse_hom.h:255-298) */
+static void
+deliver_plastic_spike( orc_net* net, int32_t src, int64_t te, double mult )
+{
+  if ( src >= net->pl_nsrc )
+    return;
+  const int64_t L = net->L, n = net->n;
+  const double t_spike = stamp_ms( net, te + 1 );
+  for ( int64_t e = net->pl_row[ src ]; e < net->pl_row[ src + 1 ]; ++e )
+  {
+    const int32_t tg = net->pl_tgt[ e ];
+    const double dd = delay_ms( net, net->pl_d[ e ] );
+    double w = net->pl_w[ e ];
+    /* get_history( t_lastspike - d, t_spike - d ): entries with
+     * t1 + eps <= t < t2 + eps (archiving_node.cpp:154-180), in order */
+    const double t1_lim = net->pl_tlast[ e ] - dd + STDP_EPS;
+    const double t2_lim = t_spike - dd + STDP_EPS;
+    int64_t fin = net->hist_len[ tg ];
+    while ( fin > 0 && net->hist_t[ tg ][ fin - 1 ] >= t2_lim )
+      --fin;
+    int64_t st = fin;
+    while ( st > 0 && net->hist_t[ tg ][ st - 1 ] >= t1_lim )
+      --st;
+    for ( int64_t k = st; k < fin; ++k )
+    {
+      const double minus_dt = net->pl_tlast[ e ] - ( net->hist_t[ tg ][ k ] + dd );
+      const double kplus = net->pl_Kplus[ e ] * exp( minus_dt * net->pl_tau_plus_inv );
+      w = w + ( net->pl_lambda * pow( w, net->pl_mu ) * kplus );
+    }
+    /* depression by the postsynaptic trace at the arrival */
+    {
+      const double kminus = k_value( net, tg, t_spike - dd );
+      const double new_w = w - ( net->pl_lambda * net->pl_alpha * w * kminus );
+      w = new_w > 0.0 ? new_w : 0.0;
+    }
+    net->pl_w[ e ] = w;
+    const int64_t slot = imod( te + net->pl_d[ e ], L );
+    const double wv = w * mult;
+    if ( net->model == ORC_IAF_PSC_DELTA )
+      net->ring[ ( slot * 2 + 0 ) * n + tg ] += wv;
+    else
+      net->ring[ ( slot * 2 + ( wv > 0 ? 0 : 1 ) ) * n + tg ] += wv;
+    net->pl_Kplus[ e ] = net->pl_Kplus[ e ] * exp( ( net->pl_tlast[ e ] - t_spike ) * net->pl_tau_plus_inv ) + 1.0;
+    net->pl_tlast[ e ] = t_spike;
+  }
+  net->syn_events += ( net->pl_row[ src + 1 ] - net->pl_row[ src ] ) * ( int64_t ) mult;
 }
 
 static void
@@ -1254,6 +1465,10 @@ deliver( orc_net* net, int nthreads )
       }
     }
   }
+  /* plastic connections: the slice's spikes in emission order per source */
+  if ( net->pl_nnz > 0 )
+    for ( int64_t s = 0; s < net->sp_len; ++s )
+      deliver_plastic_spike( net, net->sp_src[ s ], net->sp_t[ s ], ( double ) net->sp_mult[ s ] );
   net->sp_len = 0;
 }
 

@@ -88,6 +88,12 @@ int64_t orc_syn_events( orc_net* net );
 
 /* Propagator restatement (libnestutil/iaf_propagator.cpp) for pinning. */
 double orc_iaf_propagator_exp( double tau_syn, double tau_m, double c_m, double h );
+/* stdp_pl_synapse_hom connections (models/stdp_pl_synapse_hom.h) as a CSR over
+ * neuron sources, with the common properties lambda, alpha, mu, tau_plus;
+ * the postsynaptic neurons' tau_minus is the variable "tau_minus" */
+int orc_set_plastic( orc_net* net, int64_t n_src, const int64_t* row_ptr, const int32_t* tgt, const double* w,
+  const int32_t* d, double lambda, double alpha, double mu, double tau_plus );
+int orc_get_plastic( orc_net* net, double* w );
 /* IAFPropagatorAlpha::evaluate (libnestutil/iaf_propagator.cpp:95-118): out[0] = P31, out[1] = P32 */
 void orc_iaf_propagator_alpha( double tau_syn, double tau_m, double c_m, double h, double* out );
 

@@ -55,6 +55,8 @@ def lib():
         L.orc_get_trace.argtypes = [P, P, i64]
         L.orc_iaf_propagator_exp.restype = dbl
         L.orc_iaf_propagator_exp.argtypes = [dbl, dbl, dbl, dbl]
+        L.orc_set_plastic.argtypes = [P, i64, P, P, P, P, dbl, dbl, dbl, dbl]
+        L.orc_get_plastic.argtypes = [P, P]
         L.orc_iaf_propagator_alpha.restype = None
         L.orc_iaf_propagator_alpha.argtypes = [dbl, dbl, dbl, dbl, P]
         L.orc_philox4x32.argtypes = [P, P, ctypes.c_int, P]
@@ -115,6 +117,30 @@ class OracleNet:
         row_ptr = np.zeros(n_src + 1, dtype=np.int64)
         np.cumsum(counts, out=row_ptr[1:])
         self.set_csr(row_ptr, np.asarray(tgt)[order], np.asarray(w)[order], np.asarray(d)[order], nthreads)
+
+    def set_plastic(self, src, tgt, w, d, lam=0.1, alpha=1.0, mu=0.4, tau_plus=20.0, n_src=None):
+        """stdp_pl_synapse_hom connections (sources are neurons), any order;
+        grouped by source keeping their order."""
+        src = np.asarray(src, dtype=np.int64)
+        n_src = self.n if n_src is None else int(n_src)
+        order = np.argsort(src, kind="stable")
+        row_ptr = np.zeros(n_src + 1, dtype=np.int64)
+        np.cumsum(np.bincount(src, minlength=n_src), out=row_ptr[1:])
+        self._pl_order = order
+        tg = np.ascontiguousarray(np.asarray(tgt)[order], dtype=np.int32)
+        ww = np.ascontiguousarray(np.asarray(w, dtype=np.float64)[order])
+        dd = np.ascontiguousarray(np.asarray(d)[order], dtype=np.int32)
+        self._chk(self.L.orc_set_plastic(self.ptr, n_src, _p(row_ptr), _p(tg), _p(ww), _p(dd), float(lam), float(alpha),
+                                         float(mu), float(tau_plus)))
+
+    def plastic_weights(self):
+        """Weights of the plastic connections, in the order they were given."""
+        k = len(self._pl_order)
+        out = np.empty(k, dtype=np.float64)
+        self._chk(self.L.orc_get_plastic(self.ptr, _p(out)))
+        res = np.empty(k, dtype=np.float64)
+        res[self._pl_order] = out
+        return res
 
     def set_sched(self, steps, srcs):
         steps = np.ascontiguousarray(steps, dtype=np.int64)
@@ -223,4 +249,10 @@ def net_from_kernel(K, nthreads=0):
         start, stop = c["pois_window"]
         net.set_poisson(c["pois_rate"], c["pois_w"], c["pois_d"], K.rng_seed, start, stop)
     net.set_record(c["rec_flags"])
+    if c.get("pl") is not None:
+        p, cm = c["pl"], c["pl"]["common"]
+        psrc = np.repeat(np.arange(c["N"]), np.diff(p["row"]))
+        # weights come back in the engine's CSR order (c["pl"]["order"] maps it to the front-end's)
+        net.set_plastic(psrc, p["tgt"], p["w"], p["d"], lam=cm["lambda"], alpha=cm["alpha"], mu=cm["mu"],
+                        tau_plus=cm["tau_plus"], n_src=c["N"])
     return net, c

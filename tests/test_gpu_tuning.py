@@ -2,7 +2,9 @@
 autotuner itself.
 
 Every configuration -- update kernel (one thread per neuron with 4 or 8
-lags of inputs gathered, two-phase with 256- or 128-thread CTAs), resident
+lags of inputs gathered, two-phase with 256- or 128-thread CTAs, or the
+persistent kernel that runs update and delivery of many slices in one
+cooperative launch), resident
 delivery CTAs per SM, edge chunks per delivery warp -- must compute the same
 result: on networks whose ring sums do not depend on the order of the adds
 (the FP32 form's integer rings; dyadic FP64 weights) the rasters and final
@@ -19,7 +21,10 @@ from nestgpu import _abi
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = [(0, -1, -1), (1, -1, -1), (2, -1, -1), (3, -1, -1), (0, 1, 1), (3, 2, 8), (2, 8, 2)]
+# (update variant, delivery CTAs per SM, chunks per warp); variant 5 is the
+# persistent slice kernel (update and delivery of many slices in one launch)
+CONFIGS = [(0, -1, -1), (1, -1, -1), (2, -1, -1), (3, -1, -1), (0, 1, 1), (3, 2, 8), (2, 8, 2), (5, -1, -1),
+           (5, 2, 1)]
 
 
 def _exp_engine(precision, n=6000, md=15, seed=3):
@@ -100,16 +105,18 @@ def test_autotuner_measures_then_caches(golden):
     fx = golden("c0_delta_balanced.npz")
     fixed = _delta_engine(fx)
     fixed.set_tuning(0, 2, -1, -1)
-    fixed.simulate(3000)
+    fixed.simulate(9000)
     ref = _finish(fixed)
     tuned = _delta_engine(fx)
     tuned.set_tuning(2)                 # measure even if the process cache knows this shape
-    tuned.simulate(3000)
+    tuned.simulate(9000)                # long enough for the probe and every trial group
     a = _finish(tuned)
     _same(a, ref)
     t = a[4]
     assert t["state"] == "tuned"
-    assert len(t["candidates"]) >= 8
+    # every update kernel; then the delivery launch shapes unless the
+    # persistent kernel (which delivers inside itself) won
+    assert len(t["candidates"]) >= (5 if t["update_variant"] == 5 else 8)
     assert all(c["us_per_slice"] > 0 for c in t["candidates"])
     best = min(t["candidates"], key=lambda c: c["us_per_slice"])
     assert (t["update_variant"], t["deliver_ctas_per_sm"], t["deliver_chunks_per_warp"]) in \
@@ -117,7 +124,7 @@ def test_autotuner_measures_then_caches(golden):
     assert (best["update_variant"], best["deliver_ctas_per_sm"], best["deliver_chunks_per_warp"]) == \
         (t["update_variant"], t["deliver_ctas_per_sm"], t["deliver_chunks_per_warp"])
     again = _delta_engine(fx)
-    again.simulate(3000)                # default mode: the process cache first
+    again.simulate(9000)                # default mode: the process cache first
     b = _finish(again)
     _same(b, ref)
     assert b[4]["state"] == "cached"
@@ -145,3 +152,32 @@ def test_tuning_arguments_checked():
     with pytest.raises(_abi.EngineError):
         eng.set_option("gather", 1)      # a static engine has no per-target gather
     eng.close()
+
+
+@pytest.mark.parametrize("precision", [_abi.NG_FP64, _abi.NG_FP32])
+def test_aeif_binning_changes_no_result(precision):
+    """aeif_cond_alpha neurons ordered by their RKF45 step size before each
+    slice (so a warp's neurons need similar numbers of sub-steps) give the
+    raster and state of the identity order: only which thread computes a
+    neuron changes."""
+    def run(binning):
+        n = 3000
+        rng = np.random.default_rng(21)
+        deg = rng.integers(40, 160, n)
+        row = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+        nnz = int(row[-1])
+        eng = _abi.Engine([(_abi.NG_AEIF_COND_ALPHA, n)], 0.1, 15, 30, precision=precision)
+        eng.set_option("aeif_binning", binning)
+        eng.set_var(0, "tau_syn_ex", np.full(n, 1.0))
+        eng.set_var(0, "V_m", rng.uniform(-70.6, -52.0, n))
+        eng.set_connections(row, rng.integers(0, n, nnz).astype(np.int32),
+                            rng.choice([1.0, 0.5, -2.0, -4.0], nnz), rng.integers(15, 31, nnz).astype(np.int32))
+        eng.set_recording(np.ones(n, dtype=np.uint8))
+        eng.set_poisson(np.full(n, 15000.0), np.full(n, 1.0), np.full(n, 15, dtype=np.int32), 0, 10**9, 5)
+        for k in (7, 1493, 1500):
+            eng.simulate(k)
+        return _finish(eng, "V_m")
+
+    a, b = run(0), run(1)
+    assert len(a[0]) > 500
+    _same(a, b)
