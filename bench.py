@@ -92,6 +92,7 @@ def parse():
     ap.add_argument("--no-layered", action="store_true")
     ap.add_argument("--no-aeif", action="store_true")
     ap.add_argument("--no-slice-calls", action="store_true")
+    ap.add_argument("--no-hpc", action="store_true", help="skip the hpc_benchmark (STDP) network")
     ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--forms", default="plain,fp32,batched",
                     help="forms of the Brunel network to time besides the plain FP64 headline")
@@ -632,6 +633,60 @@ def measure_aeif(args, dev, sim_ms=500.0):
     return out
 
 
+def measure_hpc(args, dev, sim_ms=1000.0):
+    """The reference's hpc_benchmark network at scale 1 (11,250 iaf_psc_alpha
+    neurons, in-degrees 9,000 + 2,250: 1.27e8 connections, of which the
+    8.1e7 E->E ones are stdp_pl_synapse_hom), built through the front-end:
+    real-time factor with plastic E->E connections in the FP64 and FP32 forms,
+    and with them static (FP64) for the cost of the plasticity."""
+    import torch
+
+    import nestgpu as nest
+    from nestgpu import workloads
+    from nestgpu.kernel import KERNEL
+
+    out = {"workload": "hpc_benchmark scale 1: 11,250 iaf_psc_alpha, CE 9,000, CI 2,250, E->E "
+                       "stdp_pl_synapse_hom (alpha 0.0513, lambda 0.1, mu 0.4, tau_plus 15 ms), delay 1.5 ms, "
+                       "100 ms warm-up then 1,000 ms"}
+    for form, prec, plastic in (("fp64_stdp", "fp64", True), ("fp32_stdp", "fp32", True),
+                                ("fp64_static", "fp64", False)):
+        t0 = time.perf_counter()
+        E, I, _ = workloads.hpc_benchmark(nest, scale=1.0, precision=prec, plastic=plastic, record=False)
+        nest.Prepare()
+        build = time.perf_counter() - t0
+        eng = KERNEL.engine
+        st = torch.cuda.current_stream(dev)
+        eng.set_stream(st.cuda_stream)
+        nest.Run(100.0)
+        KERNEL.settle()
+        torch.cuda.synchronize(dev)
+        sampler = ClockSampler(dev.index)
+        sampler.start()
+        s0 = eng.stats()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        nest.Run(sim_ms)
+        KERNEL.settle()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        s1 = eng.stats()
+        clocks = sampler.stop()
+        n = len(E) + len(I)
+        r = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": (s1["syn_events"] - s0["syn_events"]) / (ms * 1e-3),
+             "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / n / (sim_ms * 1e-3), "build_s": build,
+             "connections": KERNEL.num_connections(), "clocks": clocks,
+             "tuned": {k: eng.tuned()[k] for k in ("state", "update_kernel", "deliver_ctas_per_sm")}}
+        if plastic:
+            w = np.asarray(nest.GetConnections(synapse_model="stdp_pl_synapse_hom_hpc").get("weight"))
+            r["weight_mean"], r["weight_sd"] = float(w.mean()), float(w.std())
+        nest.Cleanup()
+        nest.ResetKernel()
+        out[form] = r
+    return out
+
+
 def measure_slice_calls(args, dev):
     """The network driven the way NEST's node loop drives an engine node
     (gpu_engine::update): one ng_update per min_delay slice, enqueued without
@@ -787,6 +842,8 @@ def run_engine(args):
         guarded("serving_sweep", measure_serving)
     if not args.no_slice_calls:
         guarded("slice_calls", measure_slice_calls)
+    if not args.no_hpc:
+        guarded("hpc_benchmark", measure_hpc)
     cpu = None
     if rank == 0 and not args.no_cpu:
         from nestgpu import workloads

@@ -5,6 +5,7 @@ a kernel on a small instance (run from the repository root):
   python bench_cases.py layered --scale 0.5 --ms 300 --precision fp32
   python bench_cases.py aeif --neurons 10000 --ms 60
   python bench_cases.py serving --requests 40 --capacity-neurons 300000 --capacity-edges 200000000 --slices 40
+  python bench_cases.py hpc --scale 0.5 --ms 200 --precision fp64
 
 Each case builds its network, simulates, prints one summary line and exits 0.
 The c1 case is bench.py's headline network (12,500 iaf_psc_exp neurons,
@@ -27,16 +28,16 @@ import sys
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["c1", "layered", "aeif", "serving"])
+    ap.add_argument("case", choices=["c1", "layered", "aeif", "serving", "hpc"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--scale", type=float, default=1.0, help="layered: population size factor")
+    ap.add_argument("--scale", type=float, default=1.0, help="layered, hpc: population size factor")
     ap.add_argument("--neurons", type=int, default=50000, help="aeif: network size (80 % excitatory)")
     ap.add_argument("--ms", type=float, default=100.0, help="simulated time")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests admitted at once")
     ap.add_argument("--capacity-neurons", type=int, default=300_000)
     ap.add_argument("--capacity-edges", type=int, default=200_000_000)
     ap.add_argument("--slices", type=int, default=40, help="serving: min_delay slices simulated")
-    ap.add_argument("--runs", type=int, default=4, help="c1: Simulate(ms) calls")
+    ap.add_argument("--runs", type=int, default=4, help="c1, hpc: Simulate(ms) calls")
     ap.add_argument("--fixed", default="", help="c1: fixed launch configuration 'variant,ctas_per_sm,chunks_per_warp' "
                                                   "instead of the autotuner (which measures differently under a profiler)")
     ap.add_argument("--ring32", action="store_true", help="layered: 32-bit ring cells")
@@ -46,6 +47,15 @@ def main(argv=None):
     from nestgpu import serving, workloads
     from nestgpu.kernel import KERNEL
 
+    if a.case == "hpc":
+        # the hpc_benchmark network (iaf_psc_alpha, E->E stdp_pl_synapse_hom_hpc)
+        workloads.hpc_benchmark(nest, scale=a.scale, precision=a.precision, record=False)
+        for _ in range(a.runs):
+            nest.Simulate(a.ms)
+        st = nest.engine_stats()
+        print(f"hpc: steps {st['clock_steps']} spikes {st['spikes']} syn_events {st['syn_events']}", flush=True)
+        nest.ResetKernel()
+        return 0
     if a.case == "c1":
         workloads.c1(nest, precision=a.precision, seed=4242)
         if a.fixed:

@@ -705,8 +705,9 @@ struct ng_engine
   // ---- stdp_pl_synapse_hom connections (ng_set_plastic_connections)
   bool plastic_on = false;
   DevBuf pl_row, pl_tgt, pl_dly, pl_w, pl_Kplus, pl_tlast, pl_ninc, pl_tauinv, pl_Kminus, pl_last, pl_hist_t, pl_hist_K,
-    pl_hist_n;
+    pl_hist_n, pl_hist_lo, pl_drop_t, pl_drop_K, pl_nflush, pl_in_row, pl_in_edge, pl_in_src, pl_wrun;
   int64_t pl_nnz = 0, pl_nsrc = 0;
+  double pl_dmax_ms = 0;
   double pl_lambda = 0.1, pl_alpha = 1.0, pl_mu = 0.4, pl_tau_plus = 20.0;
   std::vector< double > tau_minus_host;  // per neuron, the postsynaptic trace's time constant (ArchivingNode)
   int pk_occ = -1;           // its resident CTAs per SM (-1: not known yet)
@@ -758,7 +759,7 @@ struct ng_engine
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
       &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t, &row_ue, &row_ls, &ent_late, &pk, &pl_row,
       &pl_tgt, &pl_dly, &pl_w, &pl_Kplus, &pl_tlast, &pl_ninc, &pl_tauinv, &pl_Kminus, &pl_last, &pl_hist_t, &pl_hist_K,
-      &pl_hist_n };
+      &pl_hist_n, &pl_hist_lo, &pl_drop_t, &pl_drop_K, &pl_nflush, &pl_in_row, &pl_in_edge, &pl_in_src, &pl_wrun };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -1246,6 +1247,7 @@ struct ng_engine
     p.tgt = ( const int32_t* ) pl_tgt.p;
     p.dly = ( const int32_t* ) pl_dly.p;
     p.w = ( double* ) pl_w.p;
+    p.w_run = ( double* ) pl_wrun.p;
     p.Kplus = ( double* ) pl_Kplus.p;
     p.tlast = ( double* ) pl_tlast.p;
     p.n_src = pl_nsrc;
@@ -1256,6 +1258,14 @@ struct ng_engine
     p.hist_t = ( double* ) pl_hist_t.p;
     p.hist_K = ( double* ) pl_hist_K.p;
     p.hist_n = ( int64_t* ) pl_hist_n.p;
+    p.hist_lo = ( int64_t* ) pl_hist_lo.p;
+    p.drop_t = ( double* ) pl_drop_t.p;
+    p.drop_K = ( double* ) pl_drop_K.p;
+    p.n_flush = ( int32_t* ) pl_nflush.p;
+    p.in_row = ( const int64_t* ) pl_in_row.p;
+    p.in_edge = ( const uint32_t* ) pl_in_edge.p;
+    p.in_src = ( const int32_t* ) pl_in_src.p;
+    p.dmax_ms = pl_dmax_ms;
     p.lambda = pl_lambda;
     p.alpha = pl_alpha;
     p.mu = pl_mu;
@@ -1271,15 +1281,17 @@ struct ng_engine
   {
     if ( plastic_on )
     {
-      // plastic connections of the closing slice: postsynaptic histories first
+      // plastic connections of the closing slice: the presynaptic spikes (which
+      // read only earlier slices' postsynaptic spikes), then the histories
       const StdpNet p = stdp();
       const unsigned ga = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( N + 255 ) / 256, 4 * sms ) );
-      const unsigned gd = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( pl_nsrc * 32 + 255 ) / 256, 8 * sms ) );
-      k_stdp_archive<<< ga, 256, 0, stream >>>( d, p );
+      const unsigned gd = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( pl_nsrc, 8 * sms ) );
       if ( prec == NG_FP64 )
         k_stdp_deliver< false ><<< gd, 256, 0, stream >>>( d, p );
       else
         k_stdp_deliver< true ><<< gd, 256, 0, stream >>>( d, p );
+      k_stdp_archive<<< ga, 256, 0, stream >>>( d, p );
+      k_stdp_flush<<< ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( N, 8 * sms ) ), 256, 0, stream >>>( d, p );
     }
     if ( gather_live )
       k_gather<<< ( unsigned ) sms, G_THREADS, G_SMEM, stream >>>( d );
@@ -1695,8 +1707,8 @@ struct ng_engine
     if ( c.err & ERR_NUMERIC )
       return fail( NG_ERR_NUMERIC, "NumericalInstability: aeif_cond_alpha state exploded (V_m < -1e3 or |w| > 1e6)" );
     if ( c.err & ERR_STDP_HISTORY )
-      return fail( NG_ERR_CAPACITY, "stdp_pl_synapse_hom: a postsynaptic spike history of " + std::to_string( STDP_HIST )
-          + " entries did not reach back to a presynaptic neuron's previous spike" );
+      return fail( NG_ERR_CAPACITY, "stdp_pl_synapse_hom: more than " + std::to_string( STDP_HIST - 32 )
+          + " postsynaptic spikes of one neuron within max_delay (its spike history ring is full)" );
     if ( c.err & ERR_BARRIER )
       return fail( NG_ERR_CUDA, "persistent slice kernel: a grid barrier gave up waiting (a CTA did not arrive)" );
     if ( c.err & ( ERR_SPIKE_LIST | ERR_LOG | ERR_TRACE ) )
@@ -2769,6 +2781,8 @@ ng_set_plastic_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr,
   const int64_t nnz = row_ptr[ n_src ];
   if ( row_ptr[ 0 ] != 0 || nnz < 0 || ( nnz > 0 && ( !target || !weight || !delay_steps ) ) )
     return fail( NG_ERR_ARG, "ng_set_plastic_connections: bad CSR" );
+  if ( nnz >= ( int64_t ) 0xffffffffll )
+    return fail( NG_ERR_ARG, "ng_set_plastic_connections: at most 2^32 - 1 plastic connections" );
   std::vector< uint8_t > ninc( ( size_t ) e->N, 0 );
   for ( int64_t s2 = 0; s2 < n_src; ++s2 )
     if ( row_ptr[ s2 + 1 ] < row_ptr[ s2 ] )
@@ -2783,22 +2797,49 @@ ng_set_plastic_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr,
       return fail( NG_ERR_ARG, "stdp_pl_synapse_hom: weights must be >= 0 (the power law of the facilitation)" );
     ninc[ ( size_t ) target[ k ] ] = 1;
   }
+  // the target-major index (the flush walks a neuron's incoming connections)
+  const size_t N = ( size_t ) e->N;
+  std::vector< int64_t > in_row( N + 1, 0 );
+  for ( int64_t k = 0; k < nnz; ++k )
+    ++in_row[ ( size_t ) target[ k ] + 1 ];
+  for ( size_t i = 0; i < N; ++i )
+    in_row[ i + 1 ] += in_row[ i ];
+  std::vector< uint32_t > in_edge( ( size_t ) std::max< int64_t >( nnz, 1 ) );
+  std::vector< int32_t > in_src( ( size_t ) std::max< int64_t >( nnz, 1 ) );
+  {
+    std::vector< int64_t > fill( in_row.begin(), in_row.end() - 1 );
+    int32_t dmax = 0;
+    for ( int64_t s2 = 0; s2 < n_src; ++s2 )
+      for ( int64_t k = row_ptr[ s2 ]; k < row_ptr[ s2 + 1 ]; ++k )
+      {
+        const int64_t q = fill[ ( size_t ) target[ k ] ]++;
+        in_edge[ ( size_t ) q ] = ( uint32_t ) k;
+        in_src[ ( size_t ) q ] = ( int32_t ) s2;
+        dmax = std::max( dmax, delay_steps[ k ] );
+      }
+    e->pl_dmax_ms = ( double ) dmax * ( ( double ) e->tics_per_step / e->cfg.tics_per_ms );
+  }
   cudaSetDevice( e->cfg.device );
   int rc;
-  const size_t N = ( size_t ) e->N;
   std::vector< double > inv( N );
   for ( size_t i = 0; i < N; ++i )
     inv[ i ] = 1. / e->tau_minus_host[ i ];
+  static const int64_t zero[ 1 ] = { 0 };  // the one cell of an empty plastic table
   if ( ( rc = e->upload( e->pl_row, row_ptr, ( size_t ) ( n_src + 1 ) * 8 ) )
-    || ( rc = e->upload( e->pl_tgt, target, ( size_t ) std::max< int64_t >( nnz, 1 ) * 4 ) )
-    || ( rc = e->upload( e->pl_dly, delay_steps, ( size_t ) std::max< int64_t >( nnz, 1 ) * 4 ) )
-    || ( rc = e->upload( e->pl_w, weight, ( size_t ) std::max< int64_t >( nnz, 1 ) * 8 ) )
+    || ( rc = e->upload( e->pl_tgt, nnz ? ( const void* ) target : zero, ( size_t ) std::max< int64_t >( nnz, 1 ) * 4 ) )
+    || ( rc = e->upload( e->pl_dly, nnz ? ( const void* ) delay_steps : zero, ( size_t ) std::max< int64_t >( nnz, 1 ) * 4 ) )
+    || ( rc = e->upload( e->pl_w, nnz ? ( const void* ) weight : zero, ( size_t ) std::max< int64_t >( nnz, 1 ) * 8 ) )
+    || ( rc = e->upload( e->pl_wrun, nnz ? ( const void* ) weight : zero, ( size_t ) std::max< int64_t >( nnz, 1 ) * 8 ) )
     || ( rc = e->alloc( e->pl_Kplus, ( size_t ) std::max< int64_t >( n_src, 1 ) * 8 ) )
     || ( rc = e->alloc( e->pl_tlast, ( size_t ) std::max< int64_t >( n_src, 1 ) * 8 ) )
     || ( rc = e->upload( e->pl_ninc, ninc.data(), N ) ) || ( rc = e->upload( e->pl_tauinv, inv.data(), N * 8 ) )
     || ( rc = e->alloc( e->pl_Kminus, N * 8 ) ) || ( rc = e->alloc( e->pl_last, N * 8 ) )
     || ( rc = e->alloc( e->pl_hist_t, N * STDP_HIST * 8 ) ) || ( rc = e->alloc( e->pl_hist_K, N * STDP_HIST * 8 ) )
-    || ( rc = e->alloc( e->pl_hist_n, N * 8 ) ) )
+    || ( rc = e->alloc( e->pl_hist_n, N * 8 ) ) || ( rc = e->alloc( e->pl_hist_lo, N * 8 ) )
+    || ( rc = e->alloc( e->pl_drop_t, N * 8 ) ) || ( rc = e->alloc( e->pl_drop_K, N * 8 ) )
+    || ( rc = e->alloc( e->pl_nflush, N * 4 ) ) || ( rc = e->upload( e->pl_in_row, in_row.data(), ( N + 1 ) * 8 ) )
+    || ( rc = e->upload( e->pl_in_edge, in_edge.data(), in_edge.size() * 4 ) )
+    || ( rc = e->upload( e->pl_in_src, in_src.data(), in_src.size() * 4 ) ) )
     return rc;
   if ( !e->gmask.p && ( rc = e->alloc( e->gmask, N * 4 ) ) )
     return rc;

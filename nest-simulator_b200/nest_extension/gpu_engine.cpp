@@ -69,12 +69,18 @@ vars_of( int model )
 {
   static const std::vector< Var > delta = { { "tau_m", "tau_m", false }, { "C_m", "C_m", false },
     { "t_ref", "t_ref", false }, { "I_e", "I_e", false }, { "V_th_rel", "V_th", true },
-    { "V_reset_rel", "V_reset", true }, { "V_min_rel", "V_min", true }, { "V_m_rel", "V_m", true } };
+    { "V_reset_rel", "V_reset", true }, { "V_min_rel", "V_min", true }, { "V_m_rel", "V_m", true },
+    { "tau_minus", "tau_minus", false } };
+  // (the synaptic currents are not in the iaf models' status; the engine
+  // takes the population over at time 0, where they are 0)
   static const std::vector< Var > exp = { { "tau_m", "tau_m", false }, { "C_m", "C_m", false },
     { "t_ref", "t_ref", false }, { "I_e", "I_e", false }, { "V_th_rel", "V_th", true },
     { "V_reset_rel", "V_reset", true }, { "tau_syn_ex", "tau_syn_ex", false },
-    { "tau_syn_in", "tau_syn_in", false }, { "V_m_rel", "V_m", true }, { "I_syn_ex", "I_syn_ex", false },
-    { "I_syn_in", "I_syn_in", false } };
+    { "tau_syn_in", "tau_syn_in", false }, { "V_m_rel", "V_m", true }, { "tau_minus", "tau_minus", false } };
+  static const std::vector< Var > alpha = { { "tau_m", "tau_m", false }, { "C_m", "C_m", false },
+    { "t_ref", "t_ref", false }, { "I_e", "I_e", false }, { "V_th_rel", "V_th", true },
+    { "V_reset_rel", "V_reset", true }, { "V_min_rel", "V_min", true }, { "tau_syn_ex", "tau_syn_ex", false },
+    { "tau_syn_in", "tau_syn_in", false }, { "V_m_rel", "V_m", true }, { "tau_minus", "tau_minus", false } };
   static const std::vector< Var > aeif = { { "V_peak", "V_peak", false }, { "V_reset", "V_reset", false },
     { "t_ref", "t_ref", false }, { "g_L", "g_L", false }, { "C_m", "C_m", false }, { "E_ex", "E_ex", false },
     { "E_in", "E_in", false }, { "E_L", "E_L", false }, { "Delta_T", "Delta_T", false },
@@ -82,7 +88,10 @@ vars_of( int model )
     { "tau_syn_ex", "tau_syn_ex", false }, { "tau_syn_in", "tau_syn_in", false }, { "I_e", "I_e", false },
     { "gsl_error_tol", "gsl_error_tol", false }, { "V_m", "V_m", false }, { "g_ex", "g_ex", false },
     { "g_in", "g_in", false }, { "w", "w", false } };
-  return model == NG_IAF_PSC_DELTA ? delta : model == NG_IAF_PSC_EXP ? exp : aeif;
+  return model == NG_IAF_PSC_DELTA ? delta
+    : model == NG_IAF_PSC_EXP       ? exp
+    : model == NG_IAF_PSC_ALPHA     ? alpha
+                                    : aeif;
 }
 
 // state variables written back to the neurons after a Run
@@ -93,6 +102,8 @@ state_of( int model )
   static const std::vector< Var > exp = { { "V_m_rel", "V_m", true } };
   static const std::vector< Var > aeif = { { "V_m", "V_m", false }, { "g_ex", "g_ex", false },
     { "g_in", "g_in", false }, { "w", "w", false } };
+  if ( model == NG_IAF_PSC_ALPHA )
+    return exp;
   return model == NG_IAF_PSC_DELTA ? delta : model == NG_IAF_PSC_EXP ? exp : aeif;
 }
 
@@ -103,9 +114,24 @@ model_id( const std::string& name )
     return NG_IAF_PSC_DELTA;
   if ( name == "iaf_psc_exp" )
     return NG_IAF_PSC_EXP;
+  if ( name == "iaf_psc_alpha" )
+    return NG_IAF_PSC_ALPHA;
   if ( name == "aeif_cond_alpha" )
     return NG_AEIF_COND_ALPHA;
   return -1;
+}
+
+// stdp_pl_synapse_hom (models/stdp_pl_synapse_hom.h) and its copies: a
+// connection model whose defaults hold its common properties lambda, alpha,
+// mu and tau_plus (STDPPLHomCommonProperties::get_status,
+// models/stdp_pl_synapse_hom.cpp:55-63) and none of the other STDP rules' keys
+bool
+is_stdp_pl( const std::string& name, const Dictionary& defaults )
+{
+  if ( name == "stdp_pl_synapse_hom" || name == "stdp_pl_synapse_hom_hpc" )
+    return true;
+  return defaults.known( "lambda" ) and defaults.known( "alpha" ) and defaults.known( "mu" )
+    and defaults.known( "tau_plus" ) and not defaults.known( "mu_plus" ) and not defaults.known( "Wmax" );
 }
 
 }  // namespace
@@ -149,7 +175,9 @@ gpu_engine::get_status( Dictionary& d ) const
   d[ "device" ] = P_.device;
   d[ "precision" ] = P_.precision;
   d[ "seed" ] = P_.seed;
+  d[ "sync_weights" ] = P_.sync_weights;
   d[ "spikes_routed" ] = static_cast< long >( routed_ );
+  d[ "plastic_connections" ] = static_cast< long >( pl_conns_.size() );
   if ( eng_ )
   {
     ng_stats st {};
@@ -174,6 +202,7 @@ gpu_engine::set_status( const Dictionary& d )
   d.update_value( "device", p.device );
   d.update_value( "precision", p.precision );
   d.update_value( "seed", p.seed );
+  d.update_value( "sync_weights", p.sync_weights );
   if ( p.n_nodes < 0 || p.first_node_id < 0 || p.device < 0 )
     throw nest::BadProperty( "gpu_engine: first_node_id, n_nodes and device must be >= 0" );
   if ( p.precision != "fp64" && p.precision != "fp32" )
@@ -194,6 +223,9 @@ gpu_engine::build_()
   using nest::kernel;
   if ( kernel().vp_manager.get_num_threads() != 1 || kernel().mpi_manager.get_num_processes() != 1 )
     throw nest::BadProperty( "gpu_engine: runs with local_num_threads = 1 in one process" );
+  if ( kernel().simulation_manager.get_clock().get_steps() != 0 )
+    throw nest::BadProperty( "gpu_engine: the engine takes the population over at time 0 (the synaptic "
+                             "currents and pending spikes of a simulated network are not in its status)" );
   const size_t first = static_cast< size_t >( P_.first_node_id );
   const size_t n = static_cast< size_t >( P_.n_nodes );
   std::vector< nest::Node* > nodes( n );
@@ -203,7 +235,7 @@ gpu_engine::build_()
     const int m = node ? model_id( node->get_name() ) : -1;
     if ( m < 0 || ( k > 0 && m != model_ ) )
       throw nest::BadProperty( "gpu_engine: the population must be one of iaf_psc_delta, iaf_psc_exp, "
-                               "aeif_cond_alpha, all the same model" );
+                               "iaf_psc_alpha, aeif_cond_alpha, all the same model" );
     model_ = m;
     nodes[ k ] = node;
   }
@@ -232,17 +264,48 @@ gpu_engine::build_()
   std::vector< double > rate( n, 0.0 ), pw( n, 0.0 );
   std::vector< int32_t > pd( n, 1 );
   long long g_start = -1, g_stop = -1;
+  // stdp_pl_synapse_hom connections among the population (one set of common properties)
+  std::vector< int32_t > psrc, ptgt, pdly;
+  std::vector< double > pwt;
+  pl_conns_.clear();
+  int pl_syn = -1;
+  double pl_common[ 4 ] = { 0, 0, 0, 0 };  // lambda, alpha, mu, tau_plus
   for ( const auto& c : conns )
   {
     const size_t s = static_cast< size_t >( c.get_source_node_id() );
     const size_t t = static_cast< size_t >( c.get_target_node_id() );
     const auto syn = static_cast< nest::synindex >( c.get_synapse_model_id() );
-    if ( kernel().model_manager.get_connection_model( syn, 0 ).get_name() != "static_synapse" )
-      throw nest::BadProperty( "gpu_engine: only static_synapse connections run on the engine" );
+    const std::string syn_name = kernel().model_manager.get_connection_model( syn, 0 ).get_name();
+    bool plastic = false;
+    if ( syn_name != "static_synapse" )
+    {
+      const Dictionary defaults = kernel().model_manager.get_connector_defaults( syn );
+      if ( not is_stdp_pl( syn_name, defaults ) )
+        throw nest::BadProperty( "gpu_engine: connections run on the engine as static_synapse or "
+                                 "stdp_pl_synapse_hom, not " + syn_name );
+      const double common[ 4 ] = { get_d( defaults, "lambda" ), get_d( defaults, "alpha" ), get_d( defaults, "mu" ),
+        get_d( defaults, "tau_plus" ) };
+      if ( pl_syn >= 0 and not std::equal( common, common + 4, pl_common ) )
+        throw nest::BadProperty( "gpu_engine: stdp_pl_synapse_hom models with different common properties" );
+      pl_syn = syn;
+      std::copy( common, common + 4, pl_common );
+      plastic = true;
+    }
     const Dictionary sd = kernel().connection_manager.get_synapse_status(
       s, t, static_cast< size_t >( c.get_target_thread() ), syn, static_cast< size_t >( c.get_port() ) );
     const double weight = get_d( sd, "weight" );
     const long d_steps = nest::Time::delay_ms_to_steps( get_d( sd, "delay" ) );
+    if ( plastic )
+    {
+      if ( s < first || s >= first + n )
+        throw nest::BadProperty( "gpu_engine: stdp_pl_synapse_hom connections start at the population's neurons" );
+      psrc.push_back( static_cast< int32_t >( s - first ) );
+      ptgt.push_back( static_cast< int32_t >( t - first ) );
+      pwt.push_back( weight );
+      pdly.push_back( static_cast< int32_t >( d_steps ) );
+      pl_conns_.push_back( c );
+      continue;
+    }
     if ( s >= first && s < first + n )
     {
       src.push_back( static_cast< int32_t >( s - first ) );
@@ -293,6 +356,31 @@ gpu_engine::build_()
     check( ng_set_poisson( eng_, rate.data(), pw.data(), pd.data(), g_start, g_stop,
              static_cast< uint64_t >( P_.seed ) ),
       "gpu_engine: poisson_generator drive" );
+  if ( not pl_conns_.empty() )
+  {
+    // a CSR over the population's neurons, stable in the order NEST listed them
+    const size_t m = pl_conns_.size();
+    std::vector< int64_t > row( n + 1, 0 );
+    for ( size_t k = 0; k < m; ++k )
+      ++row[ static_cast< size_t >( psrc[ k ] ) + 1 ];
+    for ( size_t i = 0; i < n; ++i )
+      row[ i + 1 ] += row[ i ];
+    std::vector< int64_t > fill( row.begin(), row.end() - 1 );
+    pl_pos_.assign( m, 0 );
+    std::vector< int32_t > ct( m ), cd( m );
+    std::vector< double > cw( m );
+    for ( size_t k = 0; k < m; ++k )
+    {
+      const int64_t q = fill[ static_cast< size_t >( psrc[ k ] ) ]++;
+      pl_pos_[ k ] = q;
+      ct[ static_cast< size_t >( q ) ] = ptgt[ k ];
+      cd[ static_cast< size_t >( q ) ] = pdly[ k ];
+      cw[ static_cast< size_t >( q ) ] = pwt[ k ];
+    }
+    check( ng_set_plastic_connections( eng_, static_cast< int64_t >( n ), row.data(), ct.data(), cw.data(), cd.data(),
+             pl_common[ 0 ], pl_common[ 1 ], pl_common[ 2 ], pl_common[ 3 ] ),
+      "gpu_engine: stdp_pl_synapse_hom connections" );
+  }
   std::vector< uint8_t > rec( n, 1 );
   check( ng_set_recording( eng_, rec.data() ), "gpu_engine: recording" );
   // the neurons stay in NEST for recorders, GetStatus and connections, but
@@ -355,6 +443,21 @@ gpu_engine::drain_and_route_()
     for ( size_t v = 0; v < sv.size(); ++v )
       d[ sv[ v ].status ] = vals[ v ][ k ] + ( sv[ v ].relative ? E_L_per_node_[ k ] : 0.0 );
     kernel().node_manager.get_node_or_proxy( first + k )->set_status_base( d );
+  }
+  // the plastic weights, so that GetConnections reads the engine's values
+  if ( P_.sync_weights and not pl_conns_.empty() )
+  {
+    std::vector< double > wv( pl_conns_.size() );
+    check( ng_get_plastic_weights( eng_, wv.data(), static_cast< int64_t >( wv.size() ) ), "gpu_engine: weights" );
+    for ( size_t k = 0; k < pl_conns_.size(); ++k )
+    {
+      const nest::ConnectionID& c = pl_conns_[ k ];
+      Dictionary d;
+      d[ "weight" ] = wv[ static_cast< size_t >( pl_pos_[ k ] ) ];
+      kernel().connection_manager.set_synapse_status( static_cast< size_t >( c.get_source_node_id() ),
+        static_cast< size_t >( c.get_target_node_id() ), static_cast< size_t >( c.get_target_thread() ),
+        static_cast< nest::synindex >( c.get_synapse_model_id() ), static_cast< size_t >( c.get_port() ), d );
+    }
   }
 }
 

@@ -29,10 +29,14 @@
  * windows and backends are the reference's own; the neurons' state is
  * written back, so GetStatus on them reads the GPU's values.
  *
- * Supported: one model per engine among iaf_psc_delta, iaf_psc_exp and
- * aeif_cond_alpha; static_synapse connections; one poisson_generator rate,
- * weight and delay per neuron; local_num_threads = 1 and one MPI process
- * (the engine owns the whole population).  Anything else raises
+ * Supported: one model per engine among iaf_psc_delta, iaf_psc_exp,
+ * iaf_psc_alpha and aeif_cond_alpha; static_synapse connections, and
+ * stdp_pl_synapse_hom connections (or copies of it) among the population's
+ * neurons with one set of common properties -- their weights are written
+ * back after each Run (sync_weights) and the neurons' tau_minus is read;
+ * one poisson_generator rate, weight and delay per neuron; local_num_threads
+ * = 1 and one MPI process (the engine owns the whole population); the
+ * engine takes the population over at time 0.  Anything else raises
  * BadProperty at Prepare.
  */
 #ifndef NESTGPU_GPU_ENGINE_H
@@ -41,6 +45,7 @@
 #include <string>
 #include <vector>
 
+#include "connection_id.h"
 #include "nest_time.h"
 #include "node.h"
 
@@ -95,12 +100,15 @@ private:
     long device = 0;
     std::string precision = "fp64";
     long seed = 1;  // key of the Philox stream that replaces the poisson_generators' draws
+    bool sync_weights = true;  // write the plastic weights back into NEST after each Run
   } P_;
 
   ng_engine* eng_ = nullptr;
   int model_ = -1;        // NG_IAF_PSC_DELTA / NG_IAF_PSC_EXP / NG_AEIF_COND_ALPHA
   double E_L_ = 0.0;      // per-population offset of the relative voltages (iaf models)
   std::vector< double > E_L_per_node_;
+  std::vector< nest::ConnectionID > pl_conns_;  // the stdp_pl_synapse_hom connections, as NEST listed them
+  std::vector< int64_t > pl_pos_;               // ... and each one's index in the engine's plastic CSR
   std::vector< int32_t > src_buf_;
   std::vector< int64_t > stamp_buf_;
   long long routed_ = 0;  // spikes handed to recording devices

@@ -1425,9 +1425,7 @@ static void
 deliver( orc_net* net, int nthreads )
 {
   const int64_t L = net->L, n = net->n;
-  const int P = net->nparts;
-  if ( P == 0 )
-    return;
+  const int P = net->nparts;  /* 0: no static connections */
   int64_t ev = 0;
   for ( int64_t s = 0; s < net->sp_len; ++s )
   {

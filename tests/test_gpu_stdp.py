@@ -123,18 +123,60 @@ def test_stdp_fp32_form_follows_fp64():
     assert abs(dw32 - dw64) <= 0.05 * abs(dw64) + 1e-3
 
 
-def test_stdp_history_overrun_is_an_error():
-    """A source firing every ~77 ms onto a target firing every ~0.9 ms: the
-    target's 64-entry history no longer reaches back to the source's previous
-    spike, and the engine says so at its next synchronisation."""
-    eng = _abi.Engine([(_abi.NG_IAF_PSC_DELTA, 2)], H, 1, 5)
-    eng.set_var(0, "I_e", np.array([375.2, 5000.0]))      # V_inf 15.008 mV: a spike every ~77 ms
-    eng.set_var(0, "t_ref", np.array([2.0, 0.1]))        # ~0.9 ms
+def test_stdp_long_silent_source_equals_oracle():
+    """A source firing every ~77 ms onto targets firing every ~0.9 ms: each
+    target's 64-entry history is flushed many times between two presynaptic
+    spikes (its oldest entries' facilitation applied early, then dropped),
+    and the weights still equal the oracle's, which keeps every entry."""
+    n = 4
+    I_e = np.array([375.2, 5000.0, 3000.0, 1000.0])     # V_inf 15.008 mV: a spike every ~77 ms; then fast ones
+    t_ref = np.array([2.0, 0.1, 0.3, 0.5])
+    row = np.array([0, 3, 3, 3, 3], dtype=np.int64)
+    tgt = np.array([1, 2, 3], np.int32)
+    w0 = np.array([1.0, 2.0, 3.0])
+    dl = np.array([1, 3, 5], np.int32)
+    eng = _abi.Engine([(_abi.NG_IAF_PSC_DELTA, n)], H, 1, 5)
+    eng.set_var(0, "I_e", I_e)
+    eng.set_var(0, "t_ref", t_ref)
+    eng.set_connections(np.array([0, 1, 1, 1, 1], dtype=np.int64), np.array([0], np.int32), np.array([0.0]),
+                        np.array([1], np.int32))
+    rule = dict(RULE, alpha=0.0513)
+    eng.set_plastic(row, tgt, w0, dl, **rule)
+    eng.set_recording(np.ones(n, dtype=np.uint8))
+    for k in (1234, 5000, 13766):
+        eng.simulate(k)
+    s, t = eng.spikes()
+    w = eng.plastic_weights()
+    eng.close()
+    net = O.OracleNet("iaf_psc_delta", n, H, 1, 5)
+    net.set("I_e", I_e)
+    net.set("t_ref", t_ref)
+    net.set_plastic(np.zeros(3, np.int64), tgt, w0, dl, n_src=n, **rule)
+    net.set_record(np.ones(n, dtype=np.uint8))
+    net.run(20000)
+    os_, ot = net.spikes()
+    assert np.sum(s == 0) >= 20 and np.sum(s == 1) > 1500
+    o1, o2 = np.lexsort((s, t)), np.lexsort((os_, ot))
+    np.testing.assert_array_equal(s[o1], os_[o2])
+    np.testing.assert_array_equal(t[o1], ot[o2])
+    assert np.all(w != w0)
+    np.testing.assert_allclose(w, net.plastic_weights(), rtol=1e-10)
+
+
+def test_stdp_history_ring_full_is_an_error():
+    """More than 32 postsynaptic spikes of one neuron within max_delay (a
+    target spiking every 0.2 ms, plastic delays of 10 ms): the entries the
+    next slice needs no longer fit the 64-entry ring, and the engine says so
+    at its next synchronisation."""
+    eng = _abi.Engine([(_abi.NG_IAF_PSC_DELTA, 2)], H, 1, 100)
+    eng.set_var(0, "I_e", np.array([375.2, 50000.0]))
+    eng.set_var(0, "t_ref", np.array([2.0, 0.1]))
     eng.set_connections(np.array([0, 1, 1], dtype=np.int64), np.array([0], np.int32), np.array([0.0]),
                         np.array([1], np.int32))
-    eng.set_plastic(np.array([0, 1], dtype=np.int64), np.array([1], np.int32), np.array([1.0]), np.array([1], np.int32))
+    eng.set_plastic(np.array([0, 1], dtype=np.int64), np.array([1], np.int32), np.array([1.0]),
+                    np.array([100], np.int32))
     with pytest.raises(_abi.EngineError) as err:
-        eng.simulate(20000)
+        eng.simulate(2000)
         eng.sync()
     assert err.value.code == _abi.NG_ERR_CAPACITY and "history" in str(err.value)
     eng.close()

@@ -44,5 +44,7 @@ def test_extension_builds_against_reference_headers():
     assert {"module", "nestgpu_init"} <= names
     undefined = subprocess.run(["nm", "-DC", "--undefined-only", so], capture_output=True, text=True).stdout
     for sym in ("nest::ModelManager::register_node_model_", "nest::ConnectionManager::get_connections",
-                "nest::ConnectionManager::send_to_devices", "ng_update", "ng_create"):
+                "nest::ConnectionManager::send_to_devices", "nest::ConnectionManager::set_synapse_status",
+                "nest::ModelManager::get_connector_defaults", "ng_update", "ng_create",
+                "ng_set_plastic_connections", "ng_get_plastic_weights"):
         assert sym in undefined, sym
