@@ -6,6 +6,13 @@ a kernel on a small instance (run from the repository root):
   python bench_cases.py aeif --neurons 10000 --ms 60
   python bench_cases.py serving --requests 40 --capacity-neurons 300000 --capacity-edges 200000000 --slices 40
   python bench_cases.py hpc --scale 0.5 --ms 200 --precision fp64
+  python bench_cases.py atomics --precision fp64
+
+The atomics case measures the device's rate of FP64 (or int64) atomic adds to
+random cells of a ring the size of the layered network's (77,169 neurons x
+80 slots x 2 channels), 9.2e6 adds per launch -- one step's deliveries at its
+mean rate -- through torch.index_add_ (atomics into global memory): the wall
+a scatter delivery of that network meets.
 
 Each case builds its network, simulates, prints one summary line and exits 0.
 The c1 case is bench.py's headline network (12,500 iaf_psc_exp neurons,
@@ -28,7 +35,7 @@ import sys
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["c1", "layered", "aeif", "serving", "hpc"])
+    ap.add_argument("case", choices=["c1", "layered", "aeif", "serving", "hpc", "atomics"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0, help="layered, hpc: population size factor")
     ap.add_argument("--neurons", type=int, default=50000, help="aeif: network size (80 % excitatory)")
@@ -47,6 +54,28 @@ def main(argv=None):
     from nestgpu import serving, workloads
     from nestgpu.kernel import KERNEL
 
+    if a.case == "atomics":
+        import torch
+
+        dev = torch.device("cuda", 0)
+        dt = torch.float64 if a.precision == "fp64" else torch.int64
+        cells, n_ev = 77169 * 80 * 2, 9_200_000
+        g = torch.Generator(device=dev).manual_seed(1)
+        ring = torch.zeros(cells, dtype=dt, device=dev)
+        idx = torch.randint(0, cells, (n_ev,), device=dev, generator=g)
+        val = torch.ones(n_ev, dtype=dt, device=dev)
+        for _ in range(3):
+            ring.index_add_(0, idx, val)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            ring.index_add_(0, idx, val)
+        e1.record()
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / 20
+        print(f"atomics ({dt}): {n_ev} random adds into {cells} cells in {us:.1f} us: {n_ev / us * 1e6:.3e} adds/s",
+              flush=True)
+        return 0
     if a.case == "hpc":
         # the hpc_benchmark network (iaf_psc_alpha, E->E stdp_pl_synapse_hom_hpc)
         workloads.hpc_benchmark(nest, scale=a.scale, precision=a.precision, record=False)

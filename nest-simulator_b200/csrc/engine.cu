@@ -705,9 +705,11 @@ struct ng_engine
   // ---- stdp_pl_synapse_hom connections (ng_set_plastic_connections)
   bool plastic_on = false;
   DevBuf pl_row, pl_tgt, pl_dly, pl_w, pl_Kplus, pl_tlast, pl_ninc, pl_tauinv, pl_Kminus, pl_last, pl_hist_t, pl_hist_K,
-    pl_hist_n, pl_hist_lo, pl_drop_t, pl_drop_K, pl_nflush, pl_in_row, pl_in_edge, pl_in_src, pl_wrun;
+    pl_hist_n, pl_hist_lo, pl_drop_t, pl_drop_K, pl_nflush, pl_in_row, pl_in_edge, pl_in_src, pl_wrun, pl_tab_fin,
+    pl_tab_km;
   int64_t pl_nnz = 0, pl_nsrc = 0;
   double pl_dmax_ms = 0;
+  int32_t pl_dconst = -1;  // the plastic delay when all are equal
   double pl_lambda = 0.1, pl_alpha = 1.0, pl_mu = 0.4, pl_tau_plus = 20.0;
   std::vector< double > tau_minus_host;  // per neuron, the postsynaptic trace's time constant (ArchivingNode)
   int pk_occ = -1;           // its resident CTAs per SM (-1: not known yet)
@@ -716,7 +718,7 @@ struct ng_engine
   int64_t deliver_want = 1;  // delivery CTAs the graph can keep busy (its chunks / 64)
   int rate_bucket = -1;
   int64_t trial_steps = 0;
-  bool aeif_binning = true;  // order aeif threads by RKF45 step size (ng_set_option "aeif_binning")
+  bool aeif_binning = false;  // order aeif threads by RKF45 step size (ng_set_option "aeif_binning"; off: measured slower)
   struct TuneCand
   {
     int variant, per_sm, group;
@@ -759,7 +761,8 @@ struct ng_engine
       &d_key, &sc_src, &sc_cnt, &sc_fill, &sc_beg, &sc_plen, &sc_total, &sc_sb, &gmask, &gin, &net_g, &net_mode,
       &net_spk, &log_sorted, &log_cnt, &log_off, &sc_bound, &seg, &net_t, &row_ue, &row_ls, &ent_late, &pk, &pl_row,
       &pl_tgt, &pl_dly, &pl_w, &pl_Kplus, &pl_tlast, &pl_ninc, &pl_tauinv, &pl_Kminus, &pl_last, &pl_hist_t, &pl_hist_K,
-      &pl_hist_n, &pl_hist_lo, &pl_drop_t, &pl_drop_K, &pl_nflush, &pl_in_row, &pl_in_edge, &pl_in_src, &pl_wrun };
+      &pl_hist_n, &pl_hist_lo, &pl_drop_t, &pl_drop_K, &pl_nflush, &pl_in_row, &pl_in_edge, &pl_in_src, &pl_wrun,
+      &pl_tab_fin, &pl_tab_km };
     for ( DevBuf* b : bufs )
       cudaFree( b->p );
     if ( host_ctl )
@@ -1266,6 +1269,9 @@ struct ng_engine
     p.in_edge = ( const uint32_t* ) pl_in_edge.p;
     p.in_src = ( const int32_t* ) pl_in_src.p;
     p.dmax_ms = pl_dmax_ms;
+    p.dconst = pl_dconst;
+    p.tab_fin = ( int32_t* ) pl_tab_fin.p;
+    p.tab_km = ( double* ) pl_tab_km.p;
     p.lambda = pl_lambda;
     p.alpha = pl_alpha;
     p.mu = pl_mu;
@@ -1286,6 +1292,12 @@ struct ng_engine
       const StdpNet p = stdp();
       const unsigned ga = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( N + 255 ) / 256, 4 * sms ) );
       const unsigned gd = ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( pl_nsrc, 8 * sms ) );
+      if ( pl_dconst >= 0 )
+      {
+        const int64_t q = N * cfg.min_delay;
+        k_stdp_arrivals<<< ( unsigned ) std::max< int64_t >( 1, std::min< int64_t >( ( q + 255 ) / 256, 8 * sms ) ), 256, 0,
+          stream >>>( d, p );
+      }
       if ( prec == NG_FP64 )
         k_stdp_deliver< false ><<< gd, 256, 0, stream >>>( d, p );
       else
@@ -1972,12 +1984,6 @@ struct ng_engine
   autotune( int64_t& n, int64_t gmax )
   {
     const int64_t md = cfg.min_delay;
-    // slices per trial group: ~256 steps (a few hundred microseconds of
-    // device time, long enough for event timing), within the spike log
-    const int64_t S = std::min< int64_t >( std::max< int64_t >( 4, ( 256 + md - 1 ) / md ), gmax / md );
-    if ( S < 2 )
-      return NG_OK;  // a trial group would not fit the spike log
-    const int64_t steps = S * md;
     bool iaf = false;
     for ( const auto& b : blk )
       iaf = iaf || b.model != NG_AEIF_COND_ALPHA;
@@ -2003,10 +2009,15 @@ struct ng_engine
     if ( variants.empty() )
       variants.push_back( upd_variant >= 0 ? upd_variant : 0 );
     const int64_t n_cand = ( int64_t ) ( variants.size() + per_sm.size() + groups.size() );
-    // the probe (3 trial lengths) and the trials must fit the call's steps;
-    // otherwise wait for a longer call
-    if ( n < ( 3 + 2 * n_cand ) * steps )
+    // slices per trial group: ~256 steps (long enough for event timing),
+    // fewer when the probe (3 groups) and the trials (2 groups each) would
+    // not fit the call's steps, at least 4; within the spike log.  A call
+    // too short for that leaves the tuning to a longer one.
+    const int64_t S = std::min( { std::max< int64_t >( 4, ( 256 + md - 1 ) / md ), n / ( ( 3 + 2 * n_cand ) * md ),
+      gmax / md } );
+    if ( S < 4 )
       return NG_OK;
+    const int64_t steps = S * md;
     const int v0 = upd_variant >= 0 ? upd_variant : ( iaf ? default_variant( blk[ 0 ].n ) : 0 );
     TuneCand best { v0, deliver_per_sm, deliver_group, 1e300 };
     tune_log.clear();
@@ -2808,7 +2819,7 @@ ng_set_plastic_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr,
   std::vector< int32_t > in_src( ( size_t ) std::max< int64_t >( nnz, 1 ) );
   {
     std::vector< int64_t > fill( in_row.begin(), in_row.end() - 1 );
-    int32_t dmax = 0;
+    int32_t dmax = 0, dmin = INT32_MAX;
     for ( int64_t s2 = 0; s2 < n_src; ++s2 )
       for ( int64_t k = row_ptr[ s2 ]; k < row_ptr[ s2 + 1 ]; ++k )
       {
@@ -2816,8 +2827,10 @@ ng_set_plastic_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr,
         in_edge[ ( size_t ) q ] = ( uint32_t ) k;
         in_src[ ( size_t ) q ] = ( int32_t ) s2;
         dmax = std::max( dmax, delay_steps[ k ] );
+        dmin = std::min( dmin, delay_steps[ k ] );
       }
     e->pl_dmax_ms = ( double ) dmax * ( ( double ) e->tics_per_step / e->cfg.tics_per_ms );
+    e->pl_dconst = ( nnz > 0 && dmin == dmax ) ? dmax : -1;
   }
   cudaSetDevice( e->cfg.device );
   int rc;
@@ -2843,6 +2856,12 @@ ng_set_plastic_connections( ng_engine* e, int64_t n_src, const int64_t* row_ptr,
     return rc;
   if ( !e->gmask.p && ( rc = e->alloc( e->gmask, N * 4 ) ) )
     return rc;
+  if ( e->pl_dconst >= 0 )
+  {
+    const size_t q = N * ( size_t ) e->cfg.min_delay;
+    if ( ( rc = e->alloc( e->pl_tab_fin, q * 4 ) ) || ( rc = e->alloc( e->pl_tab_km, q * 8 ) ) )
+      return rc;
+  }
   e->pl_nnz = nnz;
   e->pl_nsrc = n_src;
   e->pl_lambda = lambda;

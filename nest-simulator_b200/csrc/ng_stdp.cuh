@@ -74,6 +74,9 @@ struct StdpNet
   const uint32_t* in_edge;  // their indices in the CSR
   const int32_t* in_src;
   double dmax_ms;         // the largest plastic delay
+  int32_t dconst;         // the plastic delay in steps when all are equal, else -1
+  int32_t* tab_fin;       // dconst >= 0: per (neuron, lag of the slice) the end of the
+  double* tab_km;         //   facilitation range and the depression trace (k_stdp_arrivals)
   double lambda, alpha, mu, tau_plus_inv;
   double ms_per_tic;      // Time::get_ms = MS_PER_TIC * tics
   int64_t tics_per_step;
@@ -131,52 +134,99 @@ k_stdp_archive( Net d, StdpNet p )
   }
 }
 
-// weight of one connection after one presynaptic spike at t_spike
+// w^mu of the facilitation, through exp and log (w > 0; the power law's
+// value at 0 otherwise)
 __device__ __forceinline__ double
-stdp_pl_update( const StdpNet& p, int32_t tg, double w, double d_ms, double Kplus, double tlast, double t_spike,
+stdp_pow( double w, double mu )
+{
+  return w > 0.0 ? exp( mu * log( w ) ) : pow( w, mu );
+}
+
+// end of the facilitation range of an arrival at t = t_spike - d: the live
+// entries before t + eps (get_history's upper bound)
+__device__ __forceinline__ int64_t
+stdp_fin( const double* ht, int64_t lo, int64_t hn, double t )
+{
+  const double t2_lim = t + STDP_EPS;
+  int64_t fin = hn;
+  while ( fin > lo && ht[ ( fin - 1 ) & ( STDP_HIST - 1 ) ] >= t2_lim )
+    --fin;
+  return fin;
+}
+
+// the postsynaptic trace at t (get_K_value, archiving_node.cpp:87-113: the
+// latest entry strictly before t); the newest dropped entry when every live
+// one is later
+__device__ __forceinline__ double
+stdp_kminus( const StdpNet& p, int32_t tg, const double* ht, const double* hk, int64_t lo, int64_t fin, double t,
   bool& overflow )
 {
-  const int64_t hn = p.hist_n[ tg ];
-  const int64_t lo = p.hist_lo[ tg ];
-  const double* ht = p.hist_t + ( int64_t ) tg * STDP_HIST;
-  const double* hk = p.hist_K + ( int64_t ) tg * STDP_HIST;
-  // get_history( t_last - d, t_spike - d ): entries t1 + eps <= t < t2 + eps
-  // (entries before lo in the range were applied when they were dropped)
-  const double t1_lim = tlast - d_ms + STDP_EPS;
-  const double t2_lim = t_spike - d_ms + STDP_EPS;
-  int64_t fin = hn;
-  while ( fin > lo && ht[ ( fin - 1 ) % STDP_HIST ] >= t2_lim )
-    --fin;
-  int64_t st = fin;
-  while ( st > lo && ht[ ( st - 1 ) % STDP_HIST ] >= t1_lim )
-    --st;
-  // facilitation, in time order
-  for ( int64_t k = st; k < fin; ++k )
-  {
-    const double minus_dt = tlast - ( ht[ k % STDP_HIST ] + d_ms );
-    const double kplus = Kplus * exp( minus_dt * p.tau_plus_inv );
-    w = w + ( p.lambda * pow( w, p.mu ) * kplus );
-  }
-  // depression by the trace at t_spike - d (get_K_value: the latest entry
-  // strictly before, archiving_node.cpp:87-113); the newest dropped entry
-  // when every live one is later
-  const double t = t_spike - d_ms;
-  double kminus = 0.;
   int64_t k = fin - 1;
-  while ( k >= lo && !( t - ht[ k % STDP_HIST ] > STDP_EPS ) )
+  while ( k >= lo && !( t - ht[ k & ( STDP_HIST - 1 ) ] > STDP_EPS ) )
     --k;
   if ( k >= lo )
-    kminus = hk[ k % STDP_HIST ] * exp( ( ht[ k % STDP_HIST ] - t ) * p.tau_minus_inv[ tg ] );
-  else if ( lo > 0 )
+    return hk[ k & ( STDP_HIST - 1 ) ] * exp( ( ht[ k & ( STDP_HIST - 1 ) ] - t ) * p.tau_minus_inv[ tg ] );
+  if ( lo > 0 )
   {
     const double te = p.drop_t[ tg ];
     if ( t - te > STDP_EPS )
-      kminus = p.drop_K[ tg ] * exp( ( te - t ) * p.tau_minus_inv[ tg ] );
-    else
-      overflow = true;  // cannot happen: dropped entries lie max_delay before the slice
+      return p.drop_K[ tg ] * exp( ( te - t ) * p.tau_minus_inv[ tg ] );
+    overflow = true;  // cannot happen: dropped entries lie max_delay before the slice
+  }
+  return 0.;
+}
+
+// weight of one connection after one presynaptic spike at t_spike, given
+// the end of its facilitation range (fin) and the depression trace:
+// facilitation by the live entries in [t_last - d + eps, t_spike - d + eps)
+// in time order (entries before lo in the range were applied when they were
+// dropped), then depression (stdp_pl_synapse_hom::send, :255-298)
+__device__ __forceinline__ double
+stdp_pl_apply( const StdpNet& p, const double* ht, int64_t lo, int64_t fin, double w, double d_ms, double Kplus,
+  double tlast, double kminus )
+{
+  const double t1_lim = tlast - d_ms + STDP_EPS;
+  int64_t st = fin;
+  while ( st > lo && ht[ ( st - 1 ) & ( STDP_HIST - 1 ) ] >= t1_lim )
+    --st;
+  for ( int64_t k = st; k < fin; ++k )
+  {
+    const double minus_dt = tlast - ( ht[ k & ( STDP_HIST - 1 ) ] + d_ms );
+    const double kplus = Kplus * exp( minus_dt * p.tau_plus_inv );
+    w = w + ( p.lambda * stdp_pow( w, p.mu ) * kplus );
   }
   const double new_w = w - ( p.lambda * p.alpha * w * kminus );
   return new_w > 0.0 ? new_w : 0.0;
+}
+
+// With one plastic delay for all connections, every arrival at a neuron in
+// a slice happens at one of min_delay times (lag k: t = stamp(origin + k + 1)
+// - d), so the end of its facilitation range and its depression trace are
+// computed here once per (neuron, lag) instead of once per connection.
+__global__ void
+k_stdp_arrivals( Net d, StdpNet p )
+{
+  const long long origin = cta_origin( d );
+  const double d_ms = ( double ) p.dconst * ( p.ms_per_tic * ( double ) p.tics_per_step );
+  const int md = d.min_delay;
+  bool overflow = false;
+  for ( int64_t q = ( int64_t ) blockIdx.x * blockDim.x + threadIdx.x; q < d.N * md;
+        q += ( int64_t ) gridDim.x * blockDim.x )
+  {
+    const int64_t tg = q / md;
+    const int k = ( int ) ( q - tg * md );
+    if ( !p.n_inc[ tg ] )
+      continue;
+    const int64_t hn = p.hist_n[ tg ], lo = p.hist_lo[ tg ];
+    const double* ht = p.hist_t + tg * STDP_HIST;
+    const double* hk = p.hist_K + tg * STDP_HIST;
+    const double t = stdp_stamp_ms( p, origin + k + 1 ) - d_ms;
+    const int64_t fin = stdp_fin( ht, lo, hn, t );
+    p.tab_fin[ q ] = ( int32_t ) ( fin - lo );
+    p.tab_km[ q ] = stdp_kminus( p, ( int32_t ) tg, ht, hk, lo, fin, t, overflow );
+  }
+  if ( overflow )
+    atomicOr( &d.ctl->err, ERR_STDP_HISTORY );
 }
 
 // The oldest n_flush entries of a marked neuron: each incoming connection
@@ -209,7 +259,7 @@ k_stdp_flush( Net d, StdpNet p )
         if ( te >= t1_lim )
         {
           const double kplus = Kp * exp( ( tl - ( te + d_ms ) ) * p.tau_plus_inv );
-          w = w + ( p.lambda * pow( w, p.mu ) * kplus );
+          w = w + ( p.lambda * stdp_pow( w, p.mu ) * kplus );
           changed = true;
         }
       }
@@ -231,13 +281,20 @@ k_stdp_flush( Net d, StdpNet p )
 // One CTA per spiking source at a time (grid-stride over sources): the
 // CTA's threads split the source's plastic row, so a spike's thousands of
 // connections -- each a chain of dependent history loads -- run on 256
-// threads instead of 32.  Every thread reads the source's Kplus and t_last
-// before the CTA's closing barrier; thread 0 writes them after it.
+// threads instead of 32.  Thread 0 first lays out the source's spikes of
+// the slice in shared memory (lag, time, ring slot, and Kplus / t_last
+// before each spike) and advances the source's Kplus and t_last; each
+// thread then applies the spikes to its connections in time order.
 template < bool FIX >
 __global__ void __launch_bounds__( 256 )
 k_stdp_deliver( Net d, StdpNet p )
 {
+  __shared__ double s_t[ 32 ], s_Kp[ 32 ], s_tl[ 32 ];
+  __shared__ int s_k[ 32 ], s_slot0[ 32 ];
+  __shared__ int s_n;
   const long long origin = cta_origin( d );
+  const double h_ms = p.ms_per_tic * ( double ) p.tics_per_step;
+  const int md = d.min_delay;
   bool overflow = false;
   unsigned long long events = 0;
   for ( int64_t src = blockIdx.x; src < p.n_src; src += gridDim.x )
@@ -246,24 +303,61 @@ k_stdp_deliver( Net d, StdpNet p )
     const int64_t e0 = p.row[ src ], e1 = p.row[ src + 1 ];
     if ( m0 == 0 || e1 == e0 )
       continue;  // uniform over the CTA
-    const double Kp0 = p.Kplus[ src ], tl0 = p.tlast[ src ];
-    for ( int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x )
+    if ( threadIdx.x == 0 )
     {
-      const int32_t tg = p.tgt[ e ];
-      const int32_t dl = p.dly[ e ];
-      const double d_ms = ( double ) dl * ( p.ms_per_tic * ( double ) p.tics_per_step );
-      double w = p.w_run[ e ];
-      double Kp = Kp0, tl = tl0;
+      double Kp = p.Kplus[ src ], tl = p.tlast[ src ];
+      int n = 0;
       unsigned m = m0;
       while ( m )
       {
         const int k = __ffs( m ) - 1;
         m &= m - 1;
-        const long long te = origin + k;
-        const double t_spike = stdp_stamp_ms( p, te + 1 );
-        w = stdp_pl_update( p, tg, w, d_ms, Kp, tl, t_spike, overflow );
+        const double t_spike = stdp_stamp_ms( p, origin + k + 1 );
+        s_k[ n ] = k;
+        s_t[ n ] = t_spike;
+        s_Kp[ n ] = Kp;
+        s_tl[ n ] = tl;
+        s_slot0[ n ] = ( int ) ( ( origin + k ) % d.L );
+        Kp = Kp * exp( ( tl - t_spike ) * p.tau_plus_inv ) + 1.0;
+        tl = t_spike;
+        ++n;
+      }
+      s_n = n;
+      p.Kplus[ src ] = Kp;
+      p.tlast[ src ] = tl;
+      events += ( unsigned long long ) ( e1 - e0 ) * ( unsigned long long ) n;
+    }
+    __syncthreads();
+    const int ns = s_n;
+    for ( int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x )
+    {
+      const int32_t tg = p.tgt[ e ];
+      const int32_t dl = p.dly[ e ];
+      const double d_ms = ( double ) dl * h_ms;
+      double w = p.w_run[ e ];
+      const int64_t hn = p.hist_n[ tg ], lo = p.hist_lo[ tg ];
+      const double* ht = p.hist_t + ( int64_t ) tg * STDP_HIST;
+      for ( int j = 0; j < ns; ++j )
+      {
+        int64_t fin;
+        double kminus;
+        if ( p.dconst >= 0 )
+        {
+          const int64_t q = ( int64_t ) tg * md + s_k[ j ];
+          fin = lo + p.tab_fin[ q ];
+          kminus = p.tab_km[ q ];
+        }
+        else
+        {
+          const double t = s_t[ j ] - d_ms;
+          fin = stdp_fin( ht, lo, hn, t );
+          kminus = stdp_kminus( p, tg, ht, p.hist_K + ( int64_t ) tg * STDP_HIST, lo, fin, t, overflow );
+        }
+        w = stdp_pl_apply( p, ht, lo, fin, w, d_ms, s_Kp[ j ], s_tl[ j ], kminus );
         // handle(SpikeEvent&): weight x multiplicity into the channel of its sign
-        const int slot = ( int ) ( ( te + dl ) % d.L );
+        int slot = s_slot0[ j ] + dl;
+        if ( slot >= d.L )
+          slot -= d.L;
         const int ch = ( p.sign_channels && !( w > 0.0 ) ) ? 1 : 0;
         const int64_t idx = ( ( int64_t ) slot * d.C + ch ) * d.N + tg;
         if constexpr ( FIX )
@@ -271,30 +365,11 @@ k_stdp_deliver( Net d, StdpNet p )
             ( unsigned long long ) __double2ll_rn( w * ( 1.0 / d.fx_inv ) ) );
         else
           atomicAdd( ( double* ) d.ring + idx, w );
-        Kp = Kp * exp( ( tl - t_spike ) * p.tau_plus_inv ) + 1.0;
-        tl = t_spike;
       }
       p.w[ e ] = w;
       p.w_run[ e ] = w;
     }
-    if ( threadIdx.x == 0 )
-      events += ( unsigned long long ) ( e1 - e0 ) * ( unsigned long long ) __popc( m0 );
-    __syncthreads();
-    if ( threadIdx.x == 0 )
-    {
-      double Kp = Kp0, tl = tl0;
-      unsigned m = m0;
-      while ( m )
-      {
-        const int k = __ffs( m ) - 1;
-        m &= m - 1;
-        const double t_spike = stdp_stamp_ms( p, origin + k + 1 );
-        Kp = Kp * exp( ( tl - t_spike ) * p.tau_plus_inv ) + 1.0;
-        tl = t_spike;
-      }
-      p.Kplus[ src ] = Kp;
-      p.tlast[ src ] = tl;
-    }
+    __syncthreads();  // the spike table is rewritten for the next source
   }
   if ( threadIdx.x == 0 && events )
     atomicAdd( &d.ctl->syn_events, events );
