@@ -100,10 +100,12 @@ def parse():
     return ap.parse_args()
 
 
-def load_traffic(kernel, workload):
+def load_traffic(kernel, workload, slices_per_launch=None):
     """DRAM bytes per launch of `kernel` on `workload` from the ncu summary
-    profiles/roofline_traffic.txt (lines: kernel workload bytes_per_launch),
-    or None."""
+    profiles/roofline_traffic.txt (lines: kernel workload bytes [per_slice]),
+    or None.  A per_slice figure (a kernel that runs many slices per launch)
+    is scaled by the launch's slices: its traffic grows with them (the
+    captured launch ran 64 slices)."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
     if not os.path.exists(p):
         return None
@@ -111,6 +113,8 @@ def load_traffic(kernel, workload):
         for line in f:
             parts = line.split()
             if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+                if len(parts) >= 4 and parts[3] == "per_slice":
+                    return float(parts[2]) * slices_per_launch if slices_per_launch else None
                 return float(parts[2])
     return None
 
@@ -888,7 +892,7 @@ def run_engine(args):
                      "bytes_model": "per-unit bytes of the path's survey: 96 B per iaf_psc_exp neuron-step "
                                     "(FP64), 29 B per synaptic event",
                      "frac_engine_model": (dom["engine_model_gbs"] / peak) if dom["engine_model_gbs"] else None,
-                     "traffic": load_traffic(dom_name, "brunel_x1_fp64"),
+                     "traffic": load_traffic(dom_name, "brunel_x1_fp64", dom.get("slices_per_launch")),
                      "kernels": r["kernels"]},
         "e2e": r.get("e2e"),
         "cpu_baseline": cpu,

@@ -98,12 +98,12 @@ ring_ld_l2( const Net& d, int slot, int ch, int64_t i )
 
 // Warp 0's spikes of a chunk of lags as delivery work (entries at running
 // indices of the ring list) and recorder log entries, one reservation per
-// counter and warp.  The row data (start, chunks, real degree) and the
+// counter and warp; lane 0 adds the events and spikes to ev_acc / spk_acc.  The row data (start, chunks, real degree) and the
 // recorder flag of the lane's neuron are passed in registers: they do not
 // change during the launch.  Must be called by all 32 lanes of warp 0.
 __device__ __forceinline__ void
 pk_append( const Net& d, unsigned mask, int32_t src, int slot0, long long t0, long long row, int ue, int nu, int rdeg,
-  bool rec, long long lb0 )
+  bool rec, long long lb0, unsigned long long& ev_acc, unsigned long long& spk_acc )
 {
   const int cnt = __popc( mask );
   if ( __ballot_sync( FULL, cnt > 0 ) == 0 )
@@ -123,8 +123,10 @@ pk_append( const Net& d, unsigned mask, int32_t src, int slot0, long long t0, lo
       base = atomicAdd( &d.ctl->n_ent, ( unsigned long long ) tot_u );
     if ( tot_g > 0 )
       lbase = atomicAdd( &d.ctl->log_count, ( unsigned long long ) tot_g );
-    atomicAdd( &d.ctl->syn_events, ( unsigned long long ) rtot );
-    atomicAdd( &d.ctl->n_spikes, ( unsigned long long ) ctot );
+    // the statistics: once per launch (same-address atomics of every CTA
+    // in every slice would queue at one L2 line)
+    ev_acc += ( unsigned long long ) rtot;
+    spk_acc += ( unsigned long long ) ctot;
   }
   base = __shfl_sync( FULL, base, 0 );
   lbase = __shfl_sync( FULL, lbase, 0 );
@@ -188,7 +190,7 @@ constexpr int PK_NB = 32;  // neurons per CTA
 constexpr int PK_CH = 16;  // lags per phase-1 chunk
 
 template < typename Real, bool FIX, int MODEL >
-__global__ void __launch_bounds__( PK_THREADS )
+__global__ void __launch_bounds__( PK_THREADS, 3 )
 k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
 {
   constexpr bool ALPHA = MODEL == NG_IAF_PSC_ALPHA_ID;
@@ -196,6 +198,7 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
   constexpr int P1 = PK_CH * PK_NB / PK_THREADS;  // phase-1 items per thread
   __shared__ Real s_ex[ PK_CH ][ PK_NB ];
   __shared__ Real s_in[ EXP ? PK_CH : 1 ][ PK_NB ];
+  __shared__ Real s_dv[ 2 ][ PK_CH ][ PK_NB ];  // drive of (lag, neuron) of the current and the next chunk
   __shared__ unsigned s_gen;
   if ( threadIdx.x == 0 )
     s_gen = ld_volatile( &pk->gen );
@@ -279,9 +282,27 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
   if ( qact )
     drive_ctx( d, iq, dc );
   long long dcnt = 0;
+  unsigned long long ev_acc = 0, spk_acc = 0;
   const int md = d.min_delay;
   const long long nwarps = ( ( long long ) gridDim.x * blockDim.x ) >> 5;
   const long long gw = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  // The drive of a chunk's (lag, neuron) pairs: it depends on no spike, so
+  // warps 1-3 draw the next chunk's while warp 0 runs the current recurrence.
+  // Lane q draws for neuron q; warp w takes the lag pairs p = w - 1, w + 2, ...
+  // (one Philox block serves the two steps of a pair).
+  auto draw_chunk = [ & ]( int buf, long long t0c, int nlc, int w0, int nw ) {
+    for ( int pr = warp - w0; 2 * pr < nlc; pr += nw )
+#pragma unroll
+      for ( int h2 = 0; h2 < 2; ++h2 )
+      {
+        const int k = 2 * pr + h2;
+        if ( k < nlc )
+          s_dv[ buf ][ k ][ lane ] = qact ? drive_at< Real >( d, dc, iq, t0c + k, dcnt ) : Real( 0 );
+      }
+  };
+  int buf = 0;
+  draw_chunk( 0, origin0, min( PK_CH, md ), 0, PK_THREADS / 32 );
+  __syncthreads();
   int sl = 0;
   for ( ; sl < n_slices; ++sl )
   {
@@ -291,9 +312,8 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
       const int nl = min( PK_CH, md - cb );
       const long long t0 = origin + cb;
       const int slot0 = ( int ) ( t0 % d.L );
-      // ---- phase 1: ring cells and drive of (neuron q, lag k), item j = k * 32 + q
+      // ---- phase 1: ring cells of (neuron q, lag k), item j = k * 32 + q
       typename RingVal< FIX >::type rex[ P1 ], rin[ P1 ];
-      Real dvs[ P1 ];
       int slots[ P1 ];
 #pragma unroll
       for ( int m = 0; m < P1; ++m )
@@ -301,7 +321,6 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
         const int j = threadIdx.x + m * PK_THREADS;
         rex[ m ] = 0;
         rin[ m ] = 0;
-        dvs[ m ] = Real( 0 );
         slots[ m ] = -1;
         if ( j < nl * PK_NB && qact )
         {
@@ -313,7 +332,6 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
           rex[ m ] = ring_ld_l2< FIX >( d, slot, 0, iq );
           if constexpr ( EXP )
             rin[ m ] = ring_ld_l2< FIX >( d, slot, 1, iq );
-          dvs[ m ] = drive_at< Real >( d, dc, iq, t0 + k, dcnt );
         }
       }
 #pragma unroll
@@ -328,7 +346,7 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
           ex = ring_real< Real, FIX >( d, rex[ m ] );
           if constexpr ( EXP )
             inh = ring_real< Real, FIX >( d, rin[ m ] );
-          const Real dv = dvs[ m ];
+          const Real dv = s_dv[ buf ][ j >> 5 ][ j & 31 ];
           if ( dv != Real( 0 ) )
           {
             if constexpr ( EXP )
@@ -417,8 +435,17 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
               smask |= 1u << k;
           }
         }
-        pk_append( d, smask, ( int32_t ) i, slot0, t0, row, ue, nu, rdeg, rec, lb0 );
+        pk_append( d, smask, ( int32_t ) i, slot0, t0, row, ue, nu, rdeg, rec, lb0, ev_acc, spk_acc );
       }
+      else
+      {
+        // the next chunk's drive, beside the recurrence
+        const bool more = cb + PK_CH < md;
+        if ( more || sl + 1 < n_slices )
+          draw_chunk( buf ^ 1, more ? t0 + PK_CH : origin + md, more ? min( PK_CH, md - cb - PK_CH ) : min( PK_CH, md ),
+            1, PK_THREADS / 32 - 1 );
+      }
+      buf ^= 1;
       __syncthreads();  // s_ex / s_in are refilled by the next chunk
     }
     if ( !pk_grid_sync( pk, gen ) )
@@ -457,6 +484,11 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
       break;
   }
   flush_drive_count( d, dcnt );
+  if ( threadIdx.x == 0 && ( ev_acc | spk_acc ) )
+  {
+    atomicAdd( &d.ctl->syn_events, ev_acc );
+    atomicAdd( &d.ctl->n_spikes, spk_acc );
+  }
   if ( blockIdx.x == 0 && threadIdx.x == 0 )
   {
     // the graph form's state at a slice boundary: empty work list, clock advanced
