@@ -1973,6 +1973,7 @@ struct ng_engine
     if ( ( rc = drain_group( 0, gi ) ) )
       return rc;
     float ms = 0;
+    CU( cudaEventSynchronize( ev1 ) );  // the drain may have waited on an earlier point of the stream
     CU( cudaEventElapsedTime( &ms, ev0, ev1 ) );
     *us = 1e3 * ms;
     if ( spikes )
