@@ -47,12 +47,18 @@ struct PkCtl
 // (measured: 1.97 us against 3.0 us per barrier on 391 CTAs).  Returns false
 // if the polls gave up or another CTA's did; all threads of the CTA get the
 // same answer.
+// The other threads of the CTA may work between the arrival and the final
+// __syncthreads (`while_waiting`, run by every thread but thread 0): work
+// that depends on nothing the barrier orders.
+template < typename F >
 __device__ __forceinline__ bool
-pk_grid_sync( PkCtl* pk, unsigned& gen )
+pk_grid_sync( PkCtl* pk, unsigned& gen, F&& while_waiting )
 {
   __shared__ int s_ok;
   __syncthreads();
-  if ( threadIdx.x == 0 )
+  if ( threadIdx.x != 0 )
+    while_waiting();
+  else
   {
     int ok = 1;
     const unsigned target = ( gen + 1u ) * gridDim.x;
@@ -79,6 +85,12 @@ pk_grid_sync( PkCtl* pk, unsigned& gen )
   __syncthreads();
   ++gen;
   return s_ok != 0;
+}
+
+__device__ __forceinline__ bool
+pk_grid_sync( PkCtl* pk, unsigned& gen )
+{
+  return pk_grid_sync( pk, gen, [] {} );
 }
 
 // A ring cell read through L2 only: the cell was written by other SMs'
@@ -436,13 +448,10 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
         }
         pk_append( d, smask, ( int32_t ) i, slot0, t0, row, ue, nu, rdeg, rec, lb0, ev_acc, spk_acc );
       }
-      else
+      else if ( cb + PK_CH < md )
       {
-        // the next chunk's drive, beside the recurrence
-        const bool more = cb + PK_CH < md;
-        if ( more || sl + 1 < n_slices )
-          draw_chunk( buf ^ 1, more ? t0 + PK_CH : origin + md, more ? min( PK_CH, md - cb - PK_CH ) : min( PK_CH, md ),
-            1, PK_THREADS / 32 - 1 );
+        // the next chunk's drive (same slice), beside the recurrence
+        draw_chunk( buf ^ 1, t0 + PK_CH, min( PK_CH, md - cb - PK_CH ), 1, PK_THREADS / 32 - 1 );
       }
       buf ^= 1;
       __syncthreads();  // s_ex / s_in are refilled by the next chunk
@@ -459,7 +468,10 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
     }
     else
     {
-      const long long G = max( 1ll, min( ( long long ) d.deliver_group, nent / nwarps ) );
+      // whole groups of consecutive chunks per warp (rounded up: a warp walks
+      // its group with the next chunk's loads in flight, where a second
+      // round of single chunks would wait a full round trip)
+      const long long G = max( 1ll, min( ( long long ) d.deliver_group, ( nent + nwarps - 1 ) / nwarps ) );
       for ( long long base = gw * G; base < nent; base += nwarps * G )
       {
         const int cnt = ( int ) min( G, nent - base );
@@ -479,7 +491,14 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
       }
     }
     ent_start = ent_end;
-    if ( !pk_grid_sync( pk, gen ) )
+    // the next slice's first chunk of drive, while thread 0 waits at the barrier
+    // (buf already names the buffer after the slice's last chunk; the other
+    // one was last read by a chunk before it)
+    const bool next = sl + 1 < n_slices;
+    if ( !pk_grid_sync( pk, gen, [ & ] {
+           if ( next && warp > 0 )
+             draw_chunk( buf, origin + md, min( PK_CH, md ), 1, PK_THREADS / 32 - 1 );
+         } ) )
       break;
   }
   flush_drive_count( d, dcnt );
