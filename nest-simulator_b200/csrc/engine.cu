@@ -713,6 +713,7 @@ struct ng_engine
   double pl_lambda = 0.1, pl_alpha = 1.0, pl_mu = 0.4, pl_tau_plus = 20.0;
   std::vector< double > tau_minus_host;  // per neuron, the postsynaptic trace's time constant (ArchivingNode)
   int pk_occ = -1;           // its resident CTAs per SM (-1: not known yet)
+  int pk_occ_mg = 0;         // ... and the multi-group form's
   int occ_deliver = 8;       // resident k_deliver CTAs per SM (occupancy bound)
   int deliver_group = 4;     // edge chunks one delivery warp takes per descriptor load
   int64_t deliver_want = 1;  // delivery CTAs the graph can keep busy (its chunks / 64)
@@ -1167,28 +1168,36 @@ struct ng_engine
 
   template < typename Real, bool FIX, int MODEL >
   const void*
-  pk_func() const
+  pk_func( bool mg ) const
   {
-    return reinterpret_cast< const void* >( &k_run_slices< Real, FIX, MODEL > );
+    return mg ? reinterpret_cast< const void* >( &k_run_slices_mg< Real, FIX, MODEL > )
+              : reinterpret_cast< const void* >( &k_run_slices< Real, FIX, MODEL > );
   }
 
+  // the persistent kernel: one resident wave holding every neuron's state in
+  // registers (k_run_slices), or the multi-group form for larger networks
   const void*
-  pk_kernel() const
+  pk_kernel( bool mg ) const
   {
     const int m = blk[ 0 ].model;
     if ( prec == NG_FP64 )
-      return m == NG_IAF_PSC_DELTA ? pk_func< double, false, NG_IAF_PSC_DELTA >()
-        : m == NG_IAF_PSC_EXP      ? pk_func< double, false, NG_IAF_PSC_EXP >()
-                                   : pk_func< double, false, NG_IAF_PSC_ALPHA >();
-    return m == NG_IAF_PSC_DELTA ? pk_func< float, true, NG_IAF_PSC_DELTA >()
-      : m == NG_IAF_PSC_EXP      ? pk_func< float, true, NG_IAF_PSC_EXP >()
-                                 : pk_func< float, true, NG_IAF_PSC_ALPHA >();
+      return m == NG_IAF_PSC_DELTA ? pk_func< double, false, NG_IAF_PSC_DELTA >( mg )
+        : m == NG_IAF_PSC_EXP      ? pk_func< double, false, NG_IAF_PSC_EXP >( mg )
+                                   : pk_func< double, false, NG_IAF_PSC_ALPHA >( mg );
+    return m == NG_IAF_PSC_DELTA ? pk_func< float, true, NG_IAF_PSC_DELTA >( mg )
+      : m == NG_IAF_PSC_EXP      ? pk_func< float, true, NG_IAF_PSC_EXP >( mg )
+                                 : pk_func< float, true, NG_IAF_PSC_ALPHA >( mg );
   }
 
-  // the persistent slice kernel applies: one iaf block of a static engine
-  // that fits one resident wave of its CTAs, no traces or scheduled
-  // generator spikes (whose bookkeeping is per launch), a device that
-  // supports cooperative launches
+  bool
+  pk_multi_group() const
+  {
+    return N > ( int64_t ) pk_occ * sms * PK_NB;
+  }
+
+  // the persistent slice kernel applies: one iaf block of a static engine,
+  // no traces or scheduled generator spikes (whose bookkeeping is per
+  // launch), a device that supports cooperative launches
   bool
   persistent_ok()
   {
@@ -1197,16 +1206,18 @@ struct ng_engine
       return false;
     if ( pk_occ < 0 )
     {
-      int coop = 0, occ = 0;
+      int coop = 0, occ = 0, occ_mg = 0;
       cudaDeviceGetAttribute( &coop, cudaDevAttrCooperativeLaunch, cfg.device );
-      if ( !coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, pk_kernel(), PK_THREADS, 0 ) != cudaSuccess )
-        occ = 0;
+      if ( !coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, pk_kernel( false ), PK_THREADS, 0 ) != cudaSuccess
+        || cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ_mg, pk_kernel( true ), PK_THREADS, 0 ) != cudaSuccess )
+        occ = occ_mg = 0;
       cudaGetLastError();
       pk_occ = occ;
-      if ( occ > 0 && !pk.p && alloc( pk, sizeof( PkCtl ) ) != NG_OK )
+      pk_occ_mg = occ_mg;
+      if ( occ > 0 && occ_mg > 0 && !pk.p && alloc( pk, sizeof( PkCtl ) ) != NG_OK )
         pk_occ = 0;
     }
-    return pk_occ > 0 && N <= ( int64_t ) pk_occ * sms * PK_NB;
+    return pk_occ > 0 && ( !pk_multi_group() || pk_occ_mg > 0 );
   }
 
   // k full slices in one cooperative launch; the grid covers the neurons
@@ -1218,13 +1229,14 @@ struct ng_engine
     Net dd = d;
     dd.late_min = INT32_MAX;  // every edge at its slice's close
     Block db = dblock( blk[ 0 ] );
+    const bool mg = pk_multi_group();
     const int64_t need = ( N + PK_NB - 1 ) / PK_NB;
-    const int64_t cap = ( int64_t ) pk_occ * sms;
+    const int64_t cap = ( int64_t ) ( mg ? pk_occ_mg : pk_occ ) * sms;
     const unsigned grid = ( unsigned ) std::min< int64_t >( cap, std::max< int64_t >( need, sms ) );
     PkCtl* pkc = ( PkCtl* ) pk.p;
     CU( cudaMemsetAsync( pk.p, 0, sizeof( PkCtl ), stream ) );
     void* args[] = { &dd, &db, &k, &pkc };
-    CU( cudaLaunchCooperativeKernel( pk_kernel(), dim3( grid ), dim3( PK_THREADS ), args, 0, stream ) );
+    CU( cudaLaunchCooperativeKernel( pk_kernel( mg ), dim3( grid ), dim3( PK_THREADS ), args, 0, stream ) );
     return NG_OK;
   }
 

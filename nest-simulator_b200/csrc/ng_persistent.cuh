@@ -530,4 +530,314 @@ k_run_slices( Net d, Block b, int n_slices, PkCtl* pk )
   }
 }
 
+// The same cycle for a network larger than one resident wave (many
+// networks of a batch concatenated into one block, or one large network):
+// each CTA walks its 32-neuron groups g = block, block + grid, ... in every
+// slice.  A group's state, coefficients, row data and drive context are
+// loaded at the start of its turn and the state written back at its end --
+// from L2, where the state of a network of this size stays (about 130 bytes
+// per neuron) -- instead of living in registers for the launch; the ring,
+// the delivery and the barriers are k_run_slices'.  All four warps read the
+// ring cells and draw the drive of the group's (neuron, lag) pairs, then
+// warp 0 runs the recurrence.
+#ifndef PK_MG_MIN_CTAS
+#define PK_MG_MIN_CTAS 3
+#endif
+template < typename Real, bool FIX, int MODEL >
+__global__ void __launch_bounds__( PK_THREADS, PK_MG_MIN_CTAS )
+k_run_slices_mg( Net d, Block b, int n_slices, PkCtl* pk )
+{
+  constexpr bool ALPHA = MODEL == NG_IAF_PSC_ALPHA_ID;
+  constexpr bool EXP = MODEL == NG_IAF_PSC_EXP_ID || ALPHA;
+  constexpr int P1 = PK_CH * PK_NB / PK_THREADS;  // phase-1 items per thread
+  __shared__ Real s_ex[ PK_CH ][ PK_NB ];
+  __shared__ Real s_in[ EXP ? PK_CH : 1 ][ PK_NB ];
+  __shared__ unsigned s_gen;
+  if ( threadIdx.x == 0 )
+    s_gen = ld_volatile( &pk->gen );
+  const long long origin0 = ld_volatile( &d.ctl->origin );
+  const long long lb0 = ld_volatile( &d.ctl->log_base );
+  unsigned long long ent_start = ld_volatile( &d.ctl->n_ent );
+  __syncthreads();
+  unsigned gen = s_gen;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  Real* s0 = ( Real* ) b.s[ 0 ];
+  Real* s1 = ( Real* ) b.s[ 1 ];
+  Real* s2 = ( Real* ) b.s[ 2 ];
+  Real* s3 = ( Real* ) b.s[ 3 ];
+  Real* s4 = ( Real* ) b.s[ 4 ];
+  const int64_t n_groups = ( b.n + PK_NB - 1 ) / PK_NB;
+  long long dcnt = 0;
+  unsigned long long ev_acc = 0, spk_acc = 0;
+  const int md = d.min_delay;
+  const long long nwarps = ( ( long long ) gridDim.x * blockDim.x ) >> 5;
+  const long long gw = ( ( long long ) blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  int sl = 0;
+  for ( ; sl < n_slices; ++sl )
+  {
+    const long long origin = origin0 + ( long long ) sl * md;
+    for ( int64_t g = blockIdx.x; g < n_groups; g += gridDim.x )
+    {
+      const int64_t nb0 = g * PK_NB;
+      const int64_t li = nb0 + lane;
+      const bool qact = li < b.n;                // this lane's neuron (every warp)
+      const bool act = warp == 0 && qact;        // ... whose recurrence this lane runs
+      const int64_t i = b.off + ( qact ? li : 0 );
+      DriveCtx dc;
+      dc.n = 0;
+      if ( qact )
+        drive_ctx( d, i, dc );
+      Real V = 0, x1 = 0, x2 = 0, i0 = 0, i1 = 0, Ie = 0;
+      Real c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, Vth = 0, Vreset = 0, c9 = 0;
+      AlphaCoef< Real > ac {};
+      int r = 0, refr = 0;
+      long long row = 0;
+      int ue = 0, nu = 0, rdeg = 0;
+      bool rec = false;
+      if ( act )
+      {
+        const double* ct = b.ctab + ( int64_t ) b.cls[ li ] * CT_STRIDE;
+        if constexpr ( ALPHA )
+          alpha_coef< Real >( ct, ac );
+        if constexpr ( EXP && !ALPHA )
+        {
+          c0 = ( Real ) ct[ 0 ];
+          c1 = ( Real ) ct[ 1 ];
+          c2 = ( Real ) ct[ 2 ];
+          c3 = ( Real ) ct[ 3 ];
+          c4 = ( Real ) ct[ 4 ];
+          c5 = ( Real ) ct[ 5 ];
+          Vth = ( Real ) ct[ 6 ];
+          Vreset = ( Real ) ct[ 7 ];
+          refr = ( int ) ct[ 8 ];
+          c9 = ( Real ) ct[ 9 ];
+        }
+        if constexpr ( EXP )
+        {
+          V = s0[ li ];
+          x1 = s1[ li ];
+          x2 = s2[ li ];
+          i0 = s3[ li ];
+          i1 = s4[ li ];
+          Ie = ( ( const Real* ) b.s[ 5 ] )[ li ];
+        }
+        else
+        {
+          c0 = ( Real ) ct[ 0 ];
+          c1 = ( Real ) ct[ 1 ];
+          Vth = ( Real ) ct[ 2 ];
+          Vreset = ( Real ) ct[ 3 ];
+          c2 = ( Real ) ct[ 4 ];
+          refr = ( int ) ct[ 5 ];
+          V = s0[ li ];
+          x1 = s1[ li ];
+          Ie = s2[ li ];
+        }
+        r = b.r[ li ];
+        const RowWork rw = row_work( d, ( int32_t ) i );
+        row = rw.row;
+        ue = rw.ue;
+        nu = rw.nu;
+        rdeg = d.real_deg[ i ];
+        rec = d.rec == nullptr || d.rec[ i ] != 0;
+      }
+      for ( int cb = 0; cb < md; cb += PK_CH )
+      {
+        const int nl = min( PK_CH, md - cb );
+        const long long t0 = origin + cb;
+        const int slot0 = ( int ) ( t0 % d.L );
+        // ---- phase 1: ring cells and drive of (neuron q, lag k), item j = k * 32 + q
+        typename RingVal< FIX >::type rex[ P1 ], rin[ P1 ];
+        Real dvs[ P1 ];
+        int slots[ P1 ];
+#pragma unroll
+        for ( int m = 0; m < P1; ++m )
+        {
+          const int j = threadIdx.x + m * PK_THREADS;
+          rex[ m ] = 0;
+          rin[ m ] = 0;
+          dvs[ m ] = Real( 0 );
+          slots[ m ] = -1;
+          if ( j < nl * PK_NB && qact )
+          {
+            const int k = j >> 5;
+            int slot = slot0 + k;
+            if ( slot >= d.L )
+              slot -= d.L;
+            slots[ m ] = slot;
+            rex[ m ] = ring_ld_l2< FIX >( d, slot, 0, i );
+            if constexpr ( EXP )
+              rin[ m ] = ring_ld_l2< FIX >( d, slot, 1, i );
+            dvs[ m ] = drive_at< Real >( d, dc, i, t0 + k, dcnt );
+          }
+        }
+#pragma unroll
+        for ( int m = 0; m < P1; ++m )
+        {
+          const int j = threadIdx.x + m * PK_THREADS;
+          if ( j >= nl * PK_NB )
+            continue;
+          Real ex = 0, inh = 0;
+          if ( slots[ m ] >= 0 )
+          {
+            ex = ring_real< Real, FIX >( d, rex[ m ] );
+            if constexpr ( EXP )
+              inh = ring_real< Real, FIX >( d, rin[ m ] );
+            const Real dv = dvs[ m ];
+            if ( dv != Real( 0 ) )
+            {
+              if constexpr ( EXP )
+              {
+                if ( dv > Real( 0 ) )
+                  ex = ex + dv;
+                else
+                  inh = inh + dv;
+              }
+              else
+              {
+                ex = ex + dv;
+              }
+            }
+          }
+          s_ex[ j >> 5 ][ j & 31 ] = ex;
+          if constexpr ( EXP )
+            s_in[ j >> 5 ][ j & 31 ] = inh;
+        }
+#pragma unroll
+        for ( int m = 0; m < P1; ++m )
+        {
+          if ( slots[ m ] < 0 )
+            continue;
+          ring_clear< FIX >( d, slots[ m ], 0, i );
+          if constexpr ( EXP )
+            ring_clear< FIX >( d, slots[ m ], 1, i );
+        }
+        __syncthreads();
+        // ---- phase 2: the recurrence, one lane per neuron (iaf_psc_delta:272-329,
+        // iaf_psc_exp:288-348, iaf_psc_alpha update)
+        if ( warp == 0 )
+        {
+          unsigned smask = 0;
+          if ( act )
+          {
+            for ( int k = 0; k < nl; ++k )
+            {
+              bool spk = false;
+              const Real in_ex = s_ex[ k ][ lane ];
+              if constexpr ( ALPHA )
+              {
+                spk = alpha_step< Real >( ac, V, x1, x2, i0, i1, r, Ie, in_ex, s_in[ k ][ lane ] );
+              }
+              else if constexpr ( EXP )
+              {
+                const Real in_in = s_in[ k ][ lane ];
+                if ( r == 0 )
+                  V = V * c0 + x1 * c1 + x2 * c2 + ( Ie + i0 ) * c3;
+                else
+                  --r;
+                x1 *= c4;
+                x2 *= c5;
+                x1 += c9 * i1;
+                x1 += in_ex;
+                x2 += in_in;
+                if ( V >= Vth )
+                {
+                  r = refr;
+                  V = Vreset;
+                  spk = true;
+                }
+                i0 = Real( 0 );
+                i1 = Real( 0 );
+              }
+              else
+              {
+                if ( r == 0 )
+                {
+                  V = c1 * ( x1 + Ie ) + c0 * V + in_ex;
+                  V = ( V < c2 ? c2 : V );
+                }
+                else
+                {
+                  --r;
+                }
+                if ( V >= Vth )
+                {
+                  r = refr;
+                  V = Vreset;
+                  spk = true;
+                }
+                x1 = Real( 0 );
+              }
+              if ( spk )
+                smask |= 1u << k;
+            }
+          }
+          pk_append( d, smask, ( int32_t ) i, slot0, t0, row, ue, nu, rdeg, rec, lb0, ev_acc, spk_acc );
+        }
+        __syncthreads();  // s_ex / s_in are refilled by the next chunk
+      }
+      if ( act )
+      {
+        s0[ li ] = V;
+        s1[ li ] = x1;
+        if constexpr ( EXP )
+        {
+          s2[ li ] = x2;
+          s3[ li ] = i0;
+          s4[ li ] = i1;
+        }
+        b.r[ li ] = r;
+      }
+    }
+    if ( !pk_grid_sync( pk, gen ) )
+      break;
+    // ---- delivery of the slice's spikes (k_deliver's chunk loop)
+    const unsigned long long ent_end = ld_volatile( &d.ctl->n_ent );
+    const long long nent = ( long long ) ( ent_end - ent_start );
+    if ( nent > d.ent_cap )
+    {
+      if ( threadIdx.x == 0 )
+        atomicOr( &d.ctl->err, ERR_SPIKE_LIST );
+    }
+    else
+    {
+      const long long G = max( 1ll, min( ( long long ) d.deliver_group, ( nent + nwarps - 1 ) / nwarps ) );
+      for ( long long base = gw * G; base < nent; base += nwarps * G )
+      {
+        const int cnt = ( int ) min( G, nent - base );
+        const int4 my = lane < cnt ? __ldcg( d.ent + ( long long ) ( ( ent_start + base + lane ) % d.ent_cap ) )
+                                   : make_int4( 0, 0, 0, 0 );
+        ChunkLane< FIX > cur, nxt;
+        load_chunk< FIX >( d, shfl_int4( my, 0 ), lane, cur );
+        for ( int k = 0; k < cnt; ++k )
+        {
+          const int4 en = shfl_int4( my, min( k + 1, 31 ) );
+          if ( k + 1 < cnt )
+            load_chunk< FIX >( d, en, lane, nxt );
+          apply_chunk< FIX, false >( d, cur );
+          cur = nxt;
+        }
+      }
+    }
+    ent_start = ent_end;
+    if ( !pk_grid_sync( pk, gen ) )
+      break;
+  }
+  flush_drive_count( d, dcnt );
+  if ( threadIdx.x == 0 && ( ev_acc | spk_acc ) )
+  {
+    atomicAdd( &d.ctl->syn_events, ev_acc );
+    atomicAdd( &d.ctl->n_spikes, spk_acc );
+  }
+  if ( blockIdx.x == 0 && threadIdx.x == 0 )
+  {
+    d.ctl->n_ent = 0ull;
+    d.ctl->origin = origin0 + ( long long ) sl * md;
+    if ( ld_volatile( &pk->err ) )
+      atomicOr( &d.ctl->err, ERR_BARRIER );
+    __threadfence();
+  }
+}
+
 }  // namespace ng

@@ -284,7 +284,8 @@ UPDATE_VARIANTS = {0: "k_update_iaf (one thread per neuron, 4 lags of inputs at 
                    2: "k_update_iaf2 (two-phase, 32 neurons per 256-thread CTA)",
                    3: "k_update_iaf2 (two-phase, 32 neurons per 128-thread CTA)",
                    4: "k_update_aeif",
-                   5: "k_run_slices (persistent: node update and delivery of many slices in one cooperative launch)"}
+                   5: "k_run_slices (persistent: node update and delivery of many slices in one cooperative launch; "
+                      "k_run_slices_mg for networks larger than one resident wave)"}
 UPDATE_KERNELS = {0: "k_update_iaf", 1: "k_update_iaf", 2: "k_update_iaf2", 3: "k_update_iaf2", 4: "k_update_aeif",
                   5: "k_run_slices"}
 

@@ -181,3 +181,39 @@ def test_aeif_binning_changes_no_result(precision):
     a, b = run(0), run(1)
     assert len(a[0]) > 500
     _same(a, b)
+
+
+@pytest.mark.parametrize("precision,model", [
+    (_abi.NG_FP64, _abi.NG_IAF_PSC_EXP), (_abi.NG_FP32, _abi.NG_IAF_PSC_EXP),
+    (_abi.NG_FP64, _abi.NG_IAF_PSC_DELTA), (_abi.NG_FP64, _abi.NG_IAF_PSC_ALPHA),
+])
+def test_persistent_multi_group_equals_graph_form(precision, model):
+    """A network larger than one resident wave of the persistent kernel
+    (30,000 neurons: each CTA walks several 32-neuron groups per slice, their
+    state reloaded from memory) gives the graph form's raster, state and
+    event count bit for bit (dyadic weights: order-independent ring sums)."""
+    def run(variant):
+        n, md = 30000, 15
+        rng = np.random.default_rng(8)
+        deg = rng.integers(100, 300, n)
+        row = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+        nnz = int(row[-1])
+        tgt = rng.integers(0, n, nnz).astype(np.int32)
+        w = rng.choice([40.0, 20.5, -80.0, -161.25], nnz, p=[0.4, 0.4, 0.1, 0.1])
+        if model == _abi.NG_IAF_PSC_DELTA:
+            w = w / 128.0
+        d = rng.integers(md, 2 * md + 6, nnz).astype(np.int32)
+        eng = _abi.Engine([(model, n)], 0.1, md, 2 * md + 5, precision=precision)
+        eng.set_tuning(0, variant, -1, -1)
+        eng.set_var(0, "V_m_rel", rng.uniform(0.0, 14.0, n))
+        eng.set_connections(row, tgt, w, d)
+        eng.set_recording(np.ones(n, dtype=np.uint8))
+        drive_w = 0.3 if model == _abi.NG_IAF_PSC_DELTA else 40.0
+        eng.set_poisson(np.full(n, 9000.0), np.full(n, drive_w), np.full(n, md, dtype=np.int32), 0, 10**9, 11)
+        for k in (7, 23, 970, 1500):
+            eng.simulate(k)
+        return _finish(eng)
+    a, b = run(0), run(5)
+    assert len(a[0]) > 5000
+    assert b[4]["update_variant"] == 5
+    _same(a, b)
