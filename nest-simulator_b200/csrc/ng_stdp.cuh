@@ -285,8 +285,11 @@ k_stdp_flush( Net d, StdpNet p )
 // the slice in shared memory (lag, time, ring slot, and Kplus / t_last
 // before each spike) and advances the source's Kplus and t_last; each
 // thread then applies the spikes to its connections in time order.
+// (registers capped for four CTAs per SM: more resident warps hide the
+// dependent history loads better than spill-free code -- measured RTF 0.407
+// against 0.424 with 80 registers, 0.420 with 48 on the hpc_benchmark network)
 template < bool FIX >
-__global__ void __launch_bounds__( 256 )
+__global__ void __launch_bounds__( 256, 4 )
 k_stdp_deliver( Net d, StdpNet p )
 {
   __shared__ double s_t[ 32 ], s_Kp[ 32 ], s_tl[ 32 ];
@@ -332,10 +335,11 @@ k_stdp_deliver( Net d, StdpNet p )
     for ( int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x )
     {
       const int32_t tg = p.tgt[ e ];
-      const int32_t dl = p.dly[ e ];
+      const int32_t dl = p.dconst >= 0 ? p.dconst : p.dly[ e ];
       const double d_ms = ( double ) dl * h_ms;
       double w = p.w_run[ e ];
-      const int64_t hn = p.hist_n[ tg ], lo = p.hist_lo[ tg ];
+      const int64_t lo = p.hist_lo[ tg ];
+      const int64_t hn = p.dconst >= 0 ? lo : p.hist_n[ tg ];  // (the arrival tables hold the range end)
       const double* ht = p.hist_t + ( int64_t ) tg * STDP_HIST;
       for ( int j = 0; j < ns; ++j )
       {
