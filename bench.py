@@ -577,9 +577,13 @@ def measure_layered(args, dev, sim_ms=1000.0):
     drawn on the device): real-time factor in the FP64 and FP32 forms."""
     from nestgpu import workloads
 
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import spikestats as S
+
     spec = workloads.layered_spec()
     out = {"workload": "layered 8-population iaf_psc_exp network, 77,169 neurons, pairwise_bernoulli "
                        "p ~ U[0.01, 0.15], 1,000 ms", "neurons": sum(spec["sizes"])}
+    summaries = {}
     steps = int(round(sim_ms / 0.1))
     for form in ("fp64", "fp32", "fp32_ring32"):
         prec = form[:4]
@@ -597,6 +601,9 @@ def measure_layered(args, dev, sim_ms=1000.0):
         ks = kernel_split(eng, 200)
         out["synapses"] = eng.net_connection_count(nid)
         tuned = eng.tuned()
+        sp, stp = eng.net_spikes(nid)
+        summaries[form] = S.summary(sp.astype(np.int64), stp.astype(np.int64), out["neurons"], 0.1, 300.0,
+                                    300.0 + sim_ms, n_pairs=3000, seed=1)
         eng.close()
         ev = s1["syn_events"] - s0["syn_events"]
         out[form] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
@@ -604,6 +611,11 @@ def measure_layered(args, dev, sim_ms=1000.0):
                      "build_s": build, "kernels": ks, "clocks": clocks, "tuned": tuned,
                      "host_ms": {k: s1[k] - s0[k] for k in ("simulate_ms", "wait_ms", "drain_ms")}}
     out["fp32_ring32"]["ring_bound"] = workloads.layered_ring_bound(spec)
+    # the precision forms against FP64 on the same graph, state and drive
+    # (300-1,300 ms: rate, CV-ISI and correlation distributions)
+    for form in ("fp32", "fp32_ring32"):
+        c = S.compare(summaries[form], summaries["fp64"])
+        out[form]["accuracy_vs_fp64"] = {k: c[k] for k in ("rate_err", "cv_isi_err", "ks_cv", "ks_corr")}
     return out
 
 
@@ -612,15 +624,19 @@ def measure_aeif(args, dev, sim_ms=500.0):
     FP32 state (FP64 error control in both)."""
     from nestgpu import workloads
 
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import spikestats as S
+
     spec = workloads.aeif_spec()
     n = spec["n_exc"] + spec["n_inh"]
     out = {"workload": "50,000 aeif_cond_alpha neurons, fixed_indegree K=1,000, 10 kHz x 0.5 nS drive, 500 ms",
            "neurons": n}
+    summaries = {}
     steps = int(round(sim_ms / 0.1))
     for prec in ("fp64", "fp32"):
         t0 = time.perf_counter()
         eng = workloads.aeif_engine(spec, prec, device=dev.index)
-        workloads.aeif_add(eng, spec, 10 * steps)
+        nid = workloads.aeif_add(eng, spec, 10 * steps)
         build = time.perf_counter() - t0
         eng.simulate(2000)  # 200 ms warm-up (autotuner trials, graphs built)
         s0 = eng.stats()
@@ -628,12 +644,40 @@ def measure_aeif(args, dev, sim_ms=500.0):
         s1 = eng.stats()
         ks = kernel_split(eng, 150)
         tuned = eng.tuned()
+        sp, stp = eng.net_spikes(nid)
+        summaries[prec] = S.summary(sp.astype(np.int64), stp.astype(np.int64), n, 0.1, 200.0, 200.0 + sim_ms,
+                                    n_pairs=3000, seed=1)
         eng.close()
         ev = s1["syn_events"] - s0["syn_events"]
         out[prec] = {"rtf": ms / sim_ms, "ms": ms, "syn_events_per_s": ev / (ms * 1e-3), "syn_events": ev,
                      "mean_rate_hz": (s1["spikes"] - s0["spikes"]) / n / (sim_ms * 1e-3), "build_s": build,
                      "kernels": ks, "tuned": {k: tuned[k] for k in ("state", "deliver_ctas_per_sm",
                                                                   "deliver_chunks_per_warp")}}
+    c = S.compare(summaries["fp32"], summaries["fp64"])
+    out["fp32"]["accuracy_vs_fp64"] = {k: c[k] for k in ("rate_err", "cv_isi_err", "ks_cv", "ks_corr")}
+    # one realization's rate varies by up to 7 % across seeds in the FP64 form
+    # itself: the pooled error over three more realizations (500 ms each), as
+    # tests/test_gpu_statistics.py states it
+    spikes = {"fp64": 0, "fp32": 0}
+    cvs = {"fp64": [], "fp32": []}
+    ks = []
+    for seed in (77, 78, 79):
+        sm = {}
+        for prec in ("fp64", "fp32"):
+            sp_spec = dict(spec, seed=seed)
+            eng = workloads.aeif_engine(sp_spec, prec, device=dev.index)
+            nid = workloads.aeif_add(eng, sp_spec, 10 ** 6)
+            eng.simulate(5000)
+            sp, stp = eng.net_spikes(nid)
+            eng.close()
+            spikes[prec] += len(sp)
+            sm[prec] = S.summary(sp.astype(np.int64), stp.astype(np.int64), n, 0.1, 100.0, 500.0, n_pairs=3000,
+                                 seed=1)
+            cvs[prec].append(sm[prec]["cv_isi_mean"])
+        ks.append(S.compare(sm["fp32"], sm["fp64"])["ks_corr"])
+    out["fp32"]["accuracy_pooled_3_realizations"] = {
+        "rate_err": spikes["fp32"] / spikes["fp64"] - 1.0,
+        "cv_isi_err": float(np.mean(cvs["fp32"]) - np.mean(cvs["fp64"])), "ks_corr_max": float(max(ks))}
     return out
 
 
