@@ -1277,21 +1277,38 @@ k_update_iaf2( Net d, Block b, int from, int to, int sched )
 struct AeifPar
 {
   double V_peak, V_reset, g_L, C_m, E_ex, E_in, E_L, Delta_T, tau_w, a, b, V_th, tau_ex, tau_in, I_e;
+  // reciprocals of the divisors, set once per launch (aeif_reciprocals)
+  double inv_Delta_T, inv_C_m, inv_tau_w, inv_tau_ex, inv_tau_in;
 };
 
+__device__ __forceinline__ void
+aeif_reciprocals( AeifPar& p )
+{
+  p.inv_Delta_T = p.Delta_T == 0. ? 0. : 1.0 / p.Delta_T;
+  p.inv_C_m = 1.0 / p.C_m;
+  p.inv_tau_w = 1.0 / p.tau_w;
+  p.inv_tau_ex = 1.0 / p.tau_ex;
+  p.inv_tau_in = 1.0 / p.tau_in;
+}
+
+// The right-hand side of aeif_cond_alpha (aeif_cond_alpha.cpp:74-126), with
+// each division by a parameter taken as a multiplication by its reciprocal
+// (within an ulp per operation of the reference's quotients): seven FP64
+// divisions per evaluation, seven evaluations per RKF45 attempt, were most
+// of an attempt's instructions and two of them sat on the V chain.
 __device__ __forceinline__ void
 aeif_rhs( const AeifPar& p, bool refr, const double* y, double* f )
 {
   const double V = refr ? p.V_reset : fmin( y[ 0 ], p.V_peak );
   const double I_syn_exc = y[ 2 ] * ( V - p.E_ex );
   const double I_syn_inh = y[ 4 ] * ( V - p.E_in );
-  const double I_spike = p.Delta_T == 0. ? 0. : ( p.g_L * p.Delta_T * exp( ( V - p.V_th ) / p.Delta_T ) );
-  f[ 0 ] = refr ? 0. : ( -p.g_L * ( V - p.E_L ) + I_spike - I_syn_exc - I_syn_inh - y[ 5 ] + p.I_e ) / p.C_m;
-  f[ 1 ] = -y[ 1 ] / p.tau_ex;
-  f[ 2 ] = y[ 1 ] - y[ 2 ] / p.tau_ex;
-  f[ 3 ] = -y[ 3 ] / p.tau_in;
-  f[ 4 ] = y[ 3 ] - y[ 4 ] / p.tau_in;
-  f[ 5 ] = ( p.a * ( V - p.E_L ) - y[ 5 ] ) / p.tau_w;
+  const double I_spike = p.Delta_T == 0. ? 0. : ( p.g_L * p.Delta_T * exp( ( V - p.V_th ) * p.inv_Delta_T ) );
+  f[ 0 ] = refr ? 0. : ( -p.g_L * ( V - p.E_L ) + I_spike - I_syn_exc - I_syn_inh - y[ 5 ] + p.I_e ) * p.inv_C_m;
+  f[ 1 ] = -y[ 1 ] * p.inv_tau_ex;
+  f[ 2 ] = y[ 1 ] - y[ 2 ] * p.inv_tau_ex;
+  f[ 3 ] = -y[ 3 ] * p.inv_tau_in;
+  f[ 4 ] = y[ 3 ] - y[ 4 ] * p.inv_tau_in;
+  f[ 5 ] = ( p.a * ( V - p.E_L ) - y[ 5 ] ) * p.inv_tau_w;
 }
 
 // Fehlberg 4(5): advance with the fifth-order weights; error = 5th - 4th.
@@ -1467,6 +1484,7 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
     Vpk = ct[ 17 ];
     refr = ( int ) ct[ 18 ];
     p.I_e = ( double ) ( ( const Real* ) b.s[ 6 ] )[ li ];
+    aeif_reciprocals( p );
 #pragma unroll
     for ( int k = 0; k < 6; ++k )
       y[ k ] = ( double ) sy[ k ][ li ];
