@@ -1357,17 +1357,26 @@ __device__ __forceinline__ int
 control_yp( double tol, const double* err, const double* f, double& hs )
 {
   const double h_old = hs;
-  double rmax = 2.2250738585072014e-308;
+  // the largest |err_i| / D_i, found by cross-multiplied comparisons (the
+  // D_i are positive) with one division for the winner
+  double en = 0.0, ed = 1.0;
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
   {
-    const double D0 = tol * fabs( h_old * f[ i ] ) + tol;
-    const double r = fabs( err[ i ] ) / fabs( D0 );
-    rmax = r > rmax ? r : rmax;
+    const double D0 = fabs( tol * fabs( h_old * f[ i ] ) + tol );
+    const double e = fabs( err[ i ] );
+    if ( e * ed > en * D0 )
+    {
+      en = e;
+      ed = D0;
+    }
   }
+  double rmax = en / ed;
+  rmax = rmax > 2.2250738585072014e-308 ? rmax : 2.2250738585072014e-308;
   if ( rmax > 1.1 )
   {
-    double r = 0.9 / pow( rmax, 1.0 / 5.0 );
+    // (rmax^(1/5) as exp(log(rmax) / 5): rmax > 1.1 is finite and positive)
+    double r = 0.9 / exp( log( rmax ) * ( 1.0 / 5.0 ) );
     if ( r < 0.2 )
       r = 0.2;
     hs = r * h_old;
@@ -1375,7 +1384,8 @@ control_yp( double tol, const double* err, const double* f, double& hs )
   }
   if ( rmax < 0.5 )
   {
-    double r = 0.9 / pow( rmax, 1.0 / 6.0 );
+    // 0.9 / rmax^(1/6) >= 5 below (0.9 / 5)^6: the growth is capped there
+    double r = rmax <= 3.4012224e-05 ? 5.0 : 0.9 / exp( log( rmax ) * ( 1.0 / 6.0 ) );
     if ( r > 5.0 )
       r = 5.0;
     if ( r < 1.0 )
