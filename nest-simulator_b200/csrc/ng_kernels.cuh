@@ -1303,7 +1303,10 @@ aeif_rhs( const AeifPar& p, bool refr, const double* y, double* f )
   const double I_syn_exc = y[ 2 ] * ( V - p.E_ex );
   const double I_syn_inh = y[ 4 ] * ( V - p.E_in );
   const double I_spike = p.Delta_T == 0. ? 0. : ( p.g_L * p.Delta_T * exp( ( V - p.V_th ) * p.inv_Delta_T ) );
-  f[ 0 ] = refr ? 0. : ( -p.g_L * ( V - p.E_L ) + I_spike - I_syn_exc - I_syn_inh - y[ 5 ] + p.I_e ) * p.inv_C_m;
+  // the other currents are summed while the exponential is evaluated; the
+  // spike current joins last (one add and one multiply after the exp)
+  const double I_rest = -p.g_L * ( V - p.E_L ) - I_syn_exc - I_syn_inh - y[ 5 ] + p.I_e;
+  f[ 0 ] = refr ? 0. : ( I_rest + I_spike ) * p.inv_C_m;
   f[ 1 ] = -y[ 1 ] * p.inv_tau_ex;
   f[ 2 ] = y[ 1 ] - y[ 2 ] * p.inv_tau_ex;
   f[ 3 ] = -y[ 3 ] * p.inv_tau_in;
@@ -1315,39 +1318,47 @@ aeif_rhs( const AeifPar& p, bool refr, const double* y, double* f )
 __device__ __forceinline__ void
 rkf45( const AeifPar& p, bool refr, const double* y, const double* k1, double hs, double* yn, double* err, double* fout )
 {
+  // Each stage's weighted sum as a chain of fused multiply-adds with the
+  // newest slope last, so that only two dependent operations follow the
+  // previous stage's right-hand side.
   double k2[ 6 ], k3[ 6 ], k4[ 6 ], k5[ 6 ], k6[ 6 ], yt[ 6 ];
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
-    yt[ i ] = y[ i ] + ( 1.0 / 4.0 ) * hs * k1[ i ];
+    yt[ i ] = fma( hs, ( 1.0 / 4.0 ) * k1[ i ], y[ i ] );
   aeif_rhs( p, refr, yt, k2 );
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
-    yt[ i ] = y[ i ] + hs * ( ( 3.0 / 32.0 ) * k1[ i ] + ( 9.0 / 32.0 ) * k2[ i ] );
+    yt[ i ] = fma( hs, fma( 9.0 / 32.0, k2[ i ], ( 3.0 / 32.0 ) * k1[ i ] ), y[ i ] );
   aeif_rhs( p, refr, yt, k3 );
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
-    yt[ i ] = y[ i ] + hs * ( ( 1932.0 / 2197.0 ) * k1[ i ] + ( -7200.0 / 2197.0 ) * k2[ i ] + ( 7296.0 / 2197.0 ) * k3[ i ] );
+    yt[ i ] = fma( hs, fma( 7296.0 / 2197.0, k3[ i ], fma( -7200.0 / 2197.0, k2[ i ], ( 1932.0 / 2197.0 ) * k1[ i ] ) ),
+      y[ i ] );
   aeif_rhs( p, refr, yt, k4 );
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
-    yt[ i ] = y[ i ]
-      + hs * ( ( 439.0 / 216.0 ) * k1[ i ] + ( -8.0 ) * k2[ i ] + ( 3680.0 / 513.0 ) * k3[ i ] + ( -845.0 / 4104.0 ) * k4[ i ] );
+    yt[ i ] = fma( hs,
+      fma( -845.0 / 4104.0, k4[ i ], fma( 3680.0 / 513.0, k3[ i ], fma( -8.0, k2[ i ], ( 439.0 / 216.0 ) * k1[ i ] ) ) ),
+      y[ i ] );
   aeif_rhs( p, refr, yt, k5 );
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
-    yt[ i ] = y[ i ]
-      + hs * ( ( -8.0 / 27.0 ) * k1[ i ] + 2.0 * k2[ i ] + ( -3544.0 / 2565.0 ) * k3[ i ] + ( 1859.0 / 4104.0 ) * k4[ i ]
-        + ( -11.0 / 40.0 ) * k5[ i ] );
+    yt[ i ] = fma( hs,
+      fma( -11.0 / 40.0, k5[ i ],
+        fma( 1859.0 / 4104.0, k4[ i ], fma( -3544.0 / 2565.0, k3[ i ], fma( 2.0, k2[ i ], ( -8.0 / 27.0 ) * k1[ i ] ) ) ) ),
+      y[ i ] );
   aeif_rhs( p, refr, yt, k6 );
 #pragma unroll
   for ( int i = 0; i < 6; ++i )
   {
-    const double d5 = ( 16.0 / 135.0 ) * k1[ i ] + ( 6656.0 / 12825.0 ) * k3[ i ] + ( 28561.0 / 56430.0 ) * k4[ i ]
-      + ( -9.0 / 50.0 ) * k5[ i ] + ( 2.0 / 55.0 ) * k6[ i ];
-    yn[ i ] = y[ i ] + hs * d5;
+    const double d5 = fma( 2.0 / 55.0, k6[ i ],
+      fma( -9.0 / 50.0, k5[ i ],
+        fma( 28561.0 / 56430.0, k4[ i ], fma( 6656.0 / 12825.0, k3[ i ], ( 16.0 / 135.0 ) * k1[ i ] ) ) ) );
+    yn[ i ] = fma( hs, d5, y[ i ] );
     err[ i ] = hs
-      * ( ( 1.0 / 360.0 ) * k1[ i ] + ( -128.0 / 4275.0 ) * k3[ i ] + ( -2197.0 / 75240.0 ) * k4[ i ]
-        + ( 1.0 / 50.0 ) * k5[ i ] + ( 2.0 / 55.0 ) * k6[ i ] );
+      * fma( 2.0 / 55.0, k6[ i ],
+        fma( 1.0 / 50.0, k5[ i ],
+          fma( -2197.0 / 75240.0, k4[ i ], fma( -128.0 / 4275.0, k3[ i ], ( 1.0 / 360.0 ) * k1[ i ] ) ) ) );
   }
   aeif_rhs( p, refr, yn, fout );
 }
