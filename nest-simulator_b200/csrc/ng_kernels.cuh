@@ -1535,14 +1535,20 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
     {
       double tt = 0.0;
       int guard = 0;
+      // k1 = f(y) at the start of a sub-step: the previous accepted
+      // attempt's f(y_new) when y was not reset after it (the same function
+      // of the same values), else evaluated
+      double k1[ 6 ];
+      bool k1_ok = false;
       while ( tt < h )
       {
         // one accepted sub-step (evolve_apply), retried on rejection
         const double t0 = tt;
         const double dt = h - t0;
         double h0 = hs;
-        double k1[ 6 ], yn[ 6 ], err[ 6 ], fo[ 6 ];
-        aeif_rhs( p, r > 0, y, k1 );
+        double yn[ 6 ], err[ 6 ], fo[ 6 ];
+        if ( !k1_ok )
+          aeif_rhs( p, r > 0, y, k1 );
         for ( ;; )
         {
           bool final_step = false;
@@ -1573,6 +1579,7 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
           unstable = true;
           break;
         }
+        k1_ok = false;
         if ( r > 0 )
         {
           y[ 0 ] = p.V_reset;
@@ -1583,6 +1590,13 @@ k_update_aeif( Net d, Block b, int from, int to, int sched, double h )
           y[ 5 ] += p.b;
           r = refr > 0 ? refr + 1 : 0;
           ++mult;
+        }
+        else
+        {
+#pragma unroll
+          for ( int k = 0; k < 6; ++k )
+            k1[ k ] = fo[ k ];
+          k1_ok = true;
         }
       }
       if ( r > 0 )
