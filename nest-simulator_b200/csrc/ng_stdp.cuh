@@ -134,12 +134,18 @@ k_stdp_archive( Net d, StdpNet p )
   }
 }
 
-// w^mu of the facilitation, through exp and log (w > 0; the power law's
-// value at 0 otherwise)
+// One facilitation term lambda w^mu Kplus exp(minus_dt / tau_plus) of
+// stdp_pl_synapse_hom::facilitate_: for w > 0 as lambda Kplus
+// exp(mu log w + minus_dt / tau_plus) -- one exponential for the power and
+// the trace's decay (within a few ulp of the reference's pow and exp); the
+// power law's value at w = 0 otherwise
 __device__ __forceinline__ double
-stdp_pow( double w, double mu )
+stdp_facilitation( const StdpNet& p, double w, double Kplus, double minus_dt )
 {
-  return w > 0.0 ? exp( mu * log( w ) ) : pow( w, mu );
+  const double a = minus_dt * p.tau_plus_inv;
+  if ( w > 0.0 )
+    return p.lambda * Kplus * exp( p.mu * log( w ) + a );
+  return p.lambda * pow( w, p.mu ) * ( Kplus * exp( a ) );
 }
 
 // end of the facilitation range of an arrival at t = t_spike - d: the live
@@ -192,8 +198,7 @@ stdp_pl_apply( const StdpNet& p, const double* ht, int64_t lo, int64_t fin, doub
   for ( int64_t k = st; k < fin; ++k )
   {
     const double minus_dt = tlast - ( ht[ k & ( STDP_HIST - 1 ) ] + d_ms );
-    const double kplus = Kplus * exp( minus_dt * p.tau_plus_inv );
-    w = w + ( p.lambda * stdp_pow( w, p.mu ) * kplus );
+    w = w + stdp_facilitation( p, w, Kplus, minus_dt );
   }
   const double new_w = w - ( p.lambda * p.alpha * w * kminus );
   return new_w > 0.0 ? new_w : 0.0;
@@ -258,8 +263,7 @@ k_stdp_flush( Net d, StdpNet p )
         const double te = ht[ k % STDP_HIST ];
         if ( te >= t1_lim )
         {
-          const double kplus = Kp * exp( ( tl - ( te + d_ms ) ) * p.tau_plus_inv );
-          w = w + ( p.lambda * stdp_pow( w, p.mu ) * kplus );
+          w = w + stdp_facilitation( p, w, Kp, tl - ( te + d_ms ) );
           changed = true;
         }
       }
