@@ -110,7 +110,7 @@ def new_engine(precision="fp32", capacity_neurons=2_000_000, capacity_edges=1_20
     return eng
 
 
-def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtime=True):
+def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtime=True, tune_slices=0):
     """Continuous batching.  Returns (requests, stats).
 
     Every live network advances in chunks of `chunk_slices` min_delay slices;
@@ -123,7 +123,14 @@ def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtim
     The chunks are enqueued with ng_simulate_async: the host reads the spikes
     of the networks that ended by the start of the running chunk while the
     device runs it, so a network is retired one chunk after its end (or at
-    once when no live network is left to advance)."""
+    once when no live network is left to advance).
+
+    With `tune_slices` > 0 and the engine's autotuner not measured yet, the
+    first chunk is `tune_slices` long: the tuner needs one call with room for
+    its trial groups (which run the live networks' own slices), and chunks of
+    `chunk_slices` are too short for it (on the serving sweep the tuned and
+    the default launch configurations measured the same, so it is off by
+    default)."""
     pending = sorted(requests, key=lambda r: r.arrival)
     waiting = []
     active = {}                       # network id -> (request, engine step at which it ends)
@@ -165,7 +172,10 @@ def run_batched(requests, eng, chunk_slices=32, clock=time.perf_counter, realtim
             eng.sync()
             ended = now_steps
         else:
-            slices = max(1, min(chunk_slices, -(-left // DELAY_STEPS)))
+            want = chunk_slices
+            if tune_slices and eng.tuned()["state"] == "pending":
+                want = max(chunk_slices, tune_slices)
+            slices = max(1, min(want, -(-left // DELAY_STEPS)))
             ended = now_steps
             eng.simulate_async(slices * DELAY_STEPS)
             now_steps += slices * DELAY_STEPS

@@ -22,6 +22,8 @@ class _StandInEngine:
         self.events = 0
         self.reads = {}
         self.log = []
+        self.tune_state = "cached"       # "pending": the autotuner waits for a long enough call
+        self.calls = []                  # steps of each simulate_async call
 
     # -- the subset of _abi.Engine the loop uses
     def stats(self):
@@ -39,8 +41,14 @@ class _StandInEngine:
         self.log.append(("add", nid, self.clock))
         return nid
 
+    def tuned(self):
+        return {"state": self.tune_state}
+
     def simulate_async(self, k):
         assert k > 0 and k % serving.DELAY_STEPS == 0
+        self.calls.append(k)
+        if self.tune_state == "pending" and k >= 112 * serving.DELAY_STEPS:
+            self.tune_state = "tuned"   # the call had room for the trial groups
         self.drained = self.clock      # the previous call's last group is drained now
         for nw in self.nets.values():
             live = max(0, min(nw["until"], self.clock + k) - max(nw["step0"], self.clock))
@@ -86,4 +94,19 @@ def test_batched_loop_single_slot():
     done, st = serving.run_batched([copy.copy(r) for r in reqs], eng, realtime=False)
     kinds = [e[0] for e in eng.log]
     assert kinds == ["add", "remove"] * 5
+    assert st["syn_events"] == sum(r.n * r.steps for r in reqs)
+
+
+def test_first_chunk_long_enough_for_the_autotuner():
+    """While the engine's autotuner waits for a long enough call, the loop's
+    first chunk is tune_slices long; after it the chunks are chunk_slices;
+    durations and events stay exact."""
+    reqs = serving.make_requests(count=20, rate_hz=0.0, seed=3)
+    eng = _StandInEngine(capacity_neurons=150_000, max_networks=8)
+    eng.tune_state = "pending"
+    done, st = serving.run_batched([copy.copy(r) for r in reqs], eng, realtime=False, chunk_slices=32,
+                                   tune_slices=112)
+    assert eng.calls[0] == 112 * serving.DELAY_STEPS
+    assert eng.tune_state == "tuned"
+    assert max(eng.calls[1:]) <= 32 * serving.DELAY_STEPS
     assert st["syn_events"] == sum(r.n * r.steps for r in reqs)
