@@ -224,25 +224,28 @@ poisson_table( double lambda )
 // CDF table of Poisson(lambda): cdf[k] = P(X <= k), summed upward in FP64,
 // up to 1 - cdf < 1e-17 or 256 entries; the last entry is set to 1 so the
 // search always ends.  Returns false when the table would be too long.
+// Stored as thresholds floor(cdf[k] * 2^53): a uniform u = m * 2^-53 (m a
+// 53-bit integer) exceeds cdf[k] exactly when m exceeds the threshold.
 bool
-poisson_cdf_table( double lambda, std::vector< double >& cdf )
+poisson_cdf_table( double lambda, std::vector< uint64_t >& cdf )
 {
   cdf.clear();
   if ( lambda > 100.0 )
     return false;
+  const auto thr = []( double F ) { return ( uint64_t ) std::floor( F * 9007199254740992.0 ); };
   double p = std::exp( -lambda ), F = p;
-  cdf.push_back( F );
+  cdf.push_back( thr( F ) );
   for ( int k = 1; k < 256; ++k )
   {
     p = p * lambda / ( double ) k;
     F += p;
-    cdf.push_back( F );
+    cdf.push_back( thr( F ) );
     if ( 1.0 - F < 1e-17 && ( double ) k > lambda )
       break;
   }
   if ( 1.0 - F > 1e-15 )
     return false;
-  cdf.back() = 1.0;
+  cdf.back() = thr( 1.0 );
   return true;
 }
 
@@ -313,6 +316,11 @@ struct ng_engine
   cudaStream_t copy_stream = nullptr;
   uint2* pinned_log = nullptr;
   size_t pinned_log_bytes = 0;
+  // pinned staging of an admission's per-neuron uploads (ng_net_add): kept
+  // across calls, so an admission neither pins nor first-touches fresh host
+  // memory; reused only after the admission stream has drained
+  char* adm_pin = nullptr;
+  size_t adm_pin_bytes = 0;
   ng_stats stats {};
   int profiling = 0;
   int graph_slices = 0;
@@ -454,7 +462,7 @@ struct ng_engine
   std::vector< GatherNet > host_g;
   std::unordered_map< std::string, int32_t > cls_ids;     // engine-wide coefficient classes
   int64_t cls_cap = 0, cdf_cap = 0;
-  std::vector< double > cdf_host;
+  std::vector< uint64_t > cdf_host;
   std::unordered_map< double, int2 > cdf_tables;
   int fx_S = 0;
 
@@ -770,6 +778,8 @@ struct ng_engine
       cudaFreeHost( host_ctl );
     if ( pinned_log )
       cudaFreeHost( pinned_log );
+    if ( adm_pin )
+      cudaFreeHost( adm_pin );
     for ( auto& nw : nets )
       free_blocks( nw.blocks );
     if ( host_off )
@@ -1010,7 +1020,7 @@ struct ng_engine
     d.pois_w = ( const double* ) pois_w.p;
     d.pois_d = ( const int32_t* ) pois_d.p;
     d.pois_cdf_ref = ( const int2* ) pois_ref.p;
-    d.pois_cdf = ( const double* ) pois_cdf.p;
+    d.pois_cdf = ( const uint64_t* ) pois_cdf.p;
     d.pois_start = pois_start;
     d.pois_stop = pois_stop;
     d.key0 = key0;
@@ -1708,6 +1718,22 @@ struct ng_engine
     if ( cudaMallocHost( &pinned_log, bytes ) != cudaSuccess )
       return fail( NG_ERR_MEMORY, "cannot allocate pinned host memory for the spike log" );
     pinned_log_bytes = bytes;
+    return NG_OK;
+  }
+
+  int
+  grow_adm_pin( size_t bytes )
+  {
+    if ( bytes <= adm_pin_bytes )
+      return NG_OK;
+    const size_t want = std::max( { bytes, 2 * adm_pin_bytes, ( size_t ) 4 << 20 } );
+    if ( adm_pin )
+      cudaFreeHost( adm_pin );
+    adm_pin = nullptr;
+    adm_pin_bytes = 0;
+    if ( cudaMallocHost( &adm_pin, want ) != cudaSuccess )
+      return fail( NG_ERR_MEMORY, "cannot allocate pinned host memory for admissions" );
+    adm_pin_bytes = want;
     return NG_OK;
   }
 
@@ -2956,7 +2982,7 @@ ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const
   const int64_t n = e->N;
   std::vector< double4 > tab( ( size_t ) n );
   std::vector< int2 > ref( ( size_t ) n, make_int2( 0, 0 ) );
-  std::vector< double > cdf;
+  std::vector< uint64_t > cdf;
   std::unordered_map< double, int2 > tables;  // one CDF table per distinct lambda
   bool any = false;
   for ( int64_t i = 0; i < n; ++i )
@@ -2973,7 +2999,7 @@ ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const
     if ( it == tables.end() )
     {
       int2 r2 = make_int2( ( int ) cdf.size(), -1 );
-      std::vector< double > t2;
+      std::vector< uint64_t > t2;
       if ( poisson_cdf_table( lam, t2 ) )
       {
         r2.y = ( int ) t2.size();
@@ -2984,13 +3010,13 @@ ng_set_poisson( ng_engine* e, const double* rate_hz, const double* weight, const
     ref[ i ] = it->second;
   }
   if ( cdf.empty() )
-    cdf.push_back( 1.0 );
+    cdf.push_back( 1ull << 53 );
   int rc;
   if ( ( rc = e->upload( e->pois, tab.data(), tab.size() * sizeof( double4 ) ) ) )
     return rc;
   if ( ( rc = e->upload( e->pois_ref, ref.data(), ref.size() * sizeof( int2 ) ) ) )
     return rc;
-  if ( ( rc = e->upload( e->pois_cdf, cdf.data(), cdf.size() * sizeof( double ) ) ) )
+  if ( ( rc = e->upload( e->pois_cdf, cdf.data(), cdf.size() * sizeof( uint64_t ) ) ) )
     return rc;
   if ( ( rc = e->upload( e->pois_w, weight, ( size_t ) n * sizeof( double ) ) ) )
     return rc;
@@ -3466,6 +3492,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   int64_t g0 = -1, gn = 0;  // gather table run, if any
   int64_t sg0 = -1, sgn = 0;  // segment table run, if any
   auto undo = [ & ]( int code ) {
+    cudaStreamSynchronize( e->adm_stream );  // its copies read the pinned staging
     ng_engine::give_run( e->free_neurons, n0, n );
     ng_engine::give_run( e->free_edges, e0, ne_need );
     if ( g0 >= 0 )
@@ -3493,32 +3520,46 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     else if ( vs->kind == STATE )
       state_src[ vs->slot ] = desc->var_values[ v ];
   }
-  // host sources of the uploads live until the function returns (after its
-  // last stream synchronisation), so no copy waits for the device here: an
-  // admission's host work overlaps slices still running on the device
-  std::vector< std::vector< char > > st_tmp( ( size_t ) n_states( model ) );
-  std::vector< double > hs;
+  // the per-neuron uploads (state, RKF45 step, drive tables) are staged in
+  // the engine's pinned buffer, which stays untouched until the function
+  // returns (after its last synchronisation of the admission stream), so no
+  // copy waits for the device here: an admission's host work overlaps slices
+  // still running on the device
+  const size_t n_st = ( size_t ) n_states( model );
+  const auto al16 = []( size_t x ) { return ( x + 15 ) & ~( size_t ) 15; };
+  const size_t st_bytes = al16( ( size_t ) n * e->rsz );
+  const size_t hs_bytes = model == NG_AEIF_COND_ALPHA ? al16( ( size_t ) n * 8 ) : 0;
+  const size_t drv_bytes = al16( ( size_t ) n * sizeof( double4 ) ) + al16( ( size_t ) n * 8 )
+    + al16( ( size_t ) n * 8 ) + al16( ( size_t ) n * 4 );
   {
-    for ( int sl = 0; sl < n_states( model ); ++sl )
+    const int rcp = e->grow_adm_pin( n_st * st_bytes + hs_bytes + drv_bytes );
+    if ( rcp )
+      return undo( rcp );
+  }
+  char* stage = e->adm_pin;
+  {
+    for ( size_t sl = 0; sl < n_st; ++sl )
     {
-      std::vector< char >& tmp = st_tmp[ ( size_t ) sl ];
-      tmp.resize( ( size_t ) n * e->rsz );
+      char* tmp = stage;
+      stage += st_bytes;
       for ( int64_t i = 0; i < n; ++i )
       {
-        const double v = state_src[ sl ] ? state_src[ sl ][ i ] : default_state( model, sl );
+        const double v = state_src[ sl ] ? state_src[ sl ][ i ] : default_state( model, ( int ) sl );
         if ( e->rsz == 8 )
-          reinterpret_cast< double* >( tmp.data() )[ i ] = v;
+          reinterpret_cast< double* >( tmp )[ i ] = v;
         else
-          reinterpret_cast< float* >( tmp.data() )[ i ] = ( float ) v;
+          reinterpret_cast< float* >( tmp )[ i ] = ( float ) v;
       }
-      CU( cudaMemcpyAsync( ( char* ) b.st[ sl ].p + n0 * e->rsz, tmp.data(), tmp.size(), cudaMemcpyHostToDevice,
+      CU( cudaMemcpyAsync( ( char* ) b.st[ sl ].p + n0 * e->rsz, tmp, ( size_t ) n * e->rsz, cudaMemcpyHostToDevice,
         e->stream ) );
     }
     CU( cudaMemsetAsync( ( int32_t* ) b.r.p + n0, 0, ( size_t ) n * 4, e->stream ) );
     if ( model == NG_AEIF_COND_ALPHA )
     {
-      hs.assign( ( size_t ) n, e->h );
-      CU( cudaMemcpyAsync( ( double* ) b.istep.p + n0, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice, e->stream ) );
+      double* hs = reinterpret_cast< double* >( stage );
+      stage += hs_bytes;
+      std::fill( hs, hs + n, e->h );
+      CU( cudaMemcpyAsync( ( double* ) b.istep.p + n0, hs, ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
     }
   }
   // coefficient classes, shared by all networks
@@ -3846,10 +3887,16 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     ng_engine::give_run( e->free_edges, e0 + ne_used, ne_need - ne_used );
   // drive: Poisson tables and CDF references of the region
   {
-    std::vector< double4 > tab( ( size_t ) n );
-    std::vector< int2 > ref( ( size_t ) n, make_int2( 0, 0 ) );
-    std::vector< double > pw( ( size_t ) n, 0.0 );
-    std::vector< int32_t > pd( ( size_t ) n, e->cfg.min_delay );
+    double4* tab = reinterpret_cast< double4* >( stage );
+    stage += al16( ( size_t ) n * sizeof( double4 ) );
+    int2* ref = reinterpret_cast< int2* >( stage );
+    stage += al16( ( size_t ) n * 8 );
+    double* pw = reinterpret_cast< double* >( stage );
+    stage += al16( ( size_t ) n * 8 );
+    int32_t* pd = reinterpret_cast< int32_t* >( stage );
+    std::fill( ref, ref + n, make_int2( 0, 0 ) );
+    std::fill( pw, pw + n, 0.0 );
+    std::fill( pd, pd + n, e->cfg.min_delay );
     const int64_t cdf_old = ( int64_t ) e->cdf_host.size();
     for ( int64_t i = 0; i < n; ++i )
     {
@@ -3877,7 +3924,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
       if ( it == e->cdf_tables.end() )
       {
         int2 r2 = make_int2( ( int ) e->cdf_host.size(), -1 );
-        std::vector< double > t2;
+        std::vector< uint64_t > t2;
         if ( poisson_cdf_table( lam, t2 ) )
         {
           if ( ( int64_t ) ( e->cdf_host.size() + t2.size() ) > e->cdf_cap )
@@ -3891,13 +3938,13 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     }
     const int64_t cdf_new = ( int64_t ) e->cdf_host.size();
     if ( cdf_new > cdf_old )
-      CU( cudaMemcpyAsync( ( double* ) e->pois_cdf.p + cdf_old, e->cdf_host.data() + cdf_old,
+      CU( cudaMemcpyAsync( ( uint64_t* ) e->pois_cdf.p + cdf_old, e->cdf_host.data() + cdf_old,
         ( size_t ) ( cdf_new - cdf_old ) * 8, cudaMemcpyHostToDevice, e->stream ) );
-    CU( cudaMemcpyAsync( ( double4* ) e->pois.p + n0, tab.data(), ( size_t ) n * sizeof( double4 ), cudaMemcpyHostToDevice,
+    CU( cudaMemcpyAsync( ( double4* ) e->pois.p + n0, tab, ( size_t ) n * sizeof( double4 ), cudaMemcpyHostToDevice,
       e->stream ) );
-    CU( cudaMemcpyAsync( ( int2* ) e->pois_ref.p + n0, ref.data(), ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
-    CU( cudaMemcpyAsync( ( double* ) e->pois_w.p + n0, pw.data(), ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
-    CU( cudaMemcpyAsync( ( int32_t* ) e->pois_d.p + n0, pd.data(), ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int2* ) e->pois_ref.p + n0, ref, ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( double* ) e->pois_w.p + n0, pw, ( size_t ) n * 8, cudaMemcpyHostToDevice, e->stream ) );
+    CU( cudaMemcpyAsync( ( int32_t* ) e->pois_d.p + n0, pd, ( size_t ) n * 4, cudaMemcpyHostToDevice, e->stream ) );
     CU( cudaStreamSynchronize( e->stream ) );
   }
   // activation, in the engine's stream order behind the prepared region and

@@ -127,7 +127,7 @@ struct Net
   const uint8_t* rec;
   const double4* pois;  // lambda, p_m, F_m, m (walk from the mode, long tables)
   const int2* pois_cdf_ref;  // per neuron: (offset, length) into pois_cdf; length 0 = no drive, -1 = walk
-  const double* pois_cdf;    // concatenated CDF tables, one per distinct rate
+  const uint64_t* pois_cdf;  // concatenated CDF tables, one per distinct rate, as 53-bit thresholds
   const double* pois_w;
   const int32_t* pois_d;
   int64_t pois_start, pois_stop;
@@ -201,6 +201,24 @@ __host__ __device__ inline double
 u53( uint32_t a, uint32_t b )
 {
   return ( ( double ) ( a >> 5 ) * 67108864.0 + ( double ) ( b >> 6 ) ) * ( 1.0 / 9007199254740992.0 );
+}
+
+// The 53-bit integer m of u53(a, b) = m * 2^-53.  For a CDF value F in
+// [0, 1], u > F holds exactly when m > floor(F * 2^53) (F * 2^53 is exact),
+// so the inversion compares integers: no int->double conversion and no FP64
+// compare per draw.
+__host__ __device__ inline uint64_t
+u53_bits( uint32_t a, uint32_t b )
+{
+  return ( ( uint64_t ) ( a >> 5 ) << 26 ) | ( uint64_t ) ( b >> 6 );
+}
+
+// (double) x, exactly, without a conversion instruction: 2^52 + x has x in
+// the low mantissa bits.
+__device__ __forceinline__ double
+u32_to_f64( uint32_t x )
+{
+  return __hiloint2double( 0x43300000, ( int ) x ) - 4503599627370496.0;
 }
 
 // tab = (lambda, p_m, F_m, m): walk from the mode m up while u > F or down

@@ -466,8 +466,8 @@ cta_origin( const Net& d )
 // would otherwise force every one of them to be re-read at every lag.
 struct DriveCtx
 {
-  const double* cdf;
-  double c[ 4 ];      // the first table entries (1.0 past the table's end)
+  const uint64_t* cdf;
+  uint64_t c[ 4 ];    // the first table thresholds (2^53 past the table's end: never exceeded)
   double w;
   long long t_off;    // global step -> network-local step
   int n;              // table length; 0: no drive; -1: walk from the mode
@@ -515,7 +515,7 @@ drive_ctx( const Net& d, int64_t i, DriveCtx& c )
   c.cdf = d.pois_cdf + tb.x;
 #pragma unroll
   for ( int q = 0; q < 4; ++q )
-    c.c[ q ] = q < tb.y ? __ldg( c.cdf + q ) : 1.0;
+    c.c[ q ] = q < tb.y ? __ldg( c.cdf + q ) : ( 1ull << 53 );
 }
 
 // One Philox4x32-10 block serves two generator steps: counter (neuron,
@@ -537,28 +537,32 @@ drive_at( const Net& d, DriveCtx& c, int64_t i, long long t, long long& cnt )
       c.o );
     c.pair = tp;
   }
-  const double u = ( tg & 1 ) ? u53( c.o[ 2 ], c.o[ 3 ] ) : u53( c.o[ 0 ], c.o[ 1 ] );
+  const uint32_t ua = ( tg & 1 ) ? c.o[ 2 ] : c.o[ 0 ];
+  const uint32_t ub = ( tg & 1 ) ? c.o[ 3 ] : c.o[ 1 ];
   long long k;
   if ( c.n > 0 )
   {
-    // j = first index with u <= cdf[j] (or the last one)
+    // j = first index with u <= cdf[j] (or the last one), compared as the
+    // 53-bit integers of u and of the thresholds (u53_bits)
+    const uint64_t m = u53_bits( ua, ub );
     int j = 0;
 #pragma unroll
     for ( int q = 0; q < 4; ++q )
-      if ( j == q && q < c.n - 1 && u > c.c[ q ] )
+      if ( j == q && q < c.n - 1 && m > c.c[ q ] )
         j = q + 1;
-    while ( j >= 4 && j < c.n - 1 && u > __ldg( c.cdf + j ) )
+    while ( j >= 4 && j < c.n - 1 && m > __ldg( c.cdf + j ) )
       ++j;
     k = j;
   }
   else
   {
-    k = poisson_from_mode( d.pois[ i ], u );
+    k = poisson_from_mode( d.pois[ i ], u53( ua, ub ) );
   }
   cnt += k;
   if ( k <= 0 )
     return Real( 0 );
-  return ( Real ) ( c.w * ( double ) k );
+  // k < 2^32: a table index or a count walked from the mode
+  return ( Real ) ( c.w * u32_to_f64( ( uint32_t ) k ) );
 }
 
 // Ring cell of (slot, channel, neuron): read it, then, separately and only
@@ -762,8 +766,13 @@ alpha_step( const AlphaCoef< Real >& c, Real& V, Real& Iex, Real& Iin, Real& dIe
 //               state: s0 = V_m - E_L, s1 = i_syn_ex, s2 = i_syn_in,
 //                      s3 = i_0, s4 = i_1, s5 = I_e
 // ---------------------------------------------------------------------
+// Launched with CTAs of 128 threads.  The FP32 form (fixed-point rings)
+// caps its registers for five resident CTAs per SM (96 registers, a few
+// spills outside the lag loop): on the serving workload, whose many small
+// networks fill several waves, the extra resident warps hide more of the
+// ring-load and drive latency (update time -6 %).
 template < typename Real, bool FIX, int MODEL, int SUB >
-__global__ void __launch_bounds__( 256 )
+__global__ void __launch_bounds__( 128, FIX ? 5 : 1 )
 k_update_iaf( Net d, Block b, int from, int to, int sched )
 {
   const long long origin = cta_origin( d );

@@ -492,14 +492,31 @@ class Engine:
         return out[:n.value]
 
     # ---- serving
+    def _per_neuron(self, slot, value, n, dtype):
+        """`value` as a contiguous array of n entries.  A scalar is written
+        into a buffer kept per slot and reused by later admissions (the
+        library copies the values before ng_net_add returns): a server
+        admitting networks back to back then allocates, and first-touches,
+        no host memory per admission."""
+        v = np.asarray(value, dtype=dtype)
+        if v.ndim > 0:
+            return np.ascontiguousarray(np.broadcast_to(v, (n,)))
+        bufs = self.__dict__.setdefault("_fill", {})
+        buf = bufs.get(slot)
+        if buf is None or buf.dtype != v.dtype or len(buf) < n:
+            buf = np.empty(max(n, 2 * (0 if buf is None else len(buf))), dtype=dtype)
+            bufs[slot] = buf
+        out = buf[:n]
+        out.fill(v)
+        return out
+
     def net_add(self, n, steps, seed, var_values, build=None, edges=None, poisson=None, record=True):
         """Admit a network; returns its id, or None if it does not fit now.
 
         build: a dict of NGFixedIndegree fields, or an NGPairwiseBernoulli;
         edges: (source, target, weight, delay_steps) in network-local ids."""
         names = list(var_values)
-        arrays = [np.ascontiguousarray(np.broadcast_to(np.asarray(var_values[k], dtype=np.float64), (n,)))
-                  for k in names]
+        arrays = [self._per_neuron(("var", j), var_values[k], n, np.float64) for j, k in enumerate(names)]
         cnames = (ctypes.c_char_p * max(1, len(names)))(*[k.encode() for k in names])
         cvals = (ctypes.c_void_p * max(1, len(arrays)))(*[a.ctypes.data for a in arrays])
         desc = NGNetDesc(n=int(n), steps=int(steps), seed=int(seed) & (2**64 - 1), record=1 if record else 0,
@@ -521,9 +538,9 @@ class Engine:
             desc.source, desc.target, desc.weight, desc.delay_steps = (src.ctypes.data, tgt.ctypes.data, w.ctypes.data,
                                                                       d.ctypes.data)
         if poisson is not None:
-            r = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson[0], dtype=np.float64), (n,)))
-            pw = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson[1], dtype=np.float64), (n,)))
-            pd = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson[2], dtype=np.int32), (n,)))
+            r = self._per_neuron("rate", poisson[0], n, np.float64)
+            pw = self._per_neuron("weight", poisson[1], n, np.float64)
+            pd = self._per_neuron("delay", poisson[2], n, np.int32)
             keep += [r, pw, pd]
             desc.poisson_rate, desc.poisson_weight, desc.poisson_delay = r.ctypes.data, pw.ctypes.data, pd.ctypes.data
         nid = ctypes.c_int32(-1)

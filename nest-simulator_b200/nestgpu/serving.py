@@ -87,7 +87,8 @@ def make_requests(count=256, rate_hz=20.0, seed=2026, n_min=1000, n_max=50000, t
 
 def _admit(eng, r, record=True):
     rng = np.random.default_rng(r.seed)
-    V0 = rng.normal(-58.0, 10.0, r.n) + 70.0   # V_m relative to E_L = -70 mV
+    V0 = rng.normal(-58.0, 10.0, r.n)
+    V0 += 70.0                                   # V_m relative to E_L = -70 mV
     build = dict(n_exc=r.n_exc, k_exc=r.k_exc, k_inh=r.k_inh, w_exc=J_EXC, w_inh=-r.g * J_EXC,
                  delay_steps=DELAY_STEPS, allow_autapses=0, seed=r.seed ^ 0x5A5A5A5A)
     rate = r.eta * NU_TH_HZ
