@@ -470,56 +470,62 @@ k_gather( Net d )
     {
       const uint4* col = reinterpret_cast< const uint4* >( d.gin + g.base ) + ( ( tl >> 5 ) * nb ) * 32 + ( tl & 31 );
       const int b0 = nb * part / GP, b1 = nb * ( part + 1 ) / GP;
-      for ( int jb = b0; jb < b1; jb += 2 )
-      {
-        uint4 v[ 2 ];
-        v[ 0 ] = __ldg( col + ( int64_t ) jb * 32 );
-        v[ 1 ] = jb + 1 < b1 ? __ldg( col + ( int64_t ) ( jb + 1 ) * 32 ) : make_uint4( 0, 0, 0, 0 );
+      // one 16-byte word (8 draws) into the planes
+      auto eat = [ & ]( const uint4 q, const int jw ) {
+        const uint32_t wv[ 4 ] = { q.x, q.y, q.z, q.w };
+        uint32_t x[ 8 ];
 #pragma unroll
-        for ( int h = 0; h < 2; ++h )
+        for ( int r = 0; r < 8; ++r )
+          x[ r ] = s_mask[ ( wv[ r >> 1 ] >> ( ( r & 1 ) * 16 ) ) & 0xffffu ];
+        // inhibitory draws count in the upper half (uniform across the warp)
+        const int j0 = jw * 8;
+        if ( j0 >= g.ke )
         {
-          if ( jb + h >= b1 )
-            break;
-          const uint32_t wv[ 4 ] = { v[ h ].x, v[ h ].y, v[ h ].z, v[ h ].w };
-          uint32_t x[ 8 ];
 #pragma unroll
           for ( int r = 0; r < 8; ++r )
-            x[ r ] = s_mask[ ( wv[ r >> 1 ] >> ( ( r & 1 ) * 16 ) ) & 0xffffu ];
-          // inhibitory draws count in the upper half (uniform across the warp)
-          const int j0 = ( jb + h ) * 8;
-          if ( j0 >= g.ke )
-          {
-#pragma unroll
-            for ( int r = 0; r < 8; ++r )
-              x[ r ] <<= 16;
-          }
-          else if ( j0 + 8 > g.ke )
-          {
-#pragma unroll
-            for ( int r = 0; r < 8; ++r )
-              if ( j0 + r >= g.ke )
-                x[ r ] <<= 16;
-          }
-          // Harley-Seal: 8 inputs through carry-save adders into P[0..2],
-          // the weight-8 carries rippled into P[3..]
-          uint32_t tA, tB, fA, fB, e;
-          csa( tA, P[ 0 ], x[ 0 ], x[ 1 ] );
-          csa( tB, P[ 0 ], x[ 2 ], x[ 3 ] );
-          csa( fA, P[ 1 ], tA, tB );
-          csa( tA, P[ 0 ], x[ 4 ], x[ 5 ] );
-          csa( tB, P[ 0 ], x[ 6 ], x[ 7 ] );
-          csa( fB, P[ 1 ], tA, tB );
-          csa( e, P[ 2 ], fA, fB );
-#pragma unroll
-          for ( int b2 = 3; b2 < G_PLANES; ++b2 )
-          {
-            const uint32_t t = P[ b2 ] & e;
-            P[ b2 ] ^= e;
-            e = t;
-            if ( e == 0u )
-              break;
-          }
+            x[ r ] <<= 16;
         }
+        else if ( j0 + 8 > g.ke )
+        {
+#pragma unroll
+          for ( int r = 0; r < 8; ++r )
+            if ( j0 + r >= g.ke )
+              x[ r ] <<= 16;
+        }
+        // Harley-Seal: 8 inputs through carry-save adders into P[0..2],
+        // the weight-8 carries rippled into P[3..]
+        uint32_t tA, tB, fA, fB, e;
+        csa( tA, P[ 0 ], x[ 0 ], x[ 1 ] );
+        csa( tB, P[ 0 ], x[ 2 ], x[ 3 ] );
+        csa( fA, P[ 1 ], tA, tB );
+        csa( tA, P[ 0 ], x[ 4 ], x[ 5 ] );
+        csa( tB, P[ 0 ], x[ 6 ], x[ 7 ] );
+        csa( fB, P[ 1 ], tA, tB );
+        csa( e, P[ 2 ], fA, fB );
+#pragma unroll
+        for ( int b2 = 3; b2 < G_PLANES; ++b2 )
+        {
+          const uint32_t t = P[ b2 ] & e;
+          P[ b2 ] ^= e;
+          e = t;
+          if ( e == 0u )
+            break;
+        }
+      };
+      // two words per step, the next step's two loaded before this step's
+      // are counted (four 16-byte loads in flight per thread)
+      const uint4 z4 = make_uint4( 0, 0, 0, 0 );
+      uint4 c0 = b0 < b1 ? __ldg( col + ( int64_t ) b0 * 32 ) : z4;
+      uint4 c1 = b0 + 1 < b1 ? __ldg( col + ( int64_t ) ( b0 + 1 ) * 32 ) : z4;
+      for ( int jb = b0; jb < b1; jb += 2 )
+      {
+        const uint4 n0 = jb + 2 < b1 ? __ldg( col + ( int64_t ) ( jb + 2 ) * 32 ) : z4;
+        const uint4 n1 = jb + 3 < b1 ? __ldg( col + ( int64_t ) ( jb + 3 ) * 32 ) : z4;
+        eat( c0, jb );
+        if ( jb + 1 < b1 )
+          eat( c1, jb + 1 );
+        c0 = n0;
+        c1 = n1;
       }
     }
     // parts 1.. hand their planes to part 0, which adds them bit-parallel
