@@ -828,21 +828,28 @@ def measure_serving(args, dev):
     # warm-up: graphs, host buffers and a pool used as widely as in the run
     # (a first run after a small warm-up measured up to 25 % slower)
     serving.run_batched(fresh()[:64], eng, realtime=False)
-    b32, st = serving.run_batched(fresh(), eng, realtime=False)
+    # each server is timed twice on the whole stream and reported by its
+    # faster run (both makespans are listed): one run on a shared host moves
+    # by up to ~20 % with host memory and scheduling
+    runs32 = [serving.run_batched(fresh(), eng, realtime=False) for _ in range(2)]
+    b32, st = min(runs32, key=lambda x: x[1]["makespan_s"])
     gathered = eng.stats()["gather_slices"]
     rt, st_rt = serving.run_batched(fresh(), eng, realtime=True)
     eng.close()
     eng = serving.new_engine("fp64", capacity_neurons=60_000, capacity_edges=80_000_000, max_networks=2,
                              device=dev.index)
     serving.run_plain(fresh()[:2], eng, realtime=False)
-    p64, sp = serving.run_plain(fresh(), eng, realtime=False)
+    runs64 = [serving.run_plain(fresh(), eng, realtime=False) for _ in range(2)]
+    p64, sp = min(runs64, key=lambda x: x[1]["makespan_s"])
     eng.close()
     out["batched_fp32"] = {"syn_events_per_s": st["syn_events_per_s"], "makespan_s": st["makespan_s"],
+                           "makespans_s": [x[1]["makespan_s"] for x in runs32],
                            "syn_events": st["syn_events"], "gather_slices": gathered,
                            "latency_saturated": serving.latency_summary(b32),
                            "latency_realtime": serving.latency_summary(rt),
                            "realtime_makespan_s": st_rt["makespan_s"]}
     out["plain_fp64"] = {"syn_events_per_s": sp["syn_events_per_s"], "makespan_s": sp["makespan_s"],
+                         "makespans_s": [x[1]["makespan_s"] for x in runs64],
                          "syn_events": sp["syn_events"], "latency_saturated": serving.latency_summary(p64)}
     out["batched_over_plain"] = st["syn_events_per_s"] / sp["syn_events_per_s"]
     out["accuracy_fp32_vs_fp64"] = serving.accuracy(b32, p64)

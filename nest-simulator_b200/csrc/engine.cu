@@ -684,6 +684,20 @@ struct ng_engine
     return alloc( b, bytes );
   }
 
+  // admission scratch: grown to the next power of two (at least 1 MiB), so a
+  // stream of networks of growing size reallocates -- and, through cudaFree,
+  // waits for the running slices -- a few times, not at every new maximum
+  int
+  grow_scratch( DevBuf& b, size_t bytes )
+  {
+    if ( b.bytes >= bytes )
+      return NG_OK;
+    size_t want = ( size_t ) 1 << 20;
+    while ( want < bytes )
+      want <<= 1;
+    return alloc( b, want );
+  }
+
   // delivery work per slice: every source spiking at every lag, each spike
   // queueing ceil(padded degree / 128) chunks, plus the generator spikes
   int
@@ -3660,9 +3674,9 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     sp.nb = nb;
     const int64_t items = n * ( int64_t ) nb;
     int rc;
-    if ( ( rc = e->grow( e->sc_sb, ( size_t ) std::max< int64_t >( items, 1 ) * 4 ) )
-      || ( rc = e->grow( e->sc_cnt, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_beg, ( size_t ) n * 8 ) )
-      || ( rc = e->grow( e->sc_plen, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_total, 8 ) ) )
+    if ( ( rc = e->grow_scratch( e->sc_sb, ( size_t ) std::max< int64_t >( items, 1 ) * 4 ) )
+      || ( rc = e->grow_scratch( e->sc_cnt, ( size_t ) n * 4 ) ) || ( rc = e->grow_scratch( e->sc_beg, ( size_t ) n * 8 ) )
+      || ( rc = e->grow_scratch( e->sc_plen, ( size_t ) n * 4 ) ) || ( rc = e->grow_scratch( e->sc_total, 8 ) ) )
       return undo( rc );
     const unsigned g = ( unsigned ) std::max< int64_t >( 1, ( items + 255 ) / 256 );
     const bool ex_m = sign_channels( model ), ae_m = model == NG_AEIF_COND_ALPHA;
@@ -3730,10 +3744,10 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
     if ( fb->delay_steps < e->cfg.min_delay || fb->delay_steps > e->cfg.max_delay )
       return undo( fail( NG_ERR_ARG, "ng_net_add: delay outside [min_delay, max_delay]" ) );
     int rc;
-    if ( ( rc = e->grow( e->sc_src, ( size_t ) std::max< int64_t >( nk, 1 ) * 4 ) )
-      || ( rc = e->grow( e->sc_cnt, ( size_t ) n * 4 ) ) || ( rc = e->grow( e->sc_fill, ( size_t ) n * 4 ) )
-      || ( rc = e->grow( e->sc_beg, ( size_t ) n * 8 ) ) || ( rc = e->grow( e->sc_plen, ( size_t ) n * 4 ) )
-      || ( rc = e->grow( e->sc_total, 8 ) ) )
+    if ( ( rc = e->grow_scratch( e->sc_src, ( size_t ) std::max< int64_t >( nk, 1 ) * 4 ) )
+      || ( rc = e->grow_scratch( e->sc_cnt, ( size_t ) n * 4 ) ) || ( rc = e->grow_scratch( e->sc_fill, ( size_t ) n * 4 ) )
+      || ( rc = e->grow_scratch( e->sc_beg, ( size_t ) n * 8 ) ) || ( rc = e->grow_scratch( e->sc_plen, ( size_t ) n * 4 ) )
+      || ( rc = e->grow_scratch( e->sc_total, 8 ) ) )
       return undo( rc );
     CU( cudaMemsetAsync( e->sc_cnt.p, 0, ( size_t ) n * 4, e->stream ) );
     CU( cudaMemsetAsync( e->sc_fill.p, 0, ( size_t ) n * 4, e->stream ) );
@@ -3865,7 +3879,7 @@ ng_net_add( ng_engine* e, const ng_net_desc* desc, int32_t* net_id )
   if ( e->ring_bytes == 4 && ne_used > 0 )
   {
     int rc2;
-    if ( ( rc2 = e->grow( e->sc_bound, ( size_t ) n * 8 + 8 ) ) )
+    if ( ( rc2 = e->grow_scratch( e->sc_bound, ( size_t ) n * 8 + 8 ) ) )
       return undo( rc2 );
     CU( cudaMemsetAsync( e->sc_bound.p, 0, ( size_t ) n * 8 + 8, e->stream ) );
     unsigned long long* sums = ( unsigned long long* ) e->sc_bound.p;
