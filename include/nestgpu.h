@@ -265,8 +265,9 @@ typedef struct
 {
   int32_t mode;            /* 0: fixed, 1: autotuned */
   int32_t state;           /* 0: not tuned yet, 1: measured, 2: from the process cache, 3: fixed */
-  int32_t update_variant;  /* 0/1: one thread per neuron (4/8 lags of inputs at a time), 2/3: two-phase
-                              (256/128-thread CTAs), 4: aeif_cond_alpha's RKF45 kernel */
+  int32_t update_variant;  /* 0/1/6: one thread per neuron (4/8/2 lags of inputs at a time), 2/3:
+                              two-phase (256/128-thread CTAs), 4: aeif_cond_alpha's RKF45 kernel,
+                              5: the persistent slice kernel */
   int32_t deliver_per_sm;  /* resident delivery CTAs per SM */
   int32_t deliver_group;   /* edge chunks per delivery warp and descriptor load */
   int32_t cache_hit;
@@ -281,7 +282,7 @@ typedef struct
 
 /* mode 1: autotune at the next long enough call (process cache first);
  * mode 2: the same, measuring even where the cache has an entry; mode 0:
- * fixed configuration -- update_variant (0..3, -1: by network size),
+ * fixed configuration -- update_variant (0..3, 5, 6; -1: by network size),
  * delivery CTAs per SM and chunks per warp (-1: defaults). */
 int ng_set_tuning( ng_engine* eng, int32_t mode, int32_t update_variant, int32_t deliver_ctas_per_sm,
   int32_t deliver_chunks_per_warp );

@@ -720,9 +720,10 @@ struct ng_engine
   // same result (the kernels share their arithmetic and its order).
   int tune_mode = 1;         // 0: fixed, 1: autotune (process cache first), 2: autotune, cache ignored
   int tune_state = 0;        // 0: pending, 1: measured, 2: from the process cache, 3: fixed
-  int upd_variant = -1;      // iaf update kernel: 0/1 one thread per neuron (4/8 lags of inputs at a
-                             // time), 2/3 two-phase (256/128 threads), 5 the persistent slice kernel
-                             // (update and delivery of many slices in one launch); -1: by network size
+  int upd_variant = -1;      // iaf update kernel: 0/1/6 one thread per neuron (4/8/2 lags of inputs
+                             // at a time), 2/3 two-phase (256/128 threads), 5 the persistent slice
+                             // kernel (update and delivery of many slices in one launch); -1: by
+                             // network size (serving engines: 6)
   DevBuf pk;                 // grid-barrier state of the persistent slice kernel
   // ---- stdp_pl_synapse_hom connections (ng_set_plastic_connections)
   bool plastic_on = false;
@@ -754,6 +755,17 @@ struct ng_engine
   default_variant( int64_t n )
   {
     return n >= 20000 ? 0 : 2;
+  }
+
+  // ... on this engine: a serving engine (whose pool of many small networks
+  // is never tuned: its chunks are too short for the trials) takes the
+  // one-thread kernel with 2 lags of inputs at a time, whose smaller code
+  // measured faster there than 4 lags at a time (update -16 % on the serving
+  // sweep; the kernel is bound by instruction issue and fetch, not memory)
+  int
+  engine_default_variant( int64_t n ) const
+  {
+    return serving ? 6 : default_variant( n );
   }
 
   void
@@ -1140,10 +1152,10 @@ struct ng_engine
     // the tuned (or default) kernel; one thread per neuron for 1-2 step
     // slices and for engines with the per-target gather or the target-tiled
     // delivery (the lag bits are written there)
-    int v = upd_variant >= 0 ? upd_variant : default_variant( db.n );
+    int v = upd_variant >= 0 ? upd_variant : engine_default_variant( db.n );
     if ( span <= 2 || gather_on || tiled_on || plastic_on )
-      v = v == 1 ? 1 : 0;
-    if ( v <= 1 )
+      v = ( v == 1 || v == 6 ) ? v : 0;
+    if ( v <= 1 || v == 6 )
     {
       // CTAs of 4 warps: a large network's grid is resident in one wave
       const unsigned grid = ( unsigned ) std::max< int64_t >( 1, ( db.n + 127 ) / 128 );
@@ -1151,6 +1163,8 @@ struct ng_engine
         k_update_iaf< Real, FIX, MODEL, 1 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
       else if ( v == 0 )
         k_update_iaf< Real, FIX, MODEL, 4 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
+      else if ( v == 6 )
+        k_update_iaf< Real, FIX, MODEL, 2 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
       else
         k_update_iaf< Real, FIX, MODEL, 8 ><<< grid, 128, 0, stream >>>( d, db, from_, to_, sched );
     }
@@ -2043,7 +2057,7 @@ struct ng_engine
     std::vector< int > variants;
     if ( iaf )
     {
-      variants = { 0, 1 };
+      variants = { 0, 1, 6 };
       if ( md >= 3 && !gather_on && !tiled_on && !plastic_on )
       {
         variants.push_back( 2 );
@@ -2071,7 +2085,7 @@ struct ng_engine
     if ( S < 4 )
       return NG_OK;
     const int64_t steps = S * md;
-    const int v0 = upd_variant >= 0 ? upd_variant : ( iaf ? default_variant( blk[ 0 ].n ) : 0 );
+    const int v0 = upd_variant >= 0 ? upd_variant : ( iaf ? engine_default_variant( blk[ 0 ].n ) : 0 );
     TuneCand best { v0, deliver_per_sm, deliver_group, 1e300 };
     tune_log.clear();
     int rc;
@@ -3293,11 +3307,11 @@ ng_set_tuning( ng_engine* e, int32_t mode, int32_t update_variant, int32_t deliv
 {
   if ( !e )
     return fail( NG_ERR_ARG, "null engine" );
-  if ( mode < 0 || mode > 2 || update_variant < -1 || update_variant > 5 || update_variant == 4 || deliver_ctas_per_sm < -1
+  if ( mode < 0 || mode > 2 || update_variant < -1 || update_variant > 6 || update_variant == 4 || deliver_ctas_per_sm < -1
     || deliver_ctas_per_sm == 0 || deliver_chunks_per_warp < -1 || deliver_chunks_per_warp == 0
     || deliver_chunks_per_warp > 32 )
-    return fail( NG_ERR_ARG, "ng_set_tuning: mode 0..2, update_variant -1, 0..3 or 5, per-SM CTAs and chunks per warp -1 "
-                             "or >= 1" );
+    return fail( NG_ERR_ARG, "ng_set_tuning: mode 0..2, update_variant -1, 0..3, 5 or 6, per-SM CTAs and chunks per warp "
+                             "-1 or >= 1" );
   int rc = e->sync_pending();
   if ( rc )
     return rc;
@@ -3330,7 +3344,7 @@ ng_get_tuning( ng_engine* e, ng_tuning* out )
   bool iaf = false;
   for ( const auto& b : e->blk )
     iaf = iaf || b.model != NG_AEIF_COND_ALPHA;
-  out->update_variant = !iaf ? 4 : e->upd_variant >= 0 ? e->upd_variant : ng_engine::default_variant( e->blk[ 0 ].n );
+  out->update_variant = !iaf ? 4 : e->upd_variant >= 0 ? e->upd_variant : e->engine_default_variant( e->blk[ 0 ].n );
   out->deliver_per_sm = e->deliver_per_sm;
   out->deliver_group = e->deliver_group;
   out->cache_hit = e->tune_state == 2 ? 1 : 0;

@@ -285,9 +285,10 @@ UPDATE_VARIANTS = {0: "k_update_iaf (one thread per neuron, 4 lags of inputs at 
                    3: "k_update_iaf2 (two-phase, 32 neurons per 128-thread CTA)",
                    4: "k_update_aeif",
                    5: "k_run_slices (persistent: node update and delivery of many slices in one cooperative launch; "
-                      "k_run_slices_mg for networks larger than one resident wave)"}
+                      "k_run_slices_mg for networks larger than one resident wave)",
+                   6: "k_update_iaf (one thread per neuron, 2 lags of inputs at a time)"}
 UPDATE_KERNELS = {0: "k_update_iaf", 1: "k_update_iaf", 2: "k_update_iaf2", 3: "k_update_iaf2", 4: "k_update_aeif",
-                  5: "k_run_slices"}
+                  5: "k_run_slices", 6: "k_update_iaf"}
 
 
 def tuning_dict(t):

@@ -22,9 +22,10 @@ from nestgpu import _abi
 pytestmark = pytest.mark.gpu
 
 # (update variant, delivery CTAs per SM, chunks per warp); variant 5 is the
-# persistent slice kernel (update and delivery of many slices in one launch)
+# persistent slice kernel (update and delivery of many slices in one launch),
+# 6 the one-thread kernel with 2 lags of inputs at a time
 CONFIGS = [(0, -1, -1), (1, -1, -1), (2, -1, -1), (3, -1, -1), (0, 1, 1), (3, 2, 8), (2, 8, 2), (5, -1, -1),
-           (5, 2, 1)]
+           (5, 2, 1), (6, -1, -1), (6, 2, 4)]
 
 
 def _exp_engine(precision, n=6000, md=15, seed=3):
