@@ -282,6 +282,35 @@ def test_gather_equals_scatter(frac):
         np.testing.assert_array_equal(v0, v1)
 
 
+@pytest.mark.parametrize("variant", [0, 1])
+def test_serving_update_variants_agree(variant):
+    """A serving engine updates with variant 6 unless told otherwise (one
+    thread per neuron, 2 lags of inputs at a time); the 4- and 8-lag forms
+    give its spikes and state bit for bit, in gather and scatter slices."""
+    def run(v):
+        eng = serving.new_engine("fp32", capacity_neurons=100_000, capacity_edges=40_000_000, max_networks=8)
+        if v is not None:
+            eng.set_tuning(0, v)
+        ids = [serving._admit(eng, _req(i, n, 1200, seed=700 + i, g=g, eta=eta))
+               for i, (n, g, eta) in enumerate(((5000, 4.0, 1.6), (1800, 6.0, 2.0)))]
+        eng.simulate(1200)
+        out = [(eng.net_spikes(i), eng.net_get_var(i, "V_m_rel", n)) for i, n in zip(ids, (5000, 1800))]
+        st, t = eng.stats(), eng.tuned()
+        eng.close()
+        return out, st, t
+
+    ref, st0, t0 = run(None)
+    got, st1, t1 = run(variant)
+    assert t0["update_variant"] == 6 and t1["update_variant"] == variant
+    assert st0["syn_events"] == st1["syn_events"] and st0["gather_slices"] > 0
+    for ((s0, u0), v0), ((s1, u1), v1) in zip(ref, got):
+        assert len(s0) > 100
+        o0, o1 = np.lexsort((s0, u0)), np.lexsort((s1, u1))
+        np.testing.assert_array_equal(s0[o0], s1[o1])
+        np.testing.assert_array_equal(u0[o0], u1[o1])
+        np.testing.assert_array_equal(v0, v1)
+
+
 def test_ring32_equals_ring64_on_representable_weights():
     """32-bit ring cells hold the same sums as 64-bit ones when the weights
     are exact at both scales (multiples of 2^-10): identical spikes and
